@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the per-step particle pipeline.
+
+Workload (N=1): PCISPH dam break, 128^3 = 1,048,576 fluid particles
+(spacing 0.01, jitter +-0.001) in a 2 x 1.3 x 1.3 container with two shells
+of boundary particles (~276k), h = 0.02, 1% density error, 3-50
+predict-correct iterations, dt = 5e-4, full Morton sort every step.
+Metric: fluid particle-steps per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0. Under torchrun (N > 1) every rank runs its own
+replica of the scene (the single-scene path does not shard: replicas only),
+value = all ranks' particle-steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at 1M PCISPH (<1% density err)"
+UNIT = "particle-steps/s"
+RADIX_PASSES = 4  # 30-bit Morton keys, 8-bit digits
+
+
+def scene_for(args):
+    from unifiedparticleframeworkcuda_b200 import scenes
+    if args.scene == "c2":
+        return scenes.pcisph_dam(128, 128, 128)
+    if args.scene == "c2-small":
+        return scenes.pcisph_dam(64, 64, 64)
+    if args.scene == "c1":
+        return scenes.wcsph_dam(32)
+    raise SystemExit("unknown scene " + args.scene)
+
+
+def workload_name(args):
+    return {"c2": "pcisph_dam_break_1M", "c2-small": "pcisph_dam_break_262k",
+            "c1": "wcsph_dam_break_32k"}[args.scene]
+
+
+def algorithmic_bytes(nf, nb, steps, total_iters, method):
+    """Algorithmic HBM bytes of `steps` steps: every SoA array counted once per
+    pass, neighbour re-reads counted zero. PCISPH: N_f (241 + 20P + 112 k) +
+    N_b 20 (1 + 2k) per step; WCSPH: N_f (193 + 20P) + N_b 40."""
+    if method == "pcisph":
+        return steps * (nf * (241 + 20 * RADIX_PASSES) + nb * 20) + total_iters * (112 * nf + 40 * nb)
+    return steps * (nf * (193 + 20 * RADIX_PASSES) + nb * 40)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 7 and f[0].replace(".", "").isdigit():
+                    rows.append(f)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][1]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[2]) for r in rows)}
+
+
+def cpu_baseline(sc_params_fn, seconds=15.0):
+    """The oracle (FP32 OpenMP restatement of the reference CPU path) on a
+    bounded sample of the same workload: a 64^3-fluid dam with the same
+    spacing, h, dt and boundary (fluid particle-steps/s do not depend on the
+    block's size beyond cache effects)."""
+    from oracle import pyoracle
+    from unifiedparticleframeworkcuda_b200 import scenes
+    import unifiedparticleframeworkcuda_b200 as upf
+    pyoracle.build(with_ref=False)
+    sc = scenes.pcisph_dam(64, 64, 64)
+    p = upf.derive_params(sc.params)
+    threads = os.cpu_count() or 1
+    o = pyoracle.OracleSim(p, sc.pos, sc.vel, sc.type, threads=threads, keep_fields=False)
+    o.step()  # warm-up
+    t0 = time.perf_counter()
+    steps = 0
+    iters = 0
+    while True:
+        info = o.step()
+        steps += 1
+        iters += info.iterations
+        if time.perf_counter() - t0 >= seconds and steps >= 2:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    nf = sc.n_fluid
+    return {"value": nf * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d fluid + %d boundary particles (pcisph_dam 64^3), %d steps, mean %.1f iterations, %.1f s"
+                      % (nf, sc.n_boundary, steps, iters / steps, dt)}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU algorithm (the oracle port; the
+    reference's UnifiedPhysics.cpp does not compile here) on the host cores."""
+    if rank != 0:
+        return
+    from oracle import pyoracle
+    import unifiedparticleframeworkcuda_b200 as upf
+    from unifiedparticleframeworkcuda_b200 import scenes
+    pyoracle.build(with_ref=False)
+    # bounded sample per step: a 64^3-fluid slab of the workload
+    sc = scenes.pcisph_dam(64, 64, 64)
+    p = upf.derive_params(sc.params)
+    threads = os.cpu_count() or 1
+    o = pyoracle.OracleSim(p, sc.pos, sc.vel, sc.type, threads=threads, keep_fields=False)
+    for _ in range(args.warmup):
+        o.step()
+    t0 = time.perf_counter()
+    iters = 0
+    for _ in range(args.steps):
+        iters += o.step().iterations
+    dt = time.perf_counter() - t0
+    o.close()
+    v = sc.n_fluid * args.steps / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": workload_name(args), "sample_fluid_particles": sc.n_fluid,
+                                        "sample_boundary_particles": sc.n_boundary,
+                                        "mean_iterations": iters / max(args.steps, 1)},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "pcisph_dam 64^3 fluid (%d) + %d boundary per step" % (sc.n_fluid, sc.n_boundary)},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import unifiedparticleframeworkcuda_b200 as upf
+    from unifiedparticleframeworkcuda_b200 import build as upfbuild
+
+    if rank == 0:
+        upfbuild.build()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sc = scene_for(args)
+    p = upf.derive_params(sc.params)
+    if args.block_size:
+        p.block_size = args.block_size
+    method = "pcisph" if p.method == upf.METHOD_PCISPH else "wcsph"
+    stream = torch.cuda.Stream(device=dev)
+    s = upf.ParticleSystem(p, capacity=sc.n, device=local_rank, derive=False)
+    s.set_stream(stream.cuda_stream)
+    s.set_particles(sc.pos, sc.vel, sc.type)
+    nf, nb = sc.n_fluid, sc.n_boundary
+
+    # warm-up
+    s.step(args.warmup)
+    s.synchronize()
+    s.reset_counters()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        s.step(args.steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    elapsed_ms = start.elapsed_time(end)
+    s.synchronize()
+    stats = s.stats()
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_ms = float(t.item())
+    total_iters = stats.total_iterations if method == "pcisph" else 0
+    mean_k = total_iters / max(stats.total_steps, 1)
+    value = nf * args.steps * world / (max_ms / 1e3)
+
+    # per-phase timings (one profiled step through the phase entry points)
+    prof = [s.profile_step() for _ in range(3)]
+    pr = prof[-1]
+    # dominant kernel: the loop's predicted-density or pressure-force pass
+    dens_ms = pr.density_ms_total / max(pr.iterations, 1)
+    pf_ms = pr.pforce_ms_total / max(pr.iterations, 1)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    if method == "pcisph":
+        # algorithmic bytes per liquid particle: density pass reads predicted
+        # position 16 + pressure 4, writes pressure 4 + density 4 = 28;
+        # pressure-force pass reads position 16, pressure 4, velocity 16,
+        # force 16, writes pressure force 16 + next prediction 16 = 84
+        if pf_ms >= dens_ms:
+            kname, kms, kbytes = "k_pcisph_pressure_force", pf_ms, 84 * nf
+        else:
+            kname, kms, kbytes = "k_pcisph_density", dens_ms, 28 * nf
+    else:
+        kname, kms, kbytes = "k_wcsph_force_integrate", pr.integrate_ms, (16 + 16 + 4 + 4 + 16 + 16 + 4) * nf
+    achieved = kbytes / (kms / 1e3) / 1e9
+    step_bytes = algorithmic_bytes(nf, nb, args.steps, total_iters, method)
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = tr.get(args.scene, {}).get(kname)
+    except Exception:
+        pass
+
+    # end to end through the C ABI with host buffers: per step, upload the
+    # state from pinned host memory, step, read the result back
+    e2e = None
+    if not args.no_e2e:
+        n = s.n_dynamic
+        hpos = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+        hvel = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+        hden = torch.empty((n,), dtype=torch.float32, pin_memory=True)
+        hpre = torch.empty((n,), dtype=torch.float32, pin_memory=True)
+        htyp = torch.empty((n,), dtype=torch.int32, pin_memory=True)
+        hid = torch.empty((n,), dtype=torch.int32, pin_memory=True)
+        import ctypes as C
+        L = upf.lib()
+        fp = C.POINTER(C.c_float)
+        cnt = C.c_uint32()
+
+        def readback():
+            upf.check(L.upf_get_particles(s.handle, C.cast(hpos.data_ptr(), fp), C.cast(hvel.data_ptr(), fp),
+                                          C.cast(hden.data_ptr(), fp), C.cast(hpre.data_ptr(), fp),
+                                          C.cast(htyp.data_ptr(), C.POINTER(C.c_int32)),
+                                          C.cast(hid.data_ptr(), C.POINTER(C.c_uint32)), C.byref(cnt)),
+                      "upf_get_particles")
+
+        readback()
+        k_e2e = max(1, min(args.steps, 10))
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k_e2e):
+            upf.check(L.upf_upload_state(s.handle, C.cast(hpos.data_ptr(), fp), C.cast(hvel.data_ptr(), fp), n),
+                      "upf_upload_state")
+            s.step(1)
+            readback()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t2 = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
+        e2e = {"value": nf * k_e2e * world / (float(t2.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * (16 + 16 + 4 + 4 + 4 + 4),
+               "steps": k_e2e}
+
+    if rank != 0:
+        s.close()
+        return
+    launches_base = 1 + 1 + 1 + 3 * RADIX_PASSES + 1 + 1  # step init, nlist, forces, sort, reorder, cells
+    if method == "pcisph":
+        gpu_launches = args.steps * (launches_base + 2) + 3 * total_iters
+    else:
+        gpu_launches = args.steps * (launches_base + 1)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(args), "fluid_particles": nf, "boundary_particles": nb,
+                   "h": float(p.support_radius), "dt": float(p.dt), "block_size": int(p.block_size),
+                   "mean_iterations": mean_k, "steps_at_max_loops": stats.steps_at_max_loops,
+                   "last_density_error_percent": float(stats.density_error_percent),
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (neighbour lists %.0f MB)" % (sc.n * p.max_neighbors * 4 / 1e6)},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                     "kernel_ms": kms, "algorithmic_bytes_per_launch": kbytes,
+                     "step_achieved_gbs": step_bytes / (max_ms / 1e3) / 1e9 / world * world,
+                     "step_frac": step_bytes / (max_ms / 1e3) / 1e9 / peak},
+        "phases_ms": {"sort": pr.sort_ms, "neighbors": pr.neighbors_ms, "forces": pr.forces_ms,
+                      "loop": pr.loop_ms, "integrate": pr.integrate_ms, "iterations": pr.iterations,
+                      "density_per_launch": dens_ms, "pforce_per_launch": pf_ms},
+        "e2e": e2e,
+        "gpu_launches": gpu_launches,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(None, seconds=args.cpu_seconds)
+    print(json.dumps(out), flush=True)
+    s.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1"])
+    ap.add_argument("--block-size", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,320 @@
+/*
+ * upf.h — C ABI of the B200-native per-step particle pipeline.
+ *
+ * Plain C: opaque handles, POD structs, pointers and sizes; no C++ or torch
+ * types cross this boundary. Every function returns a upf_status (0 = OK) and
+ * records a message retrievable through upf_last_error().
+ *
+ * The reference drives its GPU path through an `extern "C"` block that takes
+ * a C++ `dataPointers&` (src/gpu/particles.cuh:430-586). Here the handle
+ * `upf_system*` owns everything that struct held (device arrays, parameters,
+ * lookup tables, ping-pong state), so several independent simulations may
+ * live in one process. The reference-named entry points are declared in
+ * upf_legacy.h on top of this header.
+ */
+#ifndef UPF_H_
+#define UPF_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UPF_ABI_VERSION 1
+#define UPF_LUT_SIZE 300           /* bins per kernel table, src/gpu/particles.cuh:187 */
+#define UPF_LUT_ENTRIES (UPF_LUT_SIZE + 1) /* +1: the zero sentinel at index 300 */
+#define UPF_GRID_RESOLUTION 1024   /* virtual z-index grid, src/sceneConfigure/global.h:26 */
+
+/* Particle types: same numbering as ParticleObjectType
+ * (src/cpu/UnifiedParticle.h:14-23). */
+enum {
+  UPF_RIGID = 0,
+  UPF_SOFT = 1,
+  UPF_LIQUID = 2,
+  UPF_GRANULAR = 3,
+  UPF_CLOTH = 4,
+  UPF_SMOKE = 5,
+  UPF_FROZEN = 6
+};
+
+typedef enum upf_status {
+  UPF_OK = 0,
+  UPF_ERR_INVALID_ARG = 1,
+  UPF_ERR_CUDA = 2,
+  UPF_ERR_ALLOC = 3,
+  UPF_ERR_NEIGHBOR_OVERFLOW = 4, /* a particle has more neighbours than max_neighbors */
+  UPF_ERR_NAN = 5,               /* a predicted or integrated position became NaN */
+  UPF_ERR_TIMEOUT = 6,           /* a bounded device-side wait ran out */
+  UPF_ERR_STATE = 7,             /* call out of order (e.g. step before set_particles) */
+  UPF_ERR_UNSUPPORTED = 8,
+  UPF_ERR_NO_DEVICE = 9
+} upf_status;
+
+/* Solver method, UnifiedConstants::setSimulationMethod
+ * (src/sceneConfigure/UnifiedConstants.cpp:193-231). */
+enum {
+  UPF_METHOD_WCSPH = 1,  /* CPU path 'w': UnifiedPhysics::CpuParticlePhysicsPureFluidsSPH */
+  UPF_METHOD_PCISPH = 2  /* CPU path 'i': CpuParticlePhysicsVersatileCouplingPCISPH */
+};
+
+/* Optional terms. */
+enum {
+  /* Wall-weight density term of Harada et al. (UnifiedPhysics.cpp:2433-2448,
+   * 6034-6060); only used by WCSPH density. */
+  UPF_FLAG_WALL_WEIGHT = 1u << 0,
+  /* Liquid-liquid cohesion (surface tension spline, UnifiedPhysics.cpp:5283-5287)
+   * in the PCISPH external force; also the optional WCSPH surface tension
+   * (UnifiedPhysics.cpp:3055-3060, useSurfaceTension). */
+  UPF_FLAG_SURFACE_TENSION = 1u << 1,
+  /* Penalty wall force on liquid particles (CalculateBoundaryForcePerLiquidParticleHost,
+   * UnifiedPhysics.cpp:2032-2069); always on in the reference's PCISPH path. */
+  UPF_FLAG_PENALTY_WALLS = 1u << 2,
+  /* Akinci boundary pressure force from boundary/rigid particles with the
+   * lagged pressure and predicted density (CalculateBoundaryFluidPressureForceHost,
+   * UnifiedPhysics.cpp:4240-4250), LUT indexed by distance. */
+  UPF_FLAG_BOUNDARY_PRESSURE = 1u << 3,
+  /* Adhesion between liquid and boundary/rigid particles
+   * (CalculateSurfaceCohesionForcePCISPHHost, UnifiedPhysics.cpp:2000-2008). */
+  UPF_FLAG_ADHESION = 1u << 4,
+  /* Record per-iteration max predicted density into the step statistics. */
+  UPF_FLAG_RECORD_ITERATIONS = 1u << 5
+};
+
+/*
+ * Scene/solver parameters. Mirrors the scalar block the reference pushes to
+ * the device with ~40 setters (src/gpu/particles.cuh:461-503,
+ * SetDeviceConstants src/gpu/particles.cu:177-229) and the fields of
+ * UnifiedConstants (src/sceneConfigure/UnifiedConstants.h:37-222).
+ * upf_default_params() fills the reference's constructor values;
+ * upf_params_derive() fills the derived fields (mass, scales, block size,
+ * density error factor) exactly as the reference computes them.
+ */
+typedef struct upf_params {
+  int32_t method;            /* UPF_METHOD_* */
+  uint32_t flags;            /* UPF_FLAG_* */
+
+  float particle_spacing;    /* particleSpacing */
+  float particle_radius;     /* particleRadius = 0.5 * spacing */
+  float support_radius;      /* globalSupportRadius h */
+  float mass;                /* initialMass = spacing^3 * rest_density */
+  float rest_density;        /* fluidRestDensity */
+  float gas_constant;        /* fluidGasConstantWCSPH (WCSPH stiffness k) */
+  float gamma;               /* Tait exponent (7) */
+  float viscosity;           /* fluidViscConst */
+  float gravity;             /* gravityConst, applied along -y */
+  float dt;                  /* deltaT */
+
+  /* PCISPH */
+  float density_error_factor;   /* delta; 0 => computed by upf_params_derive */
+  float density_error_fudge;    /* densityErrorFactorParameter; <0 => 0.05*(dt/2e-4)^2 */
+  float max_density_error;      /* maxDensityErrorAllowed, percent */
+  int32_t min_loops;            /* minLoops (3) */
+  int32_t max_loops;            /* maxLoops (50) */
+
+  /* Surface tension / adhesion (Akinci 2013) */
+  float surface_tension_gamma;  /* 0.3 */
+  float surface_adhesion_beta;  /* 0.0 */
+
+  /* Penalty walls */
+  float force_distance;         /* 0.25 * h */
+  float max_boundary_force;     /* 64 * spacing^2 */
+
+  /* Rigid bodies (GPU Gems 3 contact model) */
+  float spring_coefficient;          /* 300 */
+  float spring_coefficient_boundary; /* 300 */
+  float damping_coefficient;         /* 0.5 */
+  float terminal_speed;              /* 20 */
+
+  /* Granular contact (Bell et al. 2005), UnifiedConstants.cpp:57-60 */
+  float granular_kr;
+  float granular_kd;
+  float granular_kt;
+  float granular_mu;
+
+  /* Virtual z-index box: key = Morton(uint16(scales * (x - zindex_origin))) */
+  float zindex_origin[3];
+  float zindex_extent[3];
+  float scales[3];              /* derived: 1024 / extent */
+  uint32_t block_size;          /* power-of-two Morton block edge (grid units); 0 => derived */
+
+  /* Collision box (clamp) and real container (wall-weight distance) */
+  float collision_min[3];
+  float collision_max[3];
+  float container_min[3];
+  float container_max[3];
+
+  /* Capacity */
+  uint32_t max_neighbors;       /* per-particle neighbour list capacity (0 => 128) */
+  uint32_t reserved[7];
+} upf_params;
+
+/* Per-step statistics (the reference prints these; here they are returned). */
+typedef struct upf_step_stats {
+  int32_t iterations;        /* PCISPH predict-correct iterations of the last step */
+  int32_t hit_max_loops;     /* 1 if iterations == max_loops */
+  float max_predicted_density;  /* after the final iteration */
+  float density_error_percent;  /* max(0.1*rho*_max - 100, 0) scaled by rest density */
+  uint32_t max_neighbor_count;
+  uint32_t error_flags;      /* bit0 neighbour overflow, bit1 NaN, bit2 timeout */
+  double kinetic_energy;     /* of liquid particles after integration */
+  double momentum[3];
+  float iteration_max_density[64]; /* per iteration of the last step (first 64) */
+  /* cumulative since creation or upf_reset_counters */
+  int32_t total_steps;
+  int32_t total_iterations;
+  int32_t steps_at_max_loops;
+  int32_t reserved;
+} upf_step_stats;
+
+typedef struct upf_system upf_system;
+
+/* ---- parameters -------------------------------------------------------- */
+
+/* Reference defaults: UnifiedConstants::UnifiedConstants
+ * (src/sceneConfigure/UnifiedConstants.cpp:7-159). */
+upf_status upf_default_params(upf_params* p);
+
+/* Derived values: mass (UnifiedConstants.cpp:168-191), scales
+ * (UnifiedConstants.cpp:308-320), Morton block size (UnifiedPhysics.cpp:2149-2159
+ * with ZIndex::SetBlockSize zIndex.cpp:27-39), density error factor
+ * (UnifiedPhysics.cpp:5525-5689, accumulated in FP64). Fields already set
+ * (non-zero) are kept. */
+upf_status upf_params_derive(upf_params* p);
+
+/* PCISPH delta from the prototype block (ComputeDensityErrorFactor,
+ * UnifiedPhysics.cpp:5525-5689), FP64 accumulation. */
+upf_status upf_density_error_factor(const upf_params* p, double* delta_out);
+
+/* The five 301-entry lookup tables (WeightingKernel::initLookupTables,
+ * src/cpu/WeightingKernel.cpp:303-320), row-major [5][301]:
+ * M4, pressure-gradient, viscosity-laplacian, surface-tension, adhesion.
+ * Replaces CreateLut*Texture (src/gpu/particles.cuh:444-448). */
+upf_status upf_build_luts(const upf_params* p, float* out_5x301);
+
+/* ---- system lifetime (MallocDeviceArrays / FreeDeviceArrays) ------------ */
+
+/* Replaces MallocDeviceArraysParticles + SetDeviceConstants +
+ * CreateLut*Texture (src/gpu/particles.cuh:432-448). capacity = maximum
+ * number of particles (dynamic + boundary). */
+upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_system** out);
+upf_status upf_destroy(upf_system* s);
+upf_status upf_get_params(const upf_system* s, upf_params* out);
+/* cudaStream_t passed as void*; NULL = the library's own stream. */
+upf_status upf_set_stream(upf_system* s, void* stream);
+
+/* Host arrays, replaces CopyZIndicesKVPairHostToDevice +
+ * CopyParticleDataHostToDevice (src/gpu/particles.cuh:436-437).
+ * pos/vel: n x 4 floats (w ignored); type: UPF_* per particle.
+ * FROZEN particles become the static boundary set (sorted once);
+ * all others are dynamic. ids are 0..n-1 in input order. */
+upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4,
+                             const int32_t* type, uint32_t n);
+
+/* Rigid bodies (MallocDeviceArraysRigidBody + CopyRigidBodyDataHostToDevice,
+ * src/gpu/particles.cuh:433,438). body_of_particle[i] = body index for every
+ * RIGID particle i of the last upf_set_particles call (-1 otherwise).
+ * Body mass, centre of mass and inverse local inertia are computed from the
+ * particles (AddToRigidBody UnifiedPhysics.cpp:825-885, FP64). */
+upf_status upf_set_rigid_bodies(upf_system* s, const int32_t* body_of_particle,
+                                uint32_t n, uint32_t num_bodies);
+
+/* ---- stepping ------------------------------------------------------------ */
+
+/* Advance nsteps full steps (ParticlePhysicsOnDevicePCISPH / ...SPH /
+ * ...FluidRigidCouplingPCISPH, src/gpu/particles.cuh:534-586). Runs as a CUDA
+ * graph; the PCISPH loop is a device-side conditional while-node (no host
+ * round trip per iteration). Asynchronous w.r.t. the host unless an error
+ * check is requested by upf_synchronize. */
+upf_status upf_step(upf_system* s, int32_t nsteps);
+upf_status upf_synchronize(upf_system* s);
+upf_status upf_get_step_stats(upf_system* s, upf_step_stats* out);
+/* Zero the cumulative counters of upf_step_stats (asynchronous, in stream order). */
+upf_status upf_reset_counters(upf_system* s);
+
+/* ---- phases (the reference's lower-level entry points) ------------------ */
+/* ZindexSorting (particles.cuh:513): sort by key, reorder, cell ranges. */
+upf_status upf_phase_sort(upf_system* s);
+/* BlockGeneration analogue (particles.cuh:515): build neighbour lists. */
+upf_status upf_phase_neighbors(upf_system* s);
+/* External forces (CalculateExternalForces*PcisphCUDA) or WCSPH density. */
+upf_status upf_phase_forces(upf_system* s);
+/* PredictionCorrectionStepPcisphCUDA (particles.cuh:537). */
+upf_status upf_phase_predict_correct(upf_system* s);
+/* Time integration + clamp + next key (UpdateLiquidParticlePosVel*, CalculateZindex). */
+upf_status upf_phase_integrate(upf_system* s);
+
+/* Replace the dynamic particles' positions and velocities from host arrays in
+ * the current device order (the order upf_get_particles returns), keeping the
+ * rest of the state; the next step re-sorts them. n must equal the dynamic
+ * particle count. This is the per-frame CopyParticleDataHostToDevice of a
+ * host-driven caller (src/gpu/particles.cuh:437). */
+upf_status upf_upload_state(upf_system* s, const float* pos4, const float* vel4, uint32_t n);
+
+/* Per-phase device timings of one step (the reference's SPH_PROFILING_VERBOSE
+ * per-phase event timers, src/gpu/particles.cu:1460-1690). Runs one full
+ * step through the phase entry points with CUDA events around each phase,
+ * and times each predicted-density and pressure-force launch. */
+typedef struct upf_phase_times {
+  float sort_ms;            /* radix sort + reorder + cell ranges */
+  float neighbors_ms;       /* neighbour lists */
+  float forces_ms;          /* external forces (PCISPH) / density (WCSPH) */
+  float loop_ms;            /* whole predict-correct loop, host-driven */
+  float integrate_ms;       /* integration (+ WCSPH force) */
+  float density_ms_total;   /* sum over the loop's predicted-density launches */
+  float pforce_ms_total;    /* sum over the loop's pressure-force launches */
+  int32_t iterations;
+  int32_t launches;         /* device kernels launched by the step */
+} upf_phase_times;
+upf_status upf_profile_step(upf_system* s, upf_phase_times* out);
+
+/* ---- readback (CopyParticlesCUDA, src/gpu/particles.cuh:505) ------------ */
+
+/* Dynamic particles in current device order. Any pointer may be NULL.
+ * pos4/vel4/force4/pforce4: n x 4 floats. Returns count in *n_out. */
+upf_status upf_get_particles(upf_system* s, float* pos4, float* vel4, float* density,
+                             float* pressure, int32_t* type, uint32_t* id, uint32_t* n_out);
+/* Per-particle step fields of the last step, in the sorted order of that step:
+ * external force, correction pressure force, predicted density. */
+upf_status upf_get_step_fields(upf_system* s, float* force4, float* pforce4,
+                               float* predicted_density, uint32_t* id, uint32_t* n_out);
+/* Neighbour lists of the dynamic particles (after upf_phase_neighbors), as
+ * ids: counts[n], lists[n * cap] (row-major, first counts[i] valid). */
+upf_status upf_get_neighbors(upf_system* s, uint32_t* counts, uint32_t* lists_ids,
+                             uint32_t cap, uint32_t* n_out);
+/* Sorted keys and cell ranges of the dynamic set (after upf_phase_sort). */
+upf_status upf_get_sorted_keys(upf_system* s, uint32_t* keys, uint32_t* ids, uint32_t* n_out);
+upf_status upf_get_cell_ranges(upf_system* s, uint32_t* start, uint32_t* end, uint32_t* ncells_out);
+
+/* ---- stateless device building blocks ----------------------------------- */
+/* Device pointers; stream as void* (NULL = default stream). */
+
+/* 30-bit Morton key per particle (ZIndex::CalcIndex, src/cpu/zIndex.h:40-45,
+ * called as zIndex.CalcIndex(fc_->scales * p.position_), UnifiedPhysics.cpp:4005). */
+upf_status upf_morton_keys(const float* pos4_dev, uint32_t n, const float origin[3],
+                           const float scales[3], uint32_t* keys_dev, void* stream);
+
+/* Stable LSD radix sort of (key, value) pairs on the low key_bits bits.
+ * Replaces RadixSort (src/gpu/radixsort.cuh:115-117). keys/vals are sorted in
+ * place; temp is caller-provided scratch of upf_radix_sort_temp_bytes(n). */
+size_t upf_radix_sort_temp_bytes(uint32_t n);
+upf_status upf_radix_sort_pairs(uint32_t* keys_dev, uint32_t* vals_dev, uint32_t n,
+                                int32_t key_bits, void* temp_dev, size_t temp_bytes,
+                                void* stream);
+
+/* Cell start/end for sorted keys at cell = key >> shift (empty cells start=end=0).
+ * Replaces ClearIndexArrays + CalculateBlocksKernel (particles_kernel.cu:656-726). */
+upf_status upf_cell_ranges(const uint32_t* sorted_keys_dev, uint32_t n, int32_t shift,
+                           uint32_t ncells, uint32_t* start_dev, uint32_t* end_dev,
+                           void* stream);
+
+/* ---- errors ------------------------------------------------------------- */
+const char* upf_last_error(void);
+const char* upf_status_string(upf_status st);
+int32_t upf_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UPF_H_ */

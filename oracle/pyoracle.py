@@ -1,0 +1,224 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes loader for the CPU oracle (liboracle.so)
+and the reference pin library (_ref/libupfref.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, as the checker. The product package never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from unifiedparticleframeworkcuda_b200._abi import UpfParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REFLIB = os.path.join(HERE, "_ref", "libupfref.so")
+REFERENCE_SRC = "/root/reference/src"
+
+_lib = None
+_ref = None
+
+
+def build(with_ref: bool = True) -> None:
+    """Compile the oracle (and the reference pins when the reference tree is
+    present) with oracle/Makefile."""
+    targets = ["all"]
+    if with_ref and os.path.isdir(REFERENCE_SRC):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+class StepInfo(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32),
+        ("max_predicted_density", C.c_float),
+        ("density_error_percent", C.c_float),
+        ("max_neighbor_count", C.c_uint32),
+        ("kinetic_energy", C.c_double),
+        ("momentum", C.c_double * 3),
+        ("iteration_max_density", C.c_float * 64),
+    ]
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build(with_ref=False)
+        L = C.CDLL(LIB)
+        P = C.POINTER(UpfParams)
+        fp, u32p, i32p = C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
+        L.orc_default_params.argtypes = [P]
+        L.orc_params_derive.argtypes = [P]
+        L.orc_params_derive.restype = C.c_int
+        L.orc_density_error_factor.argtypes = [P, C.c_int]
+        L.orc_density_error_factor.restype = C.c_double
+        L.orc_build_luts.argtypes = [P, fp]
+        L.orc_morton.argtypes = [P, C.c_float, C.c_float, C.c_float]
+        L.orc_morton.restype = C.c_uint32
+        L.orc_morton_table.argtypes = [u32p]
+        L.orc_box_query.argtypes = [C.c_uint32, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), u32p, u32p, C.c_int]
+        L.orc_box_query.restype = C.c_int
+        L.orc_create.argtypes = [P, fp, fp, i32p, C.c_uint32, C.c_int, C.c_int]
+        L.orc_create.restype = C.c_void_p
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_step.argtypes = [C.c_void_p, C.POINTER(StepInfo)]
+        L.orc_step.restype = C.c_int
+        L.orc_count.argtypes = [C.c_void_p]
+        L.orc_count.restype = C.c_uint32
+        L.orc_keep_fields.argtypes = [C.c_void_p, C.c_int]
+        L.orc_get.argtypes = [C.c_void_p, fp, fp, fp, fp, i32p, u32p, u32p]
+        L.orc_get_step_fields.argtypes = [C.c_void_p, fp, fp, fp, fp, fp, fp, u32p]
+        L.orc_neighbors.argtypes = [C.c_void_p, u32p, u32p, C.c_uint32]
+        L.orc_neighbors.restype = C.c_uint32
+        L.orc_set_rigid_bodies.argtypes = [C.c_void_p, i32p, C.c_uint32, C.c_uint32]
+        L.orc_set_rigid_bodies.restype = C.c_int
+        L.orc_get_rigid.argtypes = [C.c_void_p, fp, fp, fp, fp]
+        L.orc_get_rigid.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REFLIB)
+
+
+def ref():
+    """The reference's own CPU code (zIndex, WeightingKernel, UnifiedConstants)."""
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REFLIB)
+        fp, u32p = C.POINTER(C.c_float), C.POINTER(C.c_uint32)
+        L.ref_morton_table.argtypes = [u32p]
+        L.ref_box_query.argtypes = [C.c_uint32, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), u32p, u32p, C.c_int]
+        L.ref_box_query.restype = C.c_int
+        L.ref_block_size.argtypes = [C.c_int]
+        L.ref_block_size.restype = C.c_uint32
+        L.ref_luts.argtypes = [C.c_float, fp]
+        L.ref_kernels.argtypes = [C.c_float, C.c_float, fp]
+        L.ref_lut_lookup.argtypes = [C.c_float, fp, C.c_int, fp]
+        L.ref_default_constants.argtypes = [fp]
+        _ref = L
+    return _ref
+
+
+# ---------------------------------------------------------------- helpers
+def default_params() -> UpfParams:
+    p = UpfParams()
+    lib().orc_default_params(C.byref(p))
+    return p
+
+
+def derive(p: UpfParams) -> UpfParams:
+    q = p.copy()
+    rc = lib().orc_params_derive(C.byref(q))
+    if rc != 0:
+        raise ValueError("orc_params_derive failed")
+    return q
+
+
+def luts(p: UpfParams) -> np.ndarray:
+    out = np.zeros((5, 301), np.float32)
+    lib().orc_build_luts(C.byref(p), _ptr(out, C.c_float))
+    return out
+
+
+def morton_table() -> np.ndarray:
+    out = np.zeros((1024, 3), np.uint32)
+    lib().orc_morton_table(_ptr(out, C.c_uint32))
+    return out
+
+
+def box_query(block_size, mn, mx, cap=4096):
+    a = np.asarray(mn, np.uint16)
+    b = np.asarray(mx, np.uint16)
+    f = np.zeros(cap, np.uint32)
+    l = np.zeros(cap, np.uint32)
+    n = lib().orc_box_query(block_size, _ptr(a, C.c_uint16), _ptr(b, C.c_uint16), _ptr(f, C.c_uint32), _ptr(l, C.c_uint32), cap)
+    return f[:n].copy(), l[:n].copy()
+
+
+class OracleSim:
+    """One oracle simulation (all particle types in one array, as in the
+    reference's UnifiedPhysics)."""
+
+    def __init__(self, params: UpfParams, pos4, vel4, types, fp64=False, threads=0, keep_fields=True):
+        self.params = params
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        vel4 = np.ascontiguousarray(vel4, np.float32)
+        types = np.ascontiguousarray(types, np.int32)
+        self.n = pos4.shape[0]
+        self._h = lib().orc_create(C.byref(params), _ptr(pos4, C.c_float), _ptr(vel4, C.c_float),
+                                   _ptr(types, C.c_int32), self.n, int(fp64), int(threads))
+        lib().orc_keep_fields(self._h, int(keep_fields))
+
+    def close(self):
+        if self._h:
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self) -> StepInfo:
+        info = StepInfo()
+        rc = lib().orc_step(self._h, C.byref(info))
+        if rc != 0:
+            raise RuntimeError("oracle step failed")
+        return info
+
+    def set_rigid_bodies(self, body, num_bodies):
+        body = np.ascontiguousarray(body, np.int32)
+        rc = lib().orc_set_rigid_bodies(self._h, _ptr(body, C.c_int32), body.shape[0], num_bodies)
+        if rc != 0:
+            raise RuntimeError("oracle rigid bodies not supported for this scene")
+
+    def state(self):
+        n = self.n
+        pos = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        den = np.zeros(n, np.float32)
+        pre = np.zeros(n, np.float32)
+        typ = np.zeros(n, np.int32)
+        ids = np.zeros(n, np.uint32)
+        key = np.zeros(n, np.uint32)
+        lib().orc_get(self._h, _ptr(pos, C.c_float), _ptr(vel, C.c_float), _ptr(den, C.c_float),
+                      _ptr(pre, C.c_float), _ptr(typ, C.c_int32), _ptr(ids, C.c_uint32), _ptr(key, C.c_uint32))
+        return dict(pos=pos, vel=vel, density=den, pressure=pre, type=typ, id=ids, key=key)
+
+    def step_fields(self):
+        n = self.n
+        f = np.zeros((n, 4), np.float32)
+        fp = np.zeros((n, 4), np.float32)
+        rs = np.zeros(n, np.float32)
+        pc = np.zeros(n, np.float32)
+        den = np.zeros(n, np.float32)
+        pr = np.zeros(n, np.float32)
+        ids = np.zeros(n, np.uint32)
+        lib().orc_get_step_fields(self._h, _ptr(f, C.c_float), _ptr(fp, C.c_float), _ptr(rs, C.c_float),
+                                  _ptr(pc, C.c_float), _ptr(den, C.c_float), _ptr(pr, C.c_float),
+                                  _ptr(ids, C.c_uint32))
+        return dict(force=f, pforce=fp, predicted_density=rs, corr_pressure=pc, density=den,
+                    pressure=pr, id=ids)
+
+    def neighbors(self):
+        """CSR neighbour lists of the current order, as particle ids."""
+        n = self.n
+        off = np.zeros(n + 1, np.uint32)
+        total = lib().orc_neighbors(self._h, _ptr(off, C.c_uint32), None, 0)
+        ids = np.zeros(max(total, 1), np.uint32)
+        lib().orc_neighbors(self._h, _ptr(off, C.c_uint32), _ptr(ids, C.c_uint32), total)
+        return off, ids[:total]

@@ -1,0 +1,108 @@
+"""CPU checks of the C ABI: the library loads, exports every function that
+include/*.h declares, the ctypes mirrors have the header's layouts, and the
+host-side math (defaults, derived values, lookup tables, density error
+factor) matches the oracle. No device work is done here."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+INCLUDE = os.path.join(ROOT, "include")
+
+
+def declared_functions():
+    names = set()
+    for f in sorted(os.listdir(INCLUDE)):
+        if not f.endswith(".h"):
+            continue
+        src = open(os.path.join(INCLUDE, f)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([a-zA-Z_]\w*)\s*\(", src, flags=re.M):
+            name = m.group(1)
+            if name in ("if", "for", "while", "return", "sizeof", "defined"):
+                continue
+            names.add(name)
+    return names
+
+
+def test_library_exports_every_declared_function(upf_lib):
+    lib = upf_lib.lib()
+    names = declared_functions()
+    assert "upf_create" in names and "upf_step" in names
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_struct_layouts_match_header(upf_lib, tmp_path):
+    from unifiedparticleframeworkcuda_b200._abi import UpfParams, UpfStepStats
+    src = tmp_path / "sz.c"
+    src.write_text('#include "upf.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(upf_params), sizeof(upf_step_stats),'
+                   ' offsetof(upf_params, scales), offsetof(upf_step_stats, kinetic_energy));return 0;}\n')
+    exe = tmp_path / "sz"
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    subprocess.run([cc, "-I" + INCLUDE, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert int(out[0]) == C.sizeof(UpfParams)
+    assert int(out[1]) == C.sizeof(UpfStepStats)
+    assert int(out[2]) == UpfParams.scales.offset
+    assert int(out[3]) == UpfStepStats.kinetic_energy.offset
+
+
+def test_abi_version(upf_lib):
+    assert upf_lib.lib().upf_abi_version() == 1
+
+
+def test_invalid_arguments_return_status(upf_lib):
+    lib = upf_lib.lib()
+    assert lib.upf_default_params(None) == 1
+    assert lib.upf_params_derive(None) == 1
+    msg = lib.upf_last_error().decode()
+    assert "upf_params_derive" in msg
+    # bad parameters are rejected before any device work
+    p = upf_lib.default_params()
+    h = C.c_void_p()
+    assert lib.upf_create(C.byref(p), 0, 10, C.byref(h)) == 1  # not derived: block_size 0
+    assert "invalid parameters" in lib.upf_last_error().decode()
+    assert lib.upf_step(None, 1) == 1
+
+
+def test_host_params_match_oracle(upf_lib, oracle_lib):
+    from unifiedparticleframeworkcuda_b200 import scenes
+    for sc in (scenes.small_wcsph(), scenes.small_pcisph(), scenes.wcsph_dam(), scenes.pcisph_dam(8, 8, 8)):
+        a = upf_lib.derive_params(sc.params).as_dict()
+        b = oracle_lib.derive(sc.params).as_dict()
+        da, db = a.pop("density_error_factor"), b.pop("density_error_factor")
+        assert a == b
+        # FP64 accumulation in the library vs the FP32 restatement
+        assert abs(da - db) <= 1e-5 * max(abs(db), 1e-30)
+
+
+def test_host_luts_bit_equal_to_reference_fixture(upf_lib):
+    g = np.load(os.path.join(ROOT, "tests", "golden", "reference_tables.npz"))
+    for h, ref in zip(g["lut_h"], g["luts"]):
+        p = upf_lib.default_params()
+        p.support_radius = float(h)
+        got = upf_lib.build_luts(p)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+def test_no_device_means_error_not_fallback(upf_lib):
+    """Without a GPU the library refuses to create a system (there is no CPU
+    path to fall back to)."""
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("GPU present")
+    from unifiedparticleframeworkcuda_b200 import UpfError, scenes
+    sc = scenes.small_pcisph()
+    with pytest.raises(UpfError) as e:
+        upf_lib.ParticleSystem(sc.params, capacity=sc.n)
+    assert e.value.status == 9  # UPF_ERR_NO_DEVICE

@@ -1,0 +1,255 @@
+"""B200-native per-step particle pipeline (SPH / WCSPH / PCISPH).
+
+Python host mirror of the C ABI in include/upf.h, over ctypes. The compute
+path is the in-tree CUDA library libupf.so (sm_100a); there is no CPU
+fallback: if the library is missing or no GPU is present, the calls fail.
+
+The reference drives its GPU path from the C++ facade UnifiedPhysics
+(src/cpu/UnifiedPhysics.cpp:615-643 InitCudaVariables, 4051-4141
+CudaParticlePhysics, 404-407 CopyGPUParticles). `ParticleSystem` mirrors
+that: construct with parameters, upload particles, step, copy back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (FLAG_ADHESION, FLAG_BOUNDARY_PRESSURE, FLAG_PENALTY_WALLS,  # noqa: F401
+                   FLAG_RECORD_ITERATIONS, FLAG_SURFACE_TENSION, FLAG_WALL_WEIGHT, FROZEN,
+                   GRANULAR, LIQUID, METHOD_PCISPH, METHOD_WCSPH, RIGID, STATUS, UpfParams,
+                   UpfPhaseTimes, UpfStepStats)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libupf.so")
+
+_lib = None
+
+
+class UpfError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str):
+        self.status = status
+        super().__init__("%s: %s: %s" % (where, STATUS.get(status, status), message))
+
+
+def lib():
+    """Load libupf.so (build it first with `python -m unifiedparticleframeworkcuda_b200.build`)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError("libupf.so not built: run python -m unifiedparticleframeworkcuda_b200.build")
+        L = C.CDLL(LIBPATH)
+        P = C.POINTER(UpfParams)
+        vp, fp = C.c_void_p, C.POINTER(C.c_float)
+        u32p, i32p = C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
+        sig = {
+            "upf_default_params": [P],
+            "upf_params_derive": [P],
+            "upf_density_error_factor": [P, C.POINTER(C.c_double)],
+            "upf_build_luts": [P, fp],
+            "upf_create": [P, C.c_int, C.c_uint32, C.POINTER(vp)],
+            "upf_destroy": [vp],
+            "upf_get_params": [vp, P],
+            "upf_set_stream": [vp, vp],
+            "upf_set_particles": [vp, fp, fp, i32p, C.c_uint32],
+            "upf_set_rigid_bodies": [vp, i32p, C.c_uint32, C.c_uint32],
+            "upf_step": [vp, C.c_int32],
+            "upf_synchronize": [vp],
+            "upf_get_step_stats": [vp, C.POINTER(UpfStepStats)],
+            "upf_phase_sort": [vp],
+            "upf_phase_neighbors": [vp],
+            "upf_phase_forces": [vp],
+            "upf_phase_predict_correct": [vp],
+            "upf_phase_integrate": [vp],
+            "upf_get_particles": [vp, fp, fp, fp, fp, i32p, u32p, u32p],
+            "upf_get_step_fields": [vp, fp, fp, fp, u32p, u32p],
+            "upf_get_neighbors": [vp, u32p, u32p, C.c_uint32, u32p],
+            "upf_get_sorted_keys": [vp, u32p, u32p, u32p],
+            "upf_get_cell_ranges": [vp, u32p, u32p, u32p],
+            "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
+            "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
+            "upf_cell_ranges": [vp, C.c_uint32, C.c_int32, C.c_uint32, vp, vp, vp],
+            "upf_upload_state": [vp, fp, fp, C.c_uint32],
+            "upf_profile_step": [vp, C.POINTER(UpfPhaseTimes)],
+            "upf_reset_counters": [vp],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.upf_radix_sort_temp_bytes.argtypes = [C.c_uint32]
+        L.upf_radix_sort_temp_bytes.restype = C.c_size_t
+        L.upf_last_error.restype = C.c_char_p
+        L.upf_status_string.argtypes = [C.c_int]
+        L.upf_status_string.restype = C.c_char_p
+        L.upf_abi_version.restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != 0:
+        raise UpfError(status, where, lib().upf_last_error().decode())
+
+
+def _p(a, ctype):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+def default_params() -> UpfParams:
+    p = UpfParams()
+    check(lib().upf_default_params(C.byref(p)), "upf_default_params")
+    return p
+
+
+def derive_params(p: UpfParams) -> UpfParams:
+    q = p.copy()
+    check(lib().upf_params_derive(C.byref(q)), "upf_params_derive")
+    return q
+
+
+def density_error_factor(p: UpfParams) -> float:
+    out = C.c_double()
+    check(lib().upf_density_error_factor(C.byref(p), C.byref(out)), "upf_density_error_factor")
+    return out.value
+
+
+def build_luts(p: UpfParams) -> np.ndarray:
+    out = np.zeros((5, 301), np.float32)
+    check(lib().upf_build_luts(C.byref(p), _p(out, C.c_float)), "upf_build_luts")
+    return out
+
+
+class ParticleSystem:
+    """One simulation on one GPU (the reference's UnifiedPhysics + dataPointers)."""
+
+    def __init__(self, params: UpfParams, capacity: int, device: int = 0, derive: bool = True):
+        self.params = derive_params(params) if derive else params.copy()
+        h = C.c_void_p()
+        check(lib().upf_create(C.byref(self.params), int(device), int(capacity), C.byref(h)), "upf_create")
+        self._h = h
+        self.n_dynamic = 0
+
+    # lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().upf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # uploads
+    def set_particles(self, pos4, vel4, types):
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        vel4 = np.ascontiguousarray(vel4, np.float32)
+        types = np.ascontiguousarray(types, np.int32)
+        n = pos4.shape[0]
+        if pos4.shape != (n, 4) or vel4.shape != (n, 4) or types.shape != (n,):
+            raise ValueError("pos4/vel4 must be (n,4) and types (n,)")
+        check(lib().upf_set_particles(self._h, _p(pos4, C.c_float), _p(vel4, C.c_float), _p(types, C.c_int32), n),
+              "upf_set_particles")
+        self.n_dynamic = int(np.count_nonzero(types != FROZEN))
+
+    # stepping
+    def step(self, nsteps: int = 1):
+        check(lib().upf_step(self._h, int(nsteps)), "upf_step")
+
+    def synchronize(self):
+        check(lib().upf_synchronize(self._h), "upf_synchronize")
+
+    def stats(self) -> UpfStepStats:
+        s = UpfStepStats()
+        check(lib().upf_get_step_stats(self._h, C.byref(s)), "upf_get_step_stats")
+        return s
+
+    def reset_counters(self):
+        check(lib().upf_reset_counters(self._h), "upf_reset_counters")
+
+    def set_stream(self, stream_handle: int | None):
+        """Run on a caller's cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
+        check(lib().upf_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None), "upf_set_stream")
+
+    def upload_state(self, pos4, vel4):
+        """Host -> device copy of positions/velocities in the current device order."""
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        vel4 = np.ascontiguousarray(vel4, np.float32)
+        check(lib().upf_upload_state(self._h, _p(pos4, C.c_float), _p(vel4, C.c_float), pos4.shape[0]),
+              "upf_upload_state")
+
+    def profile_step(self) -> UpfPhaseTimes:
+        t = UpfPhaseTimes()
+        check(lib().upf_profile_step(self._h, C.byref(t)), "upf_profile_step")
+        return t
+
+    def phase(self, name: str):
+        check(getattr(lib(), "upf_phase_" + name)(self._h), "upf_phase_" + name)
+
+    # readback
+    def particles(self):
+        n = self.n_dynamic
+        pos = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        den = np.zeros(n, np.float32)
+        pre = np.zeros(n, np.float32)
+        typ = np.zeros(n, np.int32)
+        ids = np.zeros(n, np.uint32)
+        cnt = C.c_uint32()
+        check(lib().upf_get_particles(self._h, _p(pos, C.c_float), _p(vel, C.c_float), _p(den, C.c_float),
+                                      _p(pre, C.c_float), _p(typ, C.c_int32), _p(ids, C.c_uint32), C.byref(cnt)),
+              "upf_get_particles")
+        return dict(pos=pos, vel=vel, density=den, pressure=pre, type=typ, id=ids)
+
+    def step_fields(self):
+        n = self.n_dynamic
+        f = np.zeros((n, 4), np.float32)
+        fp = np.zeros((n, 4), np.float32)
+        rs = np.zeros(n, np.float32)
+        ids = np.zeros(n, np.uint32)
+        cnt = C.c_uint32()
+        check(lib().upf_get_step_fields(self._h, _p(f, C.c_float), _p(fp, C.c_float), _p(rs, C.c_float),
+                                        _p(ids, C.c_uint32), C.byref(cnt)), "upf_get_step_fields")
+        return dict(force=f, pforce=fp, predicted_density=rs, id=ids)
+
+    def neighbors(self):
+        n = self.n_dynamic
+        cap = int(self.params.max_neighbors)
+        counts = np.zeros(n, np.uint32)
+        lists = np.zeros((n, cap), np.uint32)
+        cnt = C.c_uint32()
+        check(lib().upf_get_neighbors(self._h, _p(counts, C.c_uint32), _p(lists, C.c_uint32), cap, C.byref(cnt)),
+              "upf_get_neighbors")
+        return counts, lists
+
+    def sorted_keys(self):
+        n = self.n_dynamic
+        keys = np.zeros(n, np.uint32)
+        ids = np.zeros(n, np.uint32)
+        cnt = C.c_uint32()
+        check(lib().upf_get_sorted_keys(self._h, _p(keys, C.c_uint32), _p(ids, C.c_uint32), C.byref(cnt)),
+              "upf_get_sorted_keys")
+        return keys, ids
+
+    def cell_ranges(self):
+        bpa = 1024 // int(self.params.block_size)
+        nc = bpa ** 3
+        start = np.zeros(nc, np.uint32)
+        end = np.zeros(nc, np.uint32)
+        cnt = C.c_uint32()
+        check(lib().upf_get_cell_ranges(self._h, _p(start, C.c_uint32), _p(end, C.c_uint32), C.byref(cnt)),
+              "upf_get_cell_ranges")
+        return start, end

@@ -1,0 +1,815 @@
+// upf_api.cu — the C ABI (include/upf.h): handle lifetime, uploads, the
+// CUDA-graph step and readback.
+//
+// The reference allocates with MallocDeviceArraysParticles
+// (src/gpu/particles.cu:100-166), uploads with Copy*HostToDevice
+// (particles.cu:349-646), steps with ParticlePhysicsOnDevice*
+// (particles.cu:1281-2769) and reads back with CopyParticlesCUDA
+// (particles.cu:62-72). Its PCISPH loop is host-driven: one device-to-host
+// read of the max predicted density per iteration (particles.cu:1917-1944,
+// 2139-2154). Here one step is a single CUDA graph and the loop is a
+// device-side conditional while-node fed by the loop-control kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "upf_sys.h"
+
+namespace upf {
+
+namespace {
+thread_local char g_err[512] = "";
+}
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+namespace {
+
+#define UPF_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return UPF_ERR_CUDA;                                                              \
+    }                                                                                   \
+  } while (0)
+
+template <class T>
+upf_status dalloc(System& s, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    *p = nullptr;
+    return UPF_ERR_ALLOC;
+  }
+  s.allocations.push_back(*p);
+  return UPF_OK;
+}
+
+#define UPF_TRY(call)              \
+  do {                             \
+    upf_status st_ = (call);       \
+    if (st_ != UPF_OK) return st_; \
+  } while (0)
+
+uint32_t log2u(uint32_t v) {
+  uint32_t r = 0;
+  while ((1u << r) < v) ++r;
+  return r;
+}
+
+DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
+  DevParams d{};
+  d.h = p.support_radius;
+  d.lut_factor = (float)(1.0 / (double)p.support_radius);
+  d.mass = p.mass;
+  d.inv_mass = (float)(1.0 / (double)p.mass);
+  d.rho0 = p.rest_density;
+  d.kernel_self = kernel_self(p.support_radius);
+  d.gas_b = p.rest_density * p.gas_constant / p.gamma;
+  d.gamma = p.gamma;
+  d.visc = p.viscosity;
+  d.rest_volume = p.mass / p.rest_density;
+  d.gravity = p.gravity;
+  d.dt = p.dt;
+  d.delta = p.density_error_factor;
+  d.err_scale = 100.0f / p.rest_density;
+  d.max_err = p.max_density_error;
+  d.min_loops = p.min_loops;
+  d.max_loops = p.max_loops;
+  d.st_gamma = p.surface_tension_gamma;
+  d.adh_beta = p.surface_adhesion_beta;
+  d.force_dist = p.force_distance;
+  d.inv_force_dist = 1.0f / p.force_distance;
+  d.max_boundary_force = p.max_boundary_force;
+  d.radius = p.particle_radius;
+  d.spacing = p.particle_spacing;
+  d.spring = p.spring_coefficient;
+  d.spring_boundary = p.spring_coefficient_boundary;
+  d.damping = p.damping_coefficient;
+  d.terminal_speed = p.terminal_speed;
+  d.gran_kr = p.granular_kr;
+  d.gran_kd = p.granular_kd;
+  d.gran_kt = p.granular_kt;
+  d.gran_mu = p.granular_mu;
+  d.origin = make_float3(p.zindex_origin[0], p.zindex_origin[1], p.zindex_origin[2]);
+  d.scales = make_float3(p.scales[0], p.scales[1], p.scales[2]);
+  d.cmin = make_float3(p.collision_min[0], p.collision_min[1], p.collision_min[2]);
+  d.cmax = make_float3(p.collision_max[0], p.collision_max[1], p.collision_max[2]);
+  d.wmin = make_float3(p.container_min[0], p.container_min[1], p.container_min[2]);
+  d.wmax = make_float3(p.container_max[0], p.container_max[1], p.container_max[2]);
+  d.block_shift = log2u(p.block_size);
+  d.blocks_per_axis = UPF_GRID_RESOLUTION / p.block_size;
+  d.flags = p.flags;
+  d.maxn = p.max_neighbors;
+  d.nstride = nstride;
+  return d;
+}
+
+void destroy_graph(System& s) {
+  if (s.step_exec) cudaGraphExecDestroy(s.step_exec);
+  if (s.step_graph) cudaGraphDestroy(s.step_graph);
+  s.step_exec = nullptr;
+  s.step_graph = nullptr;
+}
+
+// One step as a graph: sort -> neighbours -> forces -> [while: loop body] -> integrate.
+upf_status build_step_graph(System& s) {
+  destroy_graph(s);
+  cudaStream_t cs = nullptr, body_stream = nullptr;
+  UPF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  UPF_CUDA(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
+  auto cleanup = [&]() {
+    cudaStreamDestroy(cs);
+    cudaStreamDestroy(body_stream);
+  };
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cleanup();
+    set_error("cudaStreamBeginCapture: %s", cudaGetErrorString(e));
+    return UPF_ERR_CUDA;
+  }
+  auto fail = [&](const char* what, cudaError_t err) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(cs, &g);
+    if (g) cudaGraphDestroy(g);
+    cleanup();
+    set_error("step graph: %s: %s", what, cudaGetErrorString(err));
+    return UPF_ERR_CUDA;
+  };
+  if ((e = launch_sort_phase(s, cs)) != cudaSuccess) return fail("sort", e);
+  if ((e = launch_neighbor_phase(s, cs)) != cudaSuccess) return fail("neighbours", e);
+  if ((e = launch_force_phase(s, cs)) != cudaSuccess) return fail("forces", e);
+  if (s.prm.method == UPF_METHOD_PCISPH) {
+    if ((e = launch_loop_init(s, cs)) != cudaSuccess) return fail("loop init", e);
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    if ((e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &g, &deps, &ndeps)) != cudaSuccess)
+      return fail("capture info", e);
+    cudaGraphConditionalHandle handle;
+    if ((e = cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+      return fail("conditional handle", e);
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    if ((e = cudaGraphAddNode(&cnode, g, deps, ndeps, &np)) != cudaSuccess) return fail("while node", e);
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if ((e = cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+      return fail("capture dependencies", e);
+    if ((e = cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return fail("body capture", e);
+    cudaError_t eb = launch_loop_body(s, body_stream, handle, true);
+    cudaGraph_t body_out = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(body_stream, &body_out);
+    if (eb != cudaSuccess) return fail("loop body", eb);
+    if (ee != cudaSuccess) return fail("body end capture", ee);
+  }
+  if ((e = launch_integrate_phase(s, cs)) != cudaSuccess) return fail("integrate", e);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(cs, &graph);
+  cleanup();
+  if (e != cudaSuccess) {
+    set_error("step graph end capture: %s", cudaGetErrorString(e));
+    return UPF_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&s.step_exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    set_error("step graph instantiate: %s", cudaGetErrorString(e));
+    return UPF_ERR_CUDA;
+  }
+  s.step_graph = graph;
+  return UPF_OK;
+}
+
+upf_status check_device_errors(System& s) {
+  UPF_CUDA(cudaMemcpyAsync(s.st_host, s.st, sizeof(DevState), cudaMemcpyDeviceToHost, s.stream));
+  UPF_CUDA(cudaStreamSynchronize(s.stream));
+  const uint32_t f = s.st_host->error_flags;
+  if (f & ERR_NAN) {
+    set_error("a particle position became NaN");
+    return UPF_ERR_NAN;
+  }
+  if (f & ERR_OVERFLOW) {
+    set_error("a particle has %u neighbours, more than max_neighbors=%u", s.st_host->max_neighbors,
+              s.prm.max_neighbors);
+    return UPF_ERR_NEIGHBOR_OVERFLOW;
+  }
+  if (f & ERR_TIMEOUT) {
+    set_error("a bounded device-side wait ran out");
+    return UPF_ERR_TIMEOUT;
+  }
+  return UPF_OK;
+}
+
+__global__ void k_init_dyn(uint32_t n, DynArrays A, float rho0) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  A.lag[i] = make_float4(0.0f, 0.0f, rho0, 0.0f);
+}
+
+__global__ void k_gather_static(uint32_t n, const uint32_t* __restrict__ perm, const float4* __restrict__ in,
+                                const uint32_t* __restrict__ in_id, float4* __restrict__ out,
+                                uint32_t* __restrict__ out_id) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t j = perm[i];
+  out[i] = in[j];
+  out_id[i] = in_id[j];
+}
+
+}  // namespace
+}  // namespace upf
+
+using namespace upf;
+
+struct upf_system : System {};
+
+extern "C" {
+
+const char* upf_last_error(void) { return g_err; }
+
+const char* upf_status_string(upf_status st) {
+  switch (st) {
+    case UPF_OK: return "UPF_OK";
+    case UPF_ERR_INVALID_ARG: return "UPF_ERR_INVALID_ARG";
+    case UPF_ERR_CUDA: return "UPF_ERR_CUDA";
+    case UPF_ERR_ALLOC: return "UPF_ERR_ALLOC";
+    case UPF_ERR_NEIGHBOR_OVERFLOW: return "UPF_ERR_NEIGHBOR_OVERFLOW";
+    case UPF_ERR_NAN: return "UPF_ERR_NAN";
+    case UPF_ERR_TIMEOUT: return "UPF_ERR_TIMEOUT";
+    case UPF_ERR_STATE: return "UPF_ERR_STATE";
+    case UPF_ERR_UNSUPPORTED: return "UPF_ERR_UNSUPPORTED";
+    case UPF_ERR_NO_DEVICE: return "UPF_ERR_NO_DEVICE";
+  }
+  return "unknown";
+}
+
+int32_t upf_abi_version(void) { return UPF_ABI_VERSION; }
+
+upf_status upf_default_params(upf_params* p) {
+  if (!p) {
+    set_error("upf_default_params: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  default_params(p);
+  return UPF_OK;
+}
+
+upf_status upf_params_derive(upf_params* p) {
+  if (!p) {
+    set_error("upf_params_derive: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (derive_params(p, nullptr) != 0) {
+    set_error("upf_params_derive: particle_spacing and zindex_extent must be > 0");
+    return UPF_ERR_INVALID_ARG;
+  }
+  return UPF_OK;
+}
+
+upf_status upf_density_error_factor(const upf_params* p, double* out) {
+  if (!p || !out) {
+    set_error("upf_density_error_factor: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  *out = density_error_factor(*p);
+  return UPF_OK;
+}
+
+upf_status upf_build_luts(const upf_params* p, float* out) {
+  if (!p || !out || !(p->support_radius > 0)) {
+    set_error("upf_build_luts: bad arguments");
+    return UPF_ERR_INVALID_ARG;
+  }
+  build_luts(*p, out);
+  return UPF_OK;
+}
+
+upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_system** out) {
+  if (!p || !out || capacity == 0) {
+    set_error("upf_create: null argument or zero capacity");
+    return UPF_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  const char* why = nullptr;
+  if (validate_params(*p, &why) != 0) {
+    set_error("upf_create: invalid parameters: %s", why);
+    return UPF_ERR_INVALID_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("upf_create: no CUDA device");
+    return UPF_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error("upf_create: device %d out of range (%d devices)", device, ndev);
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaSetDevice(device));
+  UPF_CUDA(radix_init());
+  upf_system* s = new upf_system();
+  s->prm = *p;
+  s->device = device;
+  s->capacity = capacity;
+  s->nstride = (capacity + 31) & ~31u;
+  s->dp = make_dev_params(*p, s->nstride);
+  const uint32_t bpa = UPF_GRID_RESOLUTION / p->block_size;
+  s->ncells = bpa * bpa * bpa;
+  auto bail = [&](upf_status st) {
+    upf_destroy(s);
+    return st;
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    set_error("cudaStreamCreate: %s", cudaGetErrorString(e));
+    return bail(UPF_ERR_CUDA);
+  }
+  s->own_stream = true;
+  const uint32_t c = capacity;
+  upf_status st = UPF_OK;
+#define ALLOC(ptr, count)                   \
+  if ((st = dalloc(*s, &(ptr), (count))) != UPF_OK) return bail(st);
+  ALLOC(s->A.pos, c); ALLOC(s->A.vel, c); ALLOC(s->A.lag, c); ALLOC(s->A.id, c); ALLOC(s->A.type, c);
+  ALLOC(s->B.pos, c); ALLOC(s->B.vel, c); ALLOC(s->B.lag, c); ALLOC(s->B.id, c); ALLOC(s->B.type, c);
+  ALLOC(s->keysA, c); ALLOC(s->perm, c);
+  ALLOC(s->sort_tmp, radix_temp_words(c));
+  ALLOC(s->force, c); ALLOC(s->pforce, c); ALLOC(s->xs, c);
+  ALLOC(s->rho, c); ALLOC(s->press, c); ALLOC(s->wvol_dyn, c);
+  ALLOC(s->nbr, (size_t)s->nstride * p->max_neighbors);
+  ALLOC(s->ncnt, c);
+  ALLOC(s->cstart, s->ncells); ALLOC(s->cend, s->ncells);
+  ALLOC(s->sstart, s->ncells); ALLOC(s->send, s->ncells);
+  ALLOC(s->spos, c); ALLOC(s->skeys, c); ALLOC(s->sid, c); ALLOC(s->swvol, c);
+  ALLOC(s->luts, 5 * UPF_LUT_ENTRIES);
+  ALLOC(s->st, 1);
+#undef ALLOC
+  e = cudaMallocHost((void**)&s->st_host, sizeof(DevState));
+  if (e != cudaSuccess) {
+    s->st_host = nullptr;
+    set_error("cudaMallocHost: %s", cudaGetErrorString(e));
+    return bail(UPF_ERR_ALLOC);
+  }
+  std::vector<float> lut(5 * UPF_LUT_ENTRIES);
+  build_luts(*p, lut.data());
+  e = cudaMemcpy(s->luts, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(s->st, 0, sizeof(DevState));
+  if (e != cudaSuccess) {
+    set_error("upload: %s", cudaGetErrorString(e));
+    return bail(UPF_ERR_CUDA);
+  }
+  *out = s;
+  return UPF_OK;
+}
+
+upf_status upf_destroy(upf_system* s) {
+  if (!s) return UPF_OK;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  destroy_graph(*s);
+  for (void* p : s->allocations) cudaFree(p);
+  if (s->st_host) cudaFreeHost(s->st_host);
+  if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return UPF_OK;
+}
+
+upf_status upf_get_params(const upf_system* s, upf_params* out) {
+  if (!s || !out) {
+    set_error("upf_get_params: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  *out = s->prm;
+  return UPF_OK;
+}
+
+upf_status upf_set_stream(upf_system* s, void* stream) {
+  if (!s) {
+    set_error("upf_set_stream: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  if (s->own_stream) cudaStreamDestroy(s->stream);
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+  } else {
+    UPF_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->own_stream = true;
+  }
+  return UPF_OK;
+}
+
+upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4, const int32_t* type,
+                             uint32_t n) {
+  if (!s || (n && (!pos4 || !vel4 || !type))) {
+    set_error("upf_set_particles: null argument");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (n > s->capacity) {
+    set_error("upf_set_particles: %u particles exceed capacity %u", n, s->capacity);
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaSetDevice(s->device));
+  std::vector<float4> dpos, dvel, spos;
+  std::vector<uint32_t> did, sid;
+  std::vector<int32_t> dtype;
+  for (uint32_t i = 0; i < n; ++i) {
+    const int32_t t = type[i];
+    if (t < 0 || t > UPF_FROZEN) {
+      set_error("upf_set_particles: particle %u has unknown type %d", i, t);
+      return UPF_ERR_INVALID_ARG;
+    }
+    if (t != UPF_LIQUID && t != UPF_FROZEN && t != UPF_RIGID) {
+      set_error("upf_set_particles: particle %u has type %d; supported: LIQUID, RIGID, FROZEN", i, t);
+      return UPF_ERR_UNSUPPORTED;
+    }
+    float4 x = make_float4(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2], 0.0f);
+    if (t == UPF_FROZEN) {
+      spos.push_back(x);
+      sid.push_back(i);
+    } else {
+      dpos.push_back(x);
+      dvel.push_back(make_float4(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2], 0.0f));
+      did.push_back(i);
+      dtype.push_back(t);
+    }
+  }
+  System& S = *s;
+  cudaStream_t st = S.stream;
+  S.n_dyn = (uint32_t)dpos.size();
+  S.n_static = (uint32_t)spos.size();
+  if (S.n_dyn) {
+    UPF_CUDA(cudaMemcpyAsync(S.A.pos, dpos.data(), sizeof(float4) * S.n_dyn, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.vel, dvel.data(), sizeof(float4) * S.n_dyn, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.id, did.data(), sizeof(uint32_t) * S.n_dyn, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.type, dtype.data(), sizeof(int32_t) * S.n_dyn, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(morton_keys(S.A.pos, S.n_dyn, S.dp.origin, S.dp.scales, S.keysA, st));
+    k_init_dyn<<<(S.n_dyn + 255) / 256, 256, 0, st>>>(S.n_dyn, S.A, S.prm.rest_density);
+    UPF_CUDA(cudaGetLastError());
+  }
+  // boundary set: sort once by key (stable), gather positions and ids
+  if (S.n_static) {
+    float4* tmp_pos = S.xs;           // scratch: per-step fields are not live yet
+    uint32_t* tmp_id = (uint32_t*)S.rho;
+    uint32_t* perm = S.ncnt;
+    UPF_CUDA(cudaMemcpyAsync(tmp_pos, spos.data(), sizeof(float4) * S.n_static, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(tmp_id, sid.data(), sizeof(uint32_t) * S.n_static, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(morton_keys(tmp_pos, S.n_static, S.dp.origin, S.dp.scales, S.skeys, st));
+    uint32_t* kalt = S.sort_tmp;
+    uint32_t* valt = kalt + ((S.n_static + 63) & ~63u);
+    uint32_t* counts = valt + ((S.n_static + 63) & ~63u);
+    UPF_CUDA(radix_sort_pairs(S.skeys, perm, kalt, valt, counts, S.n_static, S.key_bits, true, st));
+    k_gather_static<<<(S.n_static + 255) / 256, 256, 0, st>>>(S.n_static, perm, tmp_pos, tmp_id, S.spos, S.sid);
+    UPF_CUDA(cudaGetLastError());
+    // default Akinci volume: the rest volume (UnifiedParticle.cpp:24)
+    std::vector<float> wv(S.n_static, S.prm.mass / S.prm.rest_density);
+    UPF_CUDA(cudaMemcpyAsync(S.swvol, wv.data(), sizeof(float) * S.n_static, cudaMemcpyHostToDevice, st));
+  }
+  UPF_CUDA(launch_static_setup(S, st));
+  UPF_CUDA(cudaMemsetAsync(S.st, 0, sizeof(DevState), st));
+  UPF_CUDA(cudaStreamSynchronize(st));
+  S.have_particles = true;
+  return build_step_graph(S);
+}
+
+upf_status upf_set_rigid_bodies(upf_system* s, const int32_t*, uint32_t, uint32_t) {
+  if (!s) {
+    set_error("upf_set_rigid_bodies: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  set_error("upf_set_rigid_bodies: rigid bodies are not available in this build");
+  return UPF_ERR_UNSUPPORTED;
+}
+
+upf_status upf_step(upf_system* s, int32_t nsteps) {
+  if (!s || nsteps < 0) {
+    set_error("upf_step: bad arguments");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (!s->have_particles || !s->step_exec) {
+    set_error("upf_step: call upf_set_particles first");
+    return UPF_ERR_STATE;
+  }
+  for (int32_t k = 0; k < nsteps; ++k) UPF_CUDA(cudaGraphLaunch(s->step_exec, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_synchronize(upf_system* s) {
+  if (!s) {
+    set_error("upf_synchronize: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_errors(*s);
+}
+
+upf_status upf_get_step_stats(upf_system* s, upf_step_stats* out) {
+  if (!s || !out) {
+    set_error("upf_get_step_stats: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  upf_status st = check_device_errors(*s);
+  const DevState& d = *s->st_host;
+  std::memset(out, 0, sizeof(*out));
+  out->iterations = s->prm.method == UPF_METHOD_PCISPH ? d.final_iterations : 0;
+  out->hit_max_loops = (s->prm.method == UPF_METHOD_PCISPH && d.final_iterations >= s->prm.max_loops);
+  out->max_predicted_density = d.final_max_rho;
+  out->density_error_percent = d.final_err;
+  out->max_neighbor_count = d.max_neighbors;
+  out->error_flags = d.error_flags;
+  out->kinetic_energy = d.ke;
+  for (int k = 0; k < 3; ++k) out->momentum[k] = d.mom[k];
+  for (int k = 0; k < 64; ++k) out->iteration_max_density[k] = d.iter_max_rho[k];
+  out->total_steps = d.total_steps;
+  out->total_iterations = d.total_iterations;
+  out->steps_at_max_loops = d.steps_at_max;
+  return st;
+}
+
+upf_status upf_reset_counters(upf_system* s) {
+  if (!s) {
+    set_error("upf_reset_counters: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  const size_t off = offsetof(DevState, total_steps);
+  UPF_CUDA(cudaMemsetAsync((char*)s->st + off, 0, sizeof(DevState) - off, s->stream));
+  return UPF_OK;
+}
+
+// ---- phases ---------------------------------------------------------------
+static upf_status phase_guard(upf_system* s) {
+  if (!s) {
+    set_error("phase: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (!s->have_particles) {
+    set_error("phase: call upf_set_particles first");
+    return UPF_ERR_STATE;
+  }
+  return UPF_OK;
+}
+
+upf_status upf_phase_sort(upf_system* s) {
+  UPF_TRY(phase_guard(s));
+  UPF_CUDA(launch_sort_phase(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_phase_neighbors(upf_system* s) {
+  UPF_TRY(phase_guard(s));
+  UPF_CUDA(launch_neighbor_phase(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_phase_forces(upf_system* s) {
+  UPF_TRY(phase_guard(s));
+  UPF_CUDA(launch_force_phase(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_phase_predict_correct(upf_system* s) {
+  UPF_TRY(phase_guard(s));
+  if (s->prm.method != UPF_METHOD_PCISPH) return UPF_OK;
+  UPF_CUDA(launch_loop_init(*s, s->stream));
+  // host-driven loop (the graph path runs the same body under a while-node)
+  for (int it = 0; it < s->prm.max_loops + 1; ++it) {
+    UPF_CUDA(launch_loop_body(*s, s->stream, 0, false));
+    UPF_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+    UPF_CUDA(cudaStreamSynchronize(s->stream));
+    const DevState& d = *s->st_host;
+    int cont = (d.iteration < s->prm.min_loops) || (d.too_large && d.iteration < s->prm.max_loops);
+    if (d.error_flags & ERR_NAN) cont = 0;
+    if (!cont) break;
+  }
+  return UPF_OK;
+}
+
+upf_status upf_phase_integrate(upf_system* s) {
+  UPF_TRY(phase_guard(s));
+  UPF_CUDA(launch_integrate_phase(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_upload_state(upf_system* s, const float* pos4, const float* vel4, uint32_t n) {
+  UPF_TRY(phase_guard(s));
+  if (n != s->n_dyn || (n && (!pos4 || !vel4))) {
+    set_error("upf_upload_state: need %u dynamic particles and non-null arrays", s->n_dyn);
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (!n) return UPF_OK;
+  UPF_CUDA(cudaMemcpyAsync(s->A.pos, pos4, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+  UPF_CUDA(cudaMemcpyAsync(s->A.vel, vel4, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+  UPF_CUDA(launch_upload_keys(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_profile_step(upf_system* s, upf_phase_times* out) {
+  UPF_TRY(phase_guard(s));
+  if (!out) {
+    set_error("upf_profile_step: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  std::memset(out, 0, sizeof(*out));
+  cudaStream_t st = s->stream;
+  cudaEvent_t ev[8];
+  for (auto& e : ev) UPF_CUDA(cudaEventCreate(&e));
+  auto elapsed = [&](cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  };
+  upf_status rc = UPF_OK;
+  do {
+    UPF_CUDA(cudaEventRecord(ev[0], st));
+    UPF_CUDA(launch_sort_phase(*s, st));
+    UPF_CUDA(cudaEventRecord(ev[1], st));
+    UPF_CUDA(launch_neighbor_phase(*s, st));
+    UPF_CUDA(cudaEventRecord(ev[2], st));
+    UPF_CUDA(launch_force_phase(*s, st));
+    UPF_CUDA(cudaEventRecord(ev[3], st));
+    UPF_CUDA(cudaStreamSynchronize(st));
+    out->sort_ms = elapsed(ev[0], ev[1]);
+    out->neighbors_ms = elapsed(ev[1], ev[2]);
+    out->forces_ms = elapsed(ev[2], ev[3]);
+    float loop = 0;
+    if (s->prm.method == UPF_METHOD_PCISPH) {
+      UPF_CUDA(launch_loop_init(*s, st));
+      for (int it = 0; it < s->prm.max_loops + 1; ++it) {
+        UPF_CUDA(cudaEventRecord(ev[4], st));
+        UPF_CUDA(launch_loop_density(*s, st));
+        UPF_CUDA(cudaEventRecord(ev[5], st));
+        UPF_CUDA(launch_loop_pforce(*s, st));
+        UPF_CUDA(cudaEventRecord(ev[6], st));
+        UPF_CUDA(launch_loop_ctl(*s, st, 0, false));
+        UPF_CUDA(cudaEventRecord(ev[7], st));
+        UPF_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+        UPF_CUDA(cudaStreamSynchronize(st));
+        out->density_ms_total += elapsed(ev[4], ev[5]);
+        out->pforce_ms_total += elapsed(ev[5], ev[6]);
+        loop += elapsed(ev[4], ev[7]);
+        const DevState& d = *s->st_host;
+        int cont = (d.iteration < s->prm.min_loops) || (d.too_large && d.iteration < s->prm.max_loops);
+        if (d.error_flags & ERR_NAN) cont = 0;
+        out->iterations = d.iteration;
+        if (!cont) break;
+      }
+    }
+    out->loop_ms = loop;
+    UPF_CUDA(cudaEventRecord(ev[0], st));
+    UPF_CUDA(launch_integrate_phase(*s, st));
+    UPF_CUDA(cudaEventRecord(ev[1], st));
+    UPF_CUDA(cudaStreamSynchronize(st));
+    out->integrate_ms = elapsed(ev[0], ev[1]);
+    out->launches = pipeline_launches_per_step(*s, out->iterations);
+  } while (0);
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (rc != UPF_OK) return rc;
+  return check_device_errors(*s);
+}
+
+// ---- readback -------------------------------------------------------------
+static upf_status copy_out_f4(void* dst, const float4* src, uint32_t n, cudaStream_t st) {
+  if (!dst || !n) return UPF_OK;
+  UPF_CUDA(cudaMemcpyAsync(dst, src, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+  return UPF_OK;
+}
+
+upf_status upf_get_particles(upf_system* s, float* pos4, float* vel4, float* density, float* pressure,
+                             int32_t* type, uint32_t* id, uint32_t* n_out) {
+  UPF_TRY(phase_guard(s));
+  const uint32_t n = s->n_dyn;
+  cudaStream_t st = s->stream;
+  UPF_TRY(copy_out_f4(pos4, s->A.pos, n, st));
+  UPF_TRY(copy_out_f4(vel4, s->A.vel, n, st));
+  if (density && n) UPF_CUDA(cudaMemcpyAsync(density, s->rho, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+  if (pressure && n) UPF_CUDA(cudaMemcpyAsync(pressure, s->press, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+  if (type && n) UPF_CUDA(cudaMemcpyAsync(type, s->A.type, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+  if (id && n) UPF_CUDA(cudaMemcpyAsync(id, s->A.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+  UPF_CUDA(cudaStreamSynchronize(st));
+  if (n_out) *n_out = n;
+  return UPF_OK;
+}
+
+upf_status upf_get_step_fields(upf_system* s, float* force4, float* pforce4, float* predicted_density,
+                               uint32_t* id, uint32_t* n_out) {
+  UPF_TRY(phase_guard(s));
+  const uint32_t n = s->n_dyn;
+  cudaStream_t st = s->stream;
+  UPF_TRY(copy_out_f4(force4, s->force, n, st));
+  UPF_TRY(copy_out_f4(pforce4, s->pforce, n, st));
+  if (predicted_density && n)
+    UPF_CUDA(cudaMemcpyAsync(predicted_density, s->rho, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+  if (id && n) UPF_CUDA(cudaMemcpyAsync(id, s->B.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+  UPF_CUDA(cudaStreamSynchronize(st));
+  if (n_out) *n_out = n;
+  return UPF_OK;
+}
+
+upf_status upf_get_neighbors(upf_system* s, uint32_t* counts, uint32_t* lists, uint32_t cap, uint32_t* n_out) {
+  UPF_TRY(phase_guard(s));
+  const uint32_t n = s->n_dyn;
+  if (n_out) *n_out = n;
+  if (!n) return UPF_OK;
+  cudaStream_t st = s->stream;
+  std::vector<uint32_t> cnt(n), bid(n), sid(s->n_static);
+  UPF_CUDA(cudaMemcpyAsync(cnt.data(), s->ncnt, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+  UPF_CUDA(cudaMemcpyAsync(bid.data(), s->B.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+  if (s->n_static)
+    UPF_CUDA(cudaMemcpyAsync(sid.data(), s->sid, sizeof(uint32_t) * s->n_static, cudaMemcpyDeviceToHost, st));
+  const uint32_t maxn = s->prm.max_neighbors;
+  std::vector<uint32_t> nb((size_t)s->nstride * maxn);
+  UPF_CUDA(cudaMemcpyAsync(nb.data(), s->nbr, sizeof(uint32_t) * nb.size(), cudaMemcpyDeviceToHost, st));
+  UPF_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < n; ++i) {
+    if (counts) counts[i] = cnt[i];
+    if (!lists) continue;
+    for (uint32_t k = 0; k < cnt[i] && k < cap; ++k) {
+      uint32_t code = nb[(size_t)k * s->nstride + i];
+      lists[(size_t)i * cap + k] = (code & kStaticBit) ? sid[code & ~kStaticBit] : bid[code];
+    }
+  }
+  return UPF_OK;
+}
+
+upf_status upf_get_sorted_keys(upf_system* s, uint32_t* keys, uint32_t* ids, uint32_t* n_out) {
+  UPF_TRY(phase_guard(s));
+  const uint32_t n = s->n_dyn;
+  if (keys && n) UPF_CUDA(cudaMemcpyAsync(keys, s->keysA, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (ids && n) UPF_CUDA(cudaMemcpyAsync(ids, s->B.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  if (n_out) *n_out = n;
+  return UPF_OK;
+}
+
+upf_status upf_get_cell_ranges(upf_system* s, uint32_t* start, uint32_t* end, uint32_t* ncells_out) {
+  UPF_TRY(phase_guard(s));
+  if (start) UPF_CUDA(cudaMemcpyAsync(start, s->cstart, sizeof(uint32_t) * s->ncells, cudaMemcpyDeviceToHost, s->stream));
+  if (end) UPF_CUDA(cudaMemcpyAsync(end, s->cend, sizeof(uint32_t) * s->ncells, cudaMemcpyDeviceToHost, s->stream));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  if (ncells_out) *ncells_out = s->ncells;
+  return UPF_OK;
+}
+
+// ---- stateless building blocks ---------------------------------------------
+upf_status upf_morton_keys(const float* pos4, uint32_t n, const float origin[3], const float scales[3],
+                           uint32_t* keys, void* stream) {
+  if (n && (!pos4 || !keys || !origin || !scales)) {
+    set_error("upf_morton_keys: null argument");
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(morton_keys((const float4*)pos4, n, make_float3(origin[0], origin[1], origin[2]),
+                       make_float3(scales[0], scales[1], scales[2]), keys, (cudaStream_t)stream));
+  return UPF_OK;
+}
+
+size_t upf_radix_sort_temp_bytes(uint32_t n) { return radix_temp_bytes(n); }
+
+upf_status upf_radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int32_t key_bits, void* temp,
+                                size_t temp_bytes, void* stream) {
+  if (n == 0) return UPF_OK;
+  if (!keys || !vals || !temp || key_bits < 1 || key_bits > 32) {
+    set_error("upf_radix_sort_pairs: bad arguments");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (temp_bytes < radix_temp_bytes(n)) {
+    set_error("upf_radix_sort_pairs: temp_bytes %zu < required %zu", temp_bytes, radix_temp_bytes(n));
+    return UPF_ERR_INVALID_ARG;
+  }
+  uint32_t* kalt = (uint32_t*)temp;
+  uint32_t* valt = kalt + ((n + 63) & ~63u);
+  uint32_t* counts = valt + ((n + 63) & ~63u);
+  UPF_CUDA(radix_sort_pairs(keys, vals, kalt, valt, counts, n, key_bits, false, (cudaStream_t)stream));
+  return UPF_OK;
+}
+
+upf_status upf_cell_ranges(const uint32_t* keys, uint32_t n, int32_t shift, uint32_t ncells, uint32_t* start,
+                           uint32_t* end, void* stream) {
+  if ((n && !keys) || !start || !end || shift < 0 || shift > 31 || ncells == 0) {
+    set_error("upf_cell_ranges: bad arguments");
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cell_ranges(keys, n, shift, ncells, start, end, (cudaStream_t)stream));
+  return UPF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// upf_common.cuh — device-side types and helpers shared by the kernels.
+//
+// Every operation that decides something discrete (neighbour membership,
+// lookup-table bin, Morton cell, clamp) is written with explicit
+// round-to-nearest intrinsics in the reference CPU path's operation order, so
+// that those decisions are bit-identical to the CPU path. The library is
+// additionally compiled with -fmad=false so that continuous sums also round
+// operation by operation like the CPU path (no contraction into FMA).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/upf.h"
+
+namespace upf {
+
+constexpr int kLut = UPF_LUT_SIZE;
+constexpr uint32_t kStaticBit = 0x80000000u;  // neighbour index refers to the boundary set
+
+enum LutId { LUT_M4 = 0, LUT_PGRAD = 1, LUT_VISC = 2, LUT_ST = 3, LUT_ADH = 4 };
+
+// Error flag bits in DevState::error_flags
+enum : uint32_t { ERR_OVERFLOW = 1u, ERR_NAN = 2u, ERR_TIMEOUT = 4u };
+
+// Everything a kernel needs from upf_params, by value.
+struct DevParams {
+  float h;            // support radius
+  float lut_factor;   // (float)(1.0 / h): the reference's function-static factor
+  float mass;
+  float inv_mass;     // (float)(1.0 / mass)
+  float rho0;
+  float kernel_self;  // KernelM4(0, h)
+  float gas_b;        // rest_density * gas_constant / gamma
+  float gamma;
+  float visc;
+  float rest_volume;  // mass / rho0
+  float gravity;
+  float dt;
+  float delta;        // PCISPH density error factor
+  float err_scale;    // 100 / rho0
+  float max_err;
+  int min_loops, max_loops;
+  float st_gamma, adh_beta;
+  float force_dist, inv_force_dist, max_boundary_force;
+  float radius, spacing;
+  float spring, spring_boundary, damping, terminal_speed;
+  float gran_kr, gran_kd, gran_kt, gran_mu;
+  float3 origin, scales;
+  float3 cmin, cmax;       // collision box
+  float3 wmin, wmax;       // real container
+  uint32_t block_shift;    // log2(block_size)
+  uint32_t blocks_per_axis;
+  uint32_t flags;
+  uint32_t maxn;
+  uint32_t nstride;        // neighbour-list column stride
+};
+
+// Device-side scalars of one system.
+struct DevState {
+  uint32_t max_rho_bits;   // running max predicted density (positive floats order as uints)
+  int32_t iteration;
+  int32_t too_large;
+  uint32_t error_flags;
+  uint32_t max_neighbors;
+  int32_t final_iterations;
+  float final_max_rho;
+  float final_err;
+  double ke;
+  double mom[3];
+  float iter_max_rho[64];
+  int32_t total_steps;
+  int32_t total_iterations;
+  int32_t steps_at_max;
+};
+
+// ---- exact float helpers --------------------------------------------------
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+
+// |a - b| as vmml computes it: sqrtf((dx*dx + dy*dy) + dz*dz)
+__device__ __forceinline__ float dist3(float4 a, float4 b) {
+  float dx = fsub(a.x, b.x), dy = fsub(a.y, b.y), dz = fsub(a.z, b.z);
+  return __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
+}
+
+// LUT bin of WeightingKernel::kernel*Lut: int index = dist * factor * 300
+__device__ __forceinline__ int lut_index(float d, float factor) {
+  return (int)fmul(fmul(d, factor), (float)kLut);
+}
+// PCISPH dist_lut: uint(dist * 300 / h), clamped to 300
+__device__ __forceinline__ unsigned dist_lut(float d, float h) {
+  unsigned dl = (unsigned)__fdiv_rn(fmul(d, (float)kLut), h);
+  return dl > (unsigned)kLut ? (unsigned)kLut : dl;
+}
+
+// Morton interleave of a 10-bit coordinate (x -> bits 3i, y -> 3i+1, z -> 3i+2),
+// the z_table_ of ZIndex::ZIndex (src/cpu/zIndex.cpp:10-24).
+__host__ __device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+
+// float -> unsigned short truncation of the key coordinate, clamped to the grid
+__device__ __forceinline__ uint32_t grid_coord(float c) {
+  if (!(c > 0.0f)) return 0;
+  if (c >= 1023.0f) return 1023;
+  return (uint32_t)c;
+}
+
+// zIndex.CalcIndex(scales * (x - origin))
+__device__ __forceinline__ uint32_t morton_key(float4 x, const float3& origin, const float3& scales) {
+  uint32_t cx = grid_coord(fmul(scales.x, fsub(x.x, origin.x)));
+  uint32_t cy = grid_coord(fmul(scales.y, fsub(x.y, origin.y)));
+  uint32_t cz = grid_coord(fmul(scales.z, fsub(x.z, origin.z)));
+  return morton3(cx, cy, cz);
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace upf

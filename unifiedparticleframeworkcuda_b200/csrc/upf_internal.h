@@ -1,0 +1,41 @@
+// upf_internal.h — declarations shared between the library's translation
+// units (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/upf.h"
+
+namespace upf {
+
+struct DevParams;
+struct DevState;
+
+// upf_params.cpp (host math, compiled with -ffp-contract=off)
+void default_params(upf_params* p);
+int derive_params(upf_params* p, double* delta_fp64);
+void build_luts(const upf_params& p, float* out_5x301);
+float kernel_self(float h);
+int validate_params(const upf_params& p, const char** why);
+double density_error_factor(const upf_params& p);
+
+// upf_sort.cu
+uint32_t radix_tiles(uint32_t n);
+size_t radix_temp_words(uint32_t n);
+size_t radix_temp_bytes(uint32_t n);
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                             uint32_t* counts, uint32_t n, int key_bits, bool iota_values,
+                             cudaStream_t st);
+int radix_launches(int key_bits);
+cudaError_t radix_init();
+cudaError_t morton_keys(const float4* pos, uint32_t n, float3 origin, float3 scales, uint32_t* keys,
+                        cudaStream_t st);
+cudaError_t cell_ranges(const uint32_t* keys, uint32_t n, int shift, uint32_t ncells, uint32_t* start,
+                        uint32_t* end, cudaStream_t st);
+
+// error reporting (upf_api.cu)
+void set_error(const char* fmt, ...);
+
+}  // namespace upf

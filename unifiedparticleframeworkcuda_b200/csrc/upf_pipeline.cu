@@ -1,0 +1,798 @@
+// upf_pipeline.cu — the per-step kernels.
+//
+// Step = sort (Morton keys -> radix sort -> reorder -> cell ranges)
+//      -> neighbour lists
+//      -> WCSPH: density/pressure, then force + integration
+//         PCISPH: external forces, then the predict-correct loop
+//                 (predicted density + pressure update, pressure force +
+//                 next prediction, loop control), then integration.
+// Every kernel is one thread per particle over the sorted working set; the
+// neighbour loops read the column-major lists, so a warp's list reads are
+// coalesced and its position gathers hit the Morton-ordered neighbourhood in
+// L1/L2.
+//
+// Reference kernels replaced (src/gpu/particles_kernel.cu):
+//   FillZindicesKernel 3360, CopySortedParticleValuesKernel* 543-654,
+//   ClearIndexArrays/CalculateBlocksKernel/RedistributeBlocks* 656-810,
+//   CalculateDensitiesInBlocksKernelWCSPH 1529-1708,
+//   CalculateForcesInBlocksKernelWCSPH 2399-2653,
+//   CalculateExternalForcesInBlocksKernelPCISPH 3397-3621,
+//   PredictPositionAndVelocityBlocksKernelPCISPH 3624-3660,
+//   ComputePredictedDensityAndPressureBlocksKernelPCISPH 3662-3842,
+//   ComputeCorrectivePressureForceBlocksKernelPCISPH 4034-4211,
+//   ReduceMax + GetReductionFinalMax (particles.cu:2840-2932, kernel.cu:3381),
+//   TimeIntegrationBlocksKernelPCISPHPureFluid 5033-5104.
+// The arithmetic follows the reference's CPU path (src/cpu/UnifiedPhysics.cpp),
+// which is the parity target; each kernel cites the function it restates.
+#include <cuda_runtime.h>
+
+#include "upf_sys.h"
+
+namespace upf {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ float mx0(float a, float b) { return (a >= b) ? a : b; }  // MAX macro
+
+__device__ __forceinline__ float lut_at(const float* s, float d, float factor) {
+  int idx = lut_index(d, factor);
+  return idx >= kLut ? 0.0f : s[idx];
+}
+
+__device__ __forceinline__ void stage_lut(float* dst, const float* __restrict__ src) {
+  for (int k = threadIdx.x; k < UPF_LUT_ENTRIES; k += blockDim.x) dst[k] = src[k];
+}
+
+__device__ __forceinline__ float4 f4(float x, float y, float z) { return make_float4(x, y, z, 0.0f); }
+
+// ---------------------------------------------------------------- reorder
+// CopySortedParticleValuesKernel* (particles_kernel.cu:543-654): gather the
+// state into sorted order.
+__global__ void __launch_bounds__(kBlock) k_reorder(uint32_t n, const uint32_t* __restrict__ perm,
+                                                     DynArrays A, DynArrays B, bool with_lag) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t j = perm[i];
+  B.pos[i] = A.pos[j];
+  B.vel[i] = A.vel[j];
+  B.id[i] = A.id[j];
+  B.type[i] = A.type[j];
+  if (with_lag) B.lag[i] = A.lag[j];
+}
+
+// ---------------------------------------------------------------- neighbours
+// GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
+// (zIndex.cpp:43-73): candidates are the Morton blocks covering the query box
+// (with a one-grid-unit margin, so the candidate set is a superset of the
+// reference's), visited in ascending Morton order; within a block the dynamic
+// and boundary ranges are merged by key. The list therefore comes out in the
+// reference's ascending sorted-index order, and membership is the reference's
+// exact test: j != i and |x_i - x_j| < h in float.
+__global__ void __launch_bounds__(kBlock) k_build_nlist(
+    DevParams P, uint32_t n, const float4* __restrict__ pos, const uint32_t* __restrict__ keys,
+    const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, uint32_t ns,
+    const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
+    const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, uint32_t* __restrict__ nbr,
+    uint32_t* __restrict__ ncnt, DevState* __restrict__ st) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 xi = pos[i];
+  const float h = P.h;
+  int lo[3], hi[3];
+  {
+    const float c[3] = {(xi.x - P.origin.x) * P.scales.x, (xi.y - P.origin.y) * P.scales.y,
+                        (xi.z - P.origin.z) * P.scales.z};
+    const float r[3] = {h * P.scales.x, h * P.scales.y, h * P.scales.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float l = c[a] - r[a] - 1.0f, u = c[a] + r[a] + 1.0f;
+      int li = (l <= 0.0f) ? 0 : (l >= 1023.0f ? 1023 : (int)l);
+      int ui = (u <= 0.0f) ? 0 : (u >= 1023.0f ? 1023 : (int)u);
+      lo[a] = li >> P.block_shift;
+      hi[a] = ui >> P.block_shift;
+    }
+  }
+  const uint32_t maxn = P.maxn, stride = P.nstride;
+  uint32_t cnt = 0;
+  auto append = [&](uint32_t code) {
+    if (cnt < maxn) nbr[(size_t)cnt * stride + i] = code;
+    cnt++;
+  };
+  auto visit = [&](uint32_t c) {
+    uint32_t ds = cstart[c], de = cend[c];
+    uint32_t ss = 0, se = 0;
+    if (ns) {
+      ss = sstart[c];
+      se = send[c];
+    }
+    while (ds < de || ss < se) {
+      bool take_dyn = (ds < de) && (ss >= se || keys[ds] <= skeys[ss]);
+      if (take_dyn) {
+        uint32_t j = ds++;
+        if (j != i && dist3(xi, pos[j]) < h) append(j);
+      } else {
+        uint32_t j = ss++;
+        if (dist3(xi, spos[j]) < h) append(j | kStaticBit);
+      }
+    }
+  };
+  const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+  const int nblk = nx * ny * nz;
+  if (nblk <= 64) {
+    uint32_t codes[64];
+    int m = 0;
+    for (int bz = lo[2]; bz <= hi[2]; ++bz)
+      for (int by = lo[1]; by <= hi[1]; ++by)
+        for (int bx = lo[0]; bx <= hi[0]; ++bx) {
+          uint32_t c = morton3(bx, by, bz);
+          int q = m++;
+          while (q > 0 && codes[q - 1] > c) {
+            codes[q] = codes[q - 1];
+            --q;
+          }
+          codes[q] = c;
+        }
+    for (int q = 0; q < m; ++q) visit(codes[q]);
+  } else {
+    for (int bz = lo[2]; bz <= hi[2]; ++bz)
+      for (int by = lo[1]; by <= hi[1]; ++by)
+        for (int bx = lo[0]; bx <= hi[0]; ++bx) visit(morton3(bx, by, bz));
+  }
+  ncnt[i] = cnt < maxn ? cnt : maxn;
+  if (cnt > maxn) atomicOr(&st->error_flags, (uint32_t)ERR_OVERFLOW);
+  atomicMax(&st->max_neighbors, cnt);
+}
+
+// ---------------------------------------------------------------- WCSPH
+// DistanceToWall (UnifiedPhysics.cpp:5926-5990) and WallWeight (6032-6060)
+__device__ float wall_weight(const DevParams& P, const float* m4, float4 x) {
+  const float L = P.wmax.x - P.wmin.x, H = P.wmax.y - P.wmin.y, W = P.wmax.z - P.wmin.z;
+  float res = mx0(L, mx0(H, W));
+  float d;
+  d = mx0(x.y - P.wmin.y, 0.0f); res = (res <= d) ? res : d;
+  d = mx0(P.wmax.y - x.y, 0.0f); res = (res <= d) ? res : d;
+  d = mx0(x.x - P.wmin.x, 0.0f); res = (res <= d) ? res : d;
+  d = mx0(P.wmax.x - x.x, 0.0f); res = (res <= d) ? res : d;
+  d = mx0(x.z - P.wmin.z, 0.0f); res = (res <= d) ? res : d;
+  d = mx0(P.wmax.z - x.z, 0.0f); res = (res <= d) ? res : d;
+  const float eff = P.h - P.radius;
+  if (res >= eff) return 0.0f;
+  const float s = P.spacing;
+  float d1 = res + P.radius;
+  float d2 = d1 + s;
+  float d3 = sqrtf(d1 * d1 + s * s);
+  float d4 = sqrtf(d1 * d1 + (s * 2) * (s * 2));
+  float d5 = sqrtf(d2 * d2 + s * s);
+  float d6 = sqrtf(d2 * d2 + (s * 2) * (s * 2));
+  float k1 = lut_at(m4, d1, P.lut_factor), k2 = lut_at(m4, d2, P.lut_factor),
+        k3 = lut_at(m4, d3, P.lut_factor), k4 = lut_at(m4, d4, P.lut_factor),
+        k5 = lut_at(m4, d5, P.lut_factor), k6 = lut_at(m4, d6, P.lut_factor);
+  return P.mass * (k1 + k2 + 2 * (k3 + k4 + k5 + k6));
+}
+
+// CalculateDensityPressurePureFluidSPH + CalculatePressureWCSPH
+// (UnifiedPhysics.cpp:2408-2501), liquid particles.
+__global__ void __launch_bounds__(kBlock) k_wcsph_density(
+    DevParams P, uint32_t n, const float4* __restrict__ pos, const int32_t* __restrict__ type,
+    const float4* __restrict__ spos, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
+    const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press) {
+  __shared__ float m4[UPF_LUT_ENTRIES];
+  stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
+  __syncthreads();
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (type[i] != UPF_LIQUID) return;
+  const float4 xi = pos[i];
+  const float m = P.mass;
+  float den = P.kernel_self * m;
+  const uint32_t c = ncnt[i];
+  for (uint32_t k = 0; k < c; ++k) {
+    uint32_t code = nbr[(size_t)k * P.nstride + i];
+    float4 xj = (code & kStaticBit) ? spos[code & ~kStaticBit] : pos[code];
+    float d = dist3(xi, xj);
+    if (d < P.h) {
+      float kv = lut_at(m4, d, P.lut_factor);
+      den += kv * m;
+    }
+  }
+  if (P.flags & UPF_FLAG_WALL_WEIGHT) den += wall_weight(P, m4, xi);
+  const float frac = den / P.rho0;
+  const float powg = powf(frac, P.gamma);
+  const float pr = P.gas_b * (powg - 1.0f);
+  rho[i] = den;
+  press[i] = (0.0f >= pr) ? 0.0f : pr;
+}
+
+// WeightingKernel::kernelSplineSurfaceTension (WeightingKernel.cpp:210-231)
+__device__ float cohesion_spline(float dist, float sr) {
+  const float c = 32.0f / ((3.14159274f * sr * sr * sr * sr * sr * sr * sr * sr * sr));
+  if (dist > 0.5 * sr && dist <= sr) return c * (sr - dist) * (sr - dist) * (sr - dist) * dist * dist * dist;
+  if (dist > 0 && dist <= 0.5 * sr)
+    return c * (2.0f * (sr - dist) * (sr - dist) * (sr - dist) * dist * dist * dist -
+                sr * sr * sr * sr * sr * sr / 64.0f);
+  return 0.0f;
+}
+
+// BoundaryHandlingBoxPerNonRigidParticle (UnifiedPhysics.cpp:4000-4044)
+__device__ __forceinline__ void clamp_box(const DevParams& P, float4& x, float4& v, float damping) {
+  if (x.y < P.cmin.y) { x.y = P.cmin.y; v.y *= damping; }
+  if (x.y > P.cmax.y) { x.y = P.cmax.y; v.y *= damping; }
+  if (x.x < P.cmin.x) { x.x = P.cmin.x; v.x *= damping; }
+  if (x.x > P.cmax.x) { x.x = P.cmax.x; v.x *= damping; }
+  if (x.z < P.cmin.z) { x.z = P.cmin.z; v.z *= damping; }
+  if (x.z > P.cmax.z) { x.z = P.cmax.z; v.z *= damping; }
+}
+
+__device__ __forceinline__ void block_stats(DevState* st, double ke, double mx, double my, double mz) {
+  __shared__ double red[4][kBlock / 32];
+  ke = warp_sum(ke);
+  mx = warp_sum(mx);
+  my = warp_sum(my);
+  mz = warp_sum(mz);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][w] = ke; red[1][w] = mx; red[2][w] = my; red[3][w] = mz;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0, c = 0, d = 0;
+    for (int k = 0; k < (int)(blockDim.x / 32); ++k) {
+      a += red[0][k]; b += red[1][k]; c += red[2][k]; d += red[3][k];
+    }
+    atomicAdd(&st->ke, a);
+    atomicAdd(&st->mom[0], b);
+    atomicAdd(&st->mom[1], c);
+    atomicAdd(&st->mom[2], d);
+  }
+}
+
+// UpdateLiquidParticlePosVelSphCPU (UnifiedPhysics.cpp:3705-3742) + boundary
+// handling with damping -0.5 + new key (UnifiedPhysics.cpp:3972-3998):
+// writes the A copy.
+__device__ __forceinline__ void integrate_store(const DevParams& P, uint32_t i, float4 x, float4 v, float3 F,
+                                                DynArrays& A, uint32_t* keysA, const DynArrays& B,
+                                                double& ke, double& mx, double& my, double& mz) {
+  v.x = v.x + F.x * P.inv_mass * P.dt;
+  v.y = v.y + F.y * P.inv_mass * P.dt;
+  v.z = v.z + F.z * P.inv_mass * P.dt;
+  x.x = x.x + v.x * P.dt;
+  x.y = x.y + v.y * P.dt;
+  x.z = x.z + v.z * P.dt;
+  clamp_box(P, x, v, -0.5f);
+  A.pos[i] = x;
+  A.vel[i] = v;
+  keysA[i] = morton_key(x, P.origin, P.scales);
+  const double m = P.mass;
+  ke = 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+  mx = m * v.x;
+  my = m * v.y;
+  mz = m * v.z;
+  if (isnan(x.x) || isnan(x.y) || isnan(x.z)) ke = nan("");
+}
+
+// CalculateLiquidParticleForces (UnifiedPhysics.cpp:3009-3083) + gravity +
+// integration (the reference's GPU path fuses these too,
+// CalculateForcesInBlocksKernelWCSPH particles_kernel.cu:2399-2653).
+__global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
+    DevParams P, uint32_t n, DynArrays B, DynArrays A, uint32_t* __restrict__ keysA,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    const float* __restrict__ rho, const float* __restrict__ press, float4* __restrict__ force,
+    DevState* __restrict__ st) {
+  __shared__ float pg[UPF_LUT_ENTRIES], vl[UPF_LUT_ENTRIES];
+  stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
+  stage_lut(vl, luts + LUT_VISC * UPF_LUT_ENTRIES);
+  __syncthreads();
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0, mx = 0, my = 0, mz = 0;
+  if (i < n) {
+    const int32_t ti = B.type[i];
+    float4 xi = B.pos[i], vi = B.vel[i];
+    if (ti == UPF_LIQUID) {
+      const float m = P.mass, h = P.h;
+      const float di = rho[i], pi = press[i];
+      const float invD = (float)(1.0 / (double)di);
+      const float pVol = m * invD;
+      float fx = 0, fy = 0, fz = 0;
+      const uint32_t c = ncnt[i];
+      for (uint32_t k = 0; k < c; ++k) {
+        uint32_t code = nbr[(size_t)k * P.nstride + i];
+        if (code & kStaticBit) continue;  // boundary particles are never liquid
+        if (B.type[code] != UPF_LIQUID) continue;
+        const float4 xj = B.pos[code];
+        float d = dist3(xi, xj);
+        if (!(d < h)) continue;
+        const float kv = lut_at(vl, d, P.lut_factor);
+        const float dj = rho[code], pj = press[code];
+        const float nVol = m / dj;
+        const float dvx = xi.x - xj.x, dvy = xi.y - xj.y, dvz = xi.z - xj.z;
+        const float g = lut_at(pg, d, P.lut_factor);
+        const float grad = pi * invD * invD + pj / (dj * dj);
+        fx = fx - dvx * g * grad * m * m;
+        fy = fy - dvy * g * grad * m * m;
+        fz = fz - dvz * g * grad * m * m;
+        const float4 vj = B.vel[code];
+        const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+        fx = fx - vx * pVol * nVol * P.visc * kv;
+        fy = fy - vy * pVol * nVol * P.visc * kv;
+        fz = fz - vz * pVol * nVol * P.visc * kv;
+        if ((P.flags & UPF_FLAG_SURFACE_TENSION) && d >= h * 0.25f) {
+          const float sp = cohesion_spline(d, h);
+          const float inv = 1.0f / d;
+          fx = fx - dvx * P.st_gamma * m * m * sp * inv;
+          fy = fy - dvy * P.st_gamma * m * m * sp * inv;
+          fz = fz - dvz * P.st_gamma * m * m * sp * inv;
+        }
+      }
+      fy -= m * P.gravity;
+      force[i] = f4(fx, fy, fz);
+      integrate_store(P, i, xi, vi, make_float3(fx, fy, fz), A, keysA, B, ke, mx, my, mz);
+    } else {
+      A.pos[i] = xi;
+      A.vel[i] = vi;
+      keysA[i] = morton_key(xi, P.origin, P.scales);
+      force[i] = f4(0, 0, 0);
+    }
+    A.id[i] = B.id[i];
+    A.type[i] = ti;
+  }
+  if (!(ke == ke)) {
+    atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
+    ke = 0;
+  }
+  block_stats(st, ke, mx, my, mz);
+}
+
+// ---------------------------------------------------------------- PCISPH
+// CalculateBoundaryForcePerLiquidParticleHost (UnifiedPhysics.cpp:2032-2069):
+// the scalar is evaluated in double because of the 2.0 literal.
+__device__ __forceinline__ float wall_term(float t, const DevParams& P) {
+  return (float)((double)(t * P.inv_force_dist) * 2.0 * (double)P.max_boundary_force);
+}
+
+__device__ __forceinline__ void penalty_walls(const DevParams& P, float4 x, float& fx, float& fy, float& fz) {
+  const float fd = P.force_dist;
+  if (x.x < P.cmin.x + fd) fx += wall_term(P.cmin.x + fd - x.x, P);
+  if (x.x > P.cmax.x - fd) fx += -1.0f * wall_term(x.x + fd - P.cmax.x, P);
+  if (x.y < P.cmin.y + fd) fy += wall_term(P.cmin.y + fd - x.y, P);
+  if (x.y > P.cmax.y - fd) fy += -1.0f * wall_term(x.y + fd - P.cmax.y, P);
+  if (x.z < P.cmin.z + fd) fz += wall_term(P.cmin.z + fd - x.z, P);
+  if (x.z > P.cmax.z - fd) fz += -1.0f * wall_term(x.z + fd - P.cmax.z, P);
+}
+
+// PredictPositionAndVelocity + CollisionHandling (UnifiedPhysics.cpp:5426-5454, 5739-5757)
+__device__ __forceinline__ float4 predict(const DevParams& P, float4 x, float4 v, float3 F, float3 Fp,
+                                          bool& bad) {
+  const float inv = 1.0f / P.mass;  // vmml: vector / scalar multiplies by the reciprocal
+  float vx = v.x + (F.x + Fp.x) * P.dt * inv;
+  float vy = v.y + (F.y + Fp.y) * P.dt * inv;
+  float vz = v.z + (F.z + Fp.z) * P.dt * inv;
+  float4 xs = make_float4(x.x + vx * P.dt, x.y + vy * P.dt, x.z + vz * P.dt, 0.0f);
+  if (xs.x < P.cmin.x) xs.x = P.cmin.x;
+  if (xs.x > P.cmax.x) xs.x = P.cmax.x;
+  if (xs.y < P.cmin.y) xs.y = P.cmin.y;
+  if (xs.y > P.cmax.y) xs.y = P.cmax.y;
+  if (xs.z < P.cmin.z) xs.z = P.cmin.z;
+  if (xs.z > P.cmax.z) xs.z = P.cmax.z;
+  bad = isnan(xs.x) || isnan(xs.y) || isnan(xs.z);
+  return xs;
+}
+
+// CalculateBoundaryFluidPressureForceHost (UnifiedPhysics.cpp:4240-4250),
+// indexed by distance; lagged pressure and predicted density of the liquid
+// particle, Akinci volume of the boundary particle.
+__device__ __forceinline__ void boundary_pressure(const DevParams& P, const float* pg, float d, float4 xi,
+                                                  float4 xj, float rho_prev, float p_prev, float wvol,
+                                                  float& fx, float& fy, float& fz) {
+  const float inv_den = 1.0f / rho_prev;
+  const float g = lut_at(pg, d, P.lut_factor);
+  const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
+  const float pgd = p_prev * inv_den * inv_den;
+  fx = fx + kx * pgd * P.mass * P.rho0 * wvol * (-1.0f);
+  fy = fy + ky * pgd * P.mass * P.rho0 * wvol * (-1.0f);
+  fz = fz + kz * pgd * P.mass * P.rho0 * wvol * (-1.0f);
+}
+
+// CalculateExternalForcesVersatilCouplingPCISPH (UnifiedPhysics.cpp:5252-5365),
+// liquid particles; then the first prediction of the loop.
+__global__ void __launch_bounds__(kBlock) k_pcisph_external(
+    DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const float* __restrict__ swvol,
+    const float* __restrict__ wvol_dyn, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
+    const float* __restrict__ luts, float4* __restrict__ force, float4* __restrict__ pforce,
+    float4* __restrict__ xs, float* __restrict__ press, DevState* __restrict__ st) {
+  __shared__ float vl[UPF_LUT_ENTRIES], pg[UPF_LUT_ENTRIES], stl[UPF_LUT_ENTRIES], adl[UPF_LUT_ENTRIES];
+  stage_lut(vl, luts + LUT_VISC * UPF_LUT_ENTRIES);
+  stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
+  stage_lut(stl, luts + LUT_ST * UPF_LUT_ENTRIES);
+  stage_lut(adl, luts + LUT_ADH * UPF_LUT_ENTRIES);
+  __syncthreads();
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t ti = B.type[i];
+  const float4 xi = B.pos[i];
+  press[i] = 0.0f;
+  pforce[i] = f4(0, 0, 0);
+  if (ti != UPF_LIQUID) {
+    force[i] = f4(0, 0, 0);
+    xs[i] = xi;
+    return;
+  }
+  const float4 vi = B.vel[i];
+  const float4 lag = B.lag[i];
+  const float m = P.mass, h = P.h, rv = P.rest_volume;
+  const uint32_t flags = P.flags;
+  float fx = 0, fy = 0, fz = 0;
+  const uint32_t c = ncnt[i];
+  for (uint32_t k = 0; k < c; ++k) {
+    uint32_t code = nbr[(size_t)k * P.nstride + i];
+    const bool is_static = code & kStaticBit;
+    const uint32_t j = code & ~kStaticBit;
+    const float4 xj = is_static ? spos[j] : B.pos[j];
+    const float d = dist3(xi, xj);
+    if (!(d < h)) continue;
+    const unsigned dl = dist_lut(d, h);
+    const int32_t tj = is_static ? UPF_FROZEN : B.type[j];
+    if (tj == UPF_LIQUID) {
+      const float kv = lut_at(vl, d, P.lut_factor);
+      const float4 vj = B.vel[j];
+      fx = fx - (vi.x - vj.x) * rv * rv * P.visc * kv;
+      fy = fy - (vi.y - vj.y) * rv * rv * P.visc * kv;
+      fz = fz - (vi.z - vj.z) * rv * rv * P.visc * kv;
+      if ((flags & UPF_FLAG_SURFACE_TENSION) && d >= h * 0.25f) {
+        const float sp = stl[dl];
+        const float inv = 1.0f / d;
+        fx = fx - (xi.x - xj.x) * P.st_gamma * m * m * sp * inv;
+        fy = fy - (xi.y - xj.y) * P.st_gamma * m * m * sp * inv;
+        fz = fz - (xi.z - xj.z) * P.st_gamma * m * m * sp * inv;
+      }
+    } else if (tj == UPF_FROZEN || tj == UPF_RIGID) {
+      const float wv = is_static ? swvol[j] : wvol_dyn[j];
+      // the reference passes the liquid particle's own weighted volume (its
+      // rest volume) to the pressure term, UnifiedPhysics.cpp:5292
+      if (flags & UPF_FLAG_BOUNDARY_PRESSURE)
+        boundary_pressure(P, pg, d, xi, xj, lag.z, lag.x, rv, fx, fy, fz);
+      if ((flags & UPF_FLAG_ADHESION) && d >= h * 0.25f) {
+        const float sp = adl[dl];
+        const float inv = 1.0f / d;
+        fx = fx - (xi.x - xj.x) * P.adh_beta * m * P.rho0 * wv * sp * inv;
+        fy = fy - (xi.y - xj.y) * P.adh_beta * m * P.rho0 * wv * sp * inv;
+        fz = fz - (xi.z - xj.z) * P.adh_beta * m * P.rho0 * wv * sp * inv;
+      }
+    }
+  }
+  fy -= m * P.gravity;
+  if (flags & UPF_FLAG_PENALTY_WALLS) penalty_walls(P, xi, fx, fy, fz);
+  force[i] = f4(fx, fy, fz);
+  bool bad;
+  xs[i] = predict(P, xi, vi, make_float3(fx, fy, fz), make_float3(0, 0, 0), bad);
+  if (bad) atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
+}
+
+// ComputePredictedDensityAndPressure (UnifiedPhysics.cpp:5456-5491) with the
+// maximum for the loop test reduced in the same pass.
+__global__ void __launch_bounds__(kBlock) k_pcisph_density(
+    DevParams P, uint32_t n, const int32_t* __restrict__ type, const float4* __restrict__ xs,
+    const float4* __restrict__ spos, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
+    const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press,
+    DevState* __restrict__ st) {
+  __shared__ float m4[UPF_LUT_ENTRIES];
+  __shared__ uint32_t wmax[kBlock / 32];
+  stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
+  __syncthreads();
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t best = 0;
+  if (i < n && type[i] == UPF_LIQUID) {
+    const float4 xi = xs[i];
+    const float m = P.mass;
+    float den = P.kernel_self * m;
+    const uint32_t c = ncnt[i];
+    for (uint32_t k = 0; k < c; ++k) {
+      uint32_t code = nbr[(size_t)k * P.nstride + i];
+      const float4 xj = (code & kStaticBit) ? spos[code & ~kStaticBit] : xs[code];
+      const float d = dist3(xi, xj);
+      if (d < P.h) {
+        const float kv = lut_at(m4, d, P.lut_factor);
+        den += kv * m;
+      }
+    }
+    const float err = mx0(den - P.rho0, 0.0f);
+    press[i] = press[i] + mx0(err * P.delta, 0.0f);
+    rho[i] = den;
+    best = __float_as_uint(den);  // densities are positive: uint order == float order
+  }
+  best = warp_max(best);
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t v = threadIdx.x < (blockDim.x >> 5) ? wmax[threadIdx.x] : 0u;
+    v = warp_max(v);
+    if (threadIdx.x == 0 && v) atomicMax(&st->max_rho_bits, v);
+  }
+}
+
+// ComputeCorrectivePressureForce (UnifiedPhysics.cpp:5493-5522), then the
+// prediction of the next iteration (PredictPositionAndVelocity).
+__global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
+    DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts, const float* __restrict__ press,
+    const float4* __restrict__ force, float4* __restrict__ pforce, float4* __restrict__ xs,
+    DevState* __restrict__ st) {
+  __shared__ float pg[UPF_LUT_ENTRIES];
+  stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
+  __syncthreads();
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (B.type[i] != UPF_LIQUID) return;
+  const float4 xi = B.pos[i];
+  const float m = P.mass, rho0 = P.rho0;
+  const float densSq = rho0 * rho0;
+  const float pi = press[i];
+  float fx = 0, fy = 0, fz = 0;
+  const uint32_t c = ncnt[i];
+  for (uint32_t k = 0; k < c; ++k) {
+    uint32_t code = nbr[(size_t)k * P.nstride + i];
+    const bool is_static = code & kStaticBit;
+    const uint32_t j = code & ~kStaticBit;
+    const float4 xj = is_static ? spos[j] : B.pos[j];
+    const float d = dist3(xi, xj);
+    if (d < P.h) {
+      const float pj = is_static ? 0.0f : press[j];
+      const float g = lut_at(pg, d, P.lut_factor);
+      const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
+      const float grad = pi / densSq + pj / (rho0 * rho0);
+      fx = fx - kx * grad * m * m;
+      fy = fy - ky * grad * m * m;
+      fz = fz - kz * grad * m * m;
+    }
+  }
+  pforce[i] = f4(fx, fy, fz);
+  const float4 F = force[i];
+  bool bad;
+  xs[i] = predict(P, xi, B.vel[i], make_float3(F.x, F.y, F.z), make_float3(fx, fy, fz), bad);
+  if (bad) atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
+}
+
+__global__ void k_loop_init(DevState* st) {
+  st->iteration = 0;
+  st->too_large = 1;
+  st->max_rho_bits = 0;
+  st->ke = 0;
+  st->mom[0] = st->mom[1] = st->mom[2] = 0;
+}
+
+__global__ void k_step_init(DevState* st, int count_step) {
+  st->ke = 0;
+  st->mom[0] = st->mom[1] = st->mom[2] = 0;
+  st->max_neighbors = 0;
+  if (count_step) st->total_steps += 1;  // PCISPH counts its steps in the loop control
+}
+
+// Loop control of PredictionCorrectionStep (UnifiedPhysics.cpp:5376-5420):
+// continue while iteration < min_loops, or the error is still too large and
+// iteration < max_loops. The "too large" flag is sticky-false, as in the
+// reference. Runs on the device and feeds the graph's conditional node.
+__global__ void k_loop_ctl(DevParams P, DevState* st, cudaGraphConditionalHandle h, int use_handle) {
+  const int it = st->iteration + 1;
+  st->iteration = it;
+  const float maxd = __uint_as_float(st->max_rho_bits);
+  const float e = mx0(P.err_scale * maxd - 100.0f, 0.0f);
+  if (it <= 64) st->iter_max_rho[it - 1] = maxd;
+  if (e < P.max_err) st->too_large = 0;
+  int cont = (it < P.min_loops) || (st->too_large && it < P.max_loops);
+  if (st->error_flags & ERR_NAN) cont = 0;
+  st->final_iterations = it;
+  st->final_max_rho = maxd;
+  st->final_err = e;
+  st->max_rho_bits = 0;
+  if (!cont) {
+    st->total_steps += 1;
+    st->total_iterations += it;
+    if (it >= P.max_loops) st->steps_at_max += 1;
+  }
+  if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
+// Integration for PCISPH: force + pressure force (UnifiedPhysics.cpp:3710-3712),
+// and the lagged pressure state carried to the next step.
+__global__ void __launch_bounds__(kBlock) k_pcisph_integrate(
+    DevParams P, uint32_t n, DynArrays B, DynArrays A, uint32_t* __restrict__ keysA,
+    const float4* __restrict__ force, const float4* __restrict__ pforce, const float* __restrict__ rho,
+    const float* __restrict__ press, DevState* __restrict__ st) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0, mx = 0, my = 0, mz = 0;
+  if (i < n) {
+    const int32_t ti = B.type[i];
+    const float4 xi = B.pos[i], vi = B.vel[i];
+    const float4 lag = B.lag[i];
+    if (ti == UPF_LIQUID) {
+      const float4 F = force[i], Fp = pforce[i];
+      integrate_store(P, i, xi, vi, make_float3(F.x + Fp.x, F.y + Fp.y, F.z + Fp.z), A, keysA, B, ke, mx, my,
+                      mz);
+      A.lag[i] = make_float4(lag.y, press[i], rho[i], 0.0f);
+    } else {
+      A.pos[i] = xi;
+      A.vel[i] = vi;
+      keysA[i] = morton_key(xi, P.origin, P.scales);
+      A.lag[i] = lag;
+    }
+    A.id[i] = B.id[i];
+    A.type[i] = ti;
+  }
+  if (!(ke == ke)) {
+    atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
+    ke = 0;
+  }
+  block_stats(st, ke, mx, my, mz);
+}
+
+// Akinci volume of the static boundary (CalculateWeightedVolume,
+// UnifiedPhysics.cpp:2703-2746): V_b = 1 / sum over boundary neighbours of W.
+__global__ void __launch_bounds__(kBlock) k_static_wvol(DevParams P, uint32_t ns, const float4* __restrict__ spos,
+                                                         const uint32_t* __restrict__ sstart,
+                                                         const uint32_t* __restrict__ send,
+                                                         const float* __restrict__ luts, float* __restrict__ wvol) {
+  __shared__ float m4[UPF_LUT_ENTRIES];
+  stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
+  __syncthreads();
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  const float4 xi = spos[i];
+  const float h = P.h;
+  int lo[3], hi[3];
+  const float c[3] = {(xi.x - P.origin.x) * P.scales.x, (xi.y - P.origin.y) * P.scales.y,
+                      (xi.z - P.origin.z) * P.scales.z};
+  const float r[3] = {h * P.scales.x, h * P.scales.y, h * P.scales.z};
+  for (int a = 0; a < 3; ++a) {
+    float l = c[a] - r[a] - 1.0f, u = c[a] + r[a] + 1.0f;
+    int li = (l <= 0.0f) ? 0 : (l >= 1023.0f ? 1023 : (int)l);
+    int ui = (u <= 0.0f) ? 0 : (u >= 1023.0f ? 1023 : (int)u);
+    lo[a] = li >> P.block_shift;
+    hi[a] = ui >> P.block_shift;
+  }
+  // accumulate in the reference's ascending order: blocks by Morton code
+  uint32_t codes[64];
+  int m = 0;
+  const int nblk = (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+  float inv = 0.0f;
+  auto visit = [&](uint32_t cc) {
+    for (uint32_t j = sstart[cc]; j < send[cc]; ++j) {
+      if (j == i) continue;
+      float d = dist3(xi, spos[j]);
+      if (d < h) inv += lut_at(m4, d, P.lut_factor);
+    }
+  };
+  if (nblk <= 64) {
+    for (int bz = lo[2]; bz <= hi[2]; ++bz)
+      for (int by = lo[1]; by <= hi[1]; ++by)
+        for (int bx = lo[0]; bx <= hi[0]; ++bx) {
+          uint32_t cc = morton3(bx, by, bz);
+          int q = m++;
+          while (q > 0 && codes[q - 1] > cc) {
+            codes[q] = codes[q - 1];
+            --q;
+          }
+          codes[q] = cc;
+        }
+    for (int q = 0; q < m; ++q) visit(codes[q]);
+  } else {
+    for (int bz = lo[2]; bz <= hi[2]; ++bz)
+      for (int by = lo[1]; by <= hi[1]; ++by)
+        for (int bx = lo[0]; bx <= hi[0]; ++bx) visit(morton3(bx, by, bz));
+  }
+  if (inv != 0.0f) wvol[i] = (float)(1.0 / (double)inv);
+}
+
+inline uint32_t grid_of(uint32_t n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+// ----------------------------------------------------------------- launchers
+cudaError_t launch_sort_phase(System& s, cudaStream_t st) {
+  const uint32_t n = s.n_dyn;
+  if (n == 0) return cudaSuccess;
+  uint32_t* kalt = s.sort_tmp;
+  uint32_t* valt = kalt + ((n + 63) & ~63u);
+  uint32_t* counts = valt + ((n + 63) & ~63u);
+  cudaError_t e = radix_sort_pairs(s.keysA, s.perm, kalt, valt, counts, n, s.key_bits, true, st);
+  if (e != cudaSuccess) return e;
+  k_reorder<<<grid_of(n), kBlock, 0, st>>>(n, s.perm, s.A, s.B, s.prm.method == UPF_METHOD_PCISPH);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cell_ranges(s.keysA, n, 3 * (int)s.dp.block_shift, s.ncells, s.cstart, s.cend, st);
+}
+
+cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
+  const uint32_t n = s.n_dyn;
+  k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
+  if (n == 0) return cudaGetLastError();
+  k_build_nlist<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
+                                                s.skeys, s.sstart, s.send, s.nbr, s.ncnt, s.st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_force_phase(System& s, cudaStream_t st) {
+  const uint32_t n = s.n_dyn;
+  if (n == 0) return cudaSuccess;
+  if (s.prm.method == UPF_METHOD_WCSPH) {
+    k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.spos, s.nbr, s.ncnt, s.luts, s.rho,
+                                                   s.press);
+  } else {
+    k_pcisph_external<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.swvol, s.wvol_dyn, s.nbr, s.ncnt,
+                                                     s.luts, s.force, s.pforce, s.xs, s.press, s.st);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loop_init(System& s, cudaStream_t st) {
+  k_loop_init<<<1, 1, 0, st>>>(s.st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loop_density(System& s, cudaStream_t st) {
+  const uint32_t n = s.n_dyn;
+  if (n)
+    k_pcisph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.type, s.xs, s.spos, s.nbr, s.ncnt, s.luts, s.rho,
+                                                    s.press, s.st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
+  const uint32_t n = s.n_dyn;
+  if (n)
+    k_pcisph_pressure_force<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.nbr, s.ncnt, s.luts, s.press,
+                                                           s.force, s.pforce, s.xs, s.st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loop_ctl(System& s, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle) {
+  k_loop_ctl<<<1, 1, 0, st>>>(s.dp, s.st, h, use_handle ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loop_body(System& s, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle) {
+  cudaError_t e = launch_loop_density(s, st);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_loop_pforce(s, st)) != cudaSuccess) return e;
+  return launch_loop_ctl(s, st, h, use_handle);
+}
+
+cudaError_t launch_upload_keys(System& s, cudaStream_t st) {
+  return morton_keys(s.A.pos, s.n_dyn, s.dp.origin, s.dp.scales, s.keysA, st);
+}
+
+cudaError_t launch_integrate_phase(System& s, cudaStream_t st) {
+  const uint32_t n = s.n_dyn;
+  if (n == 0) return cudaSuccess;
+  if (s.prm.method == UPF_METHOD_WCSPH) {
+    k_wcsph_force_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.nbr, s.ncnt, s.luts, s.rho,
+                                                           s.press, s.force, s.st);
+  } else {
+    k_pcisph_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.force, s.pforce, s.rho, s.press,
+                                                      s.st);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_static_setup(System& s, cudaStream_t st) {
+  // boundary set: keys -> stable sort -> gather -> cell ranges -> Akinci volumes
+  const uint32_t ns = s.n_static;
+  cudaError_t e = cudaMemsetAsync(s.sstart, 0, sizeof(uint32_t) * s.ncells, st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(s.send, 0, sizeof(uint32_t) * s.ncells, st);
+  if (e != cudaSuccess) return e;
+  if (ns == 0) return cudaSuccess;
+  e = cell_ranges(s.skeys, ns, 3 * (int)s.dp.block_shift, s.ncells, s.sstart, s.send, st);
+  if (e != cudaSuccess) return e;
+  k_static_wvol<<<grid_of(ns), kBlock, 0, st>>>(s.dp, ns, s.spos, s.sstart, s.send, s.luts, s.swvol);
+  return cudaGetLastError();
+}
+
+int pipeline_launches_per_step(const System& s, int iterations) {
+  int sort = radix_launches(s.key_bits) + 1 /*reorder*/ + 1 /*cells*/;
+  int nl = 2;  // step init + neighbour lists
+  if (s.prm.method == UPF_METHOD_WCSPH) return sort + nl + 2;
+  return sort + nl + 1 /*external*/ + 1 /*loop init*/ + 3 * iterations + 1 /*integrate*/;
+}
+
+}  // namespace upf

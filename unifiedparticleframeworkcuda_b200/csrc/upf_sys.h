@@ -1,0 +1,111 @@
+// upf_sys.h — the state behind one upf_system handle (library-internal).
+//
+// Device layout (structure of arrays, float4 for 3-vectors so each gather is
+// one 16-byte transaction):
+//   dynamic set (liquid, rigid, granular particles), two copies:
+//     A = state after integration, in the order of the last sort, with the
+//         Morton keys of the new positions (input to the next sort);
+//     B = the sorted working copy a step reads (gathered from A by the sort
+//         permutation).
+//   boundary set (FROZEN particles): sorted once at upload; static.
+//   per-step fields (indexed like B): external force, correction pressure
+//   force, predicted position, predicted density, correction pressure.
+//   neighbour lists: column-major nbr[k * stride + i] (coalesced reads when
+//   consecutive threads take consecutive particles), bit 31 marks an index
+//   into the boundary set.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "upf_common.cuh"
+#include "upf_internal.h"
+
+namespace upf {
+
+struct DynArrays {
+  float4* pos = nullptr;
+  float4* vel = nullptr;
+  float4* lag = nullptr;   // (previous correction pressure, last final correction pressure, last predicted density, -)
+  uint32_t* id = nullptr;
+  int32_t* type = nullptr;
+};
+
+struct RigidArrays {
+  int32_t* body = nullptr;      // body index of each dynamic particle (-1: not rigid), A/B like the rest
+  float4* r0 = nullptr;         // initial relative position of rigid particles
+};
+
+struct System {
+  upf_params prm{};
+  DevParams dp{};
+  int device = 0;
+  uint32_t capacity = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  uint32_t n_dyn = 0, n_static = 0;
+  bool have_particles = false;
+
+  DynArrays A, B;
+  uint32_t* keysA = nullptr;   // keys of A (sorted in place by the sort)
+  uint32_t* perm = nullptr;    // sort values (permutation into A)
+  uint32_t* sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
+
+  // per-step fields (B order)
+  float4* force = nullptr;
+  float4* pforce = nullptr;
+  float4* xs = nullptr;
+  float* rho = nullptr;
+  float* press = nullptr;
+  float* wvol_dyn = nullptr;   // Akinci volume of dynamic rigid particles
+
+  // neighbour lists
+  uint32_t* nbr = nullptr;
+  uint32_t* ncnt = nullptr;
+  uint32_t nstride = 0;
+
+  // cells
+  uint32_t ncells = 0;
+  uint32_t* cstart = nullptr;
+  uint32_t* cend = nullptr;
+  uint32_t* sstart = nullptr;
+  uint32_t* send = nullptr;
+
+  // boundary set
+  float4* spos = nullptr;
+  uint32_t* skeys = nullptr;
+  uint32_t* sid = nullptr;
+  float* swvol = nullptr;
+
+  // lookup tables (5 x 301 floats)
+  float* luts = nullptr;
+
+  DevState* st = nullptr;      // device scalars
+  DevState* st_host = nullptr; // pinned mirror
+
+  // CUDA graph of one full step
+  cudaGraphExec_t step_exec = nullptr;
+  cudaGraph_t step_graph = nullptr;
+  int key_bits = 30;
+
+  std::vector<void*> allocations;
+};
+
+// upf_pipeline.cu: phase launchers (all asynchronous on s.stream)
+cudaError_t launch_sort_phase(System& s, cudaStream_t st);
+cudaError_t launch_neighbor_phase(System& s, cudaStream_t st);
+cudaError_t launch_force_phase(System& s, cudaStream_t st);
+cudaError_t launch_loop_init(System& s, cudaStream_t st);
+cudaError_t launch_loop_body(System& s, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle);
+cudaError_t launch_loop_density(System& s, cudaStream_t st);
+cudaError_t launch_loop_pforce(System& s, cudaStream_t st);
+cudaError_t launch_loop_ctl(System& s, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle);
+cudaError_t launch_upload_keys(System& s, cudaStream_t st);
+cudaError_t launch_integrate_phase(System& s, cudaStream_t st);
+cudaError_t launch_static_setup(System& s, cudaStream_t st);
+int pipeline_launches_per_step(const System& s, int iterations);
+
+}  // namespace upf

@@ -1,0 +1,208 @@
+"""Seeded synthetic scenes (the reference builds its scenes in
+src/sceneConfigure/Scene.cpp; no dataset is involved).
+
+Random numbers come from an in-repo splitmix64 stream (the reference's
+`drand48` macro is integer division and always 0, src/sceneConfigure/global.h:12),
+so the oracle and the device path consume identical arrays.
+
+Every generator returns a `Scene`: float32 positions/velocities (n x 4),
+int32 types, and the upf parameters (not yet derived).
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from ._abi import (FLAG_BOUNDARY_PRESSURE, FLAG_PENALTY_WALLS, FLAG_SURFACE_TENSION,
+                   FROZEN, LIQUID, METHOD_PCISPH, METHOD_WCSPH, UpfParams)
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, n: int, stream: int = 0) -> np.ndarray:
+    """The first n outputs of splitmix64 started at seed + stream * 2^32."""
+    with np.errstate(over="ignore"):
+        s0 = np.uint64((seed + (stream << 32)) & 0xFFFFFFFFFFFFFFFF)
+        z = s0 + _GOLDEN * np.arange(1, n + 1, dtype=np.uint64)
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform(seed: int, n: int, stream: int = 0) -> np.ndarray:
+    """Uniform doubles in [0, 1)."""
+    return (splitmix64(seed, n, stream) >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+
+
+def normal(seed: int, n: int, stream: int = 0) -> np.ndarray:
+    """Standard normals (Box-Muller over two splitmix64 streams)."""
+    u1 = uniform(seed, n, 2 * stream + 1)
+    u2 = uniform(seed, n, 2 * stream + 2)
+    return np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * np.pi * u2)
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    params: UpfParams
+    pos: np.ndarray    # (n, 4) float32
+    vel: np.ndarray    # (n, 4) float32
+    type: np.ndarray   # (n,) int32
+    body: np.ndarray | None = None  # (n,) int32 body index of RIGID particles, -1 otherwise
+    num_bodies: int = 0
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    @property
+    def n_fluid(self) -> int:
+        return int(np.count_nonzero(self.type == LIQUID))
+
+    @property
+    def n_boundary(self) -> int:
+        return int(np.count_nonzero(self.type == FROZEN))
+
+
+def default_params() -> UpfParams:
+    """UnifiedConstants::UnifiedConstants defaults
+    (src/sceneConfigure/UnifiedConstants.cpp:7-159), before derivation."""
+    p = UpfParams()
+    p.method = METHOD_PCISPH
+    p.flags = FLAG_SURFACE_TENSION | FLAG_PENALTY_WALLS
+    p.particle_spacing = np.float32(1.0 / 40.0)
+    p.rest_density = 1000.0
+    p.gas_constant = 2000.0
+    p.gamma = 7.0
+    p.viscosity = 1.0
+    p.gravity = 9.81
+    p.dt = 0.0012
+    p.density_error_fudge = -1.0
+    p.max_density_error = 1.0
+    p.min_loops = 3
+    p.max_loops = 50
+    p.surface_tension_gamma = 0.3
+    p.surface_adhesion_beta = 0.0
+    p.spring_coefficient = 300.0
+    p.spring_coefficient_boundary = 300.0
+    p.damping_coefficient = 0.5
+    p.terminal_speed = 20.0
+    p.granular_kr = 1.0
+    p.granular_kd = 0.1
+    p.granular_kt = 100.0
+    p.granular_mu = 0.4
+    p.zindex_extent[:] = (2.0, 2.0, 1.5)
+    p.max_neighbors = 128
+    return p
+
+
+def _lattice(nx, ny, nz, spacing, origin, jitter, seed, stream=0):
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    g = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1).astype(np.float64)
+    n = g.shape[0]
+    pos = np.asarray(origin, np.float64)[None, :] + g * spacing
+    if jitter:
+        pos = pos + (uniform(seed, 3 * n, stream).reshape(n, 3) * 2.0 - 1.0) * jitter
+    return pos
+
+
+def box_shell(lo, hi, spacing, layers):
+    """Boundary particles: `layers` lattice shells at `spacing` covering the six
+    faces of the box [lo, hi] (the first shell on the faces, further shells
+    outside)."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    out = []
+    for k in range(layers):
+        a = lo - k * spacing
+        b = hi + k * spacing
+        cnt = np.rint((b - a) / spacing).astype(int) + 1
+        ix, iy, iz = np.meshgrid(np.arange(cnt[0]), np.arange(cnt[1]), np.arange(cnt[2]), indexing="ij")
+        on = ((ix == 0) | (ix == cnt[0] - 1) | (iy == 0) | (iy == cnt[1] - 1) |
+              (iz == 0) | (iz == cnt[2] - 1))
+        g = np.stack([ix[on], iy[on], iz[on]], axis=1).astype(np.float64)
+        out.append(a[None, :] + g * spacing)
+    return np.concatenate(out, axis=0)
+
+
+def _pack(name, params, fluid, boundary, vel_fluid=None):
+    nf, nb = fluid.shape[0], boundary.shape[0]
+    pos = np.zeros((nf + nb, 4), np.float32)
+    pos[:nf, :3] = fluid
+    pos[nf:, :3] = boundary
+    vel = np.zeros_like(pos)
+    if vel_fluid is not None:
+        vel[:nf, :3] = vel_fluid
+    typ = np.concatenate([np.full(nf, LIQUID, np.int32), np.full(nb, FROZEN, np.int32)])
+    return Scene(name, params, pos, vel, typ)
+
+
+def _set_box(p, container_lo, container_hi):
+    r = np.float32(p.particle_spacing) * np.float32(0.5)
+    p.container_min[:] = container_lo
+    p.container_max[:] = container_hi
+    p.collision_min[:] = [np.float32(v) + r for v in container_lo]
+    p.collision_max[:] = [np.float32(v) - r for v in container_hi]
+
+
+def wcsph_dam(n_side=32, seed=1234, box=1.0) -> Scene:
+    """WCSPH dam break, the CPU path's own method: n_side^3 fluid particles on a
+    lattice (spacing 0.02, jitter U(+-0.002)) in the corner of a box x box x box
+    container walled by one layer of boundary particles at the same spacing.
+    h = 0.04, rest density 1000, stiffness 1000, gamma 7, viscosity 0.01,
+    gravity 9.81, dt = 1e-3."""
+    p = default_params()
+    p.method = METHOD_WCSPH
+    p.flags = 0
+    s = 0.02
+    p.particle_spacing = s
+    p.support_radius = 0.04
+    p.gas_constant = 1000.0
+    p.gamma = 7.0
+    p.viscosity = 0.01
+    p.dt = 1e-3
+    lo = np.array([0.04, 0.04, 0.04])
+    hi = lo + box
+    _set_box(p, lo, hi)
+    p.zindex_extent[:] = (2.0, 2.0, 1.5)
+    fluid = _lattice(n_side, n_side, n_side, s, lo + s, 0.002, seed)
+    boundary = box_shell(lo, hi, s, 1)
+    return _pack("wcsph_dam_%d" % n_side, p, fluid, boundary)
+
+
+def pcisph_dam(nx=128, ny=128, nz=128, seed=4321, box=(2.0, 1.3, 1.3), layers=2,
+               spacing=0.01) -> Scene:
+    """PCISPH dam break: nx*ny*nz fluid particles (spacing 0.01, jitter
+    +-0.001) in the corner of a box[0] x box[1] x box[2] container with
+    `layers` shells of boundary particles. h = 2 * spacing, rest density
+    1000, 1% density error threshold, 3-50 iterations, dt = 5e-4."""
+    p = default_params()
+    p.method = METHOD_PCISPH
+    p.flags = FLAG_SURFACE_TENSION | FLAG_PENALTY_WALLS | FLAG_BOUNDARY_PRESSURE
+    s = spacing
+    p.particle_spacing = s
+    p.support_radius = 2.0 * s
+    p.dt = 5e-4
+    p.viscosity = 1.0
+    lo = np.array([2 * s, 2 * s, 2 * s])
+    hi = lo + np.asarray(box, np.float64)
+    _set_box(p, lo, hi)
+    ext = 1024.0 * (s / 5.0)  # 5 grid cells per spacing: 2.048 m at 0.01
+    p.zindex_extent[:] = (ext, ext, ext)
+    fluid = _lattice(nx, ny, nz, s, lo + s, 0.1 * s, seed)
+    boundary = box_shell(lo, hi, s, layers)
+    return _pack("pcisph_dam_%dx%dx%d" % (nx, ny, nz), p, fluid, boundary)
+
+
+def small_pcisph(n_side=12, seed=7, layers=2, box=(0.3, 0.2, 0.2)) -> Scene:
+    """A small PCISPH dam (oracle-sized) with the same physics as pcisph_dam."""
+    return pcisph_dam(n_side, n_side, n_side, seed=seed, box=box, layers=layers)
+
+
+def small_wcsph(n_side=12, seed=11) -> Scene:
+    """A small WCSPH dam (oracle-sized) with the same physics as wcsph_dam."""
+    return wcsph_dam(n_side, seed=seed, box=0.4)
