@@ -199,7 +199,11 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_density(
   }
   if (P.flags & UPF_FLAG_WALL_WEIGHT) den += wall_weight(P, m4, xi);
   const float frac = den / P.rho0;
-  const float powg = powf(frac, P.gamma);
+  // pow(float, float) of the reference's host build is glibc powf, which
+  // evaluates in double and rounds once; the double pow rounded to float
+  // gives the same float (CUDA's single-precision powf may differ by ulps,
+  // which the stiff Tait equation amplifies over many steps)
+  const float powg = (float)pow((double)frac, (double)P.gamma);
   const float pr = P.gas_b * (powg - 1.0f);
   rho[i] = den;
   press[i] = (0.0f >= pr) ? 0.0f : pr;
