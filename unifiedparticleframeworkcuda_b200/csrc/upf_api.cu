@@ -73,6 +73,13 @@ uint32_t log2u(uint32_t v) {
 DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   DevParams d{};
   d.h = p.support_radius;
+  {
+    // sqrt is monotone and correctly rounded: r2 < h^2 (1 - 2^-20) implies
+    // RN(sqrt(r2)) < h, and r2 > h^2 (1 + 2^-20) implies RN(sqrt(r2)) >= h
+    const double h2 = (double)p.support_radius * (double)p.support_radius;
+    d.r2_accept = std::nextafter((float)(h2 * (1.0 - std::ldexp(1.0, -20))), 0.0f);
+    d.r2_reject = std::nextafter((float)(h2 * (1.0 + std::ldexp(1.0, -20))), INFINITY);
+  }
   d.lut_factor = (float)(1.0 / (double)p.support_radius);
   d.mass = p.mass;
   d.inv_mass = (float)(1.0 / (double)p.mass);

@@ -47,6 +47,49 @@ __device__ __forceinline__ void stage_lut(float* dst, const float* __restrict__ 
 
 __device__ __forceinline__ float4 f4(float x, float y, float z) { return make_float4(x, y, z, 0.0f); }
 
+// Neighbour loop with memory-level parallelism: the list entries of a batch
+// of kUnroll neighbours are loaded together, then their gathers, then the
+// arithmetic runs in list order (so floating-point sums keep the reference's
+// sequential order). `load(code)` gathers a neighbour's data, `use(code, v)`
+// accumulates it.
+constexpr int kUnroll = 8;
+
+template <class Load, class Use>
+__device__ __forceinline__ void for_neighbors(const uint32_t* __restrict__ col, uint32_t stride, uint32_t cnt,
+                                              Load&& load, Use&& use) {
+  using T = decltype(load(0u));
+  uint32_t k = 0;
+  for (; k + kUnroll <= cnt; k += kUnroll) {
+    uint32_t code[kUnroll];
+    T v[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) code[u] = __ldg(col + (size_t)(k + u) * stride);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) v[u] = load(code[u]);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) use(code[u], v[u]);
+  }
+  if (k < cnt) {
+    uint32_t code[kUnroll];
+    T v[kUnroll];
+    const uint32_t rem = cnt - k;
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (u < rem) code[u] = __ldg(col + (size_t)(k + u) * stride);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (u < rem) v[u] = load(code[u]);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (u < rem) use(code[u], v[u]);
+  }
+}
+
+struct PosP {
+  float4 x;
+  float p;
+};
+
 // ---------------------------------------------------------------- reorder
 // CopySortedParticleValuesKernel* (particles_kernel.cu:543-654): gather the
 // state into sorted order.
@@ -63,13 +106,30 @@ __global__ void __launch_bounds__(kBlock) k_reorder(uint32_t n, const uint32_t* 
 }
 
 // ---------------------------------------------------------------- neighbours
+// Squared distance with the rounding of dist3 (no sqrt).
+__device__ __forceinline__ float dist2(float4 a, float4 b) {
+  float dx = fsub(a.x, b.x), dy = fsub(a.y, b.y), dz = fsub(a.z, b.z);
+  return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+}
+
+// Membership test of GetNeighbors (UnifiedPhysics.cpp:2270): sqrtf(r2) < h.
+// Squared distances clearly below or above h^2 decide without the square
+// root; the thin band around h^2 takes the exact test, so the result is
+// always that of the reference's float test.
+__device__ __forceinline__ bool within_h(const DevParams& P, float r2) {
+  if (r2 < P.r2_accept) return true;
+  if (r2 > P.r2_reject) return false;
+  return __fsqrt_rn(r2) < P.h;
+}
+
 // GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
 // (zIndex.cpp:43-73): candidates are the Morton blocks covering the query box
 // (with a one-grid-unit margin, so the candidate set is a superset of the
 // reference's), visited in ascending Morton order; within a block the dynamic
 // and boundary ranges are merged by key. The list therefore comes out in the
 // reference's ascending sorted-index order, and membership is the reference's
-// exact test: j != i and |x_i - x_j| < h in float.
+// exact test: j != i and |x_i - x_j| < h in float. Candidate positions are
+// gathered kUnroll at a time.
 __global__ void __launch_bounds__(kBlock) k_build_nlist(
     DevParams P, uint32_t n, const float4* __restrict__ pos, const uint32_t* __restrict__ keys,
     const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, uint32_t ns,
@@ -96,9 +156,25 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
   }
   const uint32_t maxn = P.maxn, stride = P.nstride;
   uint32_t cnt = 0;
+  uint32_t* __restrict__ out = nbr + i;
   auto append = [&](uint32_t code) {
-    if (cnt < maxn) nbr[(size_t)cnt * stride + i] = code;
+    if (cnt < maxn) out[(size_t)cnt * stride] = code;
     cnt++;
+  };
+  // one contiguous range of one set, candidates gathered kUnroll at a time
+  auto scan_range = [&](const float4* __restrict__ set, uint32_t b, uint32_t e, uint32_t tag, bool skip_self) {
+    for (; b + kUnroll <= e; b += kUnroll) {
+      float4 xj[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(set + b + u);
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const uint32_t j = b + u;
+        if (!(skip_self && j == i) && within_h(P, dist2(xi, xj[u]))) append(j | tag);
+      }
+    }
+    for (; b < e; ++b)
+      if (!(skip_self && b == i) && within_h(P, dist2(xi, __ldg(set + b)))) append(b | tag);
   };
   auto visit = [&](uint32_t c) {
     uint32_t ds = cstart[c], de = cend[c];
@@ -107,14 +183,22 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
       ss = sstart[c];
       se = send[c];
     }
-    while (ds < de || ss < se) {
+    if (ss == se) {
+      scan_range(pos, ds, de, 0u, true);
+      return;
+    }
+    if (ds == de) {
+      scan_range(spos, ss, se, kStaticBit, false);
+      return;
+    }
+    while (ds < de || ss < se) {  // both sets present: merge by key
       bool take_dyn = (ds < de) && (ss >= se || keys[ds] <= skeys[ss]);
       if (take_dyn) {
         uint32_t j = ds++;
-        if (j != i && dist3(xi, pos[j]) < h) append(j);
+        if (j != i && within_h(P, dist2(xi, pos[j]))) append(j);
       } else {
         uint32_t j = ss++;
-        if (dist3(xi, spos[j]) < h) append(j | kStaticBit);
+        if (within_h(P, dist2(xi, spos[j]))) append(j | kStaticBit);
       }
     }
   };
@@ -187,16 +271,16 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_density(
   const float4 xi = pos[i];
   const float m = P.mass;
   float den = P.kernel_self * m;
-  const uint32_t c = ncnt[i];
-  for (uint32_t k = 0; k < c; ++k) {
-    uint32_t code = nbr[(size_t)k * P.nstride + i];
-    float4 xj = (code & kStaticBit) ? spos[code & ~kStaticBit] : pos[code];
-    float d = dist3(xi, xj);
-    if (d < P.h) {
-      float kv = lut_at(m4, d, P.lut_factor);
-      den += kv * m;
-    }
-  }
+  for_neighbors(
+      nbr + i, P.nstride, ncnt[i],
+      [&](uint32_t code) { return (code & kStaticBit) ? __ldg(spos + (code & ~kStaticBit)) : __ldg(pos + code); },
+      [&](uint32_t, float4 xj) {
+        float d = dist3(xi, xj);
+        if (d < P.h) {
+          float kv = lut_at(m4, d, P.lut_factor);
+          den += kv * m;
+        }
+      });
   if (P.flags & UPF_FLAG_WALL_WEIGHT) den += wall_weight(P, m4, xi);
   const float frac = den / P.rho0;
   // pow(float, float) of the reference's host build is glibc powf, which
@@ -299,16 +383,38 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
       const float invD = (float)(1.0 / (double)di);
       const float pVol = m * invD;
       float fx = 0, fy = 0, fz = 0;
-      const uint32_t c = ncnt[i];
-      for (uint32_t k = 0; k < c; ++k) {
-        uint32_t code = nbr[(size_t)k * P.nstride + i];
-        if (code & kStaticBit) continue;  // boundary particles are never liquid
-        if (B.type[code] != UPF_LIQUID) continue;
-        const float4 xj = B.pos[code];
+      struct WNb {
+        float4 x, v;
+        float d, p;
+        int32_t t;
+      };
+      const float4* __restrict__ bpos = B.pos;
+      const float4* __restrict__ bvel = B.vel;
+      const int32_t* __restrict__ btype = B.type;
+      for_neighbors(
+          nbr + i, P.nstride, ncnt[i],
+          [&](uint32_t code) {
+            WNb s;
+            if (code & kStaticBit) {  // boundary particles are never liquid
+              s.t = UPF_FROZEN;
+              s.x = s.v = make_float4(0, 0, 0, 0);
+              s.d = s.p = 0.0f;
+            } else {
+              s.t = __ldg(btype + code);
+              s.x = __ldg(bpos + code);
+              s.v = __ldg(bvel + code);
+              s.d = __ldg(rho + code);
+              s.p = __ldg(press + code);
+            }
+            return s;
+          },
+          [&](uint32_t, const WNb& s) {
+        if (s.t != UPF_LIQUID) return;
+        const float4 xj = s.x;
         float d = dist3(xi, xj);
-        if (!(d < h)) continue;
+        if (!(d < h)) return;
         const float kv = lut_at(vl, d, P.lut_factor);
-        const float dj = rho[code], pj = press[code];
+        const float dj = s.d, pj = s.p;
         const float nVol = m / dj;
         const float dvx = xi.x - xj.x, dvy = xi.y - xj.y, dvz = xi.z - xj.z;
         const float g = lut_at(pg, d, P.lut_factor);
@@ -316,7 +422,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
         fx = fx - dvx * g * grad * m * m;
         fy = fy - dvy * g * grad * m * m;
         fz = fz - dvz * g * grad * m * m;
-        const float4 vj = B.vel[code];
+        const float4 vj = s.v;
         const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
         fx = fx - vx * pVol * nVol * P.visc * kv;
         fy = fy - vy * pVol * nVol * P.visc * kv;
@@ -328,7 +434,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
           fy = fy - dvy * P.st_gamma * m * m * sp * inv;
           fz = fz - dvz * P.st_gamma * m * m * sp * inv;
         }
-      }
+          });
       fy -= m * P.gravity;
       force[i] = f4(fx, fy, fz);
       integrate_store(P, i, xi, vi, make_float3(fx, fy, fz), A, keysA, B, ke, mx, my, mz);
@@ -427,19 +533,39 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
   const float m = P.mass, h = P.h, rv = P.rest_volume;
   const uint32_t flags = P.flags;
   float fx = 0, fy = 0, fz = 0;
-  const uint32_t c = ncnt[i];
-  for (uint32_t k = 0; k < c; ++k) {
-    uint32_t code = nbr[(size_t)k * P.nstride + i];
+  struct NbState {
+    float4 x, v;
+    int32_t t;
+  };
+  const float4* __restrict__ bpos = B.pos;
+  const float4* __restrict__ bvel = B.vel;
+  const int32_t* __restrict__ btype = B.type;
+  for_neighbors(
+      nbr + i, P.nstride, ncnt[i],
+      [&](uint32_t code) {
+        NbState s;
+        if (code & kStaticBit) {
+          s.x = __ldg(spos + (code & ~kStaticBit));
+          s.v = make_float4(0, 0, 0, 0);
+          s.t = UPF_FROZEN;
+        } else {
+          s.x = __ldg(bpos + code);
+          s.v = __ldg(bvel + code);
+          s.t = __ldg(btype + code);
+        }
+        return s;
+      },
+      [&](uint32_t code, const NbState& s) {
     const bool is_static = code & kStaticBit;
     const uint32_t j = code & ~kStaticBit;
-    const float4 xj = is_static ? spos[j] : B.pos[j];
+    const float4 xj = s.x;
     const float d = dist3(xi, xj);
-    if (!(d < h)) continue;
+    if (!(d < h)) return;
     const unsigned dl = dist_lut(d, h);
-    const int32_t tj = is_static ? UPF_FROZEN : B.type[j];
+    const int32_t tj = s.t;
     if (tj == UPF_LIQUID) {
       const float kv = lut_at(vl, d, P.lut_factor);
-      const float4 vj = B.vel[j];
+      const float4 vj = s.v;
       fx = fx - (vi.x - vj.x) * rv * rv * P.visc * kv;
       fy = fy - (vi.y - vj.y) * rv * rv * P.visc * kv;
       fz = fz - (vi.z - vj.z) * rv * rv * P.visc * kv;
@@ -464,7 +590,7 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
         fz = fz - (xi.z - xj.z) * P.adh_beta * m * P.rho0 * wv * sp * inv;
       }
     }
-  }
+      });
   fy -= m * P.gravity;
   if (flags & UPF_FLAG_PENALTY_WALLS) penalty_walls(P, xi, fx, fy, fz);
   force[i] = f4(fx, fy, fz);
@@ -490,16 +616,16 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
     const float4 xi = xs[i];
     const float m = P.mass;
     float den = P.kernel_self * m;
-    const uint32_t c = ncnt[i];
-    for (uint32_t k = 0; k < c; ++k) {
-      uint32_t code = nbr[(size_t)k * P.nstride + i];
-      const float4 xj = (code & kStaticBit) ? spos[code & ~kStaticBit] : xs[code];
-      const float d = dist3(xi, xj);
-      if (d < P.h) {
-        const float kv = lut_at(m4, d, P.lut_factor);
-        den += kv * m;
-      }
-    }
+    for_neighbors(
+        nbr + i, P.nstride, ncnt[i],
+        [&](uint32_t code) { return (code & kStaticBit) ? __ldg(spos + (code & ~kStaticBit)) : __ldg(xs + code); },
+        [&](uint32_t, float4 xj) {
+          const float d = dist3(xi, xj);
+          if (d < P.h) {
+            const float kv = lut_at(m4, d, P.lut_factor);
+            den += kv * m;
+          }
+        });
     const float err = mx0(den - P.rho0, 0.0f);
     press[i] = press[i] + mx0(err * P.delta, 0.0f);
     rho[i] = den;
@@ -533,23 +659,32 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
   const float densSq = rho0 * rho0;
   const float pi = press[i];
   float fx = 0, fy = 0, fz = 0;
-  const uint32_t c = ncnt[i];
-  for (uint32_t k = 0; k < c; ++k) {
-    uint32_t code = nbr[(size_t)k * P.nstride + i];
-    const bool is_static = code & kStaticBit;
-    const uint32_t j = code & ~kStaticBit;
-    const float4 xj = is_static ? spos[j] : B.pos[j];
-    const float d = dist3(xi, xj);
-    if (d < P.h) {
-      const float pj = is_static ? 0.0f : press[j];
-      const float g = lut_at(pg, d, P.lut_factor);
-      const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
-      const float grad = pi / densSq + pj / (rho0 * rho0);
-      fx = fx - kx * grad * m * m;
-      fy = fy - ky * grad * m * m;
-      fz = fz - kz * grad * m * m;
-    }
-  }
+  const float4* __restrict__ pos = B.pos;
+  for_neighbors(
+      nbr + i, P.nstride, ncnt[i],
+      [&](uint32_t code) {
+        PosP v;
+        if (code & kStaticBit) {
+          v.x = __ldg(spos + (code & ~kStaticBit));
+          v.p = 0.0f;
+        } else {
+          v.x = __ldg(pos + code);
+          v.p = __ldg(press + code);
+        }
+        return v;
+      },
+      [&](uint32_t, const PosP& v) {
+        const float4 xj = v.x;
+        const float d = dist3(xi, xj);
+        if (d < P.h) {
+          const float g = lut_at(pg, d, P.lut_factor);
+          const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
+          const float grad = pi / densSq + v.p / (rho0 * rho0);
+          fx = fx - kx * grad * m * m;
+          fy = fy - ky * grad * m * m;
+          fz = fz - kz * grad * m * m;
+        }
+      });
   pforce[i] = f4(fx, fy, fz);
   const float4 F = force[i];
   bool bad;
