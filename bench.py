@@ -36,7 +36,7 @@ RADIX_PASSES = 4  # 30-bit Morton keys, 8-bit digits
 def scene_for(args):
     from unifiedparticleframeworkcuda_b200 import scenes
     if args.scene == "c2":
-        return scenes.pcisph_dam(128, 128, 128)
+        return scenes.pcisph_dam(128, 128, 64)
     if args.scene == "c2-small":
         return scenes.pcisph_dam(64, 64, 64)
     if args.scene == "c1":

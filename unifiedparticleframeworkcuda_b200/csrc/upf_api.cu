@@ -119,6 +119,12 @@ DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   d.wmax = make_float3(p.container_max[0], p.container_max[1], p.container_max[2]);
   d.block_shift = log2u(p.block_size);
   d.blocks_per_axis = UPF_GRID_RESOLUTION / p.block_size;
+  {
+    // a member's query box reaches r + 1 grid units past its cell (r = scales * h,
+    // the +1 covering the truncation of the grid coordinate)
+    float r = std::max(p.scales[0], std::max(p.scales[1], p.scales[2])) * p.support_radius;
+    d.nb_radius = (int32_t)std::ceil((double)(r + 1.0f) / (double)p.block_size);
+  }
   d.flags = p.flags;
   d.maxn = p.max_neighbors;
   d.nstride = nstride;
@@ -361,9 +367,11 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   ALLOC(s->keysA, c); ALLOC(s->perm, c);
   ALLOC(s->sort_tmp, radix_temp_words(c));
   ALLOC(s->force, c); ALLOC(s->pforce, c); ALLOC(s->xs, c);
-  ALLOC(s->rho, c); ALLOC(s->press, c); ALLOC(s->wvol_dyn, c);
+  ALLOC(s->rho, c); ALLOC(s->press, c); ALLOC(s->pq, c); ALLOC(s->wvol_dyn, c);
   ALLOC(s->nbr, (size_t)s->nstride * p->max_neighbors);
+  ALLOC(s->bins, (size_t)s->nstride * p->max_neighbors);
   ALLOC(s->ncnt, c);
+  ALLOC(s->occ, c);
   ALLOC(s->cstart, s->ncells); ALLOC(s->cend, s->ncells);
   ALLOC(s->sstart, s->ncells); ALLOC(s->send, s->ncells);
   ALLOC(s->spos, c); ALLOC(s->skeys, c); ALLOC(s->sid, c); ALLOC(s->swvol, c);

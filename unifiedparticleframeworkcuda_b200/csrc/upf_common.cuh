@@ -53,6 +53,7 @@ struct DevParams {
   float3 wmin, wmax;       // real container
   uint32_t block_shift;    // log2(block_size)
   uint32_t blocks_per_axis;
+  int32_t nb_radius;       // blocks per axis around a cell that cover its members' query boxes
   uint32_t flags;
   uint32_t maxn;
   uint32_t nstride;        // neighbour-list column stride
@@ -60,6 +61,7 @@ struct DevParams {
 
 // Device-side scalars of one system.
 struct DevState {
+  uint32_t n_occupied;     // occupied cells of the dynamic set this step
   uint32_t max_rho_bits;   // running max predicted density (positive floats order as uints)
   int32_t iteration;
   int32_t too_large;

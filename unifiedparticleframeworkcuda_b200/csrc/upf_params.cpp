@@ -257,6 +257,12 @@ int validate_params(const upf_params& p, const char** why) {
   if (p.block_size < 4) return bad("block_size must be >= 4 (cell table size)");
   for (int a = 0; a < 3; ++a)
     if (!(p.scales[a] > 0)) return bad("scales must be > 0");
+  {
+    // the neighbour search visits (2R+1)^3 blocks around a cell, R <= 2
+    float r = std::max(p.scales[0], std::max(p.scales[1], p.scales[2])) * p.support_radius;
+    if (std::ceil((double)(r + 1.0f) / (double)p.block_size) > 2.0)
+      return bad("block_size too small for the support radius (need block_size >= (scales*h + 1) / 2)");
+  }
   if (p.max_neighbors == 0 || p.max_neighbors > 1024) return bad("max_neighbors must be in 1..1024");
   if (p.method == UPF_METHOD_PCISPH) {
     if (p.min_loops < 1 || p.max_loops < p.min_loops) return bad("need 1 <= min_loops <= max_loops");

@@ -85,6 +85,33 @@ __device__ __forceinline__ void for_neighbors(const uint32_t* __restrict__ col, 
   }
 }
 
+// The same, also handing each entry's stored kernel-table bin to `use`.
+template <class Load, class Use>
+__device__ __forceinline__ void for_neighbors_bin(const uint32_t* __restrict__ col, const uint16_t* __restrict__ bcol,
+                                                  uint32_t stride, uint32_t cnt, Load&& load, Use&& use) {
+  using T = decltype(load(0u));
+  uint32_t k = 0;
+  for (; k + kUnroll <= cnt; k += kUnroll) {
+    uint32_t code[kUnroll];
+    uint32_t bin[kUnroll];
+    T v[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      code[u] = __ldg(col + (size_t)(k + u) * stride);
+      bin[u] = __ldg(bcol + (size_t)(k + u) * stride);
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) v[u] = load(code[u]);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) use(code[u], bin[u], v[u]);
+  }
+  for (; k < cnt; ++k) {
+    const uint32_t code = __ldg(col + (size_t)k * stride);
+    const uint32_t bin = __ldg(bcol + (size_t)k * stride);
+    use(code, bin, load(code));
+  }
+}
+
 struct PosP {
   float4 x;
   float p;
@@ -122,111 +149,141 @@ __device__ __forceinline__ bool within_h(const DevParams& P, float r2) {
   return __fsqrt_rn(r2) < P.h;
 }
 
-// GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
-// (zIndex.cpp:43-73): candidates are the Morton blocks covering the query box
-// (with a one-grid-unit margin, so the candidate set is a superset of the
-// reference's), visited in ascending Morton order; within a block the dynamic
-// and boundary ranges are merged by key. The list therefore comes out in the
-// reference's ascending sorted-index order, and membership is the reference's
-// exact test: j != i and |x_i - x_j| < h in float. Candidate positions are
-// gathered kUnroll at a time.
-__global__ void __launch_bounds__(kBlock) k_build_nlist(
-    DevParams P, uint32_t n, const float4* __restrict__ pos, const uint32_t* __restrict__ keys,
-    const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, uint32_t ns,
-    const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
-    const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, uint32_t* __restrict__ nbr,
-    uint32_t* __restrict__ ncnt, DevState* __restrict__ st) {
+// Block coordinate of a Morton code (inverse of spread3).
+__device__ __forceinline__ uint32_t compact3(uint32_t v) {
+  v &= 0x09249249u;
+  v = (v | (v >> 2)) & 0x030C30C3u;
+  v = (v | (v >> 4)) & 0x0300F00Fu;
+  v = (v | (v >> 8)) & 0x030000FFu;
+  v = (v | (v >> 16)) & 0x000003FFu;
+  return v;
+}
+
+// Cell ranges of the dynamic set (ClearIndexArrays + CalculateBlocksKernel,
+// particles_kernel.cu:656-726) that also collect the occupied cells for the
+// neighbour pass (in any order: each cell's output does not depend on it).
+__global__ void __launch_bounds__(kBlock) k_cell_ranges_occ(const uint32_t* __restrict__ keys, uint32_t n, int shift,
+                                                             uint32_t* __restrict__ start, uint32_t* __restrict__ end,
+                                                             uint32_t* __restrict__ occ, DevState* __restrict__ st) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float4 xi = pos[i];
-  const float h = P.h;
-  int lo[3], hi[3];
-  {
-    const float c[3] = {(xi.x - P.origin.x) * P.scales.x, (xi.y - P.origin.y) * P.scales.y,
-                        (xi.z - P.origin.z) * P.scales.z};
-    const float r[3] = {h * P.scales.x, h * P.scales.y, h * P.scales.z};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      float l = c[a] - r[a] - 1.0f, u = c[a] + r[a] + 1.0f;
-      int li = (l <= 0.0f) ? 0 : (l >= 1023.0f ? 1023 : (int)l);
-      int ui = (u <= 0.0f) ? 0 : (u >= 1023.0f ? 1023 : (int)u);
-      lo[a] = li >> P.block_shift;
-      hi[a] = ui >> P.block_shift;
-    }
+  const uint32_t c = keys[i] >> shift;
+  if (i == 0 || (keys[i - 1] >> shift) != c) {
+    start[c] = i;
+    occ[atomicAdd(&st->n_occupied, 1u)] = c;
   }
+  if (i == n - 1 || (keys[i + 1] >> shift) != c) end[c] = i + 1;
+}
+
+// GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
+// (zIndex.cpp:43-73). One warp per occupied cell, a lane per particle of the
+// cell; all lanes walk the same candidate blocks (the cell's neighbourhood,
+// wide enough to cover every member's query box plus one grid unit, so the
+// candidate set is a superset of the reference's) in ascending Morton order,
+// so the loops are warp-uniform and candidate positions are broadcast loads.
+// Within a block the dynamic and boundary ranges are merged by key. The list
+// therefore comes out in the reference's ascending sorted-index order, and
+// membership is the reference's exact test: j != i and |x_i - x_j| < h in
+// float. Each entry also records its kernel-table bin at the current
+// positions (used by every pass that evaluates at current positions).
+__global__ void __launch_bounds__(kBlock) k_build_nlist(
+    DevParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ keys,
+    const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, uint32_t ns,
+    const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
+    const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, const uint32_t* __restrict__ occ,
+    uint32_t* __restrict__ nbr, uint16_t* __restrict__ bins, uint32_t* __restrict__ ncnt,
+    DevState* __restrict__ st) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t nocc = *(volatile uint32_t*)&st->n_occupied;
+  const int R = P.nb_radius;
+  const int top = (int)P.blocks_per_axis - 1;
   const uint32_t maxn = P.maxn, stride = P.nstride;
-  uint32_t cnt = 0;
-  uint32_t* __restrict__ out = nbr + i;
-  auto append = [&](uint32_t code) {
-    if (cnt < maxn) out[(size_t)cnt * stride] = code;
-    cnt++;
-  };
-  // one contiguous range of one set, candidates gathered kUnroll at a time
-  auto scan_range = [&](const float4* __restrict__ set, uint32_t b, uint32_t e, uint32_t tag, bool skip_self) {
-    for (; b + kUnroll <= e; b += kUnroll) {
-      float4 xj[kUnroll];
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(set + b + u);
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        const uint32_t j = b + u;
-        if (!(skip_self && j == i) && within_h(P, dist2(xi, xj[u]))) append(j | tag);
-      }
-    }
-    for (; b < e; ++b)
-      if (!(skip_self && b == i) && within_h(P, dist2(xi, __ldg(set + b)))) append(b | tag);
-  };
-  auto visit = [&](uint32_t c) {
-    uint32_t ds = cstart[c], de = cend[c];
-    uint32_t ss = 0, se = 0;
-    if (ns) {
-      ss = sstart[c];
-      se = send[c];
-    }
-    if (ss == se) {
-      scan_range(pos, ds, de, 0u, true);
-      return;
-    }
-    if (ds == de) {
-      scan_range(spos, ss, se, kStaticBit, false);
-      return;
-    }
-    while (ds < de || ss < se) {  // both sets present: merge by key
-      bool take_dyn = (ds < de) && (ss >= se || keys[ds] <= skeys[ss]);
-      if (take_dyn) {
-        uint32_t j = ds++;
-        if (j != i && within_h(P, dist2(xi, pos[j]))) append(j);
-      } else {
-        uint32_t j = ss++;
-        if (within_h(P, dist2(xi, spos[j]))) append(j | kStaticBit);
-      }
-    }
-  };
-  const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
-  const int nblk = nx * ny * nz;
-  if (nblk <= 64) {
-    uint32_t codes[64];
+  uint32_t codes[125];
+  uint32_t local_max = 0;
+  bool overflow = false;
+  for (uint32_t w = warp; w < nocc; w += nwarps) {
+    const uint32_t c = occ[w];
+    const uint32_t cs = cstart[c], ce = cend[c];
+    const int bx = compact3(c), by = compact3(c >> 1), bz = compact3(c >> 2);
     int m = 0;
-    for (int bz = lo[2]; bz <= hi[2]; ++bz)
-      for (int by = lo[1]; by <= hi[1]; ++by)
-        for (int bx = lo[0]; bx <= hi[0]; ++bx) {
-          uint32_t c = morton3(bx, by, bz);
+    for (int z = max(bz - R, 0); z <= min(bz + R, top); ++z)
+      for (int y = max(by - R, 0); y <= min(by + R, top); ++y)
+        for (int x = max(bx - R, 0); x <= min(bx + R, top); ++x) {
+          const uint32_t cc = morton3(x, y, z);
           int q = m++;
-          while (q > 0 && codes[q - 1] > c) {
+          while (q > 0 && codes[q - 1] > cc) {
             codes[q] = codes[q - 1];
             --q;
           }
-          codes[q] = c;
+          codes[q] = cc;
         }
-    for (int q = 0; q < m; ++q) visit(codes[q]);
-  } else {
-    for (int bz = lo[2]; bz <= hi[2]; ++bz)
-      for (int by = lo[1]; by <= hi[1]; ++by)
-        for (int bx = lo[0]; bx <= hi[0]; ++bx) visit(morton3(bx, by, bz));
+    for (uint32_t base = cs; base < ce; base += 32) {
+      const uint32_t i = base + lane;
+      const bool active = i < ce;
+      const float4 xi = pos[active ? i : cs];
+      uint32_t cnt = 0;
+      uint32_t* __restrict__ out = nbr + i;
+      uint16_t* __restrict__ ob = bins + i;
+      auto test = [&](float4 xj, uint32_t code, bool self) {
+        const float r2 = dist2(xi, xj);
+        if (active && !self && within_h(P, r2)) {
+          if (cnt < maxn) {
+            out[(size_t)cnt * stride] = code;
+            const int b = lut_index(__fsqrt_rn(r2), P.lut_factor);
+            ob[(size_t)cnt * stride] = (uint16_t)(b > kLut ? kLut : b);
+          }
+          cnt++;
+        }
+      };
+      for (int q = 0; q < m; ++q) {
+        const uint32_t cc = codes[q];
+        uint32_t ds = cstart[cc], de = cend[cc], ss = 0, se = 0;
+        if (ns) {
+          ss = sstart[cc];
+          se = send[cc];
+        }
+        if (ss == se || ds == de) {  // one set only: batched broadcast gathers
+          const bool dyn = (ss == se);
+          const float4* __restrict__ set = dyn ? pos : spos;
+          uint32_t b = dyn ? ds : ss;
+          const uint32_t e = dyn ? de : se;
+          const uint32_t tag = dyn ? 0u : kStaticBit;
+          for (; b + kUnroll <= e; b += kUnroll) {
+            float4 xj[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(set + b + u);
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) test(xj[u], (b + u) | tag, dyn && (b + u == i));
+          }
+          for (; b < e; ++b) test(__ldg(set + b), b | tag, dyn && b == i);
+        } else {  // both sets present: merge by key
+          while (ds < de || ss < se) {
+            const bool take_dyn = (ds < de) && (ss >= se || __ldg(keys + ds) <= __ldg(skeys + ss));
+            if (take_dyn) {
+              test(__ldg(pos + ds), ds, ds == i);
+              ++ds;
+            } else {
+              test(__ldg(spos + ss), ss | kStaticBit, false);
+              ++ss;
+            }
+          }
+        }
+      }
+      if (active) {
+        ncnt[i] = cnt < maxn ? cnt : maxn;
+        overflow |= cnt > maxn;
+        local_max = max(local_max, cnt);
+      }
+    }
   }
-  ncnt[i] = cnt < maxn ? cnt : maxn;
-  if (cnt > maxn) atomicOr(&st->error_flags, (uint32_t)ERR_OVERFLOW);
-  atomicMax(&st->max_neighbors, cnt);
+  local_max = warp_max(local_max);
+  const bool any_over = __any_sync(0xffffffffu, overflow);
+  if (lane == 0) {
+    if (any_over) atomicOr(&st->error_flags, (uint32_t)ERR_OVERFLOW);
+    if (local_max) atomicMax(&st->max_neighbors, local_max);
+  }
 }
 
 // ---------------------------------------------------------------- WCSPH
@@ -260,8 +317,8 @@ __device__ float wall_weight(const DevParams& P, const float* m4, float4 x) {
 // (UnifiedPhysics.cpp:2408-2501), liquid particles.
 __global__ void __launch_bounds__(kBlock) k_wcsph_density(
     DevParams P, uint32_t n, const float4* __restrict__ pos, const int32_t* __restrict__ type,
-    const float4* __restrict__ spos, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
-    const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press) {
+    const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    float* __restrict__ rho, float* __restrict__ press) {
   __shared__ float m4[UPF_LUT_ENTRIES];
   stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
   __syncthreads();
@@ -271,16 +328,19 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_density(
   const float4 xi = pos[i];
   const float m = P.mass;
   float den = P.kernel_self * m;
-  for_neighbors(
-      nbr + i, P.nstride, ncnt[i],
-      [&](uint32_t code) { return (code & kStaticBit) ? __ldg(spos + (code & ~kStaticBit)) : __ldg(pos + code); },
-      [&](uint32_t, float4 xj) {
-        float d = dist3(xi, xj);
-        if (d < P.h) {
-          float kv = lut_at(m4, d, P.lut_factor);
-          den += kv * m;
-        }
-      });
+  // densities at the positions the list was built at: every entry is within
+  // h and carries its kernel-table bin, so only the bins are read
+  const uint16_t* __restrict__ b = bins + i;
+  const uint32_t c = ncnt[i];
+  uint32_t k = 0;
+  for (; k + kUnroll <= c; k += kUnroll) {
+    uint32_t bb[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) bb[u] = __ldg(b + (size_t)(k + u) * P.nstride);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) den += m4[bb[u]] * m;
+  }
+  for (; k < c; ++k) den += m4[__ldg(b + (size_t)k * P.nstride)] * m;
   if (P.flags & UPF_FLAG_WALL_WEIGHT) den += wall_weight(P, m4, xi);
   const float frac = den / P.rho0;
   // pow(float, float) of the reference's host build is glibc powf, which
@@ -365,9 +425,9 @@ __device__ __forceinline__ void integrate_store(const DevParams& P, uint32_t i, 
 // CalculateForcesInBlocksKernelWCSPH particles_kernel.cu:2399-2653).
 __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
     DevParams P, uint32_t n, DynArrays B, DynArrays A, uint32_t* __restrict__ keysA,
-    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
-    const float* __restrict__ rho, const float* __restrict__ press, float4* __restrict__ force,
-    DevState* __restrict__ st) {
+    const uint32_t* __restrict__ nbr, const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt,
+    const float* __restrict__ luts, const float* __restrict__ rho, const float* __restrict__ press,
+    float4* __restrict__ force, DevState* __restrict__ st) {
   __shared__ float pg[UPF_LUT_ENTRIES], vl[UPF_LUT_ENTRIES];
   stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
   stage_lut(vl, luts + LUT_VISC * UPF_LUT_ENTRIES);
@@ -391,8 +451,10 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
       const float4* __restrict__ bpos = B.pos;
       const float4* __restrict__ bvel = B.vel;
       const int32_t* __restrict__ btype = B.type;
-      for_neighbors(
-          nbr + i, P.nstride, ncnt[i],
+      // positions are those the list was built at: entries are within h and
+      // carry their kernel-table bin
+      for_neighbors_bin(
+          nbr + i, bins + i, P.nstride, ncnt[i],
           [&](uint32_t code) {
             WNb s;
             if (code & kStaticBit) {  // boundary particles are never liquid
@@ -408,16 +470,14 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
             }
             return s;
           },
-          [&](uint32_t, const WNb& s) {
+          [&](uint32_t, uint32_t bin, const WNb& s) {
         if (s.t != UPF_LIQUID) return;
         const float4 xj = s.x;
-        float d = dist3(xi, xj);
-        if (!(d < h)) return;
-        const float kv = lut_at(vl, d, P.lut_factor);
+        const float kv = vl[bin];
         const float dj = s.d, pj = s.p;
         const float nVol = m / dj;
         const float dvx = xi.x - xj.x, dvy = xi.y - xj.y, dvz = xi.z - xj.z;
-        const float g = lut_at(pg, d, P.lut_factor);
+        const float g = pg[bin];
         const float grad = pi * invD * invD + pj / (dj * dj);
         fx = fx - dvx * g * grad * m * m;
         fy = fy - dvy * g * grad * m * m;
@@ -427,7 +487,9 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
         fx = fx - vx * pVol * nVol * P.visc * kv;
         fy = fy - vy * pVol * nVol * P.visc * kv;
         fz = fz - vz * pVol * nVol * P.visc * kv;
-        if ((P.flags & UPF_FLAG_SURFACE_TENSION) && d >= h * 0.25f) {
+        if (P.flags & UPF_FLAG_SURFACE_TENSION) {
+          const float d = dist3(xi, xj);
+          if (!(d >= h * 0.25f)) return;
           const float sp = cohesion_spline(d, h);
           const float inv = 1.0f / d;
           fx = fx - dvx * P.st_gamma * m * m * sp * inv;
@@ -510,7 +572,7 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
     DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const float* __restrict__ swvol,
     const float* __restrict__ wvol_dyn, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
     const float* __restrict__ luts, float4* __restrict__ force, float4* __restrict__ pforce,
-    float4* __restrict__ xs, float* __restrict__ press, DevState* __restrict__ st) {
+    float4* __restrict__ xs, float* __restrict__ press, float* __restrict__ pq, DevState* __restrict__ st) {
   __shared__ float vl[UPF_LUT_ENTRIES], pg[UPF_LUT_ENTRIES], stl[UPF_LUT_ENTRIES], adl[UPF_LUT_ENTRIES];
   stage_lut(vl, luts + LUT_VISC * UPF_LUT_ENTRIES);
   stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
@@ -522,6 +584,7 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
   const int32_t ti = B.type[i];
   const float4 xi = B.pos[i];
   press[i] = 0.0f;
+  pq[i] = 0.0f;
   pforce[i] = f4(0, 0, 0);
   if (ti != UPF_LIQUID) {
     force[i] = f4(0, 0, 0);
@@ -604,7 +667,7 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
 __global__ void __launch_bounds__(kBlock) k_pcisph_density(
     DevParams P, uint32_t n, const int32_t* __restrict__ type, const float4* __restrict__ xs,
     const float4* __restrict__ spos, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
-    const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press,
+    const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press, float* __restrict__ pq,
     DevState* __restrict__ st) {
   __shared__ float m4[UPF_LUT_ENTRIES];
   __shared__ uint32_t wmax[kBlock / 32];
@@ -627,7 +690,11 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
           }
         });
     const float err = mx0(den - P.rho0, 0.0f);
-    press[i] = press[i] + mx0(err * P.delta, 0.0f);
+    const float pnew = press[i] + mx0(err * P.delta, 0.0f);
+    press[i] = pnew;
+    // p / (rho0 * rho0): the pressure-force pass divides every neighbour's
+    // pressure by the same constant; dividing once here is bit-identical
+    pq[i] = pnew / (P.rho0 * P.rho0);
     rho[i] = den;
     best = __float_as_uint(den);  // densities are positive: uint order == float order
   }
@@ -645,9 +712,9 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
 // prediction of the next iteration (PredictPositionAndVelocity).
 __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
     DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const uint32_t* __restrict__ nbr,
-    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts, const float* __restrict__ press,
-    const float4* __restrict__ force, float4* __restrict__ pforce, float4* __restrict__ xs,
-    DevState* __restrict__ st) {
+    const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    const float* __restrict__ pq, const float4* __restrict__ force, float4* __restrict__ pforce,
+    float4* __restrict__ xs, DevState* __restrict__ st) {
   __shared__ float pg[UPF_LUT_ENTRIES];
   stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
   __syncthreads();
@@ -655,13 +722,16 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
   if (i >= n) return;
   if (B.type[i] != UPF_LIQUID) return;
   const float4 xi = B.pos[i];
-  const float m = P.mass, rho0 = P.rho0;
-  const float densSq = rho0 * rho0;
-  const float pi = press[i];
+  const float m = P.mass;
+  // grad = p_i / rho0^2 + p_j / rho0^2, both quotients precomputed by the
+  // density pass (pq); boundary particles have p = 0, so 0 / rho0^2 = 0
+  const float qi = pq[i];
   float fx = 0, fy = 0, fz = 0;
   const float4* __restrict__ pos = B.pos;
-  for_neighbors(
-      nbr + i, P.nstride, ncnt[i],
+  // positions are those the list was built at: every entry passes |x_i - x_j| < h
+  // and its kernel-table bin is stored with it
+  for_neighbors_bin(
+      nbr + i, bins + i, P.nstride, ncnt[i],
       [&](uint32_t code) {
         PosP v;
         if (code & kStaticBit) {
@@ -669,21 +739,18 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
           v.p = 0.0f;
         } else {
           v.x = __ldg(pos + code);
-          v.p = __ldg(press + code);
+          v.p = __ldg(pq + code);
         }
         return v;
       },
-      [&](uint32_t, const PosP& v) {
+      [&](uint32_t, uint32_t bin, const PosP& v) {
         const float4 xj = v.x;
-        const float d = dist3(xi, xj);
-        if (d < P.h) {
-          const float g = lut_at(pg, d, P.lut_factor);
-          const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
-          const float grad = pi / densSq + v.p / (rho0 * rho0);
-          fx = fx - kx * grad * m * m;
-          fy = fy - ky * grad * m * m;
-          fz = fz - kz * grad * m * m;
-        }
+        const float g = pg[bin];
+        const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
+        const float grad = qi + v.p;
+        fx = fx - kx * grad * m * m;
+        fy = fy - ky * grad * m * m;
+        fz = fz - kz * grad * m * m;
       });
   pforce[i] = f4(fx, fy, fz);
   const float4 F = force[i];
@@ -836,17 +903,33 @@ cudaError_t launch_sort_phase(System& s, cudaStream_t st) {
   cudaError_t e = radix_sort_pairs(s.keysA, s.perm, kalt, valt, counts, n, s.key_bits, true, st);
   if (e != cudaSuccess) return e;
   k_reorder<<<grid_of(n), kBlock, 0, st>>>(n, s.perm, s.A, s.B, s.prm.method == UPF_METHOD_PCISPH);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  return cell_ranges(s.keysA, n, 3 * (int)s.dp.block_shift, s.ncells, s.cstart, s.cend, st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.cstart, 0, sizeof(uint32_t) * s.ncells, st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(s.cend, 0, sizeof(uint32_t) * s.ncells, st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(&s.st->n_occupied, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+  k_cell_ranges_occ<<<grid_of(n), kBlock, 0, st>>>(s.keysA, n, 3 * (int)s.dp.block_shift, s.cstart, s.cend, s.occ,
+                                                    s.st);
+  return cudaGetLastError();
+}
+
+// persistent grid of the warp-per-cell neighbour pass
+static uint32_t nlist_grid() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return (uint32_t)sms * 8;
 }
 
 cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
   if (n == 0) return cudaGetLastError();
-  k_build_nlist<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
-                                                s.skeys, s.sstart, s.send, s.nbr, s.ncnt, s.st);
+  k_build_nlist<<<nlist_grid(), kBlock, 0, st>>>(s.dp, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
+                                                 s.skeys, s.sstart, s.send, s.occ, s.nbr, s.bins, s.ncnt, s.st);
   return cudaGetLastError();
 }
 
@@ -854,11 +937,11 @@ cudaError_t launch_force_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n == 0) return cudaSuccess;
   if (s.prm.method == UPF_METHOD_WCSPH) {
-    k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.spos, s.nbr, s.ncnt, s.luts, s.rho,
+    k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.bins, s.ncnt, s.luts, s.rho,
                                                    s.press);
   } else {
     k_pcisph_external<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.swvol, s.wvol_dyn, s.nbr, s.ncnt,
-                                                     s.luts, s.force, s.pforce, s.xs, s.press, s.st);
+                                                     s.luts, s.force, s.pforce, s.xs, s.press, s.pq, s.st);
   }
   return cudaGetLastError();
 }
@@ -872,15 +955,15 @@ cudaError_t launch_loop_density(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
     k_pcisph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.type, s.xs, s.spos, s.nbr, s.ncnt, s.luts, s.rho,
-                                                    s.press, s.st);
+                                                    s.press, s.pq, s.st);
   return cudaGetLastError();
 }
 
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_pressure_force<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.nbr, s.ncnt, s.luts, s.press,
-                                                           s.force, s.pforce, s.xs, s.st);
+    k_pcisph_pressure_force<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.nbr, s.bins, s.ncnt, s.luts,
+                                                           s.pq, s.force, s.pforce, s.xs, s.st);
   return cudaGetLastError();
 }
 
@@ -904,8 +987,8 @@ cudaError_t launch_integrate_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n == 0) return cudaSuccess;
   if (s.prm.method == UPF_METHOD_WCSPH) {
-    k_wcsph_force_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.nbr, s.ncnt, s.luts, s.rho,
-                                                           s.press, s.force, s.st);
+    k_wcsph_force_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.nbr, s.bins, s.ncnt,
+                                                           s.luts, s.rho, s.press, s.force, s.st);
   } else {
     k_pcisph_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.force, s.pforce, s.rho, s.press,
                                                       s.st);

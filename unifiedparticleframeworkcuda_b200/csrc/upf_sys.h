@@ -60,11 +60,14 @@ struct System {
   float4* xs = nullptr;
   float* rho = nullptr;
   float* press = nullptr;
+  float* pq = nullptr;         // press / rest_density^2 (PCISPH loop)
   float* wvol_dyn = nullptr;   // Akinci volume of dynamic rigid particles
 
   // neighbour lists
   uint32_t* nbr = nullptr;
+  uint16_t* bins = nullptr;    // kernel-table bin of each list entry at current positions
   uint32_t* ncnt = nullptr;
+  uint32_t* occ = nullptr;     // occupied cells of the dynamic set
   uint32_t nstride = 0;
 
   // cells

@@ -174,9 +174,10 @@ def wcsph_dam(n_side=32, seed=1234, box=1.0) -> Scene:
     return _pack("wcsph_dam_%d" % n_side, p, fluid, boundary)
 
 
-def pcisph_dam(nx=128, ny=128, nz=128, seed=4321, box=(2.0, 1.3, 1.3), layers=2,
+def pcisph_dam(nx=128, ny=128, nz=64, seed=4321, box=(2.0, 1.3, 1.3), layers=2,
                spacing=0.01) -> Scene:
-    """PCISPH dam break: nx*ny*nz fluid particles (spacing 0.01, jitter
+    """PCISPH dam break: nx*ny*nz fluid particles (default 128 x 128 x 64 =
+    1,048,576; spacing 0.01, jitter
     +-0.001) in the corner of a box[0] x box[1] x box[2] container with
     `layers` shells of boundary particles. h = 2 * spacing, rest density
     1000, 1% density error threshold, 3-50 iterations, dt = 5e-4."""
