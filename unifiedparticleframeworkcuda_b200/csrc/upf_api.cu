@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "upf_sys.h"
+#include "upf_tma.cuh"
 
 namespace upf {
 
@@ -129,6 +130,38 @@ DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   d.maxn = p.max_neighbors;
   d.nstride = nstride;
   return d;
+}
+
+// 2D tensor map over a column-major neighbour array [rows][cols] for the
+// TMA list stream: box = 32 columns (one warp) x kListRows rows.
+upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint32_t elem_bytes, uint64_t cols,
+                           uint64_t rows) {
+  typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeTiled encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || !fn || q != cudaDriverEntryPointSuccess) {
+      set_error("cuTensorMapEncodeTiled unavailable: %s", cudaGetErrorString(e));
+      return UPF_ERR_CUDA;
+    }
+    encode = (EncodeTiled)fn;
+  }
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {cols * elem_bytes};
+  const cuuint32_t box[2] = {32, (cuuint32_t)kListRows};
+  const cuuint32_t estride[2] = {1, 1};
+  CUresult r = encode(map, dt, 2, base, dims, strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return UPF_ERR_CUDA;
+  }
+  return UPF_OK;
 }
 
 void destroy_graph(System& s) {
@@ -378,6 +411,12 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   ALLOC(s->luts, 5 * UPF_LUT_ENTRIES);
   ALLOC(s->st, 1);
 #undef ALLOC
+  if ((st = encode_list_map(&s->nbr_map, s->nbr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, s->nstride,
+                            p->max_neighbors)) != UPF_OK)
+    return bail(st);
+  if ((st = encode_list_map(&s->bins_map, s->bins, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s->nstride,
+                            p->max_neighbors)) != UPF_OK)
+    return bail(st);
   e = cudaMallocHost((void**)&s->st_host, sizeof(DevState));
   if (e != cudaSuccess) {
     s->st_host = nullptr;

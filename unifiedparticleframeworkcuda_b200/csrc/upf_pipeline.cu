@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "upf_sys.h"
+#include "upf_tma.cuh"
 
 namespace upf {
 
@@ -176,114 +177,121 @@ __global__ void __launch_bounds__(kBlock) k_cell_ranges_occ(const uint32_t* __re
 }
 
 // GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
-// (zIndex.cpp:43-73). One warp per occupied cell, a lane per particle of the
-// cell; all lanes walk the same candidate blocks (the cell's neighbourhood,
-// wide enough to cover every member's query box plus one grid unit, so the
-// candidate set is a superset of the reference's) in ascending Morton order,
-// so the loops are warp-uniform and candidate positions are broadcast loads.
-// Within a block the dynamic and boundary ranges are merged by key. The list
-// therefore comes out in the reference's ascending sorted-index order, and
-// membership is the reference's exact test: j != i and |x_i - x_j| < h in
-// float. Each entry also records its kernel-table bin at the current
+// (zIndex.cpp:43-73), one thread per particle: candidates are the Morton
+// blocks covering the query box (with a one-grid-unit margin, so the
+// candidate set is a superset of the reference's), visited in ascending
+// Morton order; within a block the dynamic and boundary ranges are merged by
+// key. The list therefore comes out in the reference's ascending
+// sorted-index order, and membership is the reference's exact test: j != i
+// and |x_i - x_j| < h in float. Candidate positions are gathered kUnroll at
+// a time. Each entry also records its kernel-table bin at the current
 // positions (used by every pass that evaluates at current positions).
 __global__ void __launch_bounds__(kBlock) k_build_nlist(
-    DevParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ keys,
+    DevParams P, uint32_t n, const float4* __restrict__ pos, const uint32_t* __restrict__ keys,
     const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, uint32_t ns,
     const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
-    const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, const uint32_t* __restrict__ occ,
-    uint32_t* __restrict__ nbr, uint16_t* __restrict__ bins, uint32_t* __restrict__ ncnt,
-    DevState* __restrict__ st) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t nocc = *(volatile uint32_t*)&st->n_occupied;
-  const int R = P.nb_radius;
-  const int top = (int)P.blocks_per_axis - 1;
+    const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, uint32_t* __restrict__ nbr,
+    uint16_t* __restrict__ bins, uint32_t* __restrict__ ncnt, DevState* __restrict__ st) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 xi = pos[i];
+  const float h = P.h;
+  int lo[3], hi[3];
+  {
+    const float c[3] = {(xi.x - P.origin.x) * P.scales.x, (xi.y - P.origin.y) * P.scales.y,
+                        (xi.z - P.origin.z) * P.scales.z};
+    const float r[3] = {h * P.scales.x, h * P.scales.y, h * P.scales.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float l = c[a] - r[a] - 1.0f, u = c[a] + r[a] + 1.0f;
+      int li = (l <= 0.0f) ? 0 : (l >= 1023.0f ? 1023 : (int)l);
+      int ui = (u <= 0.0f) ? 0 : (u >= 1023.0f ? 1023 : (int)u);
+      lo[a] = li >> P.block_shift;
+      hi[a] = ui >> P.block_shift;
+    }
+  }
   const uint32_t maxn = P.maxn, stride = P.nstride;
-  uint32_t codes[125];
-  uint32_t local_max = 0;
-  bool overflow = false;
-  for (uint32_t w = warp; w < nocc; w += nwarps) {
-    const uint32_t c = occ[w];
-    const uint32_t cs = cstart[c], ce = cend[c];
-    const int bx = compact3(c), by = compact3(c >> 1), bz = compact3(c >> 2);
+  uint32_t cnt = 0;
+  uint32_t* __restrict__ out = nbr + i;
+  uint16_t* __restrict__ ob = bins + i;
+  auto append = [&](uint32_t code, float r2) {
+    if (cnt < maxn) {
+      out[(size_t)cnt * stride] = code;
+      const int b = lut_index(__fsqrt_rn(r2), P.lut_factor);
+      ob[(size_t)cnt * stride] = (uint16_t)(b > kLut ? kLut : b);
+    }
+    cnt++;
+  };
+  auto scan_range = [&](const float4* __restrict__ set, uint32_t b, uint32_t e, uint32_t tag, bool skip_self) {
+    for (; b + kUnroll <= e; b += kUnroll) {
+      float4 xj[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(set + b + u);
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const uint32_t j = b + u;
+        const float r2 = dist2(xi, xj[u]);
+        if (!(skip_self && j == i) && within_h(P, r2)) append(j | tag, r2);
+      }
+    }
+    for (; b < e; ++b) {
+      const float r2 = dist2(xi, __ldg(set + b));
+      if (!(skip_self && b == i) && within_h(P, r2)) append(b | tag, r2);
+    }
+  };
+  auto visit = [&](uint32_t c) {
+    uint32_t ds = cstart[c], de = cend[c];
+    uint32_t ss = 0, se = 0;
+    if (ns) {
+      ss = sstart[c];
+      se = send[c];
+    }
+    if (ss == se) {
+      scan_range(pos, ds, de, 0u, true);
+      return;
+    }
+    if (ds == de) {
+      scan_range(spos, ss, se, kStaticBit, false);
+      return;
+    }
+    while (ds < de || ss < se) {  // both sets present: merge by key
+      bool take_dyn = (ds < de) && (ss >= se || keys[ds] <= skeys[ss]);
+      if (take_dyn) {
+        uint32_t j = ds++;
+        const float r2 = dist2(xi, pos[j]);
+        if (j != i && within_h(P, r2)) append(j, r2);
+      } else {
+        uint32_t j = ss++;
+        const float r2 = dist2(xi, spos[j]);
+        if (within_h(P, r2)) append(j | kStaticBit, r2);
+      }
+    }
+  };
+  const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+  const int nblk = nx * ny * nz;
+  if (nblk <= 64) {
+    uint32_t codes[64];
     int m = 0;
-    for (int z = max(bz - R, 0); z <= min(bz + R, top); ++z)
-      for (int y = max(by - R, 0); y <= min(by + R, top); ++y)
-        for (int x = max(bx - R, 0); x <= min(bx + R, top); ++x) {
-          const uint32_t cc = morton3(x, y, z);
+    for (int bz = lo[2]; bz <= hi[2]; ++bz)
+      for (int by = lo[1]; by <= hi[1]; ++by)
+        for (int bx = lo[0]; bx <= hi[0]; ++bx) {
+          uint32_t c = morton3(bx, by, bz);
           int q = m++;
-          while (q > 0 && codes[q - 1] > cc) {
+          while (q > 0 && codes[q - 1] > c) {
             codes[q] = codes[q - 1];
             --q;
           }
-          codes[q] = cc;
+          codes[q] = c;
         }
-    for (uint32_t base = cs; base < ce; base += 32) {
-      const uint32_t i = base + lane;
-      const bool active = i < ce;
-      const float4 xi = pos[active ? i : cs];
-      uint32_t cnt = 0;
-      uint32_t* __restrict__ out = nbr + i;
-      uint16_t* __restrict__ ob = bins + i;
-      auto test = [&](float4 xj, uint32_t code, bool self) {
-        const float r2 = dist2(xi, xj);
-        if (active && !self && within_h(P, r2)) {
-          if (cnt < maxn) {
-            out[(size_t)cnt * stride] = code;
-            const int b = lut_index(__fsqrt_rn(r2), P.lut_factor);
-            ob[(size_t)cnt * stride] = (uint16_t)(b > kLut ? kLut : b);
-          }
-          cnt++;
-        }
-      };
-      for (int q = 0; q < m; ++q) {
-        const uint32_t cc = codes[q];
-        uint32_t ds = cstart[cc], de = cend[cc], ss = 0, se = 0;
-        if (ns) {
-          ss = sstart[cc];
-          se = send[cc];
-        }
-        if (ss == se || ds == de) {  // one set only: batched broadcast gathers
-          const bool dyn = (ss == se);
-          const float4* __restrict__ set = dyn ? pos : spos;
-          uint32_t b = dyn ? ds : ss;
-          const uint32_t e = dyn ? de : se;
-          const uint32_t tag = dyn ? 0u : kStaticBit;
-          for (; b + kUnroll <= e; b += kUnroll) {
-            float4 xj[kUnroll];
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(set + b + u);
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) test(xj[u], (b + u) | tag, dyn && (b + u == i));
-          }
-          for (; b < e; ++b) test(__ldg(set + b), b | tag, dyn && b == i);
-        } else {  // both sets present: merge by key
-          while (ds < de || ss < se) {
-            const bool take_dyn = (ds < de) && (ss >= se || __ldg(keys + ds) <= __ldg(skeys + ss));
-            if (take_dyn) {
-              test(__ldg(pos + ds), ds, ds == i);
-              ++ds;
-            } else {
-              test(__ldg(spos + ss), ss | kStaticBit, false);
-              ++ss;
-            }
-          }
-        }
-      }
-      if (active) {
-        ncnt[i] = cnt < maxn ? cnt : maxn;
-        overflow |= cnt > maxn;
-        local_max = max(local_max, cnt);
-      }
-    }
+    for (int q = 0; q < m; ++q) visit(codes[q]);
+  } else {
+    for (int bz = lo[2]; bz <= hi[2]; ++bz)
+      for (int by = lo[1]; by <= hi[1]; ++by)
+        for (int bx = lo[0]; bx <= hi[0]; ++bx) visit(morton3(bx, by, bz));
   }
-  local_max = warp_max(local_max);
-  const bool any_over = __any_sync(0xffffffffu, overflow);
-  if (lane == 0) {
-    if (any_over) atomicOr(&st->error_flags, (uint32_t)ERR_OVERFLOW);
-    if (local_max) atomicMax(&st->max_neighbors, local_max);
-  }
+  ncnt[i] = cnt < maxn ? cnt : maxn;
+  if (cnt > maxn) atomicOr(&st->error_flags, (uint32_t)ERR_OVERFLOW);
+  atomicMax(&st->max_neighbors, cnt);
 }
 
 // ---------------------------------------------------------------- WCSPH
@@ -664,31 +672,55 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
 
 // ComputePredictedDensityAndPressure (UnifiedPhysics.cpp:5456-5491) with the
 // maximum for the loop test reduced in the same pass.
+//
+// The warp's list rows stream through shared memory by TMA (upf_tma.cuh);
+// each lane then gathers kListRows neighbours' predicted positions at once
+// and accumulates them in list order.
 __global__ void __launch_bounds__(kBlock) k_pcisph_density(
     DevParams P, uint32_t n, const int32_t* __restrict__ type, const float4* __restrict__ xs,
-    const float4* __restrict__ spos, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
+    const float4* __restrict__ spos, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
     const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press, float* __restrict__ pq,
     DevState* __restrict__ st) {
   __shared__ float m4[UPF_LUT_ENTRIES];
   __shared__ uint32_t wmax[kBlock / 32];
+  __shared__ WarpListRing<false> rings[kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
+  ring_init(rings[warp]);
   __syncthreads();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t best = 0;
-  if (i < n && type[i] == UPF_LIQUID) {
-    const float4 xi = xs[i];
-    const float m = P.mass;
-    float den = P.kernel_self * m;
-    for_neighbors(
-        nbr + i, P.nstride, ncnt[i],
-        [&](uint32_t code) { return (code & kStaticBit) ? __ldg(spos + (code & ~kStaticBit)) : __ldg(xs + code); },
-        [&](uint32_t, float4 xj) {
-          const float d = dist3(xi, xj);
-          if (d < P.h) {
-            const float kv = lut_at(m4, d, P.lut_factor);
-            den += kv * m;
-          }
-        });
+  const bool active = i < n && type[i] == UPF_LIQUID;
+  const uint32_t cnt = active ? ncnt[i] : 0u;
+  const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
+  const float4 xi = active ? xs[i] : make_float4(0, 0, 0, 0);
+  const float m = P.mass;
+  float den = P.kernel_self * m;
+  WarpListRing<false>& ring = rings[warp];
+  const bool ok = ring_walk(ring, &cmap, &cmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
+                            [&](int s, int k0) {
+                              float4 xj[kListRows];
+#pragma unroll
+                              for (int r = 0; r < kListRows; ++r) {
+                                if (k0 + r < (int)cnt) {
+                                  const uint32_t code = ring.codes[s][r][lane];
+                                  xj[r] = (code & kStaticBit) ? __ldg(spos + (code & ~kStaticBit))
+                                                              : __ldg(xs + code);
+                                }
+                              }
+#pragma unroll
+                              for (int r = 0; r < kListRows; ++r) {
+                                if (k0 + r < (int)cnt) {
+                                  const float d = dist3(xi, xj[r]);
+                                  if (d < P.h) {
+                                    const float kv = lut_at(m4, d, P.lut_factor);
+                                    den += kv * m;
+                                  }
+                                }
+                              }
+                            });
+  if (!ok && lane == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
+  if (active) {
     const float err = mx0(den - P.rho0, 0.0f);
     const float pnew = press[i] + mx0(err * P.delta, 0.0f);
     press[i] = pnew;
@@ -711,47 +743,62 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
 // ComputeCorrectivePressureForce (UnifiedPhysics.cpp:5493-5522), then the
 // prediction of the next iteration (PredictPositionAndVelocity).
 __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
-    DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const uint32_t* __restrict__ nbr,
-    const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const __grid_constant__ CUtensorMap cmap,
+    const __grid_constant__ CUtensorMap bmap, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
     const float* __restrict__ pq, const float4* __restrict__ force, float4* __restrict__ pforce,
     float4* __restrict__ xs, DevState* __restrict__ st) {
   __shared__ float pg[UPF_LUT_ENTRIES];
+  __shared__ WarpListRing<true> rings[kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
+  ring_init(rings[warp]);
   __syncthreads();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (B.type[i] != UPF_LIQUID) return;
-  const float4 xi = B.pos[i];
+  const bool active = i < n && B.type[i] == UPF_LIQUID;
+  const uint32_t cnt = active ? ncnt[i] : 0u;
+  const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
+  const float4 xi = active ? B.pos[i] : make_float4(0, 0, 0, 0);
   const float m = P.mass;
   // grad = p_i / rho0^2 + p_j / rho0^2, both quotients precomputed by the
   // density pass (pq); boundary particles have p = 0, so 0 / rho0^2 = 0
-  const float qi = pq[i];
+  const float qi = active ? pq[i] : 0.0f;
   float fx = 0, fy = 0, fz = 0;
   const float4* __restrict__ pos = B.pos;
   // positions are those the list was built at: every entry passes |x_i - x_j| < h
   // and its kernel-table bin is stored with it
-  for_neighbors_bin(
-      nbr + i, bins + i, P.nstride, ncnt[i],
-      [&](uint32_t code) {
-        PosP v;
-        if (code & kStaticBit) {
-          v.x = __ldg(spos + (code & ~kStaticBit));
-          v.p = 0.0f;
-        } else {
-          v.x = __ldg(pos + code);
-          v.p = __ldg(pq + code);
-        }
-        return v;
-      },
-      [&](uint32_t, uint32_t bin, const PosP& v) {
-        const float4 xj = v.x;
-        const float g = pg[bin];
-        const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
-        const float grad = qi + v.p;
-        fx = fx - kx * grad * m * m;
-        fy = fy - ky * grad * m * m;
-        fz = fz - kz * grad * m * m;
-      });
+  WarpListRing<true>& ring = rings[warp];
+  const bool ok = ring_walk(ring, &cmap, &bmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
+                            [&](int s, int k0) {
+                              float4 xj[kListRows];
+                              float qj[kListRows];
+#pragma unroll
+                              for (int r = 0; r < kListRows; ++r) {
+                                if (k0 + r < (int)cnt) {
+                                  const uint32_t code = ring.codes[s][r][lane];
+                                  if (code & kStaticBit) {
+                                    xj[r] = __ldg(spos + (code & ~kStaticBit));
+                                    qj[r] = 0.0f;
+                                  } else {
+                                    xj[r] = __ldg(pos + code);
+                                    qj[r] = __ldg(pq + code);
+                                  }
+                                }
+                              }
+#pragma unroll
+                              for (int r = 0; r < kListRows; ++r) {
+                                if (k0 + r < (int)cnt) {
+                                  const float g = pg[ring.bins[s][r][lane]];
+                                  const float kx = (xi.x - xj[r].x) * g, ky = (xi.y - xj[r].y) * g,
+                                              kz = (xi.z - xj[r].z) * g;
+                                  const float grad = qi + qj[r];
+                                  fx = fx - kx * grad * m * m;
+                                  fy = fy - ky * grad * m * m;
+                                  fz = fz - kz * grad * m * m;
+                                }
+                              }
+                            });
+  if (!ok && lane == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
+  if (!active) return;
   pforce[i] = f4(fx, fy, fz);
   const float4 F = force[i];
   bool bad;
@@ -912,24 +959,12 @@ cudaError_t launch_sort_phase(System& s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// persistent grid of the warp-per-cell neighbour pass
-static uint32_t nlist_grid() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return (uint32_t)sms * 8;
-}
-
 cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
   if (n == 0) return cudaGetLastError();
-  k_build_nlist<<<nlist_grid(), kBlock, 0, st>>>(s.dp, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
-                                                 s.skeys, s.sstart, s.send, s.occ, s.nbr, s.bins, s.ncnt, s.st);
+  k_build_nlist<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
+                                                s.skeys, s.sstart, s.send, s.nbr, s.bins, s.ncnt, s.st);
   return cudaGetLastError();
 }
 
@@ -954,16 +989,16 @@ cudaError_t launch_loop_init(System& s, cudaStream_t st) {
 cudaError_t launch_loop_density(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.type, s.xs, s.spos, s.nbr, s.ncnt, s.luts, s.rho,
-                                                    s.press, s.pq, s.st);
+    k_pcisph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.type, s.xs, s.spos, s.nbr_map, s.ncnt, s.luts,
+                                                    s.rho, s.press, s.pq, s.st);
   return cudaGetLastError();
 }
 
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_pressure_force<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.nbr, s.bins, s.ncnt, s.luts,
-                                                           s.pq, s.force, s.pforce, s.xs, s.st);
+    k_pcisph_pressure_force<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.nbr_map, s.bins_map, s.ncnt,
+                                                           s.luts, s.pq, s.force, s.pforce, s.xs, s.st);
   return cudaGetLastError();
 }
 

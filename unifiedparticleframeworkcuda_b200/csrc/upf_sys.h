@@ -15,6 +15,7 @@
 //   into the boundary set.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -68,6 +69,8 @@ struct System {
   uint16_t* bins = nullptr;    // kernel-table bin of each list entry at current positions
   uint32_t* ncnt = nullptr;
   uint32_t* occ = nullptr;     // occupied cells of the dynamic set
+  CUtensorMap nbr_map;         // 2D [max_neighbors][nstride] uint32 view of nbr for TMA
+  CUtensorMap bins_map;        // same view of bins (uint16)
   uint32_t nstride = 0;
 
   // cells

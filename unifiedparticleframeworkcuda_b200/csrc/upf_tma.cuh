@@ -1,0 +1,123 @@
+// upf_tma.cuh — TMA (cp.async.bulk.tensor) streaming of the neighbour lists
+// into shared memory, one pipeline per warp.
+//
+// The neighbour lists are column-major [row k][particle i], so the rows
+// k..k+R-1 of a warp's 32 consecutive particles form a 2D box of 32 x R
+// elements. Lane 0 of each warp issues one 2D tensor copy per box into a ring
+// of kStages shared-memory stages; every lane waits on the stage's mbarrier
+// (bounded: a wait that runs out records ERR_TIMEOUT and the pass goes on
+// without that data rather than hanging). Only loads from this GPU's own
+// memory, no cluster multicast.
+#pragma once
+
+#include <cuda.h>
+#include <stdint.h>
+
+#include "upf_common.cuh"
+
+namespace upf {
+
+constexpr int kListRows = 8;     // list rows per stage
+constexpr int kListStages = 3;   // ring depth
+constexpr uint32_t kWaitSpins = 1u << 22;  // bounded wait (~seconds at worst)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; returns false (and the caller records a timeout) if the phase
+// did not complete
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t s = 0; s < kWaitSpins; ++s)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// One warp's ring of list stages. Stage s holds rows [c*R, c*R+R) of chunk c
+// (c % kListStages == s) for the warp's 32 columns: codes (uint32) and,
+// when kWithBins, bins (uint16).
+template <bool kWithBins>
+struct __align__(128) WarpListRing {
+  uint32_t codes[kListStages][kListRows][32];                   // 1 KB per stage
+  uint16_t bins[kWithBins ? kListStages : 1][kListRows][32];     // 512 B per stage
+  uint64_t full[kListStages];
+};
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <bool kWithBins>
+__device__ __forceinline__ void ring_issue(WarpListRing<kWithBins>& r, const CUtensorMap* cmap,
+                                           const CUtensorMap* bmap, int chunk, int col0) {
+  const int s = chunk % kListStages;
+  const uint32_t bytes = kListRows * 32 * (4 + (kWithBins ? 2 : 0));
+  fence_proxy_async_smem();  // the stage's previous contents were read through the generic proxy
+  mbar_arrive_expect_tx(&r.full[s], bytes);
+  tma_load_2d(&r.codes[s][0][0], cmap, &r.full[s], col0, chunk * kListRows);
+  if (kWithBins) tma_load_2d(&r.bins[s][0][0], bmap, &r.full[s], col0, chunk * kListRows);
+}
+
+// Walks the warp's lists chunk by chunk. `body(s, rows)` consumes stage s
+// (rows valid rows); lanes index their own column. Returns false if a wait
+// ran out.
+template <bool kWithBins, class Body>
+__device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins>& r, const CUtensorMap* cmap,
+                                          const CUtensorMap* bmap, int col0, uint32_t warp_max_cnt, Body&& body) {
+  const int lane = threadIdx.x & 31;
+  const int nchunks = (int)((warp_max_cnt + kListRows - 1) / kListRows);
+  if (lane == 0) {
+    for (int c = 0; c < kListStages && c < nchunks; ++c) ring_issue(r, cmap, bmap, c, col0);
+  }
+  bool ok = true;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c % kListStages;
+    const uint32_t parity = (uint32_t)(c / kListStages) & 1u;
+    ok = mbar_wait(&r.full[s], parity) && ok;
+    body(s, c * kListRows);
+    __syncwarp();
+    if (lane == 0 && c + kListStages < nchunks) ring_issue(r, cmap, bmap, c + kListStages, col0);
+  }
+  return ok;
+}
+
+template <bool kWithBins>
+__device__ __forceinline__ void ring_init(WarpListRing<kWithBins>& r) {
+  if ((threadIdx.x & 31) == 0) {
+    for (int s = 0; s < kListStages; ++s) mbar_init(&r.full[s], 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+}
+
+}  // namespace upf
