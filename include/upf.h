@@ -193,6 +193,14 @@ upf_status upf_density_error_factor(const upf_params* p, double* delta_out);
  * Replaces CreateLut*Texture (src/gpu/particles.cuh:444-448). */
 upf_status upf_build_luts(const upf_params* p, float* out_5x301);
 
+/* Exact squared-distance thresholds of the table bins: out[b] (b = 1..300) is
+ * the smallest float r2 with (int)(sqrtf(r2) * (float)(1/h) * 300) >= b,
+ * out[0] = 0, out[301] the smallest r2 with sqrtf(r2) >= h. The device picks
+ * table bins (WeightingKernel::kernel*Lut, WeightingKernel.cpp:122-128) and
+ * the support test (UnifiedPhysics.cpp:2270) from these, bit-identically to
+ * the square-root form. No counterpart in the reference. */
+upf_status upf_build_bin_thresholds(const upf_params* p, float* out_302);
+
 /* ---- system lifetime (MallocDeviceArrays / FreeDeviceArrays) ------------ */
 
 /* Replaces MallocDeviceArraysParticles + SetDeviceConstants +

@@ -106,3 +106,23 @@ def test_no_device_means_error_not_fallback(upf_lib):
     with pytest.raises(UpfError) as e:
         upf_lib.ParticleSystem(sc.params, capacity=sc.n)
     assert e.value.status == 9  # UPF_ERR_NO_DEVICE
+
+
+def test_bin_thresholds_reproduce_sqrt_binning(upf_lib):
+    """The device derives table bins from r^2 with these thresholds; they must
+    give exactly (int)(sqrtf(r2) * (float)(1/h) * 300) and sqrtf(r2) < h."""
+    rng = np.random.default_rng(3)
+    for h in (0.02, 0.04, 0.0500005, 0.0123):
+        p = upf_lib.default_params()
+        p.support_radius = h
+        thr = upf_lib.bin_thresholds(p)
+        hf = np.float32(h)
+        factor = np.float32(1.0 / np.float64(hf))
+        r2 = np.concatenate([rng.uniform(0, 1.1, 200000).astype(np.float32) * hf * hf,
+                             thr[1:].copy(), np.nextafter(thr[1:], np.float32(0))]).astype(np.float32)
+        d = np.sqrt(r2, dtype=np.float32)
+        exact = ((d * factor).astype(np.float32) * np.float32(300)).astype(np.float32).astype(np.int64)
+        got = np.searchsorted(thr[1:301], r2, side="right")  # number of thresholds <= r2
+        inside = d < hf
+        assert np.array_equal(r2 < thr[301], inside)
+        assert np.array_equal(np.minimum(exact, 300)[inside], got[inside])

@@ -48,6 +48,7 @@ def lib():
             "upf_params_derive": [P],
             "upf_density_error_factor": [P, C.POINTER(C.c_double)],
             "upf_build_luts": [P, fp],
+            "upf_build_bin_thresholds": [P, fp],
             "upf_create": [P, C.c_int, C.c_uint32, C.POINTER(vp)],
             "upf_destroy": [vp],
             "upf_get_params": [vp, P],
@@ -118,6 +119,12 @@ def density_error_factor(p: UpfParams) -> float:
 def build_luts(p: UpfParams) -> np.ndarray:
     out = np.zeros((5, 301), np.float32)
     check(lib().upf_build_luts(C.byref(p), _p(out, C.c_float)), "upf_build_luts")
+    return out
+
+
+def bin_thresholds(p: UpfParams) -> np.ndarray:
+    out = np.zeros(302, np.float32)
+    check(lib().upf_build_bin_thresholds(C.byref(p), _p(out, C.c_float)), "upf_build_bin_thresholds")
     return out
 
 

@@ -129,6 +129,7 @@ DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   d.flags = p.flags;
   d.maxn = p.max_neighbors;
   d.nstride = nstride;
+  d.static_base = nstride;
   return d;
 }
 
@@ -350,6 +351,15 @@ upf_status upf_build_luts(const upf_params* p, float* out) {
   return UPF_OK;
 }
 
+upf_status upf_build_bin_thresholds(const upf_params* p, float* out) {
+  if (!p || !out || !(p->support_radius > 0)) {
+    set_error("upf_build_bin_thresholds: bad arguments");
+    return UPF_ERR_INVALID_ARG;
+  }
+  build_bin_thresholds(*p, out);
+  return UPF_OK;
+}
+
 upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_system** out) {
   if (!p || !out || capacity == 0) {
     set_error("upf_create: null argument or zero capacity");
@@ -396,19 +406,21 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
 #define ALLOC(ptr, count)                   \
   if ((st = dalloc(*s, &(ptr), (count))) != UPF_OK) return bail(st);
   ALLOC(s->A.pos, c); ALLOC(s->A.vel, c); ALLOC(s->A.lag, c); ALLOC(s->A.id, c); ALLOC(s->A.type, c);
-  ALLOC(s->B.pos, c); ALLOC(s->B.vel, c); ALLOC(s->B.lag, c); ALLOC(s->B.id, c); ALLOC(s->B.type, c);
+  // arrays gathered by neighbour index: [dynamic (stride) | boundary tail (capacity)]
+  const size_t ct = (size_t)s->nstride + c;
+  ALLOC(s->B.pos, ct); ALLOC(s->B.vel, ct); ALLOC(s->B.lag, c); ALLOC(s->B.id, c); ALLOC(s->B.type, ct);
   ALLOC(s->keysA, c); ALLOC(s->perm, c);
   ALLOC(s->sort_tmp, radix_temp_words(c));
-  ALLOC(s->force, c); ALLOC(s->pforce, c); ALLOC(s->xs, c);
-  ALLOC(s->rho, c); ALLOC(s->press, c); ALLOC(s->pq, c); ALLOC(s->wvol_dyn, c);
+  ALLOC(s->force, c); ALLOC(s->pforce, c); ALLOC(s->xs, ct);
+  ALLOC(s->rho, ct); ALLOC(s->press, ct); ALLOC(s->pq, ct); ALLOC(s->wvol, ct);
   ALLOC(s->nbr, (size_t)s->nstride * p->max_neighbors);
   ALLOC(s->bins, (size_t)s->nstride * p->max_neighbors);
   ALLOC(s->ncnt, c);
   ALLOC(s->occ, c);
   ALLOC(s->cstart, s->ncells); ALLOC(s->cend, s->ncells);
   ALLOC(s->sstart, s->ncells); ALLOC(s->send, s->ncells);
-  ALLOC(s->spos, c); ALLOC(s->skeys, c); ALLOC(s->sid, c); ALLOC(s->swvol, c);
-  ALLOC(s->luts, 5 * UPF_LUT_ENTRIES);
+  ALLOC(s->spos, c); ALLOC(s->skeys, c); ALLOC(s->sid, c);
+  ALLOC(s->luts, 5 * UPF_LUT_ENTRIES + kThresholds);
   ALLOC(s->st, 1);
 #undef ALLOC
   if ((st = encode_list_map(&s->nbr_map, s->nbr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, s->nstride,
@@ -423,9 +435,15 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
     set_error("cudaMallocHost: %s", cudaGetErrorString(e));
     return bail(UPF_ERR_ALLOC);
   }
-  std::vector<float> lut(5 * UPF_LUT_ENTRIES);
+  std::vector<float> lut(5 * UPF_LUT_ENTRIES + kThresholds);
   build_luts(*p, lut.data());
+  build_bin_thresholds(*p, lut.data() + 5 * UPF_LUT_ENTRIES);
   e = cudaMemcpy(s->luts, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice);
+  // boundary tails: zero velocity, pressure and pressure quotient
+  if (e == cudaSuccess) e = cudaMemset(s->B.vel, 0, sizeof(float4) * ct);
+  if (e == cudaSuccess) e = cudaMemset(s->pq, 0, sizeof(float) * ct);
+  if (e == cudaSuccess) e = cudaMemset(s->press, 0, sizeof(float) * ct);
+  if (e == cudaSuccess) e = cudaMemset(s->rho, 0, sizeof(float) * ct);
   if (e == cudaSuccess) e = cudaMemset(s->st, 0, sizeof(DevState));
   if (e != cudaSuccess) {
     set_error("upload: %s", cudaGetErrorString(e));
@@ -535,9 +553,18 @@ upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4
     UPF_CUDA(radix_sort_pairs(S.skeys, perm, kalt, valt, counts, S.n_static, S.key_bits, true, st));
     k_gather_static<<<(S.n_static + 255) / 256, 256, 0, st>>>(S.n_static, perm, tmp_pos, tmp_id, S.spos, S.sid);
     UPF_CUDA(cudaGetLastError());
+    // boundary tails of the arrays gathered by neighbour index
+    const size_t tb = S.dp.static_base;
+    UPF_CUDA(cudaMemcpyAsync(S.B.pos + tb, S.spos, sizeof(float4) * S.n_static, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.xs + tb, S.spos, sizeof(float4) * S.n_static, cudaMemcpyDeviceToDevice, st));
+    std::vector<int32_t> frozen(S.n_static, UPF_FROZEN);
+    UPF_CUDA(cudaMemcpyAsync(S.B.type + tb, frozen.data(), sizeof(int32_t) * S.n_static, cudaMemcpyHostToDevice, st));
+  }
+  {
     // default Akinci volume: the rest volume (UnifiedParticle.cpp:24)
-    std::vector<float> wv(S.n_static, S.prm.mass / S.prm.rest_density);
-    UPF_CUDA(cudaMemcpyAsync(S.swvol, wv.data(), sizeof(float) * S.n_static, cudaMemcpyHostToDevice, st));
+    std::vector<float> wv((size_t)S.dp.static_base + S.n_static, S.prm.mass / S.prm.rest_density);
+    UPF_CUDA(cudaMemcpyAsync(S.wvol, wv.data(), sizeof(float) * wv.size(), cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
   }
   UPF_CUDA(launch_static_setup(S, st));
   UPF_CUDA(cudaMemsetAsync(S.st, 0, sizeof(DevState), st));
@@ -799,7 +826,8 @@ upf_status upf_get_neighbors(upf_system* s, uint32_t* counts, uint32_t* lists, u
     if (!lists) continue;
     for (uint32_t k = 0; k < cnt[i] && k < cap; ++k) {
       uint32_t code = nb[(size_t)k * s->nstride + i];
-      lists[(size_t)i * cap + k] = (code & kStaticBit) ? sid[code & ~kStaticBit] : bid[code];
+      const uint32_t base = s->dp.static_base;
+      lists[(size_t)i * cap + k] = (code >= base) ? sid[code - base] : bid[code];
     }
   }
   return UPF_OK;

@@ -16,7 +16,10 @@
 namespace upf {
 
 constexpr int kLut = UPF_LUT_SIZE;
-constexpr uint32_t kStaticBit = 0x80000000u;  // neighbour index refers to the boundary set
+// Bin thresholds: kBinThresholds[b] (b = 1..300) is the smallest float r2 whose
+// bin lut_index(sqrt_rn(r2)) is >= b; entry 301 is the smallest r2 with
+// sqrt_rn(r2) >= h (outside the support). Built on the host bit-exactly.
+constexpr int kThresholds = UPF_LUT_ENTRIES + 1;
 
 enum LutId { LUT_M4 = 0, LUT_PGRAD = 1, LUT_VISC = 2, LUT_ST = 3, LUT_ADH = 4 };
 
@@ -57,6 +60,7 @@ struct DevParams {
   uint32_t flags;
   uint32_t maxn;
   uint32_t nstride;        // neighbour-list column stride
+  uint32_t static_base;    // neighbour index of boundary particle j is static_base + j
 };
 
 // Device-side scalars of one system.
@@ -93,6 +97,23 @@ __device__ __forceinline__ float dist3(float4 a, float4 b) {
 __device__ __forceinline__ int lut_index(float d, float factor) {
   return (int)fmul(fmul(d, factor), (float)kLut);
 }
+// lut_index(sqrt_rn(r2)) from r2 without the correctly rounded square root:
+// an approximate root (relative error ~1e-7, so the scaled value is off by
+// far less than one bin) gives a guess g, and the exact thresholds `thr`
+// (kThresholds entries, see above) move it to the exact bin. Returns 300 for
+// r2 beyond the last bin (the tables' zero entry).
+__device__ __forceinline__ int bin_of_r2(float r2, float factor, const float* thr) {
+  float d = r2 * rsqrtf(r2);             // approximate sqrt; r2 == 0 gives NaN -> guess 0
+  int g = (int)(d * factor * (float)kLut);
+  g = g < 0 ? 0 : (g > kLut - 1 ? kLut - 1 : g);
+  if (thr[g + 1] <= r2) {
+    ++g;
+  } else if (g > 0 && thr[g] > r2) {
+    --g;
+  }
+  return g;
+}
+
 // PCISPH dist_lut: uint(dist * 300 / h), clamped to 300
 __device__ __forceinline__ unsigned dist_lut(float d, float h) {
   unsigned dl = (unsigned)__fdiv_rn(fmul(d, (float)kLut), h);

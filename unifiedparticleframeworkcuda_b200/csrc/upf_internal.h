@@ -18,6 +18,7 @@ void default_params(upf_params* p);
 int derive_params(upf_params* p, double* delta_fp64);
 void build_luts(const upf_params& p, float* out_5x301);
 float kernel_self(float h);
+void build_bin_thresholds(const upf_params& p, float* out_302);
 int validate_params(const upf_params& p, const char** why);
 double density_error_factor(const upf_params& p);
 

@@ -157,6 +157,49 @@ double density_error_factor_fp64(const upf_params& p) {
 
 float kernel_self(float h) { return m4(0.0f, h); }
 
+namespace {
+// bin of WeightingKernel::kernel*Lut for a squared distance: (int)(sqrtf(r2) * factor * 300)
+int bin_exact(float r2, float factor) { return (int)(sqrtf(r2) * factor * (float)UPF_LUT_SIZE); }
+
+uint32_t fbits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+float bitsf(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+// smallest non-negative float r2 with pred(r2) true (pred monotone, true at hi)
+template <class Pred>
+float first_true(uint32_t hi_bits, Pred pred) {
+  uint32_t lo = 0, hi = hi_bits;  // pred(bitsf(hi)) is true
+  if (pred(0.0f)) return 0.0f;
+  while (hi - lo > 1) {
+    uint32_t mid = lo + (hi - lo) / 2;
+    if (pred(bitsf(mid)))
+      hi = mid;
+    else
+      lo = mid;
+  }
+  return bitsf(hi);
+}
+}  // namespace
+
+// Exact squared-distance thresholds of the table bins (the device picks the
+// bin of r2 from these instead of a correctly rounded square root; sqrt,
+// the two products and the truncation are all monotone in r2).
+void build_bin_thresholds(const upf_params& p, float* out) {
+  const float h = p.support_radius;
+  const float factor = (float)(1.0 / (double)h);
+  const uint32_t top = fbits(h * h * 4.0f);
+  out[0] = 0.0f;
+  for (int b = 1; b <= UPF_LUT_SIZE; ++b)
+    out[b] = first_true(top, [&](float r2) { return bin_exact(r2, factor) >= b; });
+  out[UPF_LUT_SIZE + 1] = first_true(top, [&](float r2) { return sqrtf(r2) >= h; });
+}
+
 void build_luts(const upf_params& p, float* out) {
   const float sr = p.support_radius;
   for (int i = 0; i < UPF_LUT_SIZE; i++) {

@@ -46,6 +46,11 @@ __device__ __forceinline__ void stage_lut(float* dst, const float* __restrict__ 
   for (int k = threadIdx.x; k < UPF_LUT_ENTRIES; k += blockDim.x) dst[k] = src[k];
 }
 
+// the bin thresholds follow the five tables in the device lookup buffer
+__device__ __forceinline__ void stage_thresholds(float* dst, const float* __restrict__ luts) {
+  for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) dst[k] = luts[5 * UPF_LUT_ENTRIES + k];
+}
+
 __device__ __forceinline__ float4 f4(float x, float y, float z) { return make_float4(x, y, z, 0.0f); }
 
 // Neighbour loop with memory-level parallelism: the list entries of a batch
@@ -191,7 +196,11 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
     const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, uint32_t ns,
     const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
     const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, uint32_t* __restrict__ nbr,
-    uint16_t* __restrict__ bins, uint32_t* __restrict__ ncnt, DevState* __restrict__ st) {
+    uint16_t* __restrict__ bins, uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    DevState* __restrict__ st) {
+  __shared__ float thr[kThresholds];
+  for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) thr[k] = luts[5 * UPF_LUT_ENTRIES + k];
+  __syncthreads();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 xi = pos[i];
@@ -217,12 +226,13 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
   auto append = [&](uint32_t code, float r2) {
     if (cnt < maxn) {
       out[(size_t)cnt * stride] = code;
-      const int b = lut_index(__fsqrt_rn(r2), P.lut_factor);
-      ob[(size_t)cnt * stride] = (uint16_t)(b > kLut ? kLut : b);
+      ob[(size_t)cnt * stride] = (uint16_t)bin_of_r2(r2, P.lut_factor, thr);
     }
     cnt++;
   };
-  auto scan_range = [&](const float4* __restrict__ set, uint32_t b, uint32_t e, uint32_t tag, bool skip_self) {
+  // one contiguous range of one set; `base` turns a set index into a
+  // neighbour index (0 for dynamic, static_base for boundary particles)
+  auto scan_range = [&](const float4* __restrict__ set, uint32_t b, uint32_t e, uint32_t base, bool skip_self) {
     for (; b + kUnroll <= e; b += kUnroll) {
       float4 xj[kUnroll];
 #pragma unroll
@@ -231,12 +241,12 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
       for (int u = 0; u < kUnroll; ++u) {
         const uint32_t j = b + u;
         const float r2 = dist2(xi, xj[u]);
-        if (!(skip_self && j == i) && within_h(P, r2)) append(j | tag, r2);
+        if (!(skip_self && j == i) && r2 < thr[kThresholds - 1]) append(j + base, r2);
       }
     }
     for (; b < e; ++b) {
       const float r2 = dist2(xi, __ldg(set + b));
-      if (!(skip_self && b == i) && within_h(P, r2)) append(b | tag, r2);
+      if (!(skip_self && b == i) && r2 < thr[kThresholds - 1]) append(b + base, r2);
     }
   };
   auto visit = [&](uint32_t c) {
@@ -251,7 +261,7 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
       return;
     }
     if (ds == de) {
-      scan_range(spos, ss, se, kStaticBit, false);
+      scan_range(spos, ss, se, P.static_base, false);
       return;
     }
     while (ds < de || ss < se) {  // both sets present: merge by key
@@ -259,11 +269,11 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
       if (take_dyn) {
         uint32_t j = ds++;
         const float r2 = dist2(xi, pos[j]);
-        if (j != i && within_h(P, r2)) append(j, r2);
+        if (j != i && r2 < thr[kThresholds - 1]) append(j, r2);
       } else {
         uint32_t j = ss++;
         const float r2 = dist2(xi, spos[j]);
-        if (within_h(P, r2)) append(j | kStaticBit, r2);
+        if (r2 < thr[kThresholds - 1]) append(j + P.static_base, r2);
       }
     }
   };
@@ -465,17 +475,12 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
           nbr + i, bins + i, P.nstride, ncnt[i],
           [&](uint32_t code) {
             WNb s;
-            if (code & kStaticBit) {  // boundary particles are never liquid
-              s.t = UPF_FROZEN;
-              s.x = s.v = make_float4(0, 0, 0, 0);
-              s.d = s.p = 0.0f;
-            } else {
-              s.t = __ldg(btype + code);
-              s.x = __ldg(bpos + code);
-              s.v = __ldg(bvel + code);
-              s.d = __ldg(rho + code);
-              s.p = __ldg(press + code);
-            }
+            // boundary particles (array tails) are FROZEN and skipped below
+            s.t = __ldg(btype + code);
+            s.x = __ldg(bpos + code);
+            s.v = __ldg(bvel + code);
+            s.d = __ldg(rho + code);
+            s.p = __ldg(press + code);
             return s;
           },
           [&](uint32_t, uint32_t bin, const WNb& s) {
@@ -577,9 +582,9 @@ __device__ __forceinline__ void boundary_pressure(const DevParams& P, const floa
 // CalculateExternalForcesVersatilCouplingPCISPH (UnifiedPhysics.cpp:5252-5365),
 // liquid particles; then the first prediction of the loop.
 __global__ void __launch_bounds__(kBlock) k_pcisph_external(
-    DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const float* __restrict__ swvol,
-    const float* __restrict__ wvol_dyn, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
-    const float* __restrict__ luts, float4* __restrict__ force, float4* __restrict__ pforce,
+    DevParams P, uint32_t n, DynArrays B, const float* __restrict__ wvol, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts, float4* __restrict__ force,
+    float4* __restrict__ pforce,
     float4* __restrict__ xs, float* __restrict__ press, float* __restrict__ pq, DevState* __restrict__ st) {
   __shared__ float vl[UPF_LUT_ENTRIES], pg[UPF_LUT_ENTRIES], stl[UPF_LUT_ENTRIES], adl[UPF_LUT_ENTRIES];
   stage_lut(vl, luts + LUT_VISC * UPF_LUT_ENTRIES);
@@ -611,24 +616,17 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
   const float4* __restrict__ bpos = B.pos;
   const float4* __restrict__ bvel = B.vel;
   const int32_t* __restrict__ btype = B.type;
+  // boundary particles sit in the tails of the B arrays (type FROZEN, velocity 0)
   for_neighbors(
       nbr + i, P.nstride, ncnt[i],
       [&](uint32_t code) {
         NbState s;
-        if (code & kStaticBit) {
-          s.x = __ldg(spos + (code & ~kStaticBit));
-          s.v = make_float4(0, 0, 0, 0);
-          s.t = UPF_FROZEN;
-        } else {
-          s.x = __ldg(bpos + code);
-          s.v = __ldg(bvel + code);
-          s.t = __ldg(btype + code);
-        }
+        s.x = __ldg(bpos + code);
+        s.v = __ldg(bvel + code);
+        s.t = __ldg(btype + code);
         return s;
       },
       [&](uint32_t code, const NbState& s) {
-    const bool is_static = code & kStaticBit;
-    const uint32_t j = code & ~kStaticBit;
     const float4 xj = s.x;
     const float d = dist3(xi, xj);
     if (!(d < h)) return;
@@ -648,7 +646,7 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
         fz = fz - (xi.z - xj.z) * P.st_gamma * m * m * sp * inv;
       }
     } else if (tj == UPF_FROZEN || tj == UPF_RIGID) {
-      const float wv = is_static ? swvol[j] : wvol_dyn[j];
+      const float wv = wvol[code];
       // the reference passes the liquid particle's own weighted volume (its
       // rest volume) to the pressure term, UnifiedPhysics.cpp:5292
       if (flags & UPF_FLAG_BOUNDARY_PRESSURE)
@@ -678,14 +676,16 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
 // and accumulates them in list order.
 __global__ void __launch_bounds__(kBlock) k_pcisph_density(
     DevParams P, uint32_t n, const int32_t* __restrict__ type, const float4* __restrict__ xs,
-    const float4* __restrict__ spos, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
+    const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
     const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press, float* __restrict__ pq,
     DevState* __restrict__ st) {
   __shared__ float m4[UPF_LUT_ENTRIES];
+  __shared__ float thr[kThresholds];
   __shared__ uint32_t wmax[kBlock / 32];
   __shared__ WarpListRing<false> rings[kBlock / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
+  stage_thresholds(thr, luts);
   ring_init(rings[warp]);
   __syncthreads();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -699,21 +699,19 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
   WarpListRing<false>& ring = rings[warp];
   const bool ok = ring_walk(ring, &cmap, &cmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
                             [&](int s, int k0) {
+                              // predicted positions; boundary particles sit in the array's
+                              // tail at their fixed positions
                               float4 xj[kListRows];
 #pragma unroll
-                              for (int r = 0; r < kListRows; ++r) {
-                                if (k0 + r < (int)cnt) {
-                                  const uint32_t code = ring.codes[s][r][lane];
-                                  xj[r] = (code & kStaticBit) ? __ldg(spos + (code & ~kStaticBit))
-                                                              : __ldg(xs + code);
-                                }
-                              }
+                              for (int r = 0; r < kListRows; ++r)
+                                if (k0 + r < (int)cnt) xj[r] = __ldg(xs + ring.codes[s][r][lane]);
 #pragma unroll
                               for (int r = 0; r < kListRows; ++r) {
                                 if (k0 + r < (int)cnt) {
-                                  const float d = dist3(xi, xj[r]);
-                                  if (d < P.h) {
-                                    const float kv = lut_at(m4, d, P.lut_factor);
+                                  // d < h and the table bin of d, from d^2 (exact)
+                                  const float r2 = dist2(xi, xj[r]);
+                                  if (r2 < thr[kThresholds - 1]) {
+                                    const float kv = m4[bin_of_r2(r2, P.lut_factor, thr)];
                                     den += kv * m;
                                   }
                                 }
@@ -769,19 +767,15 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
   WarpListRing<true>& ring = rings[warp];
   const bool ok = ring_walk(ring, &cmap, &bmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
                             [&](int s, int k0) {
+                              // boundary particles sit in the arrays' tails (pq = 0 there)
                               float4 xj[kListRows];
                               float qj[kListRows];
 #pragma unroll
                               for (int r = 0; r < kListRows; ++r) {
                                 if (k0 + r < (int)cnt) {
                                   const uint32_t code = ring.codes[s][r][lane];
-                                  if (code & kStaticBit) {
-                                    xj[r] = __ldg(spos + (code & ~kStaticBit));
-                                    qj[r] = 0.0f;
-                                  } else {
-                                    xj[r] = __ldg(pos + code);
-                                    qj[r] = __ldg(pq + code);
-                                  }
+                                  xj[r] = __ldg(pos + code);
+                                  qj[r] = __ldg(pq + code);
                                 }
                               }
 #pragma unroll
@@ -964,7 +958,7 @@ cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
   k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
   if (n == 0) return cudaGetLastError();
   k_build_nlist<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
-                                                s.skeys, s.sstart, s.send, s.nbr, s.bins, s.ncnt, s.st);
+                                                s.skeys, s.sstart, s.send, s.nbr, s.bins, s.ncnt, s.luts, s.st);
   return cudaGetLastError();
 }
 
@@ -975,8 +969,8 @@ cudaError_t launch_force_phase(System& s, cudaStream_t st) {
     k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.bins, s.ncnt, s.luts, s.rho,
                                                    s.press);
   } else {
-    k_pcisph_external<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.swvol, s.wvol_dyn, s.nbr, s.ncnt,
-                                                     s.luts, s.force, s.pforce, s.xs, s.press, s.pq, s.st);
+    k_pcisph_external<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.wvol, s.nbr, s.ncnt, s.luts, s.force,
+                                                     s.pforce, s.xs, s.press, s.pq, s.st);
   }
   return cudaGetLastError();
 }
@@ -989,8 +983,8 @@ cudaError_t launch_loop_init(System& s, cudaStream_t st) {
 cudaError_t launch_loop_density(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.type, s.xs, s.spos, s.nbr_map, s.ncnt, s.luts,
-                                                    s.rho, s.press, s.pq, s.st);
+    k_pcisph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.type, s.xs, s.nbr_map, s.ncnt, s.luts, s.rho,
+                                                    s.press, s.pq, s.st);
   return cudaGetLastError();
 }
 
@@ -1041,7 +1035,8 @@ cudaError_t launch_static_setup(System& s, cudaStream_t st) {
   if (ns == 0) return cudaSuccess;
   e = cell_ranges(s.skeys, ns, 3 * (int)s.dp.block_shift, s.ncells, s.sstart, s.send, st);
   if (e != cudaSuccess) return e;
-  k_static_wvol<<<grid_of(ns), kBlock, 0, st>>>(s.dp, ns, s.spos, s.sstart, s.send, s.luts, s.swvol);
+  k_static_wvol<<<grid_of(ns), kBlock, 0, st>>>(s.dp, ns, s.spos, s.sstart, s.send, s.luts,
+                                                 s.wvol + s.dp.static_base);
   return cudaGetLastError();
 }
 

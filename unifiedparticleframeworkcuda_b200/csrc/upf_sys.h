@@ -11,8 +11,11 @@
 //   per-step fields (indexed like B): external force, correction pressure
 //   force, predicted position, predicted density, correction pressure.
 //   neighbour lists: column-major nbr[k * stride + i] (coalesced reads when
-//   consecutive threads take consecutive particles), bit 31 marks an index
-//   into the boundary set.
+//   consecutive threads take consecutive particles). Neighbour index j < stride
+//   is dynamic particle j; stride + b is boundary particle b. The arrays a
+//   neighbour loop gathers from (B.pos/vel/type, xs, pq, wvol) are allocated
+//   with stride + capacity entries and hold the boundary particles' data in
+//   that tail, so a gather needs no branch on the particle's set.
 #pragma once
 
 #include <cuda.h>
@@ -62,7 +65,7 @@ struct System {
   float* rho = nullptr;
   float* press = nullptr;
   float* pq = nullptr;         // press / rest_density^2 (PCISPH loop)
-  float* wvol_dyn = nullptr;   // Akinci volume of dynamic rigid particles
+  float* wvol = nullptr;       // Akinci volume per neighbour index (dynamic, then boundary tail)
 
   // neighbour lists
   uint32_t* nbr = nullptr;
