@@ -880,6 +880,7 @@ upf_status upf_radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, int3
   uint32_t* kalt = (uint32_t*)temp;
   uint32_t* valt = kalt + ((n + 63) & ~63u);
   uint32_t* counts = valt + ((n + 63) & ~63u);
+  UPF_CUDA(radix_init());  // once per device
   UPF_CUDA(radix_sort_pairs(keys, vals, kalt, valt, counts, n, key_bits, false, (cudaStream_t)stream));
   return UPF_OK;
 }

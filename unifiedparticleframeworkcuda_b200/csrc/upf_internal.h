@@ -23,6 +23,8 @@ int validate_params(const upf_params& p, const char** why);
 double density_error_factor(const upf_params& p);
 
 // upf_sort.cu
+constexpr uint32_t kRadixTileKeys = 8192;  // keys per sort tile (16 warps x 512)
+constexpr uint32_t kRadixDigits = 256;     // 8-bit digits
 uint32_t radix_tiles(uint32_t n);
 size_t radix_temp_words(uint32_t n);
 size_t radix_temp_bytes(uint32_t n);

@@ -14,6 +14,8 @@
 // digits keep their input order; an LSD sort of stable passes is stable.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "upf_common.cuh"
 #include "upf_internal.h"
 
@@ -28,6 +30,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kItemsPerLane = 16;
 constexpr int kWarpItems = 32 * kItemsPerLane;   // 512
 constexpr int kTile = kWarps * kWarpItems;       // 8192 keys per tile
+static_assert(kTile == (int)kRadixTileKeys && kRadix == (int)kRadixDigits, "scratch layout constants");
 
 __global__ void __launch_bounds__(kThreads) k_upsweep(const uint32_t* __restrict__ keys, uint32_t n,
                                                        int shift, uint32_t ntiles,
@@ -206,12 +209,22 @@ size_t radix_temp_words(uint32_t n) {
 
 size_t radix_temp_bytes(uint32_t n) { return radix_temp_words(n) * sizeof(uint32_t); }
 
-// Opt the downsweep kernel into its 82 KB of dynamic shared memory; called
-// once per device before any launch (and before any stream capture).
+// Opt the downsweep kernel into its 82 KB of dynamic shared memory on the
+// current device, once per device (before any launch on it, and so before
+// any stream capture that launches it).
 cudaError_t radix_init() {
-  cudaError_t e = cudaFuncSetAttribute(k_downsweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDownSmem);
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_downsweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDownSmem);
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute(k_downsweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDownSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_downsweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDownSmem);
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+  return e;
 }
 
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
