@@ -311,6 +311,22 @@ upf_status upf_radix_sort_pairs(uint32_t* keys_dev, uint32_t* vals_dev, uint32_t
                                 int32_t key_bits, void* temp_dev, size_t temp_bytes,
                                 void* stream);
 
+/* The same sort without caller scratch and without any allocation. No
+ * counterpart in the reference. For callers that cannot call cudaMalloc: hosts
+ * that own all device memory through their own pool or arena, and per-frame
+ * loops that must not pay cudaMalloc's implicit device synchronisation. The
+ * scratch is a fixed file-scope device array in the library, sized for at most
+ * UPF_NOALLOC_MAX_PAIRS pairs (17 MB); every GPU that loads the library holds it
+ * until the process exits. Larger n is rejected with UPF_ERR_INVALID_ARG.
+ * The first call on a device looks up that array's device address (once per
+ * device, with the device current); make that first call before any stream
+ * capture. All calls share the one array and it keeps the last call's
+ * contents: calls that overlap on the GPU (different streams or host threads
+ * without ordering between them) race on it. */
+#define UPF_NOALLOC_MAX_PAIRS (1u << 21)
+upf_status upf_radix_sort_pairs_noalloc(uint32_t* keys_dev, uint32_t* vals_dev, uint32_t n,
+                                        int32_t key_bits, void* stream);
+
 /* Cell start/end for sorted keys at cell = key >> shift (empty cells start=end=0).
  * Replaces ClearIndexArrays + CalculateBlocksKernel (particles_kernel.cu:656-726). */
 upf_status upf_cell_ranges(const uint32_t* sorted_keys_dev, uint32_t n, int32_t shift,

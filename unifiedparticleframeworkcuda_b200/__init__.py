@@ -70,6 +70,7 @@ def lib():
             "upf_get_cell_ranges": [vp, u32p, u32p, u32p],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
             "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
+            "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],
             "upf_cell_ranges": [vp, C.c_uint32, C.c_int32, C.c_uint32, vp, vp, vp],
             "upf_upload_state": [vp, fp, fp, C.c_uint32],
             "upf_profile_step": [vp, C.POINTER(UpfPhaseTimes)],

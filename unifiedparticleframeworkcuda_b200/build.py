@@ -22,9 +22,9 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libupf.so")
 INCLUDE = os.path.abspath(os.path.join(HERE, "..", "include"))
 
-CU_SOURCES = ["upf_sort.cu", "upf_pipeline.cu", "upf_api.cu"]
+CU_SOURCES = ["upf_sort.cu", "upf_pipeline.cu", "upf_api.cu", "upf_noalloc.cu"]
 CPP_SOURCES = ["upf_params.cpp"]
-HEADERS = ["upf_common.cuh", "upf_internal.h", "upf_sys.h"]
+HEADERS = ["upf_common.cuh", "upf_internal.h", "upf_sys.h", "upf_tma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
