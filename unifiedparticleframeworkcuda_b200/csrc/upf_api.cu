@@ -74,13 +74,6 @@ uint32_t log2u(uint32_t v) {
 DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   DevParams d{};
   d.h = p.support_radius;
-  {
-    // sqrt is monotone and correctly rounded: r2 < h^2 (1 - 2^-20) implies
-    // RN(sqrt(r2)) < h, and r2 > h^2 (1 + 2^-20) implies RN(sqrt(r2)) >= h
-    const double h2 = (double)p.support_radius * (double)p.support_radius;
-    d.r2_accept = std::nextafter((float)(h2 * (1.0 - std::ldexp(1.0, -20))), 0.0f);
-    d.r2_reject = std::nextafter((float)(h2 * (1.0 + std::ldexp(1.0, -20))), INFINITY);
-  }
   d.lut_factor = (float)(1.0 / (double)p.support_radius);
   d.mass = p.mass;
   d.inv_mass = (float)(1.0 / (double)p.mass);
@@ -416,7 +409,6 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   ALLOC(s->nbr, (size_t)s->nstride * p->max_neighbors);
   ALLOC(s->bins, (size_t)s->nstride * p->max_neighbors);
   ALLOC(s->ncnt, c);
-  ALLOC(s->occ, c);
   ALLOC(s->cstart, s->ncells); ALLOC(s->cend, s->ncells);
   ALLOC(s->sstart, s->ncells); ALLOC(s->send, s->ncells);
   ALLOC(s->spos, c); ALLOC(s->skeys, c); ALLOC(s->sid, c);

@@ -29,8 +29,6 @@ enum : uint32_t { ERR_OVERFLOW = 1u, ERR_NAN = 2u, ERR_TIMEOUT = 4u };
 // Everything a kernel needs from upf_params, by value.
 struct DevParams {
   float h;            // support radius
-  float r2_accept;    // squared distances below this are certainly < h after sqrt
-  float r2_reject;    // squared distances above this are certainly >= h after sqrt
   float lut_factor;   // (float)(1.0 / h): the reference's function-static factor
   float mass;
   float inv_mass;     // (float)(1.0 / mass)
@@ -65,7 +63,6 @@ struct DevParams {
 
 // Device-side scalars of one system.
 struct DevState {
-  uint32_t n_occupied;     // occupied cells of the dynamic set this step
   uint32_t max_rho_bits;   // running max predicted density (positive floats order as uints)
   int32_t iteration;
   int32_t too_large;

@@ -145,42 +145,6 @@ __device__ __forceinline__ float dist2(float4 a, float4 b) {
   return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
 }
 
-// Membership test of GetNeighbors (UnifiedPhysics.cpp:2270): sqrtf(r2) < h.
-// Squared distances clearly below or above h^2 decide without the square
-// root; the thin band around h^2 takes the exact test, so the result is
-// always that of the reference's float test.
-__device__ __forceinline__ bool within_h(const DevParams& P, float r2) {
-  if (r2 < P.r2_accept) return true;
-  if (r2 > P.r2_reject) return false;
-  return __fsqrt_rn(r2) < P.h;
-}
-
-// Block coordinate of a Morton code (inverse of spread3).
-__device__ __forceinline__ uint32_t compact3(uint32_t v) {
-  v &= 0x09249249u;
-  v = (v | (v >> 2)) & 0x030C30C3u;
-  v = (v | (v >> 4)) & 0x0300F00Fu;
-  v = (v | (v >> 8)) & 0x030000FFu;
-  v = (v | (v >> 16)) & 0x000003FFu;
-  return v;
-}
-
-// Cell ranges of the dynamic set (ClearIndexArrays + CalculateBlocksKernel,
-// particles_kernel.cu:656-726) that also collect the occupied cells for the
-// neighbour pass (in any order: each cell's output does not depend on it).
-__global__ void __launch_bounds__(kBlock) k_cell_ranges_occ(const uint32_t* __restrict__ keys, uint32_t n, int shift,
-                                                             uint32_t* __restrict__ start, uint32_t* __restrict__ end,
-                                                             uint32_t* __restrict__ occ, DevState* __restrict__ st) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t c = keys[i] >> shift;
-  if (i == 0 || (keys[i - 1] >> shift) != c) {
-    start[c] = i;
-    occ[atomicAdd(&st->n_occupied, 1u)] = c;
-  }
-  if (i == n - 1 || (keys[i + 1] >> shift) != c) end[c] = i + 1;
-}
-
 // GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
 // (zIndex.cpp:43-73), one thread per particle: candidates are the Morton
 // blocks covering the query box (with a one-grid-unit margin, so the
@@ -945,12 +909,7 @@ cudaError_t launch_sort_phase(System& s, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   k_reorder<<<grid_of(n), kBlock, 0, st>>>(n, s.perm, s.A, s.B, s.prm.method == UPF_METHOD_PCISPH);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(s.cstart, 0, sizeof(uint32_t) * s.ncells, st)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(s.cend, 0, sizeof(uint32_t) * s.ncells, st)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(&s.st->n_occupied, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-  k_cell_ranges_occ<<<grid_of(n), kBlock, 0, st>>>(s.keysA, n, 3 * (int)s.dp.block_shift, s.cstart, s.cend, s.occ,
-                                                    s.st);
-  return cudaGetLastError();
+  return cell_ranges(s.keysA, n, 3 * (int)s.dp.block_shift, s.ncells, s.cstart, s.cend, st);
 }
 
 cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {

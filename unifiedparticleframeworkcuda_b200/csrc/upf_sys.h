@@ -71,7 +71,6 @@ struct System {
   uint32_t* nbr = nullptr;
   uint16_t* bins = nullptr;    // kernel-table bin of each list entry at current positions
   uint32_t* ncnt = nullptr;
-  uint32_t* occ = nullptr;     // occupied cells of the dynamic set
   CUtensorMap nbr_map;         // 2D [max_neighbors][nstride] uint32 view of nbr for TMA
   CUtensorMap bins_map;        // same view of bins (uint16)
   uint32_t nstride = 0;
