@@ -209,6 +209,8 @@ def run_ours(args, rank, world, local_rank):
     s.step(args.warmup)
     s.synchronize()
     s.reset_counters()
+    # the end-to-end run below replays the same steps from this state
+    s.checkpoint(0)
     torch.cuda.synchronize()
 
     def barrier():
@@ -261,17 +263,17 @@ def run_ours(args, rank, world, local_rank):
         kname, kms, kbytes = "k_wcsph_force_integrate", pr.integrate_ms, (16 + 16 + 4 + 4 + 16 + 16 + 4) * nf
     achieved = kbytes / (kms / 1e3) / 1e9
     step_bytes = algorithmic_bytes(nf, nb, args.steps, total_iters, method)
-    traffic = None
-    try:
-        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        traffic = tr.get(args.scene, {}).get(kname)
-    except Exception:
-        pass
+    # DRAM bytes per fluid particle per launch from one ncu capture of the same
+    # kernels (profiles/pcisph_loop_kernels_262k_ncu.md), scaled by fluid count
+    traffic_per_particle = {"k_pcisph_density": 158.0, "k_pcisph_pressure_force": 261.0}
+    traffic = traffic_per_particle[kname] * nf if kname in traffic_per_particle else None
 
-    # end to end through the C ABI with host buffers: per step, upload the
+    # end to end through the C ABI with host buffers, over the same steps as
+    # the timed region (restored from the checkpoint): per step, upload the
     # state from pinned host memory, step, read the result back
     e2e = None
     if not args.no_e2e:
+        s.restore(0)
         n = s.n_dynamic
         hpos = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
         hvel = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
@@ -292,7 +294,7 @@ def run_ours(args, rank, world, local_rank):
                       "upf_get_particles")
 
         readback()
-        k_e2e = max(1, min(args.steps, 10))
+        k_e2e = args.steps
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)

@@ -260,6 +260,19 @@ upf_status upf_phase_integrate(upf_system* s);
  * host-driven caller (src/gpu/particles.cuh:437). */
 upf_status upf_upload_state(upf_system* s, const float* pos4, const float* vel4, uint32_t n);
 
+/* ---- checkpoint / resume ------------------------------------------------- */
+/* The reference only has text dumps and readers (src/cpu/UnifiedIO.cpp:14-220).
+ * Here the dynamic state (positions, velocities, lagged PCISPH state, ids,
+ * types, keys, counters) can be copied to a device-side slot and back (step
+ * checkpointing), or to/from a host buffer of upf_state_bytes() bytes (a
+ * binary snapshot to resume from). Slots are allocated on first use; all
+ * copies are stream-ordered on the system's stream. */
+upf_status upf_checkpoint(upf_system* s, int32_t slot);
+upf_status upf_restore(upf_system* s, int32_t slot);
+size_t upf_state_bytes(const upf_system* s);
+upf_status upf_state_save(upf_system* s, void* host, size_t bytes);
+upf_status upf_state_load(upf_system* s, const void* host, size_t bytes);
+
 /* Per-phase device timings of one step (the reference's SPH_PROFILING_VERBOSE
  * per-phase event timers, src/gpu/particles.cu:1460-1690). Runs one full
  * step through the phase entry points with CUDA events around each phase,

@@ -75,11 +75,17 @@ def lib():
             "upf_upload_state": [vp, fp, fp, C.c_uint32],
             "upf_profile_step": [vp, C.POINTER(UpfPhaseTimes)],
             "upf_reset_counters": [vp],
+            "upf_checkpoint": [vp, C.c_int32],
+            "upf_restore": [vp, C.c_int32],
+            "upf_state_save": [vp, vp, C.c_size_t],
+            "upf_state_load": [vp, vp, C.c_size_t],
         }
         for name, args in sig.items():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = C.c_int
+        L.upf_state_bytes.argtypes = [vp]
+        L.upf_state_bytes.restype = C.c_size_t
         L.upf_radix_sort_temp_bytes.argtypes = [C.c_uint32]
         L.upf_radix_sort_temp_bytes.restype = C.c_size_t
         L.upf_last_error.restype = C.c_char_p
@@ -184,6 +190,23 @@ class ParticleSystem:
         s = UpfStepStats()
         check(lib().upf_get_step_stats(self._h, C.byref(s)), "upf_get_step_stats")
         return s
+
+    # checkpoint / resume
+    def checkpoint(self, slot: int = 0):
+        check(lib().upf_checkpoint(self._h, int(slot)), "upf_checkpoint")
+
+    def restore(self, slot: int = 0):
+        check(lib().upf_restore(self._h, int(slot)), "upf_restore")
+
+    def save_state(self) -> bytes:
+        n = lib().upf_state_bytes(self._h)
+        buf = C.create_string_buffer(n)
+        check(lib().upf_state_save(self._h, buf, n), "upf_state_save")
+        return buf.raw
+
+    def load_state(self, data: bytes):
+        buf = C.create_string_buffer(data, len(data))
+        check(lib().upf_state_load(self._h, buf, len(data)), "upf_state_load")
 
     def reset_counters(self):
         check(lib().upf_reset_counters(self._h), "upf_reset_counters")

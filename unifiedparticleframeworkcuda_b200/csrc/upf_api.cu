@@ -696,6 +696,107 @@ upf_status upf_upload_state(upf_system* s, const float* pos4, const float* vel4,
   return UPF_OK;
 }
 
+// ---- checkpoint / resume ---------------------------------------------------
+// The dynamic state as contiguous segments (A copy + keys + device scalars).
+namespace {
+struct StateSeg {
+  void* dev;
+  size_t bytes;
+};
+int state_segments(System& s, StateSeg* seg) {
+  const size_t n = s.n_dyn;
+  seg[0] = {s.A.pos, sizeof(float4) * n};
+  seg[1] = {s.A.vel, sizeof(float4) * n};
+  seg[2] = {s.A.lag, sizeof(float4) * n};
+  seg[3] = {s.A.id, sizeof(uint32_t) * n};
+  seg[4] = {s.A.type, sizeof(int32_t) * n};
+  seg[5] = {s.keysA, sizeof(uint32_t) * n};
+  seg[6] = {s.st, sizeof(DevState)};
+  return 7;
+}
+size_t state_total(System& s) {
+  StateSeg seg[8];
+  const int k = state_segments(s, seg);
+  size_t t = 0;
+  for (int i = 0; i < k; ++i) t += (seg[i].bytes + 255) & ~size_t(255);
+  return t;
+}
+// copy all segments between the system and a flat buffer (device or host)
+upf_status state_copy(System& s, char* flat, bool to_flat, cudaMemcpyKind kind) {
+  StateSeg seg[8];
+  const int k = state_segments(s, seg);
+  size_t off = 0;
+  for (int i = 0; i < k; ++i) {
+    if (seg[i].bytes) {
+      cudaError_t e = to_flat ? cudaMemcpyAsync(flat + off, seg[i].dev, seg[i].bytes, kind, s.stream)
+                              : cudaMemcpyAsync(seg[i].dev, flat + off, seg[i].bytes, kind, s.stream);
+      if (e != cudaSuccess) {
+        set_error("state copy: %s", cudaGetErrorString(e));
+        return UPF_ERR_CUDA;
+      }
+    }
+    off += (seg[i].bytes + 255) & ~size_t(255);
+  }
+  return UPF_OK;
+}
+}  // namespace
+
+upf_status upf_checkpoint(upf_system* s, int32_t slot) {
+  UPF_TRY(phase_guard(s));
+  if (slot < 0 || slot > 4096) {
+    set_error("upf_checkpoint: slot %d out of range", slot);
+    return UPF_ERR_INVALID_ARG;
+  }
+  if ((size_t)slot >= s->checkpoint_slots.size()) s->checkpoint_slots.resize(slot + 1, nullptr);
+  if (!s->checkpoint_slots[slot]) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, state_total(*s));
+    if (e != cudaSuccess) {
+      set_error("upf_checkpoint: cudaMalloc: %s", cudaGetErrorString(e));
+      return UPF_ERR_ALLOC;
+    }
+    s->checkpoint_slots[slot] = p;
+    s->allocations.push_back(p);
+  }
+  return state_copy(*s, (char*)s->checkpoint_slots[slot], true, cudaMemcpyDeviceToDevice);
+}
+
+upf_status upf_restore(upf_system* s, int32_t slot) {
+  UPF_TRY(phase_guard(s));
+  if (slot < 0 || (size_t)slot >= s->checkpoint_slots.size() || !s->checkpoint_slots[slot]) {
+    set_error("upf_restore: slot %d holds no checkpoint", slot);
+    return UPF_ERR_INVALID_ARG;
+  }
+  return state_copy(*s, (char*)s->checkpoint_slots[slot], false, cudaMemcpyDeviceToDevice);
+}
+
+size_t upf_state_bytes(const upf_system* s) {
+  if (!s || !s->have_particles) return 0;
+  return state_total(*const_cast<upf_system*>(s));
+}
+
+upf_status upf_state_save(upf_system* s, void* host, size_t bytes) {
+  UPF_TRY(phase_guard(s));
+  if (!host || bytes < state_total(*s)) {
+    set_error("upf_state_save: need %zu bytes", state_total(*s));
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_TRY(state_copy(*s, (char*)host, true, cudaMemcpyDeviceToHost));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_state_load(upf_system* s, const void* host, size_t bytes) {
+  UPF_TRY(phase_guard(s));
+  if (!host || bytes < state_total(*s)) {
+    set_error("upf_state_load: need %zu bytes (same particle count as the saving system)", state_total(*s));
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_TRY(state_copy(*s, (char*)const_cast<void*>(host), false, cudaMemcpyHostToDevice));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  return UPF_OK;
+}
+
 upf_status upf_profile_step(upf_system* s, upf_phase_times* out) {
   UPF_TRY(phase_guard(s));
   if (!out) {

@@ -100,6 +100,7 @@ struct System {
   int key_bits = 30;
 
   std::vector<void*> allocations;
+  std::vector<void*> checkpoint_slots;  // device copies of the dynamic state (upf_checkpoint)
 };
 
 // upf_pipeline.cu: phase launchers (all asynchronous on s.stream)
