@@ -222,9 +222,13 @@ upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4
 
 /* Rigid bodies (MallocDeviceArraysRigidBody + CopyRigidBodyDataHostToDevice,
  * src/gpu/particles.cuh:433,438). body_of_particle[i] = body index for every
- * RIGID particle i of the last upf_set_particles call (-1 otherwise).
- * Body mass, centre of mass and inverse local inertia are computed from the
- * particles (AddToRigidBody UnifiedPhysics.cpp:825-885, FP64). */
+ * RIGID particle i of the last upf_set_particles call (-1 otherwise); n is
+ * that call's particle count. Body mass, centre of mass, momenta and inverse
+ * local inertia are computed from the uploaded positions and velocities
+ * (AddToRigidBody UnifiedPhysics.cpp:825-885, summed in FP64). PCISPH only;
+ * call after upf_set_particles and before the first step (UPF_ERR_STATE
+ * otherwise). num_bodies = 0 removes all bodies. Every body needs at least
+ * one particle. Setting particles again removes the bodies. */
 upf_status upf_set_rigid_bodies(upf_system* s, const int32_t* body_of_particle,
                                 uint32_t n, uint32_t num_bodies);
 
@@ -307,6 +311,11 @@ upf_status upf_get_neighbors(upf_system* s, uint32_t* counts, uint32_t* lists_id
 /* Sorted keys and cell ranges of the dynamic set (after upf_phase_sort). */
 upf_status upf_get_sorted_keys(upf_system* s, uint32_t* keys, uint32_t* ids, uint32_t* n_out);
 upf_status upf_get_cell_ranges(upf_system* s, uint32_t* start, uint32_t* end, uint32_t* ncells_out);
+/* Rigid body state (RigidBody::rigidbody_pos / velocity / angular_velocity /
+ * quaternion, src/cpu/RigidBody.h:105-134): pos3/vel3/omega3 num_bodies x 3
+ * floats, quat4 num_bodies x 4 (s, x, y, z). Any pointer may be NULL. */
+upf_status upf_get_rigid_bodies(upf_system* s, float* pos3, float* vel3, float* omega3,
+                                float* quat4, uint32_t* num_bodies_out);
 
 /* ---- stateless device building blocks ----------------------------------- */
 /* Device pointers; stream as void* (NULL = default stream). */

@@ -185,6 +185,19 @@ class OracleSim:
         rc = lib().orc_set_rigid_bodies(self._h, _ptr(body, C.c_int32), body.shape[0], num_bodies)
         if rc != 0:
             raise RuntimeError("oracle rigid bodies not supported for this scene")
+        self.num_bodies = int(num_bodies)
+
+    def rigid(self):
+        """(pos (nb,3), vel (nb,3), omega (nb,3), quat (nb,4) as (s,x,y,z))."""
+        nb = getattr(self, "num_bodies", 0)
+        pos = np.zeros((nb, 3), np.float32)
+        vel = np.zeros((nb, 3), np.float32)
+        om = np.zeros((nb, 3), np.float32)
+        q = np.zeros((nb, 4), np.float32)
+        if nb:
+            lib().orc_get_rigid(self._h, _ptr(pos, C.c_float), _ptr(vel, C.c_float), _ptr(om, C.c_float),
+                                _ptr(q, C.c_float))
+        return pos, vel, om, q
 
     def state(self):
         n = self.n

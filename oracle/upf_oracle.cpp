@@ -156,15 +156,54 @@ struct Particle {
   V3<R> r0;            // init_relative_pos_
 };
 
+// RigidBody (src/cpu/RigidBody.h:105-134): the state is float as in the
+// reference; the per-body sums (force, torque, mass, inertia) are FP64.
 template <class R>
 struct Body {
-  double mass;
-  V3<R> pos, vel, P, L, omega, force, torque;
+  R mass;
+  V3<R> pos, vel, P, L, omega;
   R q[4];              // quaternion_ (s, x, y, z)
   R rot[3][3];
   R inv_inertia_local[3][3];
   R inv_inertia_world[3][3];
 };
+
+// Matrix3x3::operator* (Matrix3x3.cpp:15-31, 34-47): sums from zero in k order
+template <class R>
+void mat_mul(const R a[3][3], const R b[3][3], R out[3][3]) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      R s = 0;
+      for (int k = 0; k < 3; ++k) s += a[i][k] * b[k][j];
+      out[i][j] = s;
+    }
+}
+template <class R>
+V3<R> mat_vec(const R a[3][3], V3<R> v) {
+  const R* x = &v.x;
+  R r[3];
+  for (int i = 0; i < 3; ++i) {
+    r[i] = 0;
+    for (int j = 0; j < 3; ++j) r[i] += a[i][j] * x[j];
+  }
+  return {r[0], r[1], r[2]};
+}
+// Vector3::normalize (vmmlib/vector3.h:516-528): returns the length
+template <class R>
+R normalize(V3<R>& v) {
+  const R l = vsqrt(lensq(v));
+  if (l == 0) return 0;
+  const R ll = R(1.0 / l);
+  v.x *= ll;
+  v.y *= ll;
+  v.z *= ll;
+  return l;
+}
+// cos/sin of a float as the reference's host build evaluates them
+inline float fcos(float x) { return cosf(x); }
+inline float fsin(float x) { return sinf(x); }
+inline double fcos(double x) { return std::cos(x); }
+inline double fsin(double x) { return std::sin(x); }
 
 // ---------------------------------------------------------------------------
 // The simulation: one particle array for every type, as in the reference.
@@ -441,10 +480,11 @@ struct Sim : SimBase {
     return force;
   }
 
-  // UpdateLiquidParticlePosVelSphCPU (UnifiedPhysics.cpp:3705-3742)
+  // UpdateLiquidParticlePosVelSphCPU (UnifiedPhysics.cpp:3705-3742); granular
+  // grains take the same symplectic Euler step with their contact force
   void integrate(Particle<R>& p) {
-    if (p.type != UPF_LIQUID) return;
-    if (prm.method == UPF_METHOD_PCISPH) p.F = p.F + p.Fp;
+    if (p.type != UPF_LIQUID && p.type != UPF_GRANULAR) return;
+    if (prm.method == UPF_METHOD_PCISPH && p.type == UPF_LIQUID) p.F = p.F + p.Fp;
     const R invMass = R(1.0 / prm.mass);
     const R dt = R(prm.dt);
     p.v = p.v + p.F * invMass * dt;
@@ -564,8 +604,10 @@ struct Sim : SimBase {
             R spline = R(tab.lut[L_ST][dl]);
             p.F = p.F - (p.x - q.x) * R(prm.surface_tension_gamma) * m * m * spline * (R(1.0f) / d);
           }
-        } else if (q.type == UPF_FROZEN || q.type == UPF_RIGID) {
-          // the liquid particle's own weighted volume, as UnifiedPhysics.cpp:5292 passes
+        } else if (q.type == UPF_FROZEN || q.type == UPF_RIGID || q.type == UPF_GRANULAR) {
+          // boundary-like neighbours (granular grains are treated as the
+          // reference treats rigid particles); the liquid particle's own
+          // weighted volume, as UnifiedPhysics.cpp:5292 passes
           if (prm.flags & UPF_FLAG_BOUNDARY_PRESSURE)
             p.F = p.F + boundary_pressure(d, p.x, q.x, p.rho_prev, p.p_prev, p.wvol);
           if ((prm.flags & UPF_FLAG_ADHESION) && d >= h * R(0.25f)) {
@@ -577,6 +619,219 @@ struct Sim : SimBase {
       }
       p.F.y -= m * R(prm.gravity);
       if (prm.flags & UPF_FLAG_PENALTY_WALLS) p.F = p.F + penalty_walls(p.x);
+    } else {
+      // predicted position of a non-liquid particle: its current position
+      // (the reference's integration leaves there the position a moving
+      // particle was advanced to, UnifiedPhysics.cpp:5781-5792)
+      p.xs = p.x;
+      if (p.type == UPF_RIGID) rigid_external(i);
+      else if (p.type == UPF_GRANULAR) granular_external(i);
+    }
+  }
+
+  // CalculateBoundaryForcePerRigidParticleHost (UnifiedPhysics.cpp:2071-2131)
+  V3<R> rigid_box_force(V3<R> x, V3<R> v) const {
+    V3<R> f = {0, 0, 0};
+    bool hit = false;
+    const R r = R(prm.particle_radius), ks = R(prm.spring_coefficient_boundary), kd = R(prm.damping_coefficient);
+    const R* xv = &x.x;
+    R* fv = &f.x;
+    for (int a = 0; a < 3; ++a) {
+      const R mn = R(prm.collision_min[a]), mx = R(prm.collision_max[a]);
+      if (xv[a] - r < mn) {
+        hit = true;
+        fv[a] += (mn + r - xv[a]) * ks;
+      }
+      if (xv[a] + r > mx) {
+        hit = true;
+        fv[a] += (R(-1.0f) * (xv[a] + r - mx)) * ks;
+      }
+    }
+    if (hit) {
+      f.x -= kd * v.x;
+      f.y -= kd * v.y;
+      f.z -= kd * v.z;
+    }
+    return f;
+  }
+
+  // Rigid branch of CalculateExternalForcesVersatilCouplingPCISPH
+  // (UnifiedPhysics.cpp:5300-5326, 5344-5348). Deviations: spring-damper
+  // contacts only between different bodies, as the reference's comment
+  // intends (UnifiedPhysics.cpp:5307); the reaction of the boundary pressure
+  // uses the liquid particle's lagged values, so the pair force is exactly
+  // antisymmetric (the reference reads a value that other threads reset
+  // concurrently).
+  void rigid_external(int i) {
+    Particle<R>& p = ps[i];
+    const R m = R(prm.mass), h = R(prm.support_radius), rho0 = R(prm.rest_density);
+    p.F = {0, 0, 0};
+    for (int j : nbr[i]) {
+      const Particle<R>& q = ps[j];
+      R d = dist(p.x, q.x);
+      if (!(d < h)) continue;
+      unsigned dl = dist_lut(d);
+      if (q.type == UPF_RIGID) {
+        if (q.body == p.body) continue;
+        const R overlap = R(2.0f) * R(prm.particle_radius) - d;
+        if (overlap > R(0.00001f)) {
+          // CalculateSpringForceHost / CalculateDampingForceHost (UnifiedPhysics.cpp:2010-2030)
+          const V3<R> rij = q.x - p.x;
+          const R ks = R(prm.spring_coefficient), kd = R(prm.damping_coefficient);
+          const V3<R> spring = {R(-1.0f) * ks * overlap * rij.x / d, R(-1.0f) * ks * overlap * rij.y / d,
+                                R(-1.0f) * ks * overlap * rij.z / d};
+          const V3<R> vij = q.v - p.v;
+          const V3<R> damp = {kd * vij.x, kd * vij.y, kd * vij.z};
+          p.F = p.F + (spring + damp);
+        }
+      } else if (q.type == UPF_LIQUID) {
+        if (prm.flags & UPF_FLAG_BOUNDARY_PRESSURE)
+          p.F = p.F - boundary_pressure(d, q.x, p.x, q.rho_prev, q.p_prev, q.wvol);
+        if ((prm.flags & UPF_FLAG_ADHESION) && d >= h * R(0.25f)) {
+          R spline = R(tab.lut[L_ADH][dl]);
+          p.F = p.F + (q.x - p.x) * R(prm.surface_adhesion_beta) * m * rho0 * q.wvol * spline * (R(1.0f) / d);
+        }
+      }
+    }
+    p.F = p.F + rigid_box_force(p.x, p.v);
+  }
+
+  // Granular grains: the contact model of CalculateForcesWithContactForces
+  // (UnifiedPhysics.cpp:3219-3338, Bell et al. 2005) against grains, rigid and
+  // boundary particles closer than collisionDistThreshold = 2 r. Deviations:
+  // the normal force is applied (the reference adds only the tangential one,
+  // UnifiedPhysics.cpp:3287) and the friction bound uses |f_n| so friction
+  // opposes slip. Liquid neighbours act on grains as on rigid particles;
+  // gravity and the rigid box penalty act as on rigid particles.
+  void granular_external(int i) {
+    Particle<R>& p = ps[i];
+    const R m = R(prm.mass), h = R(prm.support_radius), rho0 = R(prm.rest_density);
+    const R dc = R(2.0f) * R(prm.particle_radius);
+    p.F = {0, 0, 0};
+    for (int j : nbr[i]) {
+      const Particle<R>& q = ps[j];
+      R d = dist(p.x, q.x);
+      if (!(d < h)) continue;
+      unsigned dl = dist_lut(d);
+      if ((q.type == UPF_GRANULAR || q.type == UPF_RIGID || q.type == UPF_FROZEN) && d < dc) {
+        const R ksi = std::max(dc - d, R(0.0f));
+        V3<R> N = (p.x - q.x) * R(-1.0f);
+        normalize(N);
+        const V3<R> V = p.v - q.v;
+        const R ksiDot = dot(V, N);
+        V3<R> Vt = V - N * ksiDot;
+        const R fn = -R(prm.granular_kd) * ksiDot - R(prm.granular_kr) * ksi;
+        const V3<R> Fn = N * fn;
+        const R vtl = normalize(Vt);
+        const R t = std::min(R(prm.granular_mu) * std::fabs(fn), R(prm.granular_kt) * vtl);
+        const V3<R> Ft = Vt * (-t);
+        p.F = p.F + (Fn + Ft);
+      } else if (q.type == UPF_LIQUID) {
+        if (prm.flags & UPF_FLAG_BOUNDARY_PRESSURE)
+          p.F = p.F - boundary_pressure(d, q.x, p.x, q.rho_prev, q.p_prev, q.wvol);
+        if ((prm.flags & UPF_FLAG_ADHESION) && d >= h * R(0.25f)) {
+          R spline = R(tab.lut[L_ADH][dl]);
+          p.F = p.F + (q.x - p.x) * R(prm.surface_adhesion_beta) * m * rho0 * q.wvol * spline * (R(1.0f) / d);
+        }
+      }
+    }
+    p.F.y -= m * R(prm.gravity);
+    p.F = p.F + rigid_box_force(p.x, p.v);
+  }
+
+  // RigidBodyIntegrationOMP -> CalculateRigidBodyForceTorqueMomenta
+  // (UnifiedPhysics.cpp:3620-3703) with RigidBody::UpdateMomenta, PerformStep,
+  // UpdateRotationMatrix (RigidBody.cpp:15-161). Force and torque are summed
+  // in FP64 (particles in array order, gravity after each particle's force);
+  // the body update is float as in the reference. The quaternion is not
+  // renormalised (RigidBody.cpp:99 discards getNormalized()'s result).
+  void rigid_step() {
+    const int nb = (int)bodies.size();
+    if (!nb) return;
+    std::vector<double> F(3 * nb, 0.0), T(3 * nb, 0.0);
+    for (const Particle<R>& p : ps) {
+      if (p.type != UPF_RIGID || p.body < 0) continue;
+      const Body<R>& b = bodies[p.body];
+      double* f = &F[3 * p.body];
+      double* t = &T[3 * p.body];
+      const double fx = p.F.x, fy = p.F.y, fz = p.F.z;
+      const double rx = (double)p.x.x - (double)b.pos.x, ry = (double)p.x.y - (double)b.pos.y,
+                   rz = (double)p.x.z - (double)b.pos.z;
+      f[0] += fx;
+      f[1] += fy;
+      f[2] += fz;
+      t[0] += ry * fz - rz * fy;
+      t[1] += rz * fx - rx * fz;
+      t[2] += rx * fy - ry * fx;
+      f[1] += (double)(-R(prm.mass) * R(prm.gravity));
+    }
+    const R dt = R(prm.dt);
+    for (int k = 0; k < nb; ++k) {
+      Body<R>& b = bodies[k];
+      const V3<R> force = {R(F[3 * k]), R(F[3 * k + 1]), R(F[3 * k + 2])};
+      const V3<R> torque = {R(T[3 * k]), R(T[3 * k + 1]), R(T[3 * k + 2])};
+      const R terminal = b.mass * R(prm.terminal_speed);
+      // UpdateMomenta (RigidBody.cpp:147-161)
+      b.P = b.P + force * dt;
+      R* P = &b.P.x;
+      for (int a = 0; a < 3; ++a) {
+        if (P[a] > R(0.0f))
+          P[a] = std::min(P[a], terminal);
+        else
+          P[a] = std::max(P[a], -terminal);
+      }
+      b.L = b.L + torque * dt;
+      // PerformStep: UpdateInverseInertiaTensor, PerformLinearStep, PerformAngularStep
+      R rt[3][3], tmp[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) rt[j][i] = b.rot[i][j];
+      mat_mul(b.rot, b.inv_inertia_local, tmp);
+      mat_mul(tmp, rt, b.inv_inertia_world);
+      b.vel = divs(b.P, b.mass);
+      b.pos = b.pos + b.vel * dt;
+      b.omega = mat_vec(b.inv_inertia_world, b.L);
+      const R speed = vsqrt(lensq(b.omega));
+      if (speed > R(0.0f)) {
+        V3<R> axis = b.omega;
+        normalize(axis);
+        const R angle = speed * dt;
+        const R ds = fcos(angle / R(2.0f));
+        const R dvx = axis.x * fsin(angle / R(2.0f));
+        const R dvy = axis.y * fsin(angle / R(2.0f));
+        const R dvz = axis.z * fsin(angle / R(2.0f));
+        const R s = b.q[0], vx = b.q[1], vy = b.q[2], vz = b.q[3];
+        b.q[0] = s * ds - vx * dvx - vy * dvy - vz * dvz;
+        b.q[1] = ds * vx + s * dvx + dvy * vz - dvz * vy;
+        b.q[2] = ds * vy + s * dvy + dvz * vx - dvx * vz;
+        b.q[3] = ds * vz + s * dvz + dvx * vy - dvy * vx;
+      }
+      // UpdateRotationMatrix (RigidBody.cpp:96-128)
+      const R w = b.q[0], x = b.q[1], y = b.q[2], z = b.q[3];
+      const R xx = x * x, yy = y * y, zz = z * z, xy = x * y, xz = x * z, yz = y * z, wx = w * x, wy = w * y,
+              wz = w * z;
+      b.rot[0][0] = R(1.0f) - R(2.0f) * (yy + zz);
+      b.rot[0][1] = R(2.0f) * (xy - wz);
+      b.rot[0][2] = R(2.0f) * (xz + wy);
+      b.rot[1][0] = R(2.0f) * (xy + wz);
+      b.rot[1][1] = R(1.0f) - R(2.0f) * (xx + zz);
+      b.rot[1][2] = R(2.0f) * (yz - wx);
+      b.rot[2][0] = R(2.0f) * (xz - wy);
+      b.rot[2][1] = R(2.0f) * (yz + wx);
+      b.rot[2][2] = R(1.0f) - R(2.0f) * (xx + yy);
+    }
+  }
+
+  // SynRigidParticlesPerRigidBody, new method (UnifiedPhysics.cpp:3766-3782)
+  void rigid_sync() {
+    if (bodies.empty()) return;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 100)
+    for (int i = 0; i < (int)ps.size(); i++) {
+      Particle<R>& p = ps[i];
+      if (p.type != UPF_RIGID || p.body < 0) continue;
+      const Body<R>& b = bodies[p.body];
+      const V3<R> rel = mat_vec(b.rot, p.r0);
+      p.v = b.vel + cross(b.omega, rel);
+      p.x = b.pos + rel;
     }
   }
 
@@ -676,9 +931,15 @@ struct Sim : SimBase {
 #pragma omp parallel for num_threads(threads) schedule(dynamic, 100)
     for (int i = 0; i < n; i++) {
       Particle<R>& p = ps[i];
-      if (p.type == UPF_LIQUID) clamp_box(p.x, p.v, damping);
-      p.key = key_of(p.x);
+      if (p.type == UPF_LIQUID || p.type == UPF_GRANULAR) clamp_box(p.x, p.v, damping);
     }
+    // RigidBodyIntegrationOMP + SynRigidParticlesOMP (UnifiedPhysics.cpp:5011-5023).
+    // Keys are taken after the rigid particles move (the reference keys them
+    // before, so its next neighbour search uses stale rigid keys).
+    rigid_step();
+    rigid_sync();
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 100)
+    for (int i = 0; i < n; i++) ps[i].key = key_of(ps[i].x);
     finish_step_stats(info);
     sort_particles();
     if (info) {
@@ -740,8 +1001,97 @@ struct Sim : SimBase {
   }
 
   void set_keep_fields(bool on) override { keep_fields = on; }
-  int set_bodies(const int32_t*, uint32_t, uint32_t) override { return -1; }
-  int get_rigid(float*, float*, float*, float*) const override { return -1; }
+  // Rigid body assembly (AddToRigidBody UnifiedPhysics.cpp:825-885, inverse
+  // Matrix3x3::CalculateInverse Matrix3x3.cpp:121-156, relative positions
+  // UnifiedPhysics.cpp:150-158): mass, centre of mass, momenta and inertia are
+  // summed in FP64 over the body's particles in input order and the inertia
+  // is inverted in FP64 (the reference sums incrementally in float and its
+  // ComputeLocalInertiaTensorRigidBody indexes particles_[i] for indices[i]).
+  int set_bodies(const int32_t* bop, uint32_t n, uint32_t nb) override {
+    if (n != ps.size()) return -1;
+    std::vector<int> where(n);
+    for (size_t k = 0; k < ps.size(); ++k) where[ps[k].id] = (int)k;
+    const double m = prm.mass;
+    std::vector<double> M(nb, 0.0), C(3 * nb, 0.0), Pm(3 * nb, 0.0), I(9 * nb, 0.0), L(3 * nb, 0.0);
+    for (uint32_t id = 0; id < n; ++id) {
+      const int b = bop[id];
+      if (b < 0) continue;
+      if (b >= (int)nb || ps[where[id]].type != UPF_RIGID) return -2;
+      const Particle<R>& p = ps[where[id]];
+      M[b] += m;
+      C[3 * b] += m * (double)p.x.x;
+      C[3 * b + 1] += m * (double)p.x.y;
+      C[3 * b + 2] += m * (double)p.x.z;
+      Pm[3 * b] += m * (double)p.v.x;
+      Pm[3 * b + 1] += m * (double)p.v.y;
+      Pm[3 * b + 2] += m * (double)p.v.z;
+    }
+    for (uint32_t b = 0; b < nb; ++b)
+      if (M[b] > 0)
+        for (int a = 0; a < 3; ++a) C[3 * b + a] /= M[b];
+    for (uint32_t id = 0; id < n; ++id) {
+      const int b = bop[id];
+      if (b < 0) continue;
+      const Particle<R>& p = ps[where[id]];
+      const double r[3] = {(double)p.x.x - C[3 * b], (double)p.x.y - C[3 * b + 1], (double)p.x.z - C[3 * b + 2]};
+      const double v[3] = {m * (double)p.v.x, m * (double)p.v.y, m * (double)p.v.z};
+      const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) I[9 * b + 3 * i + j] += m * ((i == j ? rr : 0.0) - r[i] * r[j]);
+      L[3 * b] += r[1] * v[2] - r[2] * v[1];
+      L[3 * b + 1] += r[2] * v[0] - r[0] * v[2];
+      L[3 * b + 2] += r[0] * v[1] - r[1] * v[0];
+    }
+    bodies.assign(nb, Body<R>());
+    for (uint32_t b = 0; b < nb; ++b) {
+      Body<R>& B = bodies[b];
+      std::memset(&B, 0, sizeof(B));
+      const double* A = &I[9 * b];
+      double inv[9] = {0};
+      const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                         A[2] * (A[3] * A[7] - A[4] * A[6]);
+      if (det != 0.0) {
+        inv[0] = (A[4] * A[8] - A[5] * A[7]) / det;
+        inv[1] = (A[2] * A[7] - A[1] * A[8]) / det;
+        inv[2] = (A[1] * A[5] - A[2] * A[4]) / det;
+        inv[3] = (A[5] * A[6] - A[3] * A[8]) / det;
+        inv[4] = (A[0] * A[8] - A[2] * A[6]) / det;
+        inv[5] = (A[2] * A[3] - A[0] * A[5]) / det;
+        inv[6] = (A[3] * A[7] - A[4] * A[6]) / det;
+        inv[7] = (A[1] * A[6] - A[0] * A[7]) / det;
+        inv[8] = (A[0] * A[4] - A[1] * A[3]) / det;
+      }
+      B.mass = R(M[b]);
+      B.pos = {R(C[3 * b]), R(C[3 * b + 1]), R(C[3 * b + 2])};
+      B.P = {R(Pm[3 * b]), R(Pm[3 * b + 1]), R(Pm[3 * b + 2])};
+      B.vel = M[b] > 0 ? V3<R>{R(Pm[3 * b] / M[b]), R(Pm[3 * b + 1] / M[b]), R(Pm[3 * b + 2] / M[b])}
+                       : V3<R>{0, 0, 0};
+      B.L = {R(L[3 * b]), R(L[3 * b + 1]), R(L[3 * b + 2])};
+      B.q[0] = 1;
+      for (int i = 0; i < 3; ++i) {
+        B.rot[i][i] = 1;
+        for (int j = 0; j < 3; ++j) B.inv_inertia_local[i][j] = R(inv[3 * i + j]);
+      }
+    }
+    for (uint32_t id = 0; id < n; ++id) {
+      const int b = bop[id];
+      Particle<R>& p = ps[where[id]];
+      p.body = b;
+      if (b >= 0) p.r0 = p.x - bodies[b].pos;
+    }
+    return 0;
+  }
+
+  int get_rigid(float* pos3, float* vel3, float* omega3, float* quat4) const override {
+    for (size_t b = 0; b < bodies.size(); ++b) {
+      const Body<R>& B = bodies[b];
+      if (pos3) { pos3[3 * b] = float(B.pos.x); pos3[3 * b + 1] = float(B.pos.y); pos3[3 * b + 2] = float(B.pos.z); }
+      if (vel3) { vel3[3 * b] = float(B.vel.x); vel3[3 * b + 1] = float(B.vel.y); vel3[3 * b + 2] = float(B.vel.z); }
+      if (omega3) { omega3[3 * b] = float(B.omega.x); omega3[3 * b + 1] = float(B.omega.y); omega3[3 * b + 2] = float(B.omega.z); }
+      if (quat4) for (int k = 0; k < 4; ++k) quat4[4 * b + k] = float(B.q[k]);
+    }
+    return (int)bodies.size();
+  }
 };
 
 // FP32 restatement of ComputeDensityErrorFactor (UnifiedPhysics.cpp:5525-5689)

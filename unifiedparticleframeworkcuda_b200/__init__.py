@@ -68,6 +68,7 @@ def lib():
             "upf_get_neighbors": [vp, u32p, u32p, C.c_uint32, u32p],
             "upf_get_sorted_keys": [vp, u32p, u32p, u32p],
             "upf_get_cell_ranges": [vp, u32p, u32p, u32p],
+            "upf_get_rigid_bodies": [vp, fp, fp, fp, fp, u32p],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
             "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
             "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],
@@ -178,6 +179,31 @@ class ParticleSystem:
         check(lib().upf_set_particles(self._h, _p(pos4, C.c_float), _p(vel4, C.c_float), _p(types, C.c_int32), n),
               "upf_set_particles")
         self.n_dynamic = int(np.count_nonzero(types != FROZEN))
+        self.n_input = n
+        self.n_bodies = 0
+
+    def set_rigid_bodies(self, body_of_particle, n_bodies: int | None = None):
+        """Group RIGID particles into bodies (body index per particle of the
+        last set_particles call, -1 for none); PCISPH only, before the first
+        step."""
+        b = np.ascontiguousarray(body_of_particle, np.int32)
+        if b.shape != (self.n_input,):
+            raise ValueError("need one body index per uploaded particle")
+        nb = int(b.max()) + 1 if n_bodies is None and b.size else int(n_bodies or 0)
+        check(lib().upf_set_rigid_bodies(self._h, _p(b, C.c_int32), b.shape[0], nb), "upf_set_rigid_bodies")
+        self.n_bodies = nb
+
+    def rigid_bodies(self):
+        """(pos (nb,3), vel (nb,3), omega (nb,3), quat (nb,4) as (s,x,y,z))."""
+        nb = self.n_bodies
+        pos = np.zeros((nb, 3), np.float32)
+        vel = np.zeros((nb, 3), np.float32)
+        om = np.zeros((nb, 3), np.float32)
+        q = np.zeros((nb, 4), np.float32)
+        cnt = C.c_uint32()
+        check(lib().upf_get_rigid_bodies(self._h, _p(pos, C.c_float), _p(vel, C.c_float), _p(om, C.c_float),
+                                         _p(q, C.c_float), C.byref(cnt)), "upf_get_rigid_bodies")
+        return pos, vel, om, q
 
     # stepping
     def step(self, nsteps: int = 1):

@@ -260,6 +260,20 @@ upf_status check_device_errors(System& s) {
   return UPF_OK;
 }
 
+void free_list(std::vector<void*>& v) {
+  for (void* p : v)
+    if (p) cudaFree(p);
+  v.clear();
+}
+
+// checkpoints hold the state layout of the configuration they were taken in
+void drop_checkpoints(System& s) { free_list(s.checkpoint_slots); }
+
+void clear_rigid(System& s) {
+  free_list(s.rigid_allocations);
+  s.rb = RigidArrays{};
+}
+
 __global__ void k_init_dyn(uint32_t n, DynArrays A, float rho0) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -451,6 +465,8 @@ upf_status upf_destroy(upf_system* s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   destroy_graph(*s);
   for (void* p : s->allocations) cudaFree(p);
+  free_list(s->rigid_allocations);
+  free_list(s->checkpoint_slots);
   if (s->st_host) cudaFreeHost(s->st_host);
   if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -503,8 +519,10 @@ upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4
       set_error("upf_set_particles: particle %u has unknown type %d", i, t);
       return UPF_ERR_INVALID_ARG;
     }
-    if (t != UPF_LIQUID && t != UPF_FROZEN && t != UPF_RIGID) {
-      set_error("upf_set_particles: particle %u has type %d; supported: LIQUID, RIGID, FROZEN", i, t);
+    const bool granular_ok = s->prm.method == UPF_METHOD_PCISPH;
+    if (t != UPF_LIQUID && t != UPF_FROZEN && t != UPF_RIGID && !(t == UPF_GRANULAR && granular_ok)) {
+      set_error("upf_set_particles: particle %u has type %d; supported: LIQUID, RIGID, FROZEN%s", i, t,
+                granular_ok ? ", GRANULAR" : " (GRANULAR needs PCISPH)");
       return UPF_ERR_UNSUPPORTED;
     }
     float4 x = make_float4(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2], 0.0f);
@@ -520,6 +538,16 @@ upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4
   }
   System& S = *s;
   cudaStream_t st = S.stream;
+  UPF_CUDA(cudaStreamSynchronize(st));
+  drop_checkpoints(S);
+  clear_rigid(S);
+  S.host_pos.resize(n);
+  S.host_vel.resize(n);
+  S.host_type.assign(type, type + n);
+  for (uint32_t i = 0; i < n; ++i) {
+    S.host_pos[i] = make_float4(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2], 0.0f);
+    S.host_vel[i] = make_float4(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2], 0.0f);
+  }
   S.n_dyn = (uint32_t)dpos.size();
   S.n_static = (uint32_t)spos.size();
   if (S.n_dyn) {
@@ -562,16 +590,187 @@ upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4
   UPF_CUDA(cudaMemsetAsync(S.st, 0, sizeof(DevState), st));
   UPF_CUDA(cudaStreamSynchronize(st));
   S.have_particles = true;
+  S.stepped = false;
   return build_step_graph(S);
 }
 
-upf_status upf_set_rigid_bodies(upf_system* s, const int32_t*, uint32_t, uint32_t) {
+upf_status upf_set_rigid_bodies(upf_system* s, const int32_t* body_of_particle, uint32_t n, uint32_t n_bodies) {
   if (!s) {
     set_error("upf_set_rigid_bodies: null");
     return UPF_ERR_INVALID_ARG;
   }
-  set_error("upf_set_rigid_bodies: rigid bodies are not available in this build");
-  return UPF_ERR_UNSUPPORTED;
+  System& S = *s;
+  if (!S.have_particles || S.stepped) {
+    set_error("upf_set_rigid_bodies: call it after upf_set_particles and before the first step");
+    return UPF_ERR_STATE;
+  }
+  if (S.prm.method != UPF_METHOD_PCISPH) {
+    set_error("upf_set_rigid_bodies: rigid bodies are coupled by the PCISPH solver only");
+    return UPF_ERR_UNSUPPORTED;
+  }
+  if (n != S.host_type.size() || (n && !body_of_particle) || n_bodies > (1u << 20)) {
+    set_error("upf_set_rigid_bodies: need one body index per particle of the last upload (%zu), at most 2^20 bodies",
+              S.host_type.size());
+    return UPF_ERR_INVALID_ARG;
+  }
+  const int32_t* bop = body_of_particle;
+  // AddToRigidBody (UnifiedPhysics.cpp:825-885): mass, centre of mass and
+  // momentum, then inertia and angular momentum about the centre, summed in
+  // FP64 in input order; the inertia is inverted in FP64 by the adjugate
+  // (Matrix3x3::CalculateInverse, Matrix3x3.cpp:121-156).
+  const double m = S.prm.mass;
+  std::vector<double> M(n_bodies, 0.0), C(3 * n_bodies, 0.0), Pm(3 * n_bodies, 0.0), I(9 * n_bodies, 0.0),
+      L(3 * n_bodies, 0.0);
+  std::vector<uint32_t> start(n_bodies + 1, 0);
+  for (uint32_t id = 0; id < n; ++id) {
+    const int32_t b = bop[id];
+    if (b < 0) continue;
+    if (b >= (int32_t)n_bodies || S.host_type[id] != UPF_RIGID) {
+      set_error("upf_set_rigid_bodies: particle %u: body %d is out of range or the particle is not RIGID", id, b);
+      return UPF_ERR_INVALID_ARG;
+    }
+    const float4 x = S.host_pos[id], v = S.host_vel[id];
+    M[b] += m;
+    C[3 * b] += m * (double)x.x;
+    C[3 * b + 1] += m * (double)x.y;
+    C[3 * b + 2] += m * (double)x.z;
+    Pm[3 * b] += m * (double)v.x;
+    Pm[3 * b + 1] += m * (double)v.y;
+    Pm[3 * b + 2] += m * (double)v.z;
+    start[b + 1] += 1;
+  }
+  for (uint32_t b = 0; b < n_bodies; ++b) {
+    if (!(M[b] > 0)) {
+      set_error("upf_set_rigid_bodies: body %u has no particles", b);
+      return UPF_ERR_INVALID_ARG;
+    }
+    for (int a = 0; a < 3; ++a) C[3 * b + a] /= M[b];
+  }
+  for (uint32_t id = 0; id < n; ++id) {
+    const int32_t b = bop[id];
+    if (b < 0) continue;
+    const float4 x = S.host_pos[id], v4 = S.host_vel[id];
+    const double r[3] = {(double)x.x - C[3 * b], (double)x.y - C[3 * b + 1], (double)x.z - C[3 * b + 2]};
+    const double v[3] = {m * (double)v4.x, m * (double)v4.y, m * (double)v4.z};
+    const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) I[9 * b + 3 * i + j] += m * ((i == j ? rr : 0.0) - r[i] * r[j]);
+    L[3 * b] += r[1] * v[2] - r[2] * v[1];
+    L[3 * b + 1] += r[2] * v[0] - r[0] * v[2];
+    L[3 * b + 2] += r[0] * v[1] - r[1] * v[0];
+  }
+  std::vector<DevBody> bodies(n_bodies);
+  for (uint32_t b = 0; b < n_bodies; ++b) {
+    DevBody& B = bodies[b];
+    std::memset(&B, 0, sizeof(B));
+    const double* A = &I[9 * b];
+    double inv[9] = {0};
+    const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                       A[2] * (A[3] * A[7] - A[4] * A[6]);
+    if (det != 0.0) {
+      inv[0] = (A[4] * A[8] - A[5] * A[7]) / det;
+      inv[1] = (A[2] * A[7] - A[1] * A[8]) / det;
+      inv[2] = (A[1] * A[5] - A[2] * A[4]) / det;
+      inv[3] = (A[5] * A[6] - A[3] * A[8]) / det;
+      inv[4] = (A[0] * A[8] - A[2] * A[6]) / det;
+      inv[5] = (A[2] * A[3] - A[0] * A[5]) / det;
+      inv[6] = (A[3] * A[7] - A[4] * A[6]) / det;
+      inv[7] = (A[1] * A[6] - A[0] * A[7]) / det;
+      inv[8] = (A[0] * A[4] - A[1] * A[3]) / det;
+    }
+    B.mass = (float)M[b];
+    B.pos = make_float3((float)C[3 * b], (float)C[3 * b + 1], (float)C[3 * b + 2]);
+    B.P = make_float3((float)Pm[3 * b], (float)Pm[3 * b + 1], (float)Pm[3 * b + 2]);
+    B.vel = make_float3((float)(Pm[3 * b] / M[b]), (float)(Pm[3 * b + 1] / M[b]), (float)(Pm[3 * b + 2] / M[b]));
+    B.L = make_float3((float)L[3 * b], (float)L[3 * b + 1], (float)L[3 * b + 2]);
+    B.q[0] = 1.0f;
+    for (int i = 0; i < 3; ++i) {
+      B.rot[i][i] = 1.0f;
+      for (int j = 0; j < 3; ++j) B.iinv_local[i][j] = (float)inv[3 * i + j];
+    }
+  }
+  // the rigid list: bodies in index order, each body's particles in input order;
+  // relative positions x - (float)centre, in float as the reference stores them
+  for (uint32_t b = 0; b < n_bodies; ++b) start[b + 1] += start[b];
+  const uint32_t n_rigid = start[n_bodies];
+  std::vector<uint32_t> fill(start.begin(), start.end() - 1), id_entry(n, 0xffffffffu);
+  std::vector<int32_t> id_body(n, -1), entry_body(n_rigid);
+  std::vector<float4> entry_r0(n_rigid);
+  for (uint32_t id = 0; id < n; ++id) {
+    const int32_t b = bop[id];
+    if (b < 0) continue;
+    const uint32_t k = fill[b]++;
+    const float4 x = S.host_pos[id];
+    const float3 c = bodies[b].pos;
+    entry_r0[k] = make_float4(x.x - c.x, x.y - c.y, x.z - c.z, 0.0f);
+    entry_body[k] = b;
+    id_entry[id] = k;
+    id_body[id] = b;
+  }
+  UPF_CUDA(cudaSetDevice(S.device));
+  UPF_CUDA(cudaStreamSynchronize(S.stream));
+  drop_checkpoints(S);
+  clear_rigid(S);
+  if (n_bodies) {
+    RigidArrays r;
+    auto alloc = [&](auto** p, size_t count) -> upf_status {
+      cudaError_t e = cudaMalloc((void**)p, (count ? count : 1) * sizeof(**p));
+      if (e != cudaSuccess) {
+        *p = nullptr;
+        set_error("upf_set_rigid_bodies: cudaMalloc: %s", cudaGetErrorString(e));
+        return UPF_ERR_ALLOC;
+      }
+      S.rigid_allocations.push_back(*p);
+      return UPF_OK;
+    };
+    upf_status rc = UPF_OK;
+    if ((rc = alloc(&r.bodies, n_bodies)) != UPF_OK || (rc = alloc(&r.start, n_bodies + 1)) != UPF_OK ||
+        (rc = alloc(&r.id_body, n)) != UPF_OK || (rc = alloc(&r.id_entry, n)) != UPF_OK ||
+        (rc = alloc(&r.entry_r0, n_rigid)) != UPF_OK || (rc = alloc(&r.entry_body, n_rigid)) != UPF_OK ||
+        (rc = alloc(&r.entry_slot, n_rigid)) != UPF_OK) {
+      clear_rigid(S);
+      return rc;
+    }
+    r.n_bodies = n_bodies;
+    r.n_rigid = n_rigid;
+    r.n_ids = n;
+    cudaStream_t st = S.stream;
+    UPF_CUDA(cudaMemcpyAsync(r.bodies, bodies.data(), sizeof(DevBody) * n_bodies, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(r.start, start.data(), sizeof(uint32_t) * (n_bodies + 1), cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(r.id_body, id_body.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(r.id_entry, id_entry.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+    if (n_rigid) {
+      UPF_CUDA(cudaMemcpyAsync(r.entry_r0, entry_r0.data(), sizeof(float4) * n_rigid, cudaMemcpyHostToDevice, st));
+      UPF_CUDA(
+          cudaMemcpyAsync(r.entry_body, entry_body.data(), sizeof(int32_t) * n_rigid, cudaMemcpyHostToDevice, st));
+    }
+    UPF_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
+    S.rb = r;
+  }
+  return build_step_graph(S);
+}
+
+upf_status upf_get_rigid_bodies(upf_system* s, float* pos3, float* vel3, float* omega3, float* quat4,
+                                uint32_t* n_out) {
+  if (!s) {
+    set_error("upf_get_rigid_bodies: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  const uint32_t nb = s->rb.n_bodies;
+  if (n_out) *n_out = nb;
+  if (!nb) return UPF_OK;
+  std::vector<DevBody> h(nb);
+  UPF_CUDA(cudaMemcpyAsync(h.data(), s->rb.bodies, sizeof(DevBody) * nb, cudaMemcpyDeviceToHost, s->stream));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  for (uint32_t b = 0; b < nb; ++b) {
+    const DevBody& B = h[b];
+    if (pos3) { pos3[3 * b] = B.pos.x; pos3[3 * b + 1] = B.pos.y; pos3[3 * b + 2] = B.pos.z; }
+    if (vel3) { vel3[3 * b] = B.vel.x; vel3[3 * b + 1] = B.vel.y; vel3[3 * b + 2] = B.vel.z; }
+    if (omega3) { omega3[3 * b] = B.omega.x; omega3[3 * b + 1] = B.omega.y; omega3[3 * b + 2] = B.omega.z; }
+    if (quat4)
+      for (int k = 0; k < 4; ++k) quat4[4 * b + k] = B.q[k];
+  }
+  return UPF_OK;
 }
 
 upf_status upf_step(upf_system* s, int32_t nsteps) {
@@ -583,6 +782,7 @@ upf_status upf_step(upf_system* s, int32_t nsteps) {
     set_error("upf_step: call upf_set_particles first");
     return UPF_ERR_STATE;
   }
+  s->stepped = true;
   for (int32_t k = 0; k < nsteps; ++k) UPF_CUDA(cudaGraphLaunch(s->step_exec, s->stream));
   return UPF_OK;
 }
@@ -644,24 +844,28 @@ static upf_status phase_guard(upf_system* s) {
 
 upf_status upf_phase_sort(upf_system* s) {
   UPF_TRY(phase_guard(s));
+  s->stepped = true;
   UPF_CUDA(launch_sort_phase(*s, s->stream));
   return UPF_OK;
 }
 
 upf_status upf_phase_neighbors(upf_system* s) {
   UPF_TRY(phase_guard(s));
+  s->stepped = true;
   UPF_CUDA(launch_neighbor_phase(*s, s->stream));
   return UPF_OK;
 }
 
 upf_status upf_phase_forces(upf_system* s) {
   UPF_TRY(phase_guard(s));
+  s->stepped = true;
   UPF_CUDA(launch_force_phase(*s, s->stream));
   return UPF_OK;
 }
 
 upf_status upf_phase_predict_correct(upf_system* s) {
   UPF_TRY(phase_guard(s));
+  s->stepped = true;
   if (s->prm.method != UPF_METHOD_PCISPH) return UPF_OK;
   UPF_CUDA(launch_loop_init(*s, s->stream));
   // host-driven loop (the graph path runs the same body under a while-node)
@@ -679,6 +883,7 @@ upf_status upf_phase_predict_correct(upf_system* s) {
 
 upf_status upf_phase_integrate(upf_system* s) {
   UPF_TRY(phase_guard(s));
+  s->stepped = true;
   UPF_CUDA(launch_integrate_phase(*s, s->stream));
   return UPF_OK;
 }
@@ -712,7 +917,8 @@ int state_segments(System& s, StateSeg* seg) {
   seg[4] = {s.A.type, sizeof(int32_t) * n};
   seg[5] = {s.keysA, sizeof(uint32_t) * n};
   seg[6] = {s.st, sizeof(DevState)};
-  return 7;
+  seg[7] = {s.rb.bodies, sizeof(DevBody) * s.rb.n_bodies};
+  return 8;
 }
 size_t state_total(System& s) {
   StateSeg seg[8];
@@ -756,7 +962,6 @@ upf_status upf_checkpoint(upf_system* s, int32_t slot) {
       return UPF_ERR_ALLOC;
     }
     s->checkpoint_slots[slot] = p;
-    s->allocations.push_back(p);
   }
   return state_copy(*s, (char*)s->checkpoint_slots[slot], true, cudaMemcpyDeviceToDevice);
 }
@@ -799,6 +1004,7 @@ upf_status upf_state_load(upf_system* s, const void* host, size_t bytes) {
 
 upf_status upf_profile_step(upf_system* s, upf_phase_times* out) {
   UPF_TRY(phase_guard(s));
+  s->stepped = true;
   if (!out) {
     set_error("upf_profile_step: null");
     return UPF_ERR_INVALID_ARG;

@@ -61,6 +61,19 @@ struct DevParams {
   uint32_t static_base;    // neighbour index of boundary particle j is static_base + j
 };
 
+// One rigid body (RigidBody, src/cpu/RigidBody.h:105-134): float state as in
+// the reference; force and torque arrive from an FP64 reduction.
+struct DevBody {
+  float mass;
+  float3 pos, vel, P, L, omega;
+  float q[4];              // (s, x, y, z)
+  float rot[3][3];
+  float iinv_local[3][3];
+  float iinv_world[3][3];
+  double force[3];
+  double torque[3];
+};
+
 // Device-side scalars of one system.
 struct DevState {
   uint32_t max_rho_bits;   // running max predicted density (positive floats order as uints)

@@ -543,13 +543,150 @@ __device__ __forceinline__ void boundary_pressure(const DevParams& P, const floa
   fz = fz + kz * pgd * P.mass * P.rho0 * wvol * (-1.0f);
 }
 
-// CalculateExternalForcesVersatilCouplingPCISPH (UnifiedPhysics.cpp:5252-5365),
-// liquid particles; then the first prediction of the loop.
+// The reaction of boundary_pressure on the solid particle: the same vector as
+// the liquid particle receives, subtracted (the pair force is antisymmetric).
+__device__ __forceinline__ void boundary_pressure_reaction(const DevParams& P, const float* pg, float d,
+                                                           float4 xl, float4 xs_, float rho_prev, float p_prev,
+                                                           float wvol, float& fx, float& fy, float& fz) {
+  const float inv_den = 1.0f / rho_prev;
+  const float g = lut_at(pg, d, P.lut_factor);
+  const float kx = (xl.x - xs_.x) * g, ky = (xl.y - xs_.y) * g, kz = (xl.z - xs_.z) * g;
+  const float pgd = p_prev * inv_den * inv_den;
+  fx = fx - kx * pgd * P.mass * P.rho0 * wvol * (-1.0f);
+  fy = fy - ky * pgd * P.mass * P.rho0 * wvol * (-1.0f);
+  fz = fz - kz * pgd * P.mass * P.rho0 * wvol * (-1.0f);
+}
+
+// CalculateBoundaryForcePerRigidParticleHost (UnifiedPhysics.cpp:2071-2131):
+// spring against each box face the particle's sphere crosses, damping once if
+// any face is hit; added to the force as one vector.
+__device__ __forceinline__ void rigid_box_force(const DevParams& P, float4 x, float4 v, float& fx, float& fy,
+                                                float& fz) {
+  const float r = P.radius, ks = P.spring_boundary, kd = P.damping;
+  float f[3] = {0.0f, 0.0f, 0.0f};
+  const float xv[3] = {x.x, x.y, x.z};
+  const float mn[3] = {P.cmin.x, P.cmin.y, P.cmin.z}, mx[3] = {P.cmax.x, P.cmax.y, P.cmax.z};
+  bool hit = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (xv[a] - r < mn[a]) {
+      hit = true;
+      f[a] += (mn[a] + r - xv[a]) * ks;
+    }
+    if (xv[a] + r > mx[a]) {
+      hit = true;
+      f[a] += (-1.0f * (xv[a] + r - mx[a])) * ks;
+    }
+  }
+  if (hit) {
+    f[0] -= kd * v.x;
+    f[1] -= kd * v.y;
+    f[2] -= kd * v.z;
+  }
+  fx = fx + f[0];
+  fy = fy + f[1];
+  fz = fz + f[2];
+}
+
+// Vector3::normalize: scales v to unit length with a reciprocal taken in
+// double, returns the length (0 leaves v unchanged).
+__device__ __forceinline__ float normalize3(float& x, float& y, float& z) {
+  const float l = __fsqrt_rn(x * x + y * y + z * z);
+  if (l == 0.0f) return 0.0f;
+  const float ll = (float)(1.0 / (double)l);
+  x *= ll;
+  y *= ll;
+  z *= ll;
+  return l;
+}
+
+// External forces on a rigid or granular particle (rigid branch of
+// CalculateExternalForcesVersatilCouplingPCISPH, UnifiedPhysics.cpp:5300-5348;
+// granular contact of CalculateForcesWithContactForces, UnifiedPhysics.cpp:3219-3338).
+// Rigid: spring-damper against rigid particles of other bodies, the reaction
+// of the liquid's boundary pressure (and adhesion), the box penalty.
+// Granular: Bell et al. contact (normal spring-damper, Coulomb-bounded
+// tangential friction) against grains, rigid and boundary particles closer
+// than 2 r, the liquid reaction, gravity, the box penalty. Solid particles are
+// a minority, so the loop is plain (no batching) to keep registers for the
+// liquid path. `id_body` is null when no bodies are set.
+__device__ __forceinline__ float3 solid_external(const DevParams& P, uint32_t i, int32_t ti, float4 xi, float4 vi,
+                                              const DynArrays& B, const int32_t* __restrict__ id_body,
+                                              const uint32_t* __restrict__ nbr, uint32_t cnt, const float* pg,
+                                              const float* adl) {
+  const float m = P.mass, h = P.h, rv = P.rest_volume;
+  const float dc = 2.0f * P.radius;
+  const int32_t bi = (ti == UPF_RIGID && id_body) ? id_body[B.id[i]] : -1;
+  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t code = __ldg(nbr + (size_t)k * P.nstride + i);
+    const float4 xj = __ldg(B.pos + code);
+    const float d = dist3(xi, xj);
+    if (!(d < h)) continue;
+    const unsigned dl = dist_lut(d, h);
+    const int32_t tj = __ldg(B.type + code);
+    if (ti == UPF_RIGID) {
+      if (tj == UPF_RIGID) {
+        // dynamic rigid neighbours have code < stride, inside the id array
+        const int32_t bj = id_body ? id_body[B.id[code]] : -1;
+        if (bj == bi) continue;
+        // CalculateSpringForceHost / CalculateDampingForceHost (UnifiedPhysics.cpp:2010-2030)
+        const float overlap = 2.0f * P.radius - d;
+        if (overlap > 0.00001f) {
+          const float4 vj = __ldg(B.vel + code);
+          const float sx = -1.0f * P.spring * overlap * (xj.x - xi.x) / d;
+          const float sy = -1.0f * P.spring * overlap * (xj.y - xi.y) / d;
+          const float sz = -1.0f * P.spring * overlap * (xj.z - xi.z) / d;
+          fx = fx + (sx + P.damping * (vj.x - vi.x));
+          fy = fy + (sy + P.damping * (vj.y - vi.y));
+          fz = fz + (sz + P.damping * (vj.z - vi.z));
+        }
+        continue;
+      }
+    } else if ((tj == UPF_GRANULAR || tj == UPF_RIGID || tj == UPF_FROZEN) && d < dc) {
+      const float4 vj = __ldg(B.vel + code);
+      const float ksi = (dc - d < 0.0f) ? 0.0f : dc - d;
+      float nx = (xi.x - xj.x) * -1.0f, ny = (xi.y - xj.y) * -1.0f, nz = (xi.z - xj.z) * -1.0f;
+      normalize3(nx, ny, nz);
+      const float Vx = vi.x - vj.x, Vy = vi.y - vj.y, Vz = vi.z - vj.z;
+      const float ksi_dot = Vx * nx + Vy * ny + Vz * nz;
+      float tx = Vx - nx * ksi_dot, ty = Vy - ny * ksi_dot, tz = Vz - nz * ksi_dot;
+      const float fn = -P.gran_kd * ksi_dot - P.gran_kr * ksi;
+      const float vtl = normalize3(tx, ty, tz);
+      const float a = P.gran_mu * fabsf(fn), b = P.gran_kt * vtl;
+      const float t = (b < a) ? b : a;
+      fx = fx + (nx * fn + tx * (-t));
+      fy = fy + (ny * fn + ty * (-t));
+      fz = fz + (nz * fn + tz * (-t));
+      continue;
+    }
+    if (tj == UPF_LIQUID) {
+      // the liquid neighbour's lagged pressure and density, its rest volume
+      const float4 lj = __ldg(B.lag + code);
+      if (P.flags & UPF_FLAG_BOUNDARY_PRESSURE)
+        boundary_pressure_reaction(P, pg, d, xj, xi, lj.z, lj.x, rv, fx, fy, fz);
+      if ((P.flags & UPF_FLAG_ADHESION) && d >= h * 0.25f) {
+        const float sp = adl[dl];
+        const float inv = 1.0f / d;
+        fx = fx + (xj.x - xi.x) * P.adh_beta * m * P.rho0 * rv * sp * inv;
+        fy = fy + (xj.y - xi.y) * P.adh_beta * m * P.rho0 * rv * sp * inv;
+        fz = fz + (xj.z - xi.z) * P.adh_beta * m * P.rho0 * rv * sp * inv;
+      }
+    }
+  }
+  if (ti == UPF_GRANULAR) fy -= m * P.gravity;
+  rigid_box_force(P, xi, vi, fx, fy, fz);
+  return make_float3(fx, fy, fz);
+}
+
+// CalculateExternalForcesVersatilCouplingPCISPH (UnifiedPhysics.cpp:5252-5365):
+// liquid particles (then the first prediction of the loop), rigid and
+// granular particles (solid_external).
 __global__ void __launch_bounds__(kBlock) k_pcisph_external(
-    DevParams P, uint32_t n, DynArrays B, const float* __restrict__ wvol, const uint32_t* __restrict__ nbr,
-    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts, float4* __restrict__ force,
-    float4* __restrict__ pforce,
-    float4* __restrict__ xs, float* __restrict__ press, float* __restrict__ pq, DevState* __restrict__ st) {
+    DevParams P, uint32_t n, DynArrays B, const float* __restrict__ wvol, const int32_t* __restrict__ id_body,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    float4* __restrict__ force, float4* __restrict__ pforce, float4* __restrict__ xs, float* __restrict__ press,
+    float* __restrict__ pq, DevState* __restrict__ st) {
   __shared__ float vl[UPF_LUT_ENTRIES], pg[UPF_LUT_ENTRIES], stl[UPF_LUT_ENTRIES], adl[UPF_LUT_ENTRIES];
   stage_lut(vl, luts + LUT_VISC * UPF_LUT_ENTRIES);
   stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
@@ -564,8 +701,14 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
   pq[i] = 0.0f;
   pforce[i] = f4(0, 0, 0);
   if (ti != UPF_LIQUID) {
-    force[i] = f4(0, 0, 0);
+    // predicted position of a non-liquid particle: its current position
     xs[i] = xi;
+    if (ti == UPF_RIGID || ti == UPF_GRANULAR) {
+      const float3 F = solid_external(P, i, ti, xi, B.vel[i], B, id_body, nbr, ncnt[i], pg, adl);
+      force[i] = f4(F.x, F.y, F.z);
+    } else {
+      force[i] = f4(0, 0, 0);
+    }
     return;
   }
   const float4 vi = B.vel[i];
@@ -609,7 +752,8 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
         fy = fy - (xi.y - xj.y) * P.st_gamma * m * m * sp * inv;
         fz = fz - (xi.z - xj.z) * P.st_gamma * m * m * sp * inv;
       }
-    } else if (tj == UPF_FROZEN || tj == UPF_RIGID) {
+    } else if (tj == UPF_FROZEN || tj == UPF_RIGID || tj == UPF_GRANULAR) {
+      // granular grains count as boundary, as rigid particles do
       const float wv = wvol[code];
       // the reference passes the liquid particle's own weighted volume (its
       // rest volume) to the pressure term, UnifiedPhysics.cpp:5292
@@ -821,7 +965,16 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_integrate(
       integrate_store(P, i, xi, vi, make_float3(F.x + Fp.x, F.y + Fp.y, F.z + Fp.z), A, keysA, B, ke, mx, my,
                       mz);
       A.lag[i] = make_float4(lag.y, press[i], rho[i], 0.0f);
+    } else if (ti == UPF_GRANULAR) {
+      // integrated and clamped like liquid, without a pressure force; not
+      // part of the liquid statistics
+      const float4 F = force[i];
+      integrate_store(P, i, xi, vi, make_float3(F.x, F.y, F.z), A, keysA, B, ke, mx, my, mz);
+      if (ke == ke) ke = 0;
+      mx = my = mz = 0;
+      A.lag[i] = lag;
     } else {
+      // rigid particles are placed by the body sync that follows
       A.pos[i] = xi;
       A.vel[i] = vi;
       keysA[i] = morton_key(xi, P.origin, P.scales);
@@ -909,6 +1062,7 @@ cudaError_t launch_sort_phase(System& s, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   k_reorder<<<grid_of(n), kBlock, 0, st>>>(n, s.perm, s.A, s.B, s.prm.method == UPF_METHOD_PCISPH);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = launch_rigid_slots(s, st)) != cudaSuccess) return e;
   return cell_ranges(s.keysA, n, 3 * (int)s.dp.block_shift, s.ncells, s.cstart, s.cend, st);
 }
 
@@ -928,8 +1082,8 @@ cudaError_t launch_force_phase(System& s, cudaStream_t st) {
     k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.bins, s.ncnt, s.luts, s.rho,
                                                    s.press);
   } else {
-    k_pcisph_external<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.wvol, s.nbr, s.ncnt, s.luts, s.force,
-                                                     s.pforce, s.xs, s.press, s.pq, s.st);
+    k_pcisph_external<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.wvol, s.rb.id_body, s.nbr, s.ncnt, s.luts,
+                                                     s.force, s.pforce, s.xs, s.press, s.pq, s.st);
   }
   return cudaGetLastError();
 }
@@ -980,6 +1134,9 @@ cudaError_t launch_integrate_phase(System& s, cudaStream_t st) {
   } else {
     k_pcisph_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.force, s.pforce, s.rho, s.press,
                                                       s.st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_rigid_phase(s, st);
   }
   return cudaGetLastError();
 }
@@ -1000,10 +1157,10 @@ cudaError_t launch_static_setup(System& s, cudaStream_t st) {
 }
 
 int pipeline_launches_per_step(const System& s, int iterations) {
-  int sort = radix_launches(s.key_bits) + 1 /*reorder*/ + 1 /*cells*/;
+  int sort = radix_launches(s.key_bits) + 1 /*reorder*/ + 1 /*cells*/ + (s.rb.n_rigid ? 1 : 0) /*rigid slots*/;
   int nl = 2;  // step init + neighbour lists
   if (s.prm.method == UPF_METHOD_WCSPH) return sort + nl + 2;
-  return sort + nl + 1 /*external*/ + 1 /*loop init*/ + 3 * iterations + 1 /*integrate*/;
+  return sort + nl + 1 /*external*/ + 1 /*loop init*/ + 3 * iterations + 1 /*integrate*/ + rigid_launches_per_step(s);
 }
 
 }  // namespace upf

@@ -36,9 +36,19 @@ struct DynArrays {
   int32_t* type = nullptr;
 };
 
+// Rigid bodies. The rigid particles form a list grouped by body (body b owns
+// entries [start[b], start[b+1]), in input-id order); what is fixed per
+// particle is indexed by input id or by list entry, so nothing but the
+// entry -> sorted-index map changes when the particles are re-sorted.
 struct RigidArrays {
-  int32_t* body = nullptr;      // body index of each dynamic particle (-1: not rigid), A/B like the rest
-  float4* r0 = nullptr;         // initial relative position of rigid particles
+  uint32_t n_bodies = 0, n_rigid = 0, n_ids = 0;
+  DevBody* bodies = nullptr;
+  uint32_t* start = nullptr;    // [n_bodies + 1]
+  int32_t* id_body = nullptr;   // input id -> body index, -1 for particles of no body
+  uint32_t* id_entry = nullptr; // input id -> list entry, 0xffffffff for particles of no body
+  float4* entry_r0 = nullptr;   // list entry -> position relative to the centre of mass, body frame
+  int32_t* entry_body = nullptr;
+  uint32_t* entry_slot = nullptr; // list entry -> current sorted index (set after each sort)
 };
 
 struct System {
@@ -51,6 +61,7 @@ struct System {
 
   uint32_t n_dyn = 0, n_static = 0;
   bool have_particles = false;
+  bool stepped = false;          // a step or phase ran since the last upf_set_particles
 
   DynArrays A, B;
   uint32_t* keysA = nullptr;   // keys of A (sorted in place by the sort)
@@ -99,9 +110,22 @@ struct System {
   cudaGraph_t step_graph = nullptr;
   int key_bits = 30;
 
+  RigidArrays rb;
+  std::vector<void*> rigid_allocations;   // freed when bodies are set again
+  // host copy of the last upload (input order), for body assembly
+  std::vector<float4> host_pos, host_vel;
+  std::vector<int32_t> host_type;
+
   std::vector<void*> allocations;
-  std::vector<void*> checkpoint_slots;  // device copies of the dynamic state (upf_checkpoint)
+  std::vector<void*> checkpoint_slots;  // device copies of the dynamic state (upf_checkpoint);
+                                        // dropped when particles or bodies are set
 };
+
+// upf_rigid.cu: list entry -> sorted index after a sort; body force/torque,
+// body integration and rigid particle sync after integration
+cudaError_t launch_rigid_slots(System& s, cudaStream_t st);
+cudaError_t launch_rigid_phase(System& s, cudaStream_t st);
+int rigid_launches_per_step(const System& s);
 
 // upf_pipeline.cu: phase launchers (all asynchronous on s.stream)
 cudaError_t launch_sort_phase(System& s, cudaStream_t st);

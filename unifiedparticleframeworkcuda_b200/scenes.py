@@ -15,7 +15,7 @@ import dataclasses
 import numpy as np
 
 from ._abi import (FLAG_BOUNDARY_PRESSURE, FLAG_PENALTY_WALLS, FLAG_SURFACE_TENSION,
-                   FROZEN, LIQUID, METHOD_PCISPH, METHOD_WCSPH, UpfParams)
+                   FROZEN, GRANULAR, LIQUID, METHOD_PCISPH, METHOD_WCSPH, RIGID, UpfParams)
 
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 _M1 = np.uint64(0xBF58476D1CE4E5B9)
@@ -197,6 +197,129 @@ def pcisph_dam(nx=128, ny=128, nz=64, seed=4321, box=(2.0, 1.3, 1.3), layers=2,
     fluid = _lattice(nx, ny, nz, s, lo + s, 0.1 * s, seed)
     boundary = box_shell(lo, hi, s, layers)
     return _pack("pcisph_dam_%dx%dx%d" % (nx, ny, nz), p, fluid, boundary)
+
+
+def _random_rotation(u):
+    """Rotation matrix of a uniformly random unit quaternion (Shoemake) from
+    three uniforms."""
+    u1, u2, u3 = u
+    q = np.array([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)])
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+
+
+def sample_sphere(r, n):
+    """n points on a sphere of radius r (Fibonacci lattice)."""
+    k = np.arange(n) + 0.5
+    phi = np.arccos(1 - 2 * k / n)
+    theta = np.pi * (1 + 5 ** 0.5) * k
+    return r * np.stack([np.cos(theta) * np.sin(phi), np.sin(theta) * np.sin(phi), np.cos(phi)], axis=1)
+
+
+def sample_box(r, n):
+    """About n points on the surface of a cube of half-edge r (a k x k grid per face)."""
+    k = max(2, int(round(np.sqrt(n / 6.0))))
+    g = (np.arange(k) + 0.5) / k * 2 * r - r
+    a, b = np.meshgrid(g, g, indexing="ij")
+    a, b = a.ravel(), b.ravel()
+    faces = []
+    for axis in range(3):
+        for sgn in (-r, r):
+            p = np.zeros((a.size, 3))
+            p[:, axis] = sgn
+            p[:, (axis + 1) % 3] = a
+            p[:, (axis + 2) % 3] = b
+            faces.append(p)
+    return np.concatenate(faces)
+
+
+def sample_torus(r, n):
+    """About n points on a torus of major radius r and minor radius r/3."""
+    a = r / 3.0
+    nu = max(8, int(round(np.sqrt(n * r / a))))
+    nv = max(4, int(round(n / nu)))
+    u = (np.arange(nu) + 0.5) / nu * 2 * np.pi
+    v = (np.arange(nv) + 0.5) / nv * 2 * np.pi
+    uu, vv = np.meshgrid(u, v, indexing="ij")
+    uu, vv = uu.ravel(), vv.ravel()
+    return np.stack([(r + a * np.cos(vv)) * np.cos(uu), (r + a * np.cos(vv)) * np.sin(uu), a * np.sin(vv)], axis=1)
+
+
+def coupling_scene(fluid=(128, 64, 64), granular=(64, 32, 64), n_bodies=16, seed=99, box=(2.0, 1.3, 1.3),
+                   radius=(0.05, 0.15), samples=(2000, 8000), spacing=0.01, layers=2) -> Scene:
+    """Rigid-fluid coupling plus granular: a PCISPH fluid block at one end of
+    the container, a granular pile (friction 0.5) at the other, and
+    `n_bodies` rigid bodies (spheres, cubes and tori cycling) with radii
+    uniform in `radius`, surface-sampled with 2k-8k Akinci boundary particles
+    each (half the fluid spacing, clamped to `samples`), random orientations
+    and positions above the fluid and the pile."""
+    p = default_params()
+    p.method = METHOD_PCISPH
+    p.flags = FLAG_SURFACE_TENSION | FLAG_PENALTY_WALLS | FLAG_BOUNDARY_PRESSURE
+    s = spacing
+    p.particle_spacing = s
+    p.support_radius = 2.0 * s
+    p.dt = 5e-4
+    p.viscosity = 1.0
+    # grain contacts stiff enough to hold a pile at this dt (k omega dt < 1)
+    p.granular_kr = 200.0
+    p.granular_kd = 0.5
+    p.granular_kt = 10.0
+    p.granular_mu = 0.5
+    p.max_neighbors = 160
+    lo = np.array([2 * s, 2 * s, 2 * s])
+    hi = lo + np.asarray(box, np.float64)
+    _set_box(p, lo, hi)
+    ext = 1024.0 * (s / 5.0)
+    p.zindex_extent[:] = (ext, ext, ext)
+    fl = _lattice(*fluid, s, lo + s, 0.1 * s, seed)
+    gx = box[0] - (granular[0] + 1) * s
+    gr = _lattice(*granular, s, lo + np.array([gx, s, s]), 0.1 * s, seed, stream=1)
+    u = uniform(seed, 8 * n_bodies, stream=2).reshape(n_bodies, 8)
+    ds = 0.5 * s
+    bodies, body_ids = [], []
+    top = max(fluid[1], granular[1]) * s + lo[1]
+    cols = int(np.ceil(np.sqrt(n_bodies)))
+    for b in range(n_bodies):
+        r = radius[0] + (radius[1] - radius[0]) * u[b, 0]
+        shape = b % 3
+        area = (4 * np.pi * r * r, 24 * r * r, 4 * np.pi ** 2 * r * (r / 3.0))[shape]
+        n = int(np.clip(round(area / ds ** 2), samples[0], samples[1]))
+        pts = (sample_sphere, sample_box, sample_torus)[shape](r, n)
+        pts = pts @ _random_rotation(u[b, 1:4]).T
+        # slots on a grid above the fluid and the pile
+        cx = lo[0] + (b % cols + 0.5) / cols * box[0]
+        cz = lo[2] + ((b // cols) % cols + 0.5) / cols * box[2]
+        # between the top of the fluid/pile and the ceiling, clear of both
+        ylo, yhi = top + r + 2 * s, hi[1] - r - 3 * s
+        cy = ylo + (yhi - ylo) * (0.25 + 0.5 * u[b, 4]) if yhi > ylo else 0.5 * (ylo + yhi)
+        bodies.append(pts + np.array([cx, cy, cz]))
+        body_ids.append(np.full(pts.shape[0], b, np.int32))
+    rig = np.concatenate(bodies)
+    bid = np.concatenate(body_ids)
+    bnd = box_shell(lo, hi, s, layers)
+    pos = np.zeros((fl.shape[0] + gr.shape[0] + rig.shape[0] + bnd.shape[0], 4), np.float32)
+    parts = [fl, gr, rig, bnd]
+    types = [LIQUID, GRANULAR, RIGID, FROZEN]
+    typ, body = [], []
+    o = 0
+    for arr, t in zip(parts, types):
+        pos[o:o + arr.shape[0], :3] = arr
+        typ.append(np.full(arr.shape[0], t, np.int32))
+        body.append(bid if t == RIGID else np.full(arr.shape[0], -1, np.int32))
+        o += arr.shape[0]
+    vel = np.zeros_like(pos)
+    return Scene("coupling_%d" % fl.shape[0], p, pos, vel, np.concatenate(typ), np.concatenate(body), n_bodies)
+
+
+def small_coupling(seed=5) -> Scene:
+    """A small coupling scene (oracle-sized): 12^3 fluid, an 8x4x8 pile and
+    three small bodies."""
+    return coupling_scene(fluid=(12, 12, 12), granular=(8, 4, 8), n_bodies=3, seed=seed, box=(0.4, 0.35, 0.25),
+                          radius=(0.03, 0.05), samples=(150, 400))
 
 
 def small_pcisph(n_side=12, seed=7, layers=2, box=(0.3, 0.2, 0.2)) -> Scene:
