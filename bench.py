@@ -8,6 +8,12 @@ predict-correct iterations, dt = 5e-4, full Morton sort every step.
 Metric: fluid particle-steps per second.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--scene c2|c2-small|c1|c3]
+
+--scene c3 times the rigid-fluid coupling workload instead: 524,288 PCISPH
+fluid particles, a 131,072-grain granular pile (friction 0.5) and 16 rigid
+bodies (spheres, cubes, tori, radii 0.05-0.15, 2k-8k surface particles each);
+its metric counts every dynamic particle (fluid, grains, rigid).
 
 One JSON line on rank 0. Under torchrun (N > 1) every rank runs its own
 replica of the scene (the single-scene path does not shard: replicas only),
@@ -41,12 +47,33 @@ def scene_for(args):
         return scenes.pcisph_dam(64, 64, 64)
     if args.scene == "c1":
         return scenes.wcsph_dam(32)
+    if args.scene == "c3":
+        return scenes.coupling_scene()
     raise SystemExit("unknown scene " + args.scene)
+
+
+def cpu_sample_scene(args):
+    """The bounded CPU sample of a workload: same physics, fewer particles."""
+    from unifiedparticleframeworkcuda_b200 import scenes
+    if args.scene == "c3":
+        return scenes.coupling_scene(fluid=(64, 32, 32), granular=(32, 16, 32), n_bodies=4), \
+            "coupling 64x32x32 fluid + 32x16x32 grains + 4 bodies"
+    return scenes.pcisph_dam(64, 64, 64), "pcisph_dam 64^3"
 
 
 def workload_name(args):
     return {"c2": "pcisph_dam_break_1M", "c2-small": "pcisph_dam_break_262k",
-            "c1": "wcsph_dam_break_32k"}[args.scene]
+            "c1": "wcsph_dam_break_32k", "c3": "rigid_fluid_granular_coupling_524k"}[args.scene]
+
+
+def metric_for(args):
+    if args.scene == "c3":
+        return "particle-steps/s, rigid-fluid coupling + granular (524k fluid, 131k grains, 16 bodies)"
+    return METRIC
+
+
+def dynamic_count(sc):
+    return sc.n - sc.n_boundary
 
 
 def algorithmic_bytes(nf, nb, steps, total_iters, method):
@@ -108,19 +135,26 @@ class ClockSampler:
                 "samples": len(rows), "power_w_max": max(float(r[2]) for r in rows)}
 
 
-def cpu_baseline(sc_params_fn, seconds=15.0):
-    """The oracle (FP32 OpenMP restatement of the reference CPU path) on a
-    bounded sample of the same workload: a 64^3-fluid dam with the same
-    spacing, h, dt and boundary (fluid particle-steps/s do not depend on the
-    block's size beyond cache effects)."""
+def make_oracle(sc, threads):
     from oracle import pyoracle
-    from unifiedparticleframeworkcuda_b200 import scenes
     import unifiedparticleframeworkcuda_b200 as upf
-    pyoracle.build(with_ref=False)
-    sc = scenes.pcisph_dam(64, 64, 64)
     p = upf.derive_params(sc.params)
-    threads = os.cpu_count() or 1
     o = pyoracle.OracleSim(p, sc.pos, sc.vel, sc.type, threads=threads, keep_fields=False)
+    if sc.num_bodies:
+        o.set_rigid_bodies(sc.body, sc.num_bodies)
+    return o
+
+
+def cpu_baseline(args, seconds=15.0):
+    """The oracle (FP32 OpenMP restatement of the reference CPU path) on a
+    bounded sample of the same workload: the same spacing, h, dt and boundary
+    with fewer particles (particle-steps/s do not depend on the block's size
+    beyond cache effects)."""
+    from oracle import pyoracle
+    pyoracle.build(with_ref=False)
+    sc, label = cpu_sample_scene(args)
+    threads = os.cpu_count() or 1
+    o = make_oracle(sc, threads)
     o.step()  # warm-up
     t0 = time.perf_counter()
     steps = 0
@@ -133,10 +167,10 @@ def cpu_baseline(sc_params_fn, seconds=15.0):
             break
     dt = time.perf_counter() - t0
     o.close()
-    nf = sc.n_fluid
-    return {"value": nf * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "%d fluid + %d boundary particles (pcisph_dam 64^3), %d steps, mean %.1f iterations, %.1f s"
-                      % (nf, sc.n_boundary, steps, iters / steps, dt)}
+    nd = dynamic_count(sc)
+    return {"value": nd * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d dynamic + %d boundary particles (%s), %d steps, mean %.1f iterations, %.1f s"
+                      % (nd, sc.n_boundary, label, steps, iters / steps, dt)}
 
 
 def run_reference(args, rank, world):
@@ -145,14 +179,11 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     from oracle import pyoracle
-    import unifiedparticleframeworkcuda_b200 as upf
-    from unifiedparticleframeworkcuda_b200 import scenes
     pyoracle.build(with_ref=False)
-    # bounded sample per step: a 64^3-fluid slab of the workload
-    sc = scenes.pcisph_dam(64, 64, 64)
-    p = upf.derive_params(sc.params)
+    # bounded sample per step: a smaller block of the workload
+    sc, label = cpu_sample_scene(args)
     threads = os.cpu_count() or 1
-    o = pyoracle.OracleSim(p, sc.pos, sc.vel, sc.type, threads=threads, keep_fields=False)
+    o = make_oracle(sc, threads)
     for _ in range(args.warmup):
         o.step()
     t0 = time.perf_counter()
@@ -161,16 +192,17 @@ def run_reference(args, rank, world):
         iters += o.step().iterations
     dt = time.perf_counter() - t0
     o.close()
-    v = sc.n_fluid * args.steps / dt
+    v = dynamic_count(sc) * args.steps / dt
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_for(args), "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": {"workload": workload_name(args), "sample_fluid_particles": sc.n_fluid,
                                         "sample_boundary_particles": sc.n_boundary,
                                         "mean_iterations": iters / max(args.steps, 1)},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": "pcisph_dam 64^3 fluid (%d) + %d boundary per step" % (sc.n_fluid, sc.n_boundary)},
+                         "sample": "%s: %d dynamic + %d boundary per step" % (label, dynamic_count(sc),
+                                                                              sc.n_boundary)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -195,7 +227,10 @@ def run_ours(args, rank, world, local_rank):
     s = upf.ParticleSystem(p, capacity=sc.n, device=local_rank, derive=False)
     s.set_stream(stream.cuda_stream)
     s.set_particles(sc.pos, sc.vel, sc.type)
+    if sc.num_bodies:
+        s.set_rigid_bodies(sc.body, sc.num_bodies)
     nf, nb = sc.n_fluid, sc.n_boundary
+    nd = dynamic_count(sc)
 
     # optional settle: during the first ~150 steps (the dam's collapse) the
     # loop runs into its 50-iteration cap with density errors above 1%;
@@ -236,7 +271,7 @@ def run_ours(args, rank, world, local_rank):
     max_ms = float(t.item())
     total_iters = stats.total_iterations if method == "pcisph" else 0
     mean_k = total_iters / max(stats.total_steps, 1)
-    value = nf * args.steps * world / (max_ms / 1e3)
+    value = nd * args.steps * world / (max_ms / 1e3)
 
     # per-phase timings (one profiled step through the phase entry points)
     prof = [s.profile_step() for _ in range(3)]
@@ -310,7 +345,7 @@ def run_ours(args, rank, world, local_rank):
         t2 = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
         if world > 1:
             torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
-        e2e = {"value": nf * k_e2e * world / (float(t2.item()) / 1e3), "unit": UNIT,
+        e2e = {"value": nd * k_e2e * world / (float(t2.item()) / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * (16 + 16 + 4 + 4 + 4 + 4),
                "steps": k_e2e}
 
@@ -319,14 +354,16 @@ def run_ours(args, rank, world, local_rank):
         return
     launches_base = 1 + 1 + 1 + 3 * RADIX_PASSES + 1 + 1  # step init, nlist, forces, sort, reorder, cells
     if method == "pcisph":
-        gpu_launches = args.steps * (launches_base + 2) + 3 * total_iters
+        rigid = (1 + 2 + 1) if sc.num_bodies else 0  # slots, reduce + integrate, sync
+        gpu_launches = args.steps * (launches_base + 2 + rigid) + 3 * total_iters
     else:
         gpu_launches = args.steps * (launches_base + 1)
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric_for(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_name(args), "fluid_particles": nf, "boundary_particles": nb,
+                   "dynamic_particles": nd, "rigid_bodies": int(sc.num_bodies),
                    "h": float(p.support_radius), "dt": float(p.dt), "block_size": int(p.block_size),
                    "settle_steps": args.settle, "mean_iterations": mean_k,
                    "steps_at_max_loops": stats.steps_at_max_loops,
@@ -346,7 +383,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(None, seconds=args.cpu_seconds)
+        out["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
     print(json.dumps(out), flush=True)
     s.close()
 
@@ -357,7 +394,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1"])
+    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3"])
     ap.add_argument("--block-size", type=int, default=0)
     ap.add_argument("--settle", type=int, default=0,
                     help="untimed steps before the warm-up, e.g. 300 to time steps after the dam's initial "

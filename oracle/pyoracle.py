@@ -85,6 +85,9 @@ def lib():
         L.orc_set_rigid_bodies.restype = C.c_int
         L.orc_get_rigid.argtypes = [C.c_void_p, fp, fp, fp, fp]
         L.orc_get_rigid.restype = C.c_int
+        L.orc_rigid_body_step.argtypes = [fp, fp, fp, C.c_float, C.c_float]
+        L.orc_inverse3.argtypes = [fp, fp]
+        L.orc_inverse3.restype = C.c_int
         _lib = L
     return _lib
 
@@ -130,6 +133,23 @@ def derive(p: UpfParams) -> UpfParams:
 def luts(p: UpfParams) -> np.ndarray:
     out = np.zeros((5, 301), np.float32)
     lib().orc_build_luts(C.byref(p), _ptr(out, C.c_float))
+    return out
+
+
+def rigid_body_step(state, force, torque, dt, terminal_speed) -> np.ndarray:
+    """One FP32 body update of a 47-float body state (see orc_rigid_body_step)."""
+    st = np.array(state, np.float32).copy()
+    f = np.ascontiguousarray(force, np.float32)
+    t = np.ascontiguousarray(torque, np.float32)
+    lib().orc_rigid_body_step(_ptr(st, C.c_float), _ptr(f, C.c_float), _ptr(t, C.c_float), float(dt),
+                              float(terminal_speed))
+    return st
+
+
+def inverse3(m9) -> np.ndarray:
+    a = np.ascontiguousarray(m9, np.float32).reshape(9)
+    out = np.zeros(9, np.float32)
+    lib().orc_inverse3(_ptr(a, C.c_float), _ptr(out, C.c_float))
     return out
 
 

@@ -199,11 +199,83 @@ R normalize(V3<R>& v) {
   v.z *= ll;
   return l;
 }
-// cos/sin of a float as the reference's host build evaluates them
-inline float fcos(float x) { return cosf(x); }
-inline float fsin(float x) { return sinf(x); }
-inline double fcos(double x) { return std::cos(x); }
-inline double fsin(double x) { return std::sin(x); }
+// Matrix3x3::CalculateInverse (Matrix3x3.cpp:121-156) in FP64: adjugate over
+// determinant, row-major; a singular matrix leaves `inv` unchanged and
+// returns false.
+inline bool inverse3_fp64(const double* A, double* inv) {
+  const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                     A[2] * (A[3] * A[7] - A[4] * A[6]);
+  if (det == 0.0) return false;
+  inv[0] = (A[4] * A[8] - A[5] * A[7]) / det;
+  inv[1] = (A[2] * A[7] - A[1] * A[8]) / det;
+  inv[2] = (A[1] * A[5] - A[2] * A[4]) / det;
+  inv[3] = (A[5] * A[6] - A[3] * A[8]) / det;
+  inv[4] = (A[0] * A[8] - A[2] * A[6]) / det;
+  inv[5] = (A[2] * A[3] - A[0] * A[5]) / det;
+  inv[6] = (A[3] * A[7] - A[4] * A[6]) / det;
+  inv[7] = (A[1] * A[6] - A[0] * A[7]) / det;
+  inv[8] = (A[0] * A[4] - A[1] * A[3]) / det;
+  return true;
+}
+
+// RigidBody::UpdateMomenta, PerformStep (UpdateInverseInertiaTensor,
+// PerformLinearStep, PerformAngularStep) and UpdateRotationMatrix
+// (RigidBody.cpp:15-161, 96-128) for one body, given the step's force and
+// torque. Float as the reference; its cos/sin calls take and return double
+// (the float angle is promoted), and `axis * sin(...)` multiplies in double
+// before rounding. The quaternion is not renormalised (RigidBody.cpp:99
+// discards getNormalized()'s result). MIN/MAX are the reference's macros
+// (global.h:4-5).
+template <class R>
+void body_update(Body<R>& b, V3<R> force, V3<R> torque, R dt, R terminal_speed) {
+  const R terminal = b.mass * terminal_speed;
+  b.P = b.P + force * dt;
+  R* P = &b.P.x;
+  for (int a = 0; a < 3; ++a) {
+    if (P[a] > R(0.0f))
+      P[a] = (P[a] <= terminal) ? P[a] : terminal;
+    else
+      P[a] = (P[a] >= -terminal) ? P[a] : -terminal;
+  }
+  b.L = b.L + torque * dt;
+  R rt[3][3], tmp[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) rt[j][i] = b.rot[i][j];
+  mat_mul(b.rot, b.inv_inertia_local, tmp);
+  mat_mul(tmp, rt, b.inv_inertia_world);
+  b.vel = divs(b.P, b.mass);
+  b.pos = b.pos + b.vel * dt;
+  b.omega = mat_vec(b.inv_inertia_world, b.L);
+  const R speed = vsqrt(lensq(b.omega));
+  if (speed > R(0.0f)) {
+    V3<R> axis = b.omega;
+    normalize(axis);
+    const R angle = speed * dt;
+    const double half = (double)(angle / R(2.0f));
+    const R ds = R(std::cos(half));
+    const double sn = std::sin(half);
+    const R dvx = R((double)axis.x * sn);
+    const R dvy = R((double)axis.y * sn);
+    const R dvz = R((double)axis.z * sn);
+    const R s = b.q[0], vx = b.q[1], vy = b.q[2], vz = b.q[3];
+    b.q[0] = s * ds - vx * dvx - vy * dvy - vz * dvz;
+    b.q[1] = ds * vx + s * dvx + dvy * vz - dvz * vy;
+    b.q[2] = ds * vy + s * dvy + dvz * vx - dvx * vz;
+    b.q[3] = ds * vz + s * dvz + dvx * vy - dvy * vx;
+  }
+  const R w = b.q[0], x = b.q[1], y = b.q[2], z = b.q[3];
+  const R xx = x * x, yy = y * y, zz = z * z, xy = x * y, xz = x * z, yz = y * z, wx = w * x, wy = w * y,
+          wz = w * z;
+  b.rot[0][0] = R(1.0f) - R(2.0f) * (yy + zz);
+  b.rot[0][1] = R(2.0f) * (xy - wz);
+  b.rot[0][2] = R(2.0f) * (xz + wy);
+  b.rot[1][0] = R(2.0f) * (xy + wz);
+  b.rot[1][1] = R(1.0f) - R(2.0f) * (xx + zz);
+  b.rot[1][2] = R(2.0f) * (yz - wx);
+  b.rot[2][0] = R(2.0f) * (xz - wy);
+  b.rot[2][1] = R(2.0f) * (yz + wx);
+  b.rot[2][2] = R(1.0f) - R(2.0f) * (xx + yy);
+}
 
 // ---------------------------------------------------------------------------
 // The simulation: one particle array for every type, as in the reference.
@@ -765,59 +837,10 @@ struct Sim : SimBase {
       t[2] += rx * fy - ry * fx;
       f[1] += (double)(-R(prm.mass) * R(prm.gravity));
     }
-    const R dt = R(prm.dt);
     for (int k = 0; k < nb; ++k) {
-      Body<R>& b = bodies[k];
       const V3<R> force = {R(F[3 * k]), R(F[3 * k + 1]), R(F[3 * k + 2])};
       const V3<R> torque = {R(T[3 * k]), R(T[3 * k + 1]), R(T[3 * k + 2])};
-      const R terminal = b.mass * R(prm.terminal_speed);
-      // UpdateMomenta (RigidBody.cpp:147-161)
-      b.P = b.P + force * dt;
-      R* P = &b.P.x;
-      for (int a = 0; a < 3; ++a) {
-        if (P[a] > R(0.0f))
-          P[a] = std::min(P[a], terminal);
-        else
-          P[a] = std::max(P[a], -terminal);
-      }
-      b.L = b.L + torque * dt;
-      // PerformStep: UpdateInverseInertiaTensor, PerformLinearStep, PerformAngularStep
-      R rt[3][3], tmp[3][3];
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) rt[j][i] = b.rot[i][j];
-      mat_mul(b.rot, b.inv_inertia_local, tmp);
-      mat_mul(tmp, rt, b.inv_inertia_world);
-      b.vel = divs(b.P, b.mass);
-      b.pos = b.pos + b.vel * dt;
-      b.omega = mat_vec(b.inv_inertia_world, b.L);
-      const R speed = vsqrt(lensq(b.omega));
-      if (speed > R(0.0f)) {
-        V3<R> axis = b.omega;
-        normalize(axis);
-        const R angle = speed * dt;
-        const R ds = fcos(angle / R(2.0f));
-        const R dvx = axis.x * fsin(angle / R(2.0f));
-        const R dvy = axis.y * fsin(angle / R(2.0f));
-        const R dvz = axis.z * fsin(angle / R(2.0f));
-        const R s = b.q[0], vx = b.q[1], vy = b.q[2], vz = b.q[3];
-        b.q[0] = s * ds - vx * dvx - vy * dvy - vz * dvz;
-        b.q[1] = ds * vx + s * dvx + dvy * vz - dvz * vy;
-        b.q[2] = ds * vy + s * dvy + dvz * vx - dvx * vz;
-        b.q[3] = ds * vz + s * dvz + dvx * vy - dvy * vx;
-      }
-      // UpdateRotationMatrix (RigidBody.cpp:96-128)
-      const R w = b.q[0], x = b.q[1], y = b.q[2], z = b.q[3];
-      const R xx = x * x, yy = y * y, zz = z * z, xy = x * y, xz = x * z, yz = y * z, wx = w * x, wy = w * y,
-              wz = w * z;
-      b.rot[0][0] = R(1.0f) - R(2.0f) * (yy + zz);
-      b.rot[0][1] = R(2.0f) * (xy - wz);
-      b.rot[0][2] = R(2.0f) * (xz + wy);
-      b.rot[1][0] = R(2.0f) * (xy + wz);
-      b.rot[1][1] = R(1.0f) - R(2.0f) * (xx + zz);
-      b.rot[1][2] = R(2.0f) * (yz - wx);
-      b.rot[2][0] = R(2.0f) * (xz - wy);
-      b.rot[2][1] = R(2.0f) * (yz + wx);
-      b.rot[2][2] = R(1.0f) - R(2.0f) * (xx + yy);
+      body_update(bodies[k], force, torque, R(prm.dt), R(prm.terminal_speed));
     }
   }
 
@@ -1007,6 +1030,10 @@ struct Sim : SimBase {
   // summed in FP64 over the body's particles in input order and the inertia
   // is inverted in FP64 (the reference sums incrementally in float and its
   // ComputeLocalInertiaTensorRigidBody indexes particles_[i] for indices[i]).
+  // The inverse is stored as the body's local inverse inertia: the reference
+  // writes it into the temporary that inverted_inertia_local() returns
+  // (UnifiedPhysics.cpp:150), so its bodies keep a zero inverse inertia and
+  // never rotate.
   int set_bodies(const int32_t* bop, uint32_t n, uint32_t nb) override {
     if (n != ps.size()) return -1;
     std::vector<int> where(n);
@@ -1046,21 +1073,8 @@ struct Sim : SimBase {
     for (uint32_t b = 0; b < nb; ++b) {
       Body<R>& B = bodies[b];
       std::memset(&B, 0, sizeof(B));
-      const double* A = &I[9 * b];
       double inv[9] = {0};
-      const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
-                         A[2] * (A[3] * A[7] - A[4] * A[6]);
-      if (det != 0.0) {
-        inv[0] = (A[4] * A[8] - A[5] * A[7]) / det;
-        inv[1] = (A[2] * A[7] - A[1] * A[8]) / det;
-        inv[2] = (A[1] * A[5] - A[2] * A[4]) / det;
-        inv[3] = (A[5] * A[6] - A[3] * A[8]) / det;
-        inv[4] = (A[0] * A[8] - A[2] * A[6]) / det;
-        inv[5] = (A[2] * A[3] - A[0] * A[5]) / det;
-        inv[6] = (A[3] * A[7] - A[4] * A[6]) / det;
-        inv[7] = (A[1] * A[6] - A[0] * A[7]) / det;
-        inv[8] = (A[0] * A[4] - A[1] * A[3]) / det;
-      }
+      inverse3_fp64(&I[9 * b], inv);
       B.mass = R(M[b]);
       B.pos = {R(C[3 * b]), R(C[3 * b + 1]), R(C[3 * b + 2])};
       B.P = {R(Pm[3 * b]), R(Pm[3 * b + 1]), R(Pm[3 * b + 2])};
@@ -1343,6 +1357,34 @@ uint32_t orc_neighbors(orc_sim* s, uint32_t* offsets, uint32_t* ids, uint32_t ca
 
 int orc_get_rigid(const orc_sim* s, float* pos3, float* vel3, float* omega3, float* quat4) {
   return s->impl->get_rigid(pos3, vel3, omega3, quat4);
+}
+
+int orc_inverse3(const float* in9, float* out9) {
+  double a[9], inv[9] = {0};
+  for (int i = 0; i < 9; ++i) a[i] = in9[i];
+  const bool ok = inverse3_fp64(a, inv);
+  for (int i = 0; i < 9; ++i) out9[i] = (float)inv[i];
+  return ok ? 1 : 0;
+}
+
+void orc_rigid_body_step(float* st, const float* force3, const float* torque3, float dt, float terminal_speed) {
+  Body<float> b;
+  const float* q = st;
+  auto v3 = [&](V3<float>& v) { v = {q[0], q[1], q[2]}; q += 3; };
+  auto m3 = [&](float m[3][3]) { for (int i = 0; i < 9; ++i) m[i / 3][i % 3] = q[i]; q += 9; };
+  b.mass = *q++;
+  v3(b.pos); v3(b.vel); v3(b.P); v3(b.L); v3(b.omega);
+  for (int k = 0; k < 4; ++k) b.q[k] = *q++;
+  m3(b.rot); m3(b.inv_inertia_local); m3(b.inv_inertia_world);
+  body_update(b, V3<float>{force3[0], force3[1], force3[2]}, V3<float>{torque3[0], torque3[1], torque3[2]}, dt,
+              terminal_speed);
+  float* o = st;
+  auto w3 = [&](const V3<float>& v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o += 3; };
+  auto n3 = [&](const float m[3][3]) { for (int i = 0; i < 9; ++i) o[i] = m[i / 3][i % 3]; o += 9; };
+  *o++ = b.mass;
+  w3(b.pos); w3(b.vel); w3(b.P); w3(b.L); w3(b.omega);
+  for (int k = 0; k < 4; ++k) *o++ = b.q[k];
+  n3(b.rot); n3(b.inv_inertia_local); n3(b.inv_inertia_world);
 }
 
 }  // extern "C"

@@ -68,6 +68,15 @@ void orc_get_step_fields(const orc_sim* s, float* force4, float* pforce4,
 uint32_t orc_neighbors(orc_sim* s, uint32_t* offsets, uint32_t* ids, uint32_t cap);
 /* rigid body state: per body pos[3], vel[3], omega[3], quat[4] */
 int orc_get_rigid(const orc_sim* s, float* pos3, float* vel3, float* omega3, float* quat4);
+/* one FP32 body update (momenta, inverse world inertia, linear and angular
+ * step, rotation matrix) in place on ORC_BODY_FLOATS floats: mass, pos[3],
+ * vel[3], P[3], L[3], omega[3], q[4] (s,x,y,z), rot[9], inv_inertia_local[9],
+ * inv_inertia_world[9] (row-major) */
+#define ORC_BODY_FLOATS 47
+/* FP64 adjugate inverse of a row-major 3x3 (rounded to float); 0 if singular */
+int orc_inverse3(const float* in9, float* out9);
+void orc_rigid_body_step(float* state, const float* force3, const float* torque3, float dt,
+                         float terminal_speed);
 
 #ifdef __cplusplus
 }

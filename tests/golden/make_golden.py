@@ -1,6 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own CPU
 code (src/cpu/zIndex.cpp, src/cpu/WeightingKernel.cpp,
-src/sceneConfigure/UnifiedConstants.cpp), compiled by oracle/Makefile into
+src/sceneConfigure/UnifiedConstants.cpp, src/cpu/RigidBody.cpp,
+src/cpu/Matrix3x3.cpp), compiled by oracle/Makefile into
 oracle/_ref/libupfref.so. Run in a checkout where the reference source tree
 is available:
 
@@ -87,6 +88,63 @@ def main():
     out["default_constants"] = cst[:41]
     np.savez_compressed(os.path.join(HERE, "reference_tables.npz"), **out)
     print("wrote", os.path.join(HERE, "reference_tables.npz"))
+    rigid = rigid_vectors(R)
+    np.savez_compressed(os.path.join(HERE, "reference_rigid.npz"), **rigid)
+    print("wrote", os.path.join(HERE, "reference_rigid.npz"))
+
+
+def random_body_state(rng):
+    """A body state of 47 floats (mass, pos, vel, P, L, omega, q, rot,
+    inv_inertia_local, inv_inertia_world): unit-ish quaternion, its rotation
+    matrix, a symmetric positive definite inverse inertia."""
+    st = np.zeros(47, np.float32)
+    st[0] = rng.uniform(0.01, 10.0)
+    st[1:4] = rng.uniform(-1, 1, 3)
+    st[4:7] = rng.normal(0, 1, 3)
+    st[7:10] = rng.normal(0, 1, 3) * st[0]
+    st[10:13] = rng.normal(0, 0.01, 3)
+    st[13:16] = rng.normal(0, 1, 3)
+    q = rng.normal(0, 1, 4)
+    q = q / np.linalg.norm(q) * (1.0 + rng.normal(0, 1e-4))
+    st[16:20] = q
+    w, x, y, z = st[16:20].astype(np.float64)
+    st[20:29] = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                          [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                          [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]]).ravel()
+    a = rng.normal(0, 1, (3, 3))
+    st[29:38] = (np.linalg.inv(a @ a.T + 0.1 * np.eye(3)) * 100.0).ravel()
+    return st
+
+
+def rigid_vectors(R):
+    """RigidBody::UpdateMomenta + PerformStep + UpdateRotationMatrix on seeded
+    states (terminal-momentum clamp active in some), and
+    Matrix3x3::CalculateInverse on seeded inertia tensors."""
+    fp_t = C.POINTER(C.c_float)
+    R.ref_rigid_body_step.argtypes = [fp_t, fp_t, fp_t, C.c_float, C.c_float]
+    R.ref_inverse3.argtypes = [fp_t, fp_t]
+    R.ref_inverse3.restype = C.c_int
+    rng = np.random.default_rng(20240917)
+    n = 256
+    st_in = np.stack([random_body_state(rng) for _ in range(n)])
+    force = rng.normal(0, 5, (n, 3)).astype(np.float32)
+    torque = rng.normal(0, 0.5, (n, 3)).astype(np.float32)
+    dt = rng.choice(np.array([5e-4, 1e-3, 1e-2], np.float32), n).astype(np.float32)
+    terminal = rng.choice(np.array([20.0, 0.5], np.float32), n).astype(np.float32)
+    st_out = st_in.copy()
+    for k in range(n):
+        R.ref_rigid_body_step(fp(st_out[k]), fp(force[k]), fp(torque[k]), C.c_float(dt[k]), C.c_float(terminal[k]))
+    mats = np.zeros((64, 9), np.float32)
+    for k in range(64):
+        pts = rng.normal(0, 0.1, (rng.integers(4, 40), 3))
+        rr = (pts * pts).sum(1)
+        inertia = sum(np.eye(3) * r2 - np.outer(p, p) for p, r2 in zip(pts, rr)) * 0.001
+        mats[k] = inertia.ravel()
+    inv = np.zeros_like(mats)
+    ok = np.array([R.ref_inverse3(fp(mats[k]), fp(inv[k])) for k in range(64)], np.int32)
+    return {"body_in": st_in, "body_force": force, "body_torque": torque, "body_dt": dt,
+            "body_terminal_speed": terminal, "body_out": st_out, "inertia": mats, "inertia_inverse": inv,
+            "inertia_ok": ok}
 
 
 if __name__ == "__main__":

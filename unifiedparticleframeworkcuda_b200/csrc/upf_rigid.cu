@@ -69,8 +69,9 @@ __global__ void __launch_bounds__(kReduceThreads) k_rigid_reduce(DevParams P, De
   }
 }
 
-__device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }  // std::min
-__device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }  // std::max
+// the reference's MIN / MAX macros (global.h:4-5)
+__device__ __forceinline__ float min_ref(float a, float b) { return (a <= b) ? a : b; }
+__device__ __forceinline__ float max_ref(float a, float b) { return (a >= b) ? a : b; }
 
 __device__ __forceinline__ void mat_mul(const float a[3][3], const float b[3][3], float out[3][3]) {
   for (int i = 0; i < 3; ++i)
@@ -92,8 +93,9 @@ __device__ __forceinline__ float3 mat_vec(const float a[3][3], float3 v) {
 }
 
 // UpdateMomenta, PerformStep and UpdateRotationMatrix (RigidBody.cpp:15-161),
-// float as in the reference; cos/sin are evaluated in double and rounded once,
-// as the reference's host cosf/sinf do.
+// float as in the reference. The reference's cos/sin calls take the float
+// half-angle promoted to double, and `axis * sin(...)` multiplies in double
+// before rounding to float; the same here.
 __global__ void k_rigid_integrate(DevParams P, DevBody* __restrict__ bodies, uint32_t nb) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nb) return;
@@ -106,7 +108,7 @@ __global__ void k_rigid_integrate(DevParams P, DevBody* __restrict__ bodies, uin
   B.P.y = B.P.y + F.y * dt;
   B.P.z = B.P.z + F.z * dt;
   float* Pv = &B.P.x;
-  for (int a = 0; a < 3; ++a) Pv[a] = (Pv[a] > 0.0f) ? fmin_ref(Pv[a], terminal) : fmax_ref(Pv[a], -terminal);
+  for (int a = 0; a < 3; ++a) Pv[a] = (Pv[a] > 0.0f) ? min_ref(Pv[a], terminal) : max_ref(Pv[a], -terminal);
   B.L.x = B.L.x + T.x * dt;
   B.L.y = B.L.y + T.y * dt;
   B.L.z = B.L.z + T.z * dt;
@@ -124,10 +126,10 @@ __global__ void k_rigid_integrate(DevParams P, DevBody* __restrict__ bodies, uin
     const float ll = (float)(1.0 / (double)speed);
     const float ax = B.omega.x * ll, ay = B.omega.y * ll, az = B.omega.z * ll;
     const float angle = speed * dt;
-    const float half = angle / 2.0f;
-    const float ds = (float)cos((double)half);
-    const float sn = (float)sin((double)half);
-    const float dvx = ax * sn, dvy = ay * sn, dvz = az * sn;
+    const double half = (double)(angle / 2.0f);
+    const float ds = (float)cos(half);
+    const double sn = sin(half);
+    const float dvx = (float)((double)ax * sn), dvy = (float)((double)ay * sn), dvz = (float)((double)az * sn);
     const float s = B.q[0], vx = B.q[1], vy = B.q[2], vz = B.q[3];
     B.q[0] = s * ds - vx * dvx - vy * dvy - vz * dvz;
     B.q[1] = ds * vx + s * dvx + dvy * vz - dvz * vy;
