@@ -355,6 +355,46 @@ upf_status upf_cell_ranges(const uint32_t* sorted_keys_dev, uint32_t n, int32_t 
                            uint32_t ncells, uint32_t* start_dev, uint32_t* end_dev,
                            void* stream);
 
+/* ---- batched scenes -------------------------------------------------------
+ * No counterpart in the reference (one simulation per process, global device
+ * state). Many independent PCISPH scenes of uneven sizes advance together:
+ * every pass of a step is one launch over all scenes, the step is one CUDA
+ * graph whose predict-correct loop (a device-side while-node) runs until the
+ * last scene has converged, each scene keeping its own iteration count. Every
+ * scene's result is the one a upf_system with the same parameters and
+ * particles computes (same sort order, neighbour lists and sums).
+ * Scenes hold LIQUID particles only (walls by the collision box and
+ * UPF_FLAG_PENALTY_WALLS); params[s].method must be UPF_METHOD_PCISPH. */
+typedef struct upf_batch upf_batch;
+
+/* params: num_scenes parameter sets (derived like upf_params_derive),
+ * counts: particles per scene. */
+upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, uint32_t num_scenes,
+                            int device, upf_batch** out);
+upf_status upf_batch_destroy(upf_batch* b);
+upf_status upf_batch_set_stream(upf_batch* b, void* stream);
+/* Host arrays of all scenes' particles, concatenated in scene order
+ * (pos4/vel4: sum(counts) x 4 floats). Particle ids are 0..counts[s]-1 per
+ * scene in input order. */
+upf_status upf_batch_set_particles(upf_batch* b, const float* pos4, const float* vel4);
+upf_status upf_batch_step(upf_batch* b, int32_t nsteps);
+/* Waits for the batch's stream; reports the first scene's device error. */
+upf_status upf_batch_synchronize(upf_batch* b);
+/* Per-scene statistics of the last step: out[num_scenes]. */
+upf_status upf_batch_get_stats(upf_batch* b, upf_step_stats* out);
+upf_status upf_batch_reset_counters(upf_batch* b);
+/* One scene's particles in current device order (any pointer may be NULL). */
+upf_status upf_batch_get_particles(upf_batch* b, uint32_t scene, float* pos4, float* vel4,
+                                   float* density, float* pressure, uint32_t* id, uint32_t* n_out);
+/* Device copies of the whole batch state, as upf_checkpoint / upf_restore. */
+upf_status upf_batch_checkpoint(upf_batch* b, int32_t slot);
+upf_status upf_batch_restore(upf_batch* b, int32_t slot);
+/* Same layout as upf_batch_set_particles: all scenes' positions and
+ * velocities replace the current state (H2D), or are read back (D2H), in the
+ * batch's current device order per scene. */
+upf_status upf_batch_upload_state(upf_batch* b, const float* pos4, const float* vel4);
+upf_status upf_batch_download_state(upf_batch* b, float* pos4, float* vel4);
+
 /* ---- errors ------------------------------------------------------------- */
 const char* upf_last_error(void);
 const char* upf_status_string(upf_status st);

@@ -69,6 +69,19 @@ def lib():
             "upf_get_sorted_keys": [vp, u32p, u32p, u32p],
             "upf_get_cell_ranges": [vp, u32p, u32p, u32p],
             "upf_get_rigid_bodies": [vp, fp, fp, fp, fp, u32p],
+            "upf_batch_create": [P, u32p, C.c_uint32, C.c_int, C.POINTER(vp)],
+            "upf_batch_destroy": [vp],
+            "upf_batch_set_stream": [vp, vp],
+            "upf_batch_set_particles": [vp, fp, fp],
+            "upf_batch_step": [vp, C.c_int32],
+            "upf_batch_synchronize": [vp],
+            "upf_batch_get_stats": [vp, C.POINTER(UpfStepStats)],
+            "upf_batch_reset_counters": [vp],
+            "upf_batch_get_particles": [vp, C.c_uint32, fp, fp, fp, fp, u32p, u32p],
+            "upf_batch_checkpoint": [vp, C.c_int32],
+            "upf_batch_restore": [vp, C.c_int32],
+            "upf_batch_upload_state": [vp, fp, fp],
+            "upf_batch_download_state": [vp, fp, fp],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
             "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
             "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],
@@ -310,3 +323,96 @@ class ParticleSystem:
         check(lib().upf_get_cell_ranges(self._h, _p(start, C.c_uint32), _p(end, C.c_uint32), C.byref(cnt)),
               "upf_get_cell_ranges")
         return start, end
+
+
+class ParticleBatch:
+    """Many independent PCISPH scenes advanced together (upf_batch_*): one
+    launch per pass over all scenes, one CUDA graph per step."""
+
+    def __init__(self, params_list, counts, device: int = 0, derive: bool = True):
+        ps = [derive_params(p) if derive else p.copy() for p in params_list]
+        self.params = ps
+        arr = (UpfParams * len(ps))(*ps)
+        self.counts = np.ascontiguousarray(counts, np.uint32)
+        if self.counts.shape != (len(ps),):
+            raise ValueError("one count per scene")
+        h = C.c_void_p()
+        check(lib().upf_batch_create(arr, _p(self.counts, C.c_uint32), len(ps), int(device), C.byref(h)),
+              "upf_batch_create")
+        self._h = h
+        self.n_scenes = len(ps)
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts.astype(np.int64))])
+
+    @classmethod
+    def from_scenes(cls, scene_list, device: int = 0):
+        b = cls([sc.params for sc in scene_list], [sc.n for sc in scene_list], device=device)
+        b.set_particles(np.concatenate([sc.pos for sc in scene_list]), np.concatenate([sc.vel for sc in scene_list]))
+        return b
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().upf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_handle: int | None):
+        check(lib().upf_batch_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None),
+              "upf_batch_set_stream")
+
+    def set_particles(self, pos4, vel4):
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        vel4 = np.ascontiguousarray(vel4, np.float32)
+        n = int(self.offsets[-1])
+        if pos4.shape != (n, 4) or vel4.shape != (n, 4):
+            raise ValueError("pos4/vel4 must be (sum(counts), 4)")
+        check(lib().upf_batch_set_particles(self._h, _p(pos4, C.c_float), _p(vel4, C.c_float)),
+              "upf_batch_set_particles")
+
+    def step(self, nsteps: int = 1):
+        check(lib().upf_batch_step(self._h, int(nsteps)), "upf_batch_step")
+
+    def synchronize(self):
+        check(lib().upf_batch_synchronize(self._h), "upf_batch_synchronize")
+
+    def stats(self):
+        out = (UpfStepStats * self.n_scenes)()
+        check(lib().upf_batch_get_stats(self._h, out), "upf_batch_get_stats")
+        return list(out)
+
+    def reset_counters(self):
+        check(lib().upf_batch_reset_counters(self._h), "upf_batch_reset_counters")
+
+    def checkpoint(self, slot: int = 0):
+        check(lib().upf_batch_checkpoint(self._h, int(slot)), "upf_batch_checkpoint")
+
+    def restore(self, slot: int = 0):
+        check(lib().upf_batch_restore(self._h, int(slot)), "upf_batch_restore")
+
+    def particles(self, scene: int):
+        n = int(self.counts[scene])
+        pos = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        den = np.zeros(n, np.float32)
+        pre = np.zeros(n, np.float32)
+        ids = np.zeros(n, np.uint32)
+        cnt = C.c_uint32()
+        check(lib().upf_batch_get_particles(self._h, int(scene), _p(pos, C.c_float), _p(vel, C.c_float),
+                                            _p(den, C.c_float), _p(pre, C.c_float), _p(ids, C.c_uint32),
+                                            C.byref(cnt)), "upf_batch_get_particles")
+        return dict(pos=pos, vel=vel, density=den, pressure=pre, id=ids)
+

@@ -71,6 +71,8 @@ uint32_t log2u(uint32_t v) {
   return r;
 }
 
+}  // namespace
+
 DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   DevParams d{};
   d.h = p.support_radius;
@@ -126,6 +128,10 @@ DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   return d;
 }
 
+namespace {
+
+}  // namespace
+
 // 2D tensor map over a column-major neighbour array [rows][cols] for the
 // TMA list stream: box = 32 columns (one warp) x kListRows rows.
 upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint32_t elem_bytes, uint64_t cols,
@@ -158,16 +164,12 @@ upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt,
   return UPF_OK;
 }
 
-void destroy_graph(System& s) {
-  if (s.step_exec) cudaGraphExecDestroy(s.step_exec);
-  if (s.step_graph) cudaGraphDestroy(s.step_graph);
-  s.step_exec = nullptr;
-  s.step_graph = nullptr;
-}
-
-// One step as a graph: sort -> neighbours -> forces -> [while: loop body] -> integrate.
-upf_status build_step_graph(System& s) {
-  destroy_graph(s);
+// One step as a graph: pre -> [while: loop] -> post. The loop body is
+// captured into the body graph of a conditional while-node; the body's last
+// kernel sets the node's condition.
+upf_status capture_step_graph(const GraphParts& parts, cudaGraph_t* graph_out, cudaGraphExec_t* exec_out) {
+  *graph_out = nullptr;
+  *exec_out = nullptr;
   cudaStream_t cs = nullptr, body_stream = nullptr;
   UPF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   UPF_CUDA(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
@@ -189,11 +191,8 @@ upf_status build_step_graph(System& s) {
     set_error("step graph: %s: %s", what, cudaGetErrorString(err));
     return UPF_ERR_CUDA;
   };
-  if ((e = launch_sort_phase(s, cs)) != cudaSuccess) return fail("sort", e);
-  if ((e = launch_neighbor_phase(s, cs)) != cudaSuccess) return fail("neighbours", e);
-  if ((e = launch_force_phase(s, cs)) != cudaSuccess) return fail("forces", e);
-  if (s.prm.method == UPF_METHOD_PCISPH) {
-    if ((e = launch_loop_init(s, cs)) != cudaSuccess) return fail("loop init", e);
+  if (parts.pre && (e = parts.pre(parts.ctx, cs)) != cudaSuccess) return fail("pre", e);
+  if (parts.loop) {
     cudaStreamCaptureStatus cst;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -216,13 +215,13 @@ upf_status build_step_graph(System& s) {
     if ((e = cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0,
                                            cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return fail("body capture", e);
-    cudaError_t eb = launch_loop_body(s, body_stream, handle, true);
+    cudaError_t eb = parts.loop(parts.ctx, body_stream, handle);
     cudaGraph_t body_out = nullptr;
     cudaError_t ee = cudaStreamEndCapture(body_stream, &body_out);
     if (eb != cudaSuccess) return fail("loop body", eb);
     if (ee != cudaSuccess) return fail("body end capture", ee);
   }
-  if ((e = launch_integrate_phase(s, cs)) != cudaSuccess) return fail("integrate", e);
+  if (parts.post && (e = parts.post(parts.ctx, cs)) != cudaSuccess) return fail("post", e);
   cudaGraph_t graph = nullptr;
   e = cudaStreamEndCapture(cs, &graph);
   cleanup();
@@ -230,14 +229,44 @@ upf_status build_step_graph(System& s) {
     set_error("step graph end capture: %s", cudaGetErrorString(e));
     return UPF_ERR_CUDA;
   }
-  e = cudaGraphInstantiate(&s.step_exec, graph, 0);
+  e = cudaGraphInstantiate(exec_out, graph, 0);
   if (e != cudaSuccess) {
     cudaGraphDestroy(graph);
     set_error("step graph instantiate: %s", cudaGetErrorString(e));
     return UPF_ERR_CUDA;
   }
-  s.step_graph = graph;
+  *graph_out = graph;
   return UPF_OK;
+}
+
+namespace {
+
+void destroy_graph(System& s) {
+  if (s.step_exec) cudaGraphExecDestroy(s.step_exec);
+  if (s.step_graph) cudaGraphDestroy(s.step_graph);
+  s.step_exec = nullptr;
+  s.step_graph = nullptr;
+}
+
+// One step of a system: sort -> neighbours -> forces -> [while: loop body] -> integrate.
+upf_status build_step_graph(System& s) {
+  destroy_graph(s);
+  GraphParts parts;
+  parts.ctx = &s;
+  parts.pre = [](void* c, cudaStream_t st) {
+    System& S = *static_cast<System*>(c);
+    cudaError_t e = launch_sort_phase(S, st);
+    if (e == cudaSuccess) e = launch_neighbor_phase(S, st);
+    if (e == cudaSuccess) e = launch_force_phase(S, st);
+    if (e == cudaSuccess && S.prm.method == UPF_METHOD_PCISPH) e = launch_loop_init(S, st);
+    return e;
+  };
+  if (s.prm.method == UPF_METHOD_PCISPH)
+    parts.loop = [](void* c, cudaStream_t st, cudaGraphConditionalHandle h) {
+      return launch_loop_body(*static_cast<System*>(c), st, h, true);
+    };
+  parts.post = [](void* c, cudaStream_t st) { return launch_integrate_phase(*static_cast<System*>(c), st); };
+  return capture_step_graph(parts, &s.step_graph, &s.step_exec);
 }
 
 upf_status check_device_errors(System& s) {

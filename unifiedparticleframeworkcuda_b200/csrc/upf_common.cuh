@@ -90,6 +90,7 @@ struct DevState {
   int32_t total_steps;
   int32_t total_iterations;
   int32_t steps_at_max;
+  int32_t loop_active;     // batched scenes: the scene's predict-correct loop still runs
 };
 
 // ---- exact float helpers --------------------------------------------------

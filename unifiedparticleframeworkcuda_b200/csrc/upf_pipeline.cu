@@ -123,6 +123,37 @@ struct PosP {
   float p;
 };
 
+// What a CTA works on: one system (plain launch) or, in a batched launch,
+// the scene its slots belong to (BatchView). Batched CTAs copy the scene's
+// parameters to shared memory; `end` bounds the particle index.
+struct Scope {
+  const DevParams* P;
+  const float* luts;
+  DevState* st;
+  uint32_t end;
+  uint32_t scene;
+  bool skip;  // a loop pass of a scene whose loop has finished
+};
+
+// batched scenes: the key of a padding slot (above every 30-bit Morton key)
+constexpr uint32_t kPadKeyBatch = 1u << 30;
+
+template <bool kBatch>
+__device__ __forceinline__ Scope enter_scope(const DevParams& Pk, const float* luts, DevState* st, uint32_t n,
+                                             const BatchView& bv, DevParams* sP, bool loop_pass) {
+  if constexpr (!kBatch) {
+    return Scope{&Pk, luts, st, n, 0u, false};
+  } else {
+    const uint32_t s = bv.group_scene[(blockIdx.x * blockDim.x) / kSegAlign];
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(bv.params + s);
+    for (uint32_t k = threadIdx.x; k < sizeof(DevParams) / 4; k += blockDim.x)
+      reinterpret_cast<uint32_t*>(sP)[k] = src[k];
+    DevState* sst = bv.st + s;
+    const bool skip = loop_pass && !*reinterpret_cast<volatile int32_t*>(&sst->loop_active);
+    return Scope{sP, bv.luts + (size_t)s * kLutFloats, sst, bv.seg_end[s], s, skip};
+  }
+}
+
 // ---------------------------------------------------------------- reorder
 // CopySortedParticleValuesKernel* (particles_kernel.cu:543-654): gather the
 // state into sorted order.
@@ -155,18 +186,28 @@ __device__ __forceinline__ float dist2(float4 a, float4 b) {
 // and |x_i - x_j| < h in float. Candidate positions are gathered kUnroll at
 // a time. Each entry also records its kernel-table bin at the current
 // positions (used by every pass that evaluates at current positions).
+template <bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_build_nlist(
-    DevParams P, uint32_t n, const float4* __restrict__ pos, const uint32_t* __restrict__ keys,
-    const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, uint32_t ns,
-    const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
+    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const float4* __restrict__ pos,
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend,
+    uint32_t ns, const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
     const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, uint32_t* __restrict__ nbr,
     uint16_t* __restrict__ bins, uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
-    DevState* __restrict__ st) {
+    DevState* __restrict__ st_plain) {
+  __shared__ DevParams sP;
   __shared__ float thr[kThresholds];
-  for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) thr[k] = luts[5 * UPF_LUT_ENTRIES + k];
+  const Scope sc = enter_scope<kBatch>(Pk, luts, st_plain, n, bv, &sP, false);
+  for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) thr[k] = sc.luts[5 * UPF_LUT_ENTRIES + k];
   __syncthreads();
+  const DevParams& P = *sc.P;
+  DevState* st = sc.st;
+  if (kBatch) {
+    // the scene's own cell table (keys are the scene's Morton keys)
+    cstart += bv.cell_base[sc.scene];
+    cend += bv.cell_base[sc.scene];
+  }
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= sc.end) return;
   const float4 xi = pos[i];
   const float h = P.h;
   int lo[3], hi[3];
@@ -682,19 +723,26 @@ __device__ __forceinline__ float3 solid_external(const DevParams& P, uint32_t i,
 // CalculateExternalForcesVersatilCouplingPCISPH (UnifiedPhysics.cpp:5252-5365):
 // liquid particles (then the first prediction of the loop), rigid and
 // granular particles (solid_external).
+template <bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_pcisph_external(
-    DevParams P, uint32_t n, DynArrays B, const float* __restrict__ wvol, const int32_t* __restrict__ id_body,
-    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
-    float4* __restrict__ force, float4* __restrict__ pforce, float4* __restrict__ xs, float* __restrict__ press,
-    float* __restrict__ pq, DevState* __restrict__ st) {
+    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
+    const float* __restrict__ wvol, const int32_t* __restrict__ id_body, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, float4* __restrict__ force,
+    float4* __restrict__ pforce, float4* __restrict__ xs, float* __restrict__ press, float* __restrict__ pq,
+    DevState* __restrict__ st_plain) {
+  __shared__ DevParams sP;
   __shared__ float vl[UPF_LUT_ENTRIES], pg[UPF_LUT_ENTRIES], stl[UPF_LUT_ENTRIES], adl[UPF_LUT_ENTRIES];
+  const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, false);
+  const float* luts = sc.luts;
   stage_lut(vl, luts + LUT_VISC * UPF_LUT_ENTRIES);
   stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
   stage_lut(stl, luts + LUT_ST * UPF_LUT_ENTRIES);
   stage_lut(adl, luts + LUT_ADH * UPF_LUT_ENTRIES);
   __syncthreads();
+  const DevParams& P = *sc.P;
+  DevState* st = sc.st;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= sc.end) return;
   const int32_t ti = B.type[i];
   const float4 xi = B.pos[i];
   press[i] = 0.0f;
@@ -782,23 +830,29 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
 // The warp's list rows stream through shared memory by TMA (upf_tma.cuh);
 // each lane then gathers kListRows neighbours' predicted positions at once
 // and accumulates them in list order.
+template <bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_pcisph_density(
-    DevParams P, uint32_t n, const int32_t* __restrict__ type, const float4* __restrict__ xs,
-    const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
-    const float* __restrict__ luts, float* __restrict__ rho, float* __restrict__ press, float* __restrict__ pq,
-    DevState* __restrict__ st) {
+    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const int32_t* __restrict__ type,
+    const float4* __restrict__ xs, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
+    const float* __restrict__ luts_plain, float* __restrict__ rho, float* __restrict__ press,
+    float* __restrict__ pq, DevState* __restrict__ st_plain) {
+  __shared__ DevParams sP;
   __shared__ float m4[UPF_LUT_ENTRIES];
   __shared__ float thr[kThresholds];
   __shared__ uint32_t wmax[kBlock / 32];
   __shared__ WarpListRing<false> rings[kBlock / 32];
+  const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
+  if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
-  stage_thresholds(thr, luts);
+  stage_lut(m4, sc.luts + LUT_M4 * UPF_LUT_ENTRIES);
+  stage_thresholds(thr, sc.luts);
   ring_init(rings[warp]);
   __syncthreads();
+  const DevParams& P = *sc.P;
+  DevState* st = sc.st;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t best = 0;
-  const bool active = i < n && type[i] == UPF_LIQUID;
+  const bool active = i < sc.end && type[i] == UPF_LIQUID;
   const uint32_t cnt = active ? ncnt[i] : 0u;
   const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
   const float4 xi = active ? xs[i] : make_float4(0, 0, 0, 0);
@@ -848,19 +902,26 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
 
 // ComputeCorrectivePressureForce (UnifiedPhysics.cpp:5493-5522), then the
 // prediction of the next iteration (PredictPositionAndVelocity).
+template <bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
-    DevParams P, uint32_t n, DynArrays B, const float4* __restrict__ spos, const __grid_constant__ CUtensorMap cmap,
-    const __grid_constant__ CUtensorMap bmap, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
-    const float* __restrict__ pq, const float4* __restrict__ force, float4* __restrict__ pforce,
-    float4* __restrict__ xs, DevState* __restrict__ st) {
+    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
+    const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap bmap,
+    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, const float* __restrict__ pq,
+    const float4* __restrict__ force, float4* __restrict__ pforce, float4* __restrict__ xs,
+    DevState* __restrict__ st_plain) {
+  __shared__ DevParams sP;
   __shared__ float pg[UPF_LUT_ENTRIES];
   __shared__ WarpListRing<true> rings[kBlock / 32];
+  const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
+  if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  stage_lut(pg, luts + LUT_PGRAD * UPF_LUT_ENTRIES);
+  stage_lut(pg, sc.luts + LUT_PGRAD * UPF_LUT_ENTRIES);
   ring_init(rings[warp]);
   __syncthreads();
+  const DevParams& P = *sc.P;
+  DevState* st = sc.st;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = i < n && B.type[i] == UPF_LIQUID;
+  const bool active = i < sc.end && B.type[i] == UPF_LIQUID;
   const uint32_t cnt = active ? ncnt[i] : 0u;
   const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
   const float4 xi = active ? B.pos[i] : make_float4(0, 0, 0, 0);
@@ -927,7 +988,7 @@ __global__ void k_step_init(DevState* st, int count_step) {
 // continue while iteration < min_loops, or the error is still too large and
 // iteration < max_loops. The "too large" flag is sticky-false, as in the
 // reference. Runs on the device and feeds the graph's conditional node.
-__global__ void k_loop_ctl(DevParams P, DevState* st, cudaGraphConditionalHandle h, int use_handle) {
+__device__ __forceinline__ int loop_ctl(const DevParams& P, DevState* st) {
   const int it = st->iteration + 1;
   st->iteration = it;
   const float maxd = __uint_as_float(st->max_rho_bits);
@@ -945,18 +1006,130 @@ __global__ void k_loop_ctl(DevParams P, DevState* st, cudaGraphConditionalHandle
     st->total_iterations += it;
     if (it >= P.max_loops) st->steps_at_max += 1;
   }
+  return cont;
+}
+
+__global__ void k_loop_ctl(DevParams P, DevState* st, cudaGraphConditionalHandle h, int use_handle) {
+  const int cont = loop_ctl(P, st);
   if (use_handle) cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------- batched scenes
+constexpr uint32_t kPadKey = kPadKeyBatch;
+
+// Set-up of a batch after upload: keys of every slot (particles: Morton key
+// in the scene's grid; padding: kPadKey) and the lagged PCISPH state.
+__global__ void __launch_bounds__(kBlock) k_batch_init(const BatchView bv, uint32_t nslots, DynArrays A,
+                                                        uint32_t* __restrict__ keys, int with_lag) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nslots) return;
+  const uint32_t s = bv.group_scene[i / kSegAlign];
+  if (i < bv.seg_end[s]) {
+    const DevParams& P = bv.params[s];
+    keys[i] = morton_key(A.pos[i], P.origin, P.scales);
+    if (with_lag) A.lag[i] = make_float4(0.0f, 0.0f, P.rho0, 0.0f);
+  } else {
+    keys[i] = kPadKey;
+  }
+}
+
+// Second sort stage key: the scene of the slot each element came from.
+__global__ void __launch_bounds__(kBlock) k_scene_digits(uint32_t nslots, const uint32_t* __restrict__ perm,
+                                                          const uint32_t* __restrict__ group_scene,
+                                                          uint32_t* __restrict__ digits) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nslots) digits[i] = group_scene[perm[i] / kSegAlign];
+}
+
+// Reorder of a batch: the gather of k_reorder, plus each slot's sorted key
+// (the scene's Morton key of the gathered position; kPadKey for padding).
+__global__ void __launch_bounds__(kBlock) k_reorder_batch(const BatchView bv, uint32_t nslots,
+                                                           const uint32_t* __restrict__ perm, DynArrays A,
+                                                           DynArrays B, uint32_t* __restrict__ keys) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nslots) return;
+  const uint32_t j = perm[i];
+  const float4 x = A.pos[j];
+  B.pos[i] = x;
+  B.vel[i] = A.vel[j];
+  B.id[i] = A.id[j];
+  B.type[i] = A.type[j];
+  B.lag[i] = A.lag[j];
+  const uint32_t s = bv.group_scene[i / kSegAlign];
+  const DevParams& P = bv.params[s];
+  keys[i] = i < bv.seg_end[s] ? morton_key(x, P.origin, P.scales) : kPadKey;
+}
+
+// Cell ranges of every scene into its own table (CalculateBlocksKernel,
+// particles_kernel.cu:693-726, per scene).
+__global__ void __launch_bounds__(kBlock) k_cell_ranges_batch(const BatchView bv, const uint32_t* __restrict__ seg_begin,
+                                                               uint32_t nslots, const uint32_t* __restrict__ keys,
+                                                               uint32_t* __restrict__ cstart,
+                                                               uint32_t* __restrict__ cend) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nslots) return;
+  const uint32_t s = bv.group_scene[i / kSegAlign];
+  const uint32_t b = seg_begin[s], e = bv.seg_end[s];
+  if (i >= e) return;
+  const int shift = 3 * (int)bv.params[s].block_shift;
+  const uint32_t c = keys[i] >> shift;
+  const uint32_t base = bv.cell_base[s];
+  if (i == b || (keys[i - 1] >> shift) != c) cstart[base + c] = i;
+  if (i + 1 == e || (keys[i + 1] >> shift) != c) cend[base + c] = i + 1;
+}
+
+__global__ void k_step_init_batch(DevState* st, uint32_t nscenes) {
+  for (uint32_t s = threadIdx.x; s < nscenes; s += blockDim.x) {
+    st[s].ke = 0;
+    st[s].mom[0] = st[s].mom[1] = st[s].mom[2] = 0;
+    st[s].max_neighbors = 0;
+  }
+}
+
+__global__ void k_loop_init_batch(DevState* st, uint32_t nscenes, int32_t* any_active) {
+  for (uint32_t s = threadIdx.x; s < nscenes; s += blockDim.x) {
+    st[s].iteration = 0;
+    st[s].too_large = 1;
+    st[s].max_rho_bits = 0;
+    st[s].loop_active = 1;
+  }
+  if (threadIdx.x == 0) *any_active = nscenes > 0;
+}
+
+// Loop control of every scene still iterating (each exactly as k_loop_ctl);
+// the while-node continues while any scene does.
+__global__ void k_loop_ctl_batch(const BatchView bv, uint32_t nscenes, int32_t* any_active,
+                                 cudaGraphConditionalHandle h, int use_handle) {
+  int any = 0;
+  for (uint32_t s = threadIdx.x; s < nscenes; s += blockDim.x) {
+    DevState* st = bv.st + s;
+    if (!st->loop_active) continue;
+    const int cont = loop_ctl(bv.params[s], st);
+    st->loop_active = cont;
+    any |= cont;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    *any_active = any;
+    if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
+  }
 }
 
 // Integration for PCISPH: force + pressure force (UnifiedPhysics.cpp:3710-3712),
 // and the lagged pressure state carried to the next step.
+template <bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_pcisph_integrate(
-    DevParams P, uint32_t n, DynArrays B, DynArrays A, uint32_t* __restrict__ keysA,
-    const float4* __restrict__ force, const float4* __restrict__ pforce, const float* __restrict__ rho,
-    const float* __restrict__ press, DevState* __restrict__ st) {
+    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B, DynArrays A,
+    uint32_t* __restrict__ keysA, const float4* __restrict__ force, const float4* __restrict__ pforce,
+    const float* __restrict__ rho, const float* __restrict__ press, DevState* __restrict__ st_plain) {
+  __shared__ DevParams sP;
+  const Scope sc = enter_scope<kBatch>(Pk, nullptr, st_plain, n, bv, &sP, false);
+  if (kBatch) __syncthreads();
+  const DevParams& P = *sc.P;
+  DevState* st = sc.st;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0, mx = 0, my = 0, mz = 0;
-  if (i < n) {
+  if (i < sc.end) {
     const int32_t ti = B.type[i];
     const float4 xi = B.pos[i], vi = B.vel[i];
     const float4 lag = B.lag[i];
@@ -982,6 +1155,8 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_integrate(
     }
     A.id[i] = B.id[i];
     A.type[i] = ti;
+  } else if (kBatch && i < n) {
+    keysA[i] = kPadKeyBatch;  // padding slots sort after the scene's particles
   }
   if (!(ke == ke)) {
     atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
@@ -1070,7 +1245,7 @@ cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
   if (n == 0) return cudaGetLastError();
-  k_build_nlist<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
+  k_build_nlist<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
                                                 s.skeys, s.sstart, s.send, s.nbr, s.bins, s.ncnt, s.luts, s.st);
   return cudaGetLastError();
 }
@@ -1082,7 +1257,7 @@ cudaError_t launch_force_phase(System& s, cudaStream_t st) {
     k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.bins, s.ncnt, s.luts, s.rho,
                                                    s.press);
   } else {
-    k_pcisph_external<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.wvol, s.rb.id_body, s.nbr, s.ncnt, s.luts,
+    k_pcisph_external<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B, s.wvol, s.rb.id_body, s.nbr, s.ncnt, s.luts,
                                                      s.force, s.pforce, s.xs, s.press, s.pq, s.st);
   }
   return cudaGetLastError();
@@ -1096,7 +1271,7 @@ cudaError_t launch_loop_init(System& s, cudaStream_t st) {
 cudaError_t launch_loop_density(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.type, s.xs, s.nbr_map, s.ncnt, s.luts, s.rho,
+    k_pcisph_density<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B.type, s.xs, s.nbr_map, s.ncnt, s.luts, s.rho,
                                                     s.press, s.pq, s.st);
   return cudaGetLastError();
 }
@@ -1104,7 +1279,7 @@ cudaError_t launch_loop_density(System& s, cudaStream_t st) {
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_pressure_force<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.spos, s.nbr_map, s.bins_map, s.ncnt,
+    k_pcisph_pressure_force<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B, s.nbr_map, s.bins_map, s.ncnt,
                                                            s.luts, s.pq, s.force, s.pforce, s.xs, s.st);
   return cudaGetLastError();
 }
@@ -1132,7 +1307,7 @@ cudaError_t launch_integrate_phase(System& s, cudaStream_t st) {
     k_wcsph_force_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.nbr, s.bins, s.ncnt,
                                                            s.luts, s.rho, s.press, s.force, s.st);
   } else {
-    k_pcisph_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.force, s.pforce, s.rho, s.press,
+    k_pcisph_integrate<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B, s.A, s.keysA, s.force, s.pforce, s.rho, s.press,
                                                       s.st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1153,6 +1328,87 @@ cudaError_t launch_static_setup(System& s, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   k_static_wvol<<<grid_of(ns), kBlock, 0, st>>>(s.dp, ns, s.spos, s.sstart, s.send, s.luts,
                                                  s.wvol + s.dp.static_base);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------- batched launchers
+cudaError_t batch_launch_init(BatchSystem& b, cudaStream_t st) {
+  if (!b.n_slots) return cudaSuccess;
+  k_batch_init<<<grid_of(b.n_slots), kBlock, 0, st>>>(b.view, b.n_slots, b.A, b.keysA, 1);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_keys(BatchSystem& b, cudaStream_t st) {
+  if (!b.n_slots) return cudaSuccess;
+  k_batch_init<<<grid_of(b.n_slots), kBlock, 0, st>>>(b.view, b.n_slots, b.A, b.keysA, 0);
+  return cudaGetLastError();
+}
+
+// Two stable LSD stages: the Morton keys (padding above them), then the
+// scene index; each scene's particles end up in its own segment in Morton
+// order, exactly the order a sort of that scene alone gives.
+cudaError_t batch_launch_sort(BatchSystem& b, cudaStream_t st) {
+  const uint32_t n = b.n_slots;
+  if (!n) return cudaSuccess;
+  uint32_t* kalt = b.sort_tmp;
+  uint32_t* valt = kalt + ((n + 63) & ~63u);
+  uint32_t* counts = valt + ((n + 63) & ~63u);
+  cudaError_t e = radix_sort_pairs(b.keysA, b.perm, kalt, valt, counts, n, 31, true, st);
+  if (e != cudaSuccess) return e;
+  k_scene_digits<<<grid_of(n), kBlock, 0, st>>>(n, b.perm, b.group_scene_d, b.digits);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  e = radix_sort_pairs(b.digits, b.perm, kalt, valt, counts, n, b.scene_bits, false, st);
+  if (e != cudaSuccess) return e;
+  k_reorder_batch<<<grid_of(n), kBlock, 0, st>>>(b.view, n, b.perm, b.A, b.B, b.keysA);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(b.cstart, 0, sizeof(uint32_t) * b.n_cells, st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(b.cend, 0, sizeof(uint32_t) * b.n_cells, st)) != cudaSuccess) return e;
+  k_cell_ranges_batch<<<grid_of(n), kBlock, 0, st>>>(b.view, b.seg_begin_d, n, b.keysA, b.cstart, b.cend);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_neighbors(BatchSystem& b, cudaStream_t st) {
+  const uint32_t n = b.n_slots;
+  k_step_init_batch<<<1, 256, 0, st>>>(b.st_d, b.n_scenes);
+  if (!n) return cudaGetLastError();
+  k_build_nlist<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B.pos, b.keysA, b.cstart, b.cend, 0u,
+                                                     nullptr, nullptr, nullptr, nullptr, b.nbr, b.bins, b.ncnt,
+                                                     nullptr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_forces(BatchSystem& b, cudaStream_t st) {
+  const uint32_t n = b.n_slots;
+  if (!n) return cudaSuccess;
+  k_pcisph_external<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B, nullptr, nullptr, b.nbr,
+                                                         b.ncnt, nullptr, b.force, b.pforce, b.xs, b.press, b.pq,
+                                                         nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st) {
+  k_loop_init_batch<<<1, 256, 0, st>>>(b.st_d, b.n_scenes, b.any_active_d);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle) {
+  const uint32_t n = b.n_slots;
+  if (n) {
+    k_pcisph_density<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B.type, b.xs, b.nbr_map, b.ncnt,
+                                                          nullptr, b.rho, b.press, b.pq, nullptr);
+    k_pcisph_pressure_force<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B, b.nbr_map, b.bins_map,
+                                                                 b.ncnt, nullptr, b.pq, b.force, b.pforce, b.xs,
+                                                                 nullptr);
+  }
+  k_loop_ctl_batch<<<1, 1024, 0, st>>>(b.view, b.n_scenes, b.any_active_d, h, use_handle ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_integrate(BatchSystem& b, cudaStream_t st) {
+  const uint32_t n = b.n_slots;
+  if (!n) return cudaSuccess;
+  k_pcisph_integrate<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B, b.A, b.keysA, b.force,
+                                                          b.pforce, b.rho, b.press, nullptr);
   return cudaGetLastError();
 }
 

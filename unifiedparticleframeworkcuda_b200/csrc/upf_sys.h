@@ -51,6 +51,23 @@ struct RigidArrays {
   uint32_t* entry_slot = nullptr; // list entry -> current sorted index (set after each sort)
 };
 
+// Batched scenes (upf_batch_*): independent scenes in one index space, each
+// in its own segment that starts on a kSegAlign boundary, so every CTA of a
+// kernel over that space (CTA sizes dividing kSegAlign) belongs to one scene.
+// A CTA finds its scene in `group_scene`, and takes the scene's parameters,
+// tables, device state and particle range from the tables below.
+constexpr uint32_t kSegAlign = 256;
+constexpr uint32_t kLutFloats = 5 * UPF_LUT_ENTRIES + kThresholds;
+
+struct BatchView {
+  const DevParams* params = nullptr;     // [scenes]
+  const float* luts = nullptr;           // [scenes][kLutFloats]
+  DevState* st = nullptr;                // [scenes]
+  const uint32_t* group_scene = nullptr; // [slots / kSegAlign]
+  const uint32_t* seg_end = nullptr;     // [scenes] exclusive end of the scene's particles
+  const uint32_t* cell_base = nullptr;   // [scenes] offset of the scene's cell table
+};
+
 struct System {
   upf_params prm{};
   DevParams dp{};
@@ -120,6 +137,80 @@ struct System {
   std::vector<void*> checkpoint_slots;  // device copies of the dynamic state (upf_checkpoint);
                                         // dropped when particles or bodies are set
 };
+
+// The state behind one upf_batch handle: every array spans the batch's slot
+// space (scene s owns slots [seg_begin[s], seg_begin[s] + padded count), its
+// particles in [seg_begin[s], seg_end[s]), the rest padding that sorts last).
+struct BatchSystem {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint32_t n_scenes = 0, n_slots = 0, n_particles = 0;
+  std::vector<upf_params> prm;
+  std::vector<uint32_t> count, seg_begin, seg_end, cell_base;
+  uint32_t n_cells = 0;       // sum of the scenes' cell tables
+  uint32_t list_rows = 0;     // neighbour-list capacity (max over scenes)
+  int scene_bits = 1;         // key bits of the scene index (second sort stage)
+  bool have_particles = false;
+
+  DynArrays A, B;
+  uint32_t* keysA = nullptr;
+  uint32_t* perm = nullptr;
+  uint32_t* digits = nullptr;  // second sort stage keys (scene of each element)
+  uint32_t* sort_tmp = nullptr;
+  float4* force = nullptr;
+  float4* pforce = nullptr;
+  float4* xs = nullptr;
+  float* rho = nullptr;
+  float* press = nullptr;
+  float* pq = nullptr;
+  uint32_t* nbr = nullptr;
+  uint16_t* bins = nullptr;
+  uint32_t* ncnt = nullptr;
+  CUtensorMap nbr_map;
+  CUtensorMap bins_map;
+  uint32_t* cstart = nullptr;
+  uint32_t* cend = nullptr;
+
+  DevParams* params_d = nullptr;
+  float* luts_d = nullptr;
+  DevState* st_d = nullptr;
+  DevState* st_h = nullptr;        // pinned mirror [n_scenes]
+  uint32_t* group_scene_d = nullptr;
+  uint32_t* seg_begin_d = nullptr;
+  uint32_t* seg_end_d = nullptr;
+  uint32_t* cell_base_d = nullptr;
+  int32_t* any_active_d = nullptr; // host-driven loop: any scene still iterating
+  BatchView view;
+
+  cudaGraphExec_t step_exec = nullptr;
+  cudaGraph_t step_graph = nullptr;
+  std::vector<void*> allocations;
+  std::vector<void*> checkpoint_slots;
+};
+
+// upf_pipeline.cu: batched phase launchers (asynchronous on `st`)
+cudaError_t batch_launch_init(BatchSystem& b, cudaStream_t st);   // keys and lagged state after upload
+cudaError_t batch_launch_keys(BatchSystem& b, cudaStream_t st);   // keys only
+cudaError_t batch_launch_sort(BatchSystem& b, cudaStream_t st);
+cudaError_t batch_launch_neighbors(BatchSystem& b, cudaStream_t st);
+cudaError_t batch_launch_forces(BatchSystem& b, cudaStream_t st);
+cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st);
+cudaError_t batch_launch_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle);
+cudaError_t batch_launch_integrate(BatchSystem& b, cudaStream_t st);
+
+// upf_api.cu: one step as a CUDA graph, `loop` (if given) under a
+// conditional while-node between `pre` and `post`
+struct GraphParts {
+  cudaError_t (*pre)(void* ctx, cudaStream_t st) = nullptr;
+  cudaError_t (*loop)(void* ctx, cudaStream_t st, cudaGraphConditionalHandle h) = nullptr;
+  cudaError_t (*post)(void* ctx, cudaStream_t st) = nullptr;
+  void* ctx = nullptr;
+};
+upf_status capture_step_graph(const GraphParts& parts, cudaGraph_t* graph_out, cudaGraphExec_t* exec_out);
+DevParams make_dev_params(const upf_params& p, uint32_t nstride);
+upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint32_t elem_bytes,
+                           uint64_t cols, uint64_t rows);
 
 // upf_rigid.cu: list entry -> sorted index after a sort; body force/torque,
 // body integration and rigid particle sync after integration

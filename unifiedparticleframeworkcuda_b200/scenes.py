@@ -315,6 +315,54 @@ def coupling_scene(fluid=(128, 64, 64), granular=(64, 32, 64), n_bodies=16, seed
     return Scene("coupling_%d" % fl.shape[0], p, pos, vel, np.concatenate(typ), np.concatenate(body), n_bodies)
 
 
+def batch_scene(n, extent, seed, stream=0) -> Scene:
+    """One scene of a batch: n liquid particles in a lattice block (jitter
+    +-10% of the spacing) filling the lower half (in x) of a box of the given
+    extents, walls by the collision box and penalty forces. The spacing
+    follows from n and the box; h = 2 * spacing, dt = 5e-4 * spacing / 0.01
+    (clamped to [1e-4, 2e-3]), the Morton grid spans the box."""
+    lx, ly, lz = (float(v) for v in extent)
+    s = (0.5 * lx * 0.8 * ly * lz / n) ** (1.0 / 3.0)
+    nx = max(1, int(0.5 * lx / s))
+    nz = max(1, int(lz / s) - 1)
+    ny = int(np.ceil(n / (nx * nz)))
+    while ny * s > 0.95 * ly - 2 * s and s > 1e-4:  # keep the block inside the box
+        s *= 0.97
+        nx = max(1, int(0.5 * lx / s))
+        nz = max(1, int(lz / s) - 1)
+        ny = int(np.ceil(n / (nx * nz)))
+    p = default_params()
+    p.method = METHOD_PCISPH
+    p.flags = FLAG_SURFACE_TENSION | FLAG_PENALTY_WALLS
+    p.particle_spacing = s
+    p.support_radius = 2.0 * s
+    p.dt = float(np.clip(5e-4 * s / 0.01, 1e-4, 2e-3))
+    p.viscosity = 1.0
+    lo = np.array([2 * s, 2 * s, 2 * s])
+    hi = lo + np.array([lx, ly, lz])
+    _set_box(p, lo, hi)
+    ext = max(lx, ly, lz) + 4 * s
+    p.zindex_extent[:] = (ext, ext, ext)
+    pts = _lattice(nx, ny, nz, s, lo + s, 0.1 * s, seed, stream)
+    # lattice order is x-major: keep the first n in y-layers from the bottom
+    order = np.lexsort((pts[:, 2], pts[:, 0], pts[:, 1]))
+    fluid = pts[order[:n]]
+    return _pack("batch_%d" % n, p, fluid, np.zeros((0, 3)))
+
+
+def batch_scenes(num=256, seed=2024, counts=(2048, 65536), extents=(0.5, 2.0)) -> list:
+    """A batch of independent scenes: particle counts log-uniform in `counts`,
+    box extents uniform in `extents` per axis, from the seed."""
+    u = uniform(seed, 4 * num, stream=7).reshape(num, 4)
+    lo, hi = np.log(counts[0]), np.log(counts[1])
+    out = []
+    for k in range(num):
+        n = int(round(np.exp(lo + (hi - lo) * u[k, 0])))
+        ext = extents[0] + (extents[1] - extents[0]) * u[k, 1:4]
+        out.append(batch_scene(n, ext, seed + 17 * k, stream=k + 1))
+    return out
+
+
 def small_coupling(seed=5) -> Scene:
     """A small coupling scene (oracle-sized): 12^3 fluid, an 8x4x8 pile and
     three small bodies."""
