@@ -178,6 +178,19 @@ def run_reference(args, rank, world):
     reference's UnifiedPhysics.cpp does not compile here) on the host cores."""
     if rank != 0:
         return
+    if args.scene == "c4":
+        from unifiedparticleframeworkcuda_b200 import scenes
+        cb = batch_cpu_baseline(scenes.batch_scenes(args.batch_scenes), args.cpu_seconds)
+        print(json.dumps({
+            "impl": "reference", "metric": "batched scene-steps/s (256 PCISPH scenes, 2k-65k particles) vs "
+                                          "sequential single-scene steps",
+            "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / cb["value"] * args.batch_scenes, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched_pcisph_256_scenes"}, "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
+        return
     from oracle import pyoracle
     pyoracle.build(with_ref=False)
     # bounded sample per step: a smaller block of the workload
@@ -205,6 +218,176 @@ def run_reference(args, rank, world):
                                                                               sc.n_boundary)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def batch_cpu_baseline(scs, seconds):
+    """The oracle on a bounded sample of the batch (every 64th scene), as
+    particle-steps/s converted to scene-steps/s by the batch's mean scene size."""
+    from oracle import pyoracle
+    pyoracle.build(with_ref=False)
+    threads = os.cpu_count() or 1
+    sample = scs[::64]
+    sims = [make_oracle(sc, threads) for sc in sample]
+    for o in sims:
+        o.step()
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        for o in sims:
+            o.step()
+        steps += 1
+        if time.perf_counter() - t0 >= seconds and steps >= 2:
+            break
+    dt = time.perf_counter() - t0
+    for o in sims:
+        o.close()
+    nsample = sum(sc.n for sc in sample)
+    pps = nsample * steps / dt
+    mean_n = sum(sc.n for sc in scs) / len(scs)
+    return {"value": pps / mean_n, "unit": "scene-steps/s", "cores": threads, "kind": "port",
+            "sample": "%d of %d scenes (%d particles), %d steps, %.1f s: %.3g particle-steps/s over the batch's "
+                      "mean scene size %.0f" % (len(sample), len(scs), nsample, steps, dt, pps, mean_n)}
+
+
+def run_batch(args, rank, world, local_rank):
+    """--scene c4: the batched form. 256 scenes (log-uniform 2,048-65,536
+    particles, box extents U(0.5, 2.0)) advance together; the baseline is the
+    same scenes as 256 single-scene systems stepped one after another."""
+    import ctypes as C
+
+    import torch
+    import unifiedparticleframeworkcuda_b200 as upf
+    from unifiedparticleframeworkcuda_b200 import build as upfbuild
+    from unifiedparticleframeworkcuda_b200 import scenes
+
+    if rank == 0:
+        upfbuild.build()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    scs = scenes.batch_scenes(args.batch_scenes, seed=2024 + rank)
+    ns = len(scs)
+    npart = sum(sc.n for sc in scs)
+    stream = torch.cuda.Stream(device=dev)
+    b = upf.ParticleBatch.from_scenes(scs, device=local_rank)
+    b.set_stream(stream.cuda_stream)
+    b.step(args.warmup)
+    b.synchronize()
+    b.reset_counters()
+    b.checkpoint(0)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def timed(fn, clk=None):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    with ClockSampler(local_rank) as clk:
+        batch_ms = timed(lambda: b.step(args.steps))
+    b.synchronize()
+    stats = b.stats()
+    its = [st.total_iterations / max(st.total_steps, 1) for st in stats]
+    errs = [st.density_error_percent for st in stats]
+    value = ns * args.steps * world / (batch_ms / 1e3)
+
+    # per-pass timings of one step (dominant kernel: the loop passes)
+    prof, act = b.profile_step()
+    dens_gbs = 28.0 * act / (prof.density_ms_total / 1e3) / 1e9
+    pf_gbs = 84.0 * act / (prof.pforce_ms_total / 1e3) / 1e9
+    try:
+        peak, peak_src = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    if prof.pforce_ms_total >= prof.density_ms_total:
+        kname, achieved, kms = "k_pcisph_pressure_force<batched>", pf_gbs, prof.pforce_ms_total
+    else:
+        kname, achieved, kms = "k_pcisph_density<batched>", dens_gbs, prof.density_ms_total
+
+    # end to end: per step, upload all scenes' state (pinned host), step, read it back
+    b.restore(0)
+    hp = torch.empty((npart, 4), dtype=torch.float32, pin_memory=True)
+    hv = torch.empty((npart, 4), dtype=torch.float32, pin_memory=True)
+    L = upf.lib()
+    fp = C.POINTER(C.c_float)
+    upf.check(L.upf_batch_download_state(b.handle, C.cast(hp.data_ptr(), fp), C.cast(hv.data_ptr(), fp)), "dl")
+
+    def e2e_steps():
+        for _ in range(args.steps):
+            upf.check(L.upf_batch_upload_state(b.handle, C.cast(hp.data_ptr(), fp), C.cast(hv.data_ptr(), fp)), "ul")
+            b.step(1)
+            upf.check(L.upf_batch_download_state(b.handle, C.cast(hp.data_ptr(), fp), C.cast(hv.data_ptr(), fp)),
+                      "dl")
+
+    e2e_ms = timed(e2e_steps)
+    b.close()
+
+    # baseline: the same scenes as single-scene systems, one after another
+    systems = []
+    for sc in scs:
+        p = upf.derive_params(sc.params)
+        s = upf.ParticleSystem(p, capacity=sc.n, device=local_rank, derive=False)
+        s.set_stream(stream.cuda_stream)
+        s.set_particles(sc.pos, sc.vel, sc.type)
+        systems.append(s)
+    for s in systems:
+        s.step(args.warmup)
+    torch.cuda.synchronize()
+
+    def seq():
+        for _ in range(args.steps):
+            for s in systems:
+                s.step(1)
+
+    seq_ms = timed(seq)
+    for s in systems:
+        s.synchronize()
+        s.close()
+    seq_value = ns * args.steps * world / (seq_ms / 1e3)
+    if rank != 0:
+        return
+    radix = lambda bits: 3 * ((bits + 7) // 8)  # noqa: E731
+    per_step = radix(31) + 1 + radix(8) + 1 + 1 + 1 + 1 + 1 + 1 + 1  # sort, digits, reorder, cells, inits, nlist, ext, integrate
+    max_it = max(st.total_iterations for st in stats)
+    out = {
+        "metric": "batched scene-steps/s (256 PCISPH scenes, 2k-65k particles) vs sequential single-scene steps",
+        "value": value, "unit": "scene-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": batch_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched_pcisph_256_scenes", "scenes": ns, "particles": npart,
+                   "mean_iterations_per_scene": float(np.mean(its)), "max_iterations_per_scene": float(np.max(its)),
+                   "max_density_error_percent_last_step": float(np.max(errs)),
+                   "particle_steps_per_s": npart * args.steps * world / (batch_ms / 1e3),
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (neighbour lists %.0f MB)" % (npart * 128 * 6 / 1e6)},
+        "sequential_single_scene": {"value": seq_value, "unit": "scene-steps/s", "ms_per_step": seq_ms / args.steps,
+                                    "speedup_of_batched": value / seq_value},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "traffic": None, "kernel_ms_per_step": kms,
+                     "loop_particle_passes": act},
+        "phases_ms": {"sort": prof.sort_ms, "neighbors": prof.neighbors_ms, "forces": prof.forces_ms,
+                      "loop": prof.loop_ms, "integrate": prof.integrate_ms, "iterations": prof.iterations},
+        "e2e": {"value": ns * args.steps * world / (e2e_ms / 1e3), "unit": "scene-steps/s",
+                "h2d_bytes_per_step": npart * 32, "d2h_bytes_per_step": npart * 32},
+        "gpu_launches": args.steps * per_step + 3 * max_it,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = batch_cpu_baseline(scs, args.cpu_seconds)
+    print(json.dumps(out), flush=True)
 
 
 def run_ours(args, rank, world, local_rank):
@@ -394,7 +577,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3"])
+    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3", "c4"])
+    ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--block-size", type=int, default=0)
     ap.add_argument("--settle", type=int, default=0,
                     help="untimed steps before the warm-up, e.g. 300 to time steps after the dam's initial "
@@ -417,7 +601,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.scene == "c4":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch

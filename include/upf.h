@@ -394,6 +394,11 @@ upf_status upf_batch_restore(upf_batch* b, int32_t slot);
  * batch's current device order per scene. */
 upf_status upf_batch_upload_state(upf_batch* b, const float* pos4, const float* vel4);
 upf_status upf_batch_download_state(upf_batch* b, float* pos4, float* vel4);
+/* One batch step through its passes with CUDA events (as upf_profile_step);
+ * iterations = the largest scene's count; *active_particle_iterations (may be
+ * NULL) = the sum over loop iterations of the particles of the scenes still
+ * iterating, i.e. the particles the loop passes processed. */
+upf_status upf_batch_profile_step(upf_batch* b, upf_phase_times* out, uint64_t* active_particle_iterations);
 
 /* ---- errors ------------------------------------------------------------- */
 const char* upf_last_error(void);

@@ -82,6 +82,7 @@ def lib():
             "upf_batch_restore": [vp, C.c_int32],
             "upf_batch_upload_state": [vp, fp, fp],
             "upf_batch_download_state": [vp, fp, fp],
+            "upf_batch_profile_step": [vp, C.POINTER(UpfPhaseTimes), C.POINTER(C.c_uint64)],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
             "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
             "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],
@@ -402,6 +403,13 @@ class ParticleBatch:
 
     def restore(self, slot: int = 0):
         check(lib().upf_batch_restore(self._h, int(slot)), "upf_batch_restore")
+
+    def profile_step(self):
+        """(phase times of one step, particles processed by the loop passes)."""
+        t = UpfPhaseTimes()
+        act = C.c_uint64()
+        check(lib().upf_batch_profile_step(self._h, C.byref(t), C.byref(act)), "upf_batch_profile_step")
+        return t, int(act.value)
 
     def particles(self, scene: int):
         n = int(self.counts[scene])

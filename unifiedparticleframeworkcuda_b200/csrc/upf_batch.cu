@@ -540,4 +540,71 @@ upf_status upf_batch_download_state(upf_batch* b, float* pos4, float* vel4) {
   return UPF_OK;
 }
 
+upf_status upf_batch_profile_step(upf_batch* b, upf_phase_times* out, uint64_t* active_particle_iterations) {
+  UPF_TRY(batch_guard(b, "upf_batch_profile_step"));
+  if (!out) {
+    set_error("upf_batch_profile_step: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  std::memset(out, 0, sizeof(*out));
+  cudaStream_t st = b->stream;
+  cudaEvent_t ev[8];
+  for (auto& e : ev) UPF_CUDA(cudaEventCreate(&e));
+  auto elapsed = [&](cudaEvent_t x, cudaEvent_t y) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, x, y);
+    return ms;
+  };
+  uint64_t active = 0;
+  std::vector<DevState> h(b->n_scenes);
+  UPF_CUDA(cudaEventRecord(ev[0], st));
+  UPF_CUDA(batch_launch_sort(*b, st));
+  UPF_CUDA(cudaEventRecord(ev[1], st));
+  UPF_CUDA(batch_launch_neighbors(*b, st));
+  UPF_CUDA(cudaEventRecord(ev[2], st));
+  UPF_CUDA(batch_launch_forces(*b, st));
+  UPF_CUDA(cudaEventRecord(ev[3], st));
+  UPF_CUDA(batch_launch_loop_init(*b, st));
+  UPF_CUDA(cudaStreamSynchronize(st));
+  out->sort_ms = elapsed(ev[0], ev[1]);
+  out->neighbors_ms = elapsed(ev[1], ev[2]);
+  out->forces_ms = elapsed(ev[2], ev[3]);
+  int launches = 4 + 1 + 4 + 1 + 1 + 2 + 1 + 1 + 1;  // sort stages, digits, reorder, cells, init, nlist, ext, loop init
+  float loop = 0;
+  for (int it = 0; it < 4096; ++it) {
+    // scenes still iterating before this iteration
+    UPF_CUDA(cudaMemcpyAsync(h.data(), b->st_d, sizeof(DevState) * b->n_scenes, cudaMemcpyDeviceToHost, st));
+    UPF_CUDA(cudaStreamSynchronize(st));
+    uint64_t act = 0;
+    for (uint32_t s = 0; s < b->n_scenes; ++s)
+      if (h[s].loop_active) act += b->count[s];
+    if (!act) break;
+    active += act;
+    UPF_CUDA(cudaEventRecord(ev[4], st));
+    UPF_CUDA(batch_launch_loop_density(*b, st));
+    UPF_CUDA(cudaEventRecord(ev[5], st));
+    UPF_CUDA(batch_launch_loop_pforce(*b, st));
+    UPF_CUDA(cudaEventRecord(ev[6], st));
+    UPF_CUDA(batch_launch_loop_ctl(*b, st));
+    UPF_CUDA(cudaEventRecord(ev[7], st));
+    UPF_CUDA(cudaStreamSynchronize(st));
+    UPF_CUDA(cudaGetLastError());
+    out->density_ms_total += elapsed(ev[4], ev[5]);
+    out->pforce_ms_total += elapsed(ev[5], ev[6]);
+    loop += elapsed(ev[4], ev[7]);
+    out->iterations = it + 1;
+    launches += 3;
+  }
+  out->loop_ms = loop;
+  UPF_CUDA(cudaEventRecord(ev[0], st));
+  UPF_CUDA(batch_launch_integrate(*b, st));
+  UPF_CUDA(cudaEventRecord(ev[1], st));
+  UPF_CUDA(cudaStreamSynchronize(st));
+  out->integrate_ms = elapsed(ev[0], ev[1]);
+  out->launches = launches + 1;
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (active_particle_iterations) *active_particle_iterations = active;
+  return batch_check_errors(b);
+}
+
 }  // extern "C"

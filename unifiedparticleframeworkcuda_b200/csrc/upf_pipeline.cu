@@ -1391,17 +1391,33 @@ cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t batch_launch_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle) {
+cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
-  if (n) {
+  if (n)
     k_pcisph_density<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B.type, b.xs, b.nbr_map, b.ncnt,
                                                           nullptr, b.rho, b.press, b.pq, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st) {
+  const uint32_t n = b.n_slots;
+  if (n)
     k_pcisph_pressure_force<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B, b.nbr_map, b.bins_map,
                                                                  b.ncnt, nullptr, b.pq, b.force, b.pforce, b.xs,
                                                                  nullptr);
-  }
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_loop_ctl(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle) {
   k_loop_ctl_batch<<<1, 1024, 0, st>>>(b.view, b.n_scenes, b.any_active_d, h, use_handle ? 1 : 0);
   return cudaGetLastError();
+}
+
+cudaError_t batch_launch_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle) {
+  cudaError_t e = batch_launch_loop_density(b, st);
+  if (e == cudaSuccess) e = batch_launch_loop_pforce(b, st);
+  if (e == cudaSuccess) e = batch_launch_loop_ctl(b, st, h, use_handle);
+  return e;
 }
 
 cudaError_t batch_launch_integrate(BatchSystem& b, cudaStream_t st) {

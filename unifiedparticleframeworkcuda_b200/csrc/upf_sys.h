@@ -197,6 +197,10 @@ cudaError_t batch_launch_neighbors(BatchSystem& b, cudaStream_t st);
 cudaError_t batch_launch_forces(BatchSystem& b, cudaStream_t st);
 cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st);
 cudaError_t batch_launch_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle);
+cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st);
+cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st);
+cudaError_t batch_launch_loop_ctl(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h = 0,
+                                  bool use_handle = false);
 cudaError_t batch_launch_integrate(BatchSystem& b, cudaStream_t st);
 
 // upf_api.cu: one step as a CUDA graph, `loop` (if given) under a
