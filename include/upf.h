@@ -147,7 +147,13 @@ typedef struct upf_params {
 
   /* Capacity */
   uint32_t max_neighbors;       /* per-particle neighbour list capacity (0 => 128) */
-  uint32_t reserved[7];
+  /* Neighbour search cell edge (grid units, power of two, >= 4). The lists
+   * hold exactly the particles within h, in ascending sorted order, whatever
+   * the cell size; a cell finer than block_size visits fewer candidates at a
+   * higher cost per cell. A query box may span at most 4 cells per axis.
+   * 0 => derived: block_size. */
+  uint32_t search_cell;
+  uint32_t reserved[6];
 } upf_params;
 
 /* Per-step statistics (the reference prints these; here they are returned). */
@@ -308,7 +314,10 @@ upf_status upf_get_step_fields(upf_system* s, float* force4, float* pforce4,
  * ids: counts[n], lists[n * cap] (row-major, first counts[i] valid). */
 upf_status upf_get_neighbors(upf_system* s, uint32_t* counts, uint32_t* lists_ids,
                              uint32_t cap, uint32_t* n_out);
-/* Sorted keys and cell ranges of the dynamic set (after upf_phase_sort). */
+/* Sorted keys and cell ranges of the dynamic set (after upf_phase_sort).
+ * The cell table has one entry per search cell, (1024 / search_cell)^3;
+ * start/end must hold that many entries: call with NULL arrays to get the
+ * count in *ncells_out first. */
 upf_status upf_get_sorted_keys(upf_system* s, uint32_t* keys, uint32_t* ids, uint32_t* n_out);
 upf_status upf_get_cell_ranges(upf_system* s, uint32_t* start, uint32_t* end, uint32_t* ncells_out);
 /* Rigid body state (RigidBody::rigidbody_pos / velocity / angular_velocity /

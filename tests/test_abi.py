@@ -77,6 +77,10 @@ def test_host_params_match_oracle(upf_lib, oracle_lib):
         a = upf_lib.derive_params(sc.params).as_dict()
         b = oracle_lib.derive(sc.params).as_dict()
         da, db = a.pop("density_error_factor"), b.pop("density_error_factor")
+        # the neighbour-search cell is the library's own (the lists do not depend on it)
+        cell = a.pop("search_cell")
+        b.pop("search_cell")
+        assert cell >= 4 and cell & (cell - 1) == 0 and cell <= a["block_size"]
         assert a == b
         # FP64 accumulation in the library vs the FP32 restatement
         assert abs(da - db) <= 1e-5 * max(abs(db), 1e-30)

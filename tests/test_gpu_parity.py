@@ -53,9 +53,11 @@ def test_sort_order_keys_and_cells_bit_exact(upf_lib, oracle_lib, scene):
     dyn = st["type"] != 6
     assert np.array_equal(ids, st["id"][dyn]), "sort order differs"
     assert np.array_equal(keys, st["key"][dyn]), "Morton keys differ"
-    # cell ranges = the reference's BoxQuery blocks: keys [c*bs^3, (c+1)*bs^3)
+    # cell ranges of the search cells (aligned Morton blocks): keys [c*cs^3, (c+1)*cs^3)
     start, end = sysm.cell_ranges()
-    bs3 = int(p.block_size) ** 3
+    cs = int(p.search_cell)
+    assert start.shape[0] == (1024 // cs) ** 3 and cs <= int(p.block_size)
+    bs3 = cs ** 3
     k = st["key"][dyn].astype(np.int64)
     occupied = np.unique(k // bs3)
     want_s = np.searchsorted(k, occupied * bs3, side="left")

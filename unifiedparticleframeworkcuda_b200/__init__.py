@@ -316,8 +316,9 @@ class ParticleSystem:
         return keys, ids
 
     def cell_ranges(self):
-        bpa = 1024 // int(self.params.block_size)
-        nc = bpa ** 3
+        cnt = C.c_uint32()
+        check(lib().upf_get_cell_ranges(self._h, None, None, C.byref(cnt)), "upf_get_cell_ranges")
+        nc = int(cnt.value)
         start = np.zeros(nc, np.uint32)
         end = np.zeros(nc, np.uint32)
         cnt = C.c_uint32()

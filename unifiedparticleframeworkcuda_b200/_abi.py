@@ -78,7 +78,8 @@ class UpfParams(C.Structure):
         ("container_min", F3),
         ("container_max", F3),
         ("max_neighbors", C.c_uint32),
-        ("reserved", C.c_uint32 * 7),
+        ("search_cell", C.c_uint32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
     def copy(self):

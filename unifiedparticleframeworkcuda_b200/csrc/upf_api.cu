@@ -114,13 +114,7 @@ DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   d.wmin = make_float3(p.container_min[0], p.container_min[1], p.container_min[2]);
   d.wmax = make_float3(p.container_max[0], p.container_max[1], p.container_max[2]);
   d.block_shift = log2u(p.block_size);
-  d.blocks_per_axis = UPF_GRID_RESOLUTION / p.block_size;
-  {
-    // a member's query box reaches r + 1 grid units past its cell (r = scales * h,
-    // the +1 covering the truncation of the grid coordinate)
-    float r = std::max(p.scales[0], std::max(p.scales[1], p.scales[2])) * p.support_radius;
-    d.nb_radius = (int32_t)std::ceil((double)(r + 1.0f) / (double)p.block_size);
-  }
+  d.cell_shift = log2u(effective_search_cell(p));
   d.flags = p.flags;
   d.maxn = p.max_neighbors;
   d.nstride = nstride;
@@ -425,7 +419,7 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   s->capacity = capacity;
   s->nstride = (capacity + 31) & ~31u;
   s->dp = make_dev_params(*p, s->nstride);
-  const uint32_t bpa = UPF_GRID_RESOLUTION / p->block_size;
+  const uint32_t bpa = UPF_GRID_RESOLUTION / effective_search_cell(*p);
   s->ncells = bpa * bpa * bpa;
   auto bail = [&](upf_status st) {
     upf_destroy(s);

@@ -180,7 +180,7 @@ upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, ui
     }
     total += counts[s];
     slots += round_up(counts[s] ? counts[s] : 1, kSegAlign);
-    const uint64_t bpa = UPF_GRID_RESOLUTION / params[s].block_size;
+    const uint64_t bpa = UPF_GRID_RESOLUTION / effective_search_cell(params[s]);
     cells += bpa * bpa * bpa;
   }
   if (slots >= (1ull << 31) || cells >= (1ull << 32)) {
@@ -225,7 +225,7 @@ upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, ui
     for (uint32_t g = off / kSegAlign; g < (off + padded) / kSegAlign; ++g) group_scene[g] = s;
     off += padded;
     b->cell_base[s] = cb;
-    const uint32_t bpa = UPF_GRID_RESOLUTION / params[s].block_size;
+    const uint32_t bpa = UPF_GRID_RESOLUTION / effective_search_cell(params[s]);
     cb += bpa * bpa * bpa;
     comp_begin[s] = comp;
     comp += counts[s];

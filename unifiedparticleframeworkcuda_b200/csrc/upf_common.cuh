@@ -53,8 +53,7 @@ struct DevParams {
   float3 cmin, cmax;       // collision box
   float3 wmin, wmax;       // real container
   uint32_t block_shift;    // log2(block_size)
-  uint32_t blocks_per_axis;
-  int32_t nb_radius;       // blocks per axis around a cell that cover its members' query boxes
+  uint32_t cell_shift;     // log2(search cell edge): the cell tables and the neighbour search
   uint32_t flags;
   uint32_t maxn;
   uint32_t nstride;        // neighbour-list column stride

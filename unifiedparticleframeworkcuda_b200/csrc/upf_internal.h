@@ -20,6 +20,8 @@ void build_luts(const upf_params& p, float* out_5x301);
 float kernel_self(float h);
 void build_bin_thresholds(const upf_params& p, float* out_302);
 int validate_params(const upf_params& p, const char** why);
+uint32_t default_search_cell(const upf_params& p);
+uint32_t effective_search_cell(const upf_params& p);  // p.search_cell, or the default when 0
 double density_error_factor(const upf_params& p);
 
 // upf_sort.cu

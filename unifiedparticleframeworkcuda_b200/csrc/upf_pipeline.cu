@@ -177,10 +177,13 @@ __device__ __forceinline__ float dist2(float4 a, float4 b) {
 }
 
 // GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
-// (zIndex.cpp:43-73), one thread per particle: candidates are the Morton
-// blocks covering the query box (with a one-grid-unit margin, so the
-// candidate set is a superset of the reference's), visited in ascending
-// Morton order; within a block the dynamic and boundary ranges are merged by
+// (zIndex.cpp:43-73), one thread per particle: candidates are the search
+// cells (aligned Morton blocks of 2^cell_shift grid units, at most the
+// reference's block size) covering the query box with a one-grid-unit
+// margin. Every particle within h lies in the reference's query box, hence in
+// these cells, so the candidate set holds all of the reference's
+// neighbours. Cells are visited in ascending Morton order, each a contiguous
+// key range; within a cell the dynamic and boundary ranges are merged by
 // key. The list therefore comes out in the reference's ascending
 // sorted-index order, and membership is the reference's exact test: j != i
 // and |x_i - x_j| < h in float. Candidate positions are gathered kUnroll at
@@ -220,8 +223,8 @@ __global__ void __launch_bounds__(kBlock) k_build_nlist(
       float l = c[a] - r[a] - 1.0f, u = c[a] + r[a] + 1.0f;
       int li = (l <= 0.0f) ? 0 : (l >= 1023.0f ? 1023 : (int)l);
       int ui = (u <= 0.0f) ? 0 : (u >= 1023.0f ? 1023 : (int)u);
-      lo[a] = li >> P.block_shift;
-      hi[a] = ui >> P.block_shift;
+      lo[a] = li >> P.cell_shift;
+      hi[a] = ui >> P.cell_shift;
     }
   }
   const uint32_t maxn = P.maxn, stride = P.nstride;
@@ -1071,7 +1074,7 @@ __global__ void __launch_bounds__(kBlock) k_cell_ranges_batch(const BatchView bv
   const uint32_t s = bv.group_scene[i / kSegAlign];
   const uint32_t b = seg_begin[s], e = bv.seg_end[s];
   if (i >= e) return;
-  const int shift = 3 * (int)bv.params[s].block_shift;
+  const int shift = 3 * (int)bv.params[s].cell_shift;
   const uint32_t c = keys[i] >> shift;
   const uint32_t base = bv.cell_base[s];
   if (i == b || (keys[i - 1] >> shift) != c) cstart[base + c] = i;
@@ -1186,8 +1189,8 @@ __global__ void __launch_bounds__(kBlock) k_static_wvol(DevParams P, uint32_t ns
     float l = c[a] - r[a] - 1.0f, u = c[a] + r[a] + 1.0f;
     int li = (l <= 0.0f) ? 0 : (l >= 1023.0f ? 1023 : (int)l);
     int ui = (u <= 0.0f) ? 0 : (u >= 1023.0f ? 1023 : (int)u);
-    lo[a] = li >> P.block_shift;
-    hi[a] = ui >> P.block_shift;
+    lo[a] = li >> P.cell_shift;
+    hi[a] = ui >> P.cell_shift;
   }
   // accumulate in the reference's ascending order: blocks by Morton code
   uint32_t codes[64];
@@ -1238,7 +1241,7 @@ cudaError_t launch_sort_phase(System& s, cudaStream_t st) {
   k_reorder<<<grid_of(n), kBlock, 0, st>>>(n, s.perm, s.A, s.B, s.prm.method == UPF_METHOD_PCISPH);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = launch_rigid_slots(s, st)) != cudaSuccess) return e;
-  return cell_ranges(s.keysA, n, 3 * (int)s.dp.block_shift, s.ncells, s.cstart, s.cend, st);
+  return cell_ranges(s.keysA, n, 3 * (int)s.dp.cell_shift, s.ncells, s.cstart, s.cend, st);
 }
 
 cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
@@ -1324,7 +1327,7 @@ cudaError_t launch_static_setup(System& s, cudaStream_t st) {
   e = cudaMemsetAsync(s.send, 0, sizeof(uint32_t) * s.ncells, st);
   if (e != cudaSuccess) return e;
   if (ns == 0) return cudaSuccess;
-  e = cell_ranges(s.skeys, ns, 3 * (int)s.dp.block_shift, s.ncells, s.sstart, s.send, st);
+  e = cell_ranges(s.skeys, ns, 3 * (int)s.dp.cell_shift, s.ncells, s.sstart, s.send, st);
   if (e != cudaSuccess) return e;
   k_static_wvol<<<grid_of(ns), kBlock, 0, st>>>(s.dp, ns, s.spos, s.sstart, s.send, s.luts,
                                                  s.wvol + s.dp.static_base);
