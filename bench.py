@@ -274,6 +274,7 @@ def run_batch(args, rank, world, local_rank):
     b.set_stream(stream.cuda_stream)
     b.step(args.warmup)
     b.synchronize()
+    tuned = b.autotune(3).as_dict() if not args.no_autotune else b.launch_config().as_dict()
     b.reset_counters()
     b.checkpoint(0)
 
@@ -371,7 +372,7 @@ def run_batch(args, rank, world, local_rank):
                    "mean_iterations_per_scene": float(np.mean(its)), "max_iterations_per_scene": float(np.max(its)),
                    "max_density_error_percent_last_step": float(np.max(errs)),
                    "particle_steps_per_s": npart * args.steps * world / (batch_ms / 1e3),
-                   "parallelism": "replicas" if world > 1 else "single",
+                   "parallelism": "replicas" if world > 1 else "single", "launch_config": tuned,
                    "l2": "inputs larger than L2 (neighbour lists %.0f MB)" % (npart * 128 * 6 / 1e6)},
         "sequential_single_scene": {"value": seq_value, "unit": "scene-steps/s", "ms_per_step": seq_ms / args.steps,
                                     "speedup_of_batched": value / seq_value},
@@ -423,9 +424,11 @@ def run_ours(args, rank, world, local_rank):
         s.step(args.settle)
         s.synchronize()
 
-    # warm-up
+    # warm-up, then the launch-shape autotuner on the warmed state (untimed;
+    # it leaves the state unchanged)
     s.step(args.warmup)
     s.synchronize()
+    tuned = s.autotune(3).as_dict() if not args.no_autotune else s.launch_config().as_dict()
     s.reset_counters()
     # the end-to-end run below replays the same steps from this state
     s.checkpoint(0)
@@ -552,6 +555,7 @@ def run_ours(args, rank, world, local_rank):
                    "steps_at_max_loops": stats.steps_at_max_loops,
                    "last_density_error_percent": float(stats.density_error_percent),
                    "parallelism": "replicas" if world > 1 else "single",
+                   "launch_config": tuned,
                    "l2": "inputs larger than L2 (neighbour lists %.0f MB)" % (sc.n * p.max_neighbors * 4 / 1e6)},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
@@ -584,6 +588,7 @@ def main():
                     help="untimed steps before the warm-up, e.g. 300 to time steps after the dam's initial "
                          "collapse (the CPU reference arm always times steps from rest)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()

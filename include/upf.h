@@ -300,6 +300,30 @@ typedef struct upf_phase_times {
 } upf_phase_times;
 upf_status upf_profile_step(upf_system* s, upf_phase_times* out);
 
+/* ---- launch shapes and the autotuner (no counterpart in the reference,
+ * whose kernels run at fixed block sizes) --------------------------------
+ * CTA sizes of the neighbour-list and external-force passes, and CTA size x
+ * list rows per TMA stage of the two predict-correct passes. Valid loop-pass
+ * pairs: (128,8) (128,16) (256,4) (256,8) (512,4); batches allow up to 256
+ * threads. Shapes change timing only: every shape gives the same results. */
+typedef struct upf_launch_config {
+  int32_t nlist_threads;      /* 64, 128, 256 */
+  int32_t external_threads;   /* 128, 256 */
+  int32_t density_threads;
+  int32_t density_rows;
+  int32_t pforce_threads;
+  int32_t pforce_rows;
+  float measured_ms[4];       /* autotune: per-launch ms of the chosen shapes
+                                 (neighbour lists, external forces, predicted
+                                 density, pressure force); 0 otherwise */
+} upf_launch_config;
+upf_status upf_get_launch_config(upf_system* s, upf_launch_config* out);
+upf_status upf_set_launch_config(upf_system* s, const upf_launch_config* cfg);
+/* Times every shape of each tunable pass on the system's current state
+ * (repeats launches per shape, CUDA events), keeps the fastest of each, and
+ * leaves the simulation state as it found it. */
+upf_status upf_autotune(upf_system* s, int32_t repeats, upf_launch_config* chosen);
+
 /* ---- readback (CopyParticlesCUDA, src/gpu/particles.cuh:505) ------------ */
 
 /* Dynamic particles in current device order. Any pointer may be NULL.
@@ -408,6 +432,10 @@ upf_status upf_batch_download_state(upf_batch* b, float* pos4, float* vel4);
  * NULL) = the sum over loop iterations of the particles of the scenes still
  * iterating, i.e. the particles the loop passes processed. */
 upf_status upf_batch_profile_step(upf_batch* b, upf_phase_times* out, uint64_t* active_particle_iterations);
+/* Launch shapes of a batch (as upf_*_launch_config; at most 256 threads). */
+upf_status upf_batch_get_launch_config(upf_batch* b, upf_launch_config* out);
+upf_status upf_batch_set_launch_config(upf_batch* b, const upf_launch_config* cfg);
+upf_status upf_batch_autotune(upf_batch* b, int32_t repeats, upf_launch_config* chosen);
 
 /* ---- errors ------------------------------------------------------------- */
 const char* upf_last_error(void);

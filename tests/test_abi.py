@@ -38,11 +38,13 @@ def test_library_exports_every_declared_function(upf_lib):
 
 
 def test_struct_layouts_match_header(upf_lib, tmp_path):
-    from unifiedparticleframeworkcuda_b200._abi import UpfParams, UpfStepStats
+    from unifiedparticleframeworkcuda_b200._abi import UpfLaunchConfig, UpfParams, UpfPhaseTimes, UpfStepStats
     src = tmp_path / "sz.c"
     src.write_text('#include "upf.h"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(upf_params), sizeof(upf_step_stats),'
-                   ' offsetof(upf_params, scales), offsetof(upf_step_stats, kinetic_energy));return 0;}\n')
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(upf_params), sizeof(upf_step_stats),'
+                   ' offsetof(upf_params, scales), offsetof(upf_step_stats, kinetic_energy),'
+                   ' sizeof(upf_phase_times), sizeof(upf_launch_config), offsetof(upf_launch_config, measured_ms),'
+                   ' offsetof(upf_params, search_cell));return 0;}\n')
     exe = tmp_path / "sz"
     cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
     subprocess.run([cc, "-I" + INCLUDE, str(src), "-o", str(exe)], check=True)
@@ -51,6 +53,10 @@ def test_struct_layouts_match_header(upf_lib, tmp_path):
     assert int(out[1]) == C.sizeof(UpfStepStats)
     assert int(out[2]) == UpfParams.scales.offset
     assert int(out[3]) == UpfStepStats.kinetic_energy.offset
+    assert int(out[4]) == C.sizeof(UpfPhaseTimes)
+    assert int(out[5]) == C.sizeof(UpfLaunchConfig)
+    assert int(out[6]) == UpfLaunchConfig.measured_ms.offset
+    assert int(out[7]) == UpfParams.search_cell.offset
 
 
 def test_abi_version(upf_lib):

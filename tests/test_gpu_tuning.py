@@ -1,0 +1,102 @@
+"""Launch shapes and the autotuner: every shape of every tunable pass must
+give the same results bit for bit (shapes change timing only), the tuner
+must leave the simulation state as it found it, and invalid shapes are
+rejected."""
+import numpy as np
+import pytest
+
+from unifiedparticleframeworkcuda_b200 import UpfError, UpfLaunchConfig, scenes
+
+pytestmark = pytest.mark.gpu
+
+LOOP_PAIRS = [(128, 8), (128, 16), (256, 4), (256, 8), (512, 4)]
+
+
+def shape(nl, ext, dens, pf):
+    c = UpfLaunchConfig()
+    c.nlist_threads, c.external_threads = nl, ext
+    c.density_threads, c.density_rows = dens
+    c.pforce_threads, c.pforce_rows = pf
+    return c
+
+
+def run(upf, sc, cfg, steps=3, tune=False):
+    p = upf.derive_params(sc.params)
+    s = upf.ParticleSystem(p, capacity=sc.n, derive=False)
+    s.set_particles(sc.pos, sc.vel, sc.type)
+    if cfg is not None:
+        s.set_launch_config(cfg)
+    chosen = None
+    s.step(1)
+    if tune:
+        chosen = s.autotune(repeats=2)
+    s.step(steps - 1)
+    g = s.particles()
+    st = s.stats()
+    s.close()
+    o = np.argsort(g["id"], kind="stable")
+    return {k: v[o] for k, v in g.items()}, st, chosen
+
+
+def test_every_shape_gives_identical_results(upf_lib):
+    sc = scenes.small_pcisph()
+    ref, ref_st, _ = run(upf_lib, sc, None)
+    nls = [64, 128, 256]
+    exts = [128, 256]
+    for k, dens in enumerate(LOOP_PAIRS):
+        pf = LOOP_PAIRS[(k + 2) % len(LOOP_PAIRS)]
+        cfg = shape(nls[k % 3], exts[k % 2], dens, pf)
+        got, st, _ = run(upf_lib, sc, cfg)
+        assert st.iterations == ref_st.iterations
+        for f in ("pos", "vel", "density", "pressure"):
+            assert np.array_equal(got[f], ref[f]), (cfg.as_dict(), f)
+
+
+def test_autotune_keeps_state_and_picks_a_valid_shape(upf_lib):
+    sc = scenes.small_pcisph()
+    ref, _, _ = run(upf_lib, sc, None)
+    got, _, chosen = run(upf_lib, sc, None, tune=True)
+    for f in ("pos", "vel", "density", "pressure"):
+        assert np.array_equal(got[f], ref[f]), f
+    assert (chosen.density_threads, chosen.density_rows) in LOOP_PAIRS
+    assert (chosen.pforce_threads, chosen.pforce_rows) in LOOP_PAIRS
+    assert chosen.nlist_threads in (64, 128, 256) and chosen.external_threads in (128, 256)
+    assert all(m > 0 for m in chosen.measured_ms)
+
+
+def test_batch_shapes_and_autotune(upf_lib):
+    scs = scenes.batch_scenes(num=5, seed=13, counts=(2048, 8192))
+
+    def go(cfg, tune):
+        with upf_lib.ParticleBatch.from_scenes(scs) as b:
+            if cfg is not None:
+                b.set_launch_config(cfg)
+            b.step(1)
+            chosen = b.autotune(repeats=2) if tune else None
+            b.step(2)
+            return [b.particles(k) for k in range(len(scs))], chosen
+
+    ref, _ = go(None, False)
+    for cfg in (shape(64, 128, (128, 16), (256, 4)), shape(128, 256, (256, 4), (128, 8))):
+        got, _ = go(cfg, False)
+        for a, b in zip(got, ref):
+            assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])
+    got, chosen = go(None, True)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a["pos"], b["pos"])
+    assert chosen.density_threads <= 256 and chosen.pforce_threads <= 256
+
+
+def test_invalid_shapes_rejected(upf_lib):
+    sc = scenes.small_pcisph()
+    p = upf_lib.derive_params(sc.params)
+    with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
+        s.set_particles(sc.pos, sc.vel, sc.type)
+        for bad in (shape(96, 256, (256, 8), (256, 8)), shape(256, 256, (256, 16), (256, 8)),
+                    shape(256, 64, (256, 8), (256, 8))):
+            with pytest.raises(UpfError):
+                s.set_launch_config(bad)
+    scs = scenes.batch_scenes(num=2, seed=3, counts=(2048, 4096))
+    with upf_lib.ParticleBatch.from_scenes(scs) as b:
+        with pytest.raises(UpfError):
+            b.set_launch_config(shape(256, 256, (512, 4), (256, 8)))  # a CTA across two scenes

@@ -19,7 +19,7 @@ import numpy as np
 from ._abi import (FLAG_ADHESION, FLAG_BOUNDARY_PRESSURE, FLAG_PENALTY_WALLS,  # noqa: F401
                    FLAG_RECORD_ITERATIONS, FLAG_SURFACE_TENSION, FLAG_WALL_WEIGHT, FROZEN,
                    GRANULAR, LIQUID, METHOD_PCISPH, METHOD_WCSPH, RIGID, STATUS, UpfParams,
-                   UpfPhaseTimes, UpfStepStats)
+                   UpfLaunchConfig, UpfPhaseTimes, UpfStepStats)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libupf.so")
@@ -83,6 +83,12 @@ def lib():
             "upf_batch_upload_state": [vp, fp, fp],
             "upf_batch_download_state": [vp, fp, fp],
             "upf_batch_profile_step": [vp, C.POINTER(UpfPhaseTimes), C.POINTER(C.c_uint64)],
+            "upf_get_launch_config": [vp, C.POINTER(UpfLaunchConfig)],
+            "upf_set_launch_config": [vp, C.POINTER(UpfLaunchConfig)],
+            "upf_autotune": [vp, C.c_int32, C.POINTER(UpfLaunchConfig)],
+            "upf_batch_get_launch_config": [vp, C.POINTER(UpfLaunchConfig)],
+            "upf_batch_set_launch_config": [vp, C.POINTER(UpfLaunchConfig)],
+            "upf_batch_autotune": [vp, C.c_int32, C.POINTER(UpfLaunchConfig)],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
             "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
             "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],
@@ -271,6 +277,21 @@ class ParticleSystem:
         check(getattr(lib(), "upf_phase_" + name)(self._h), "upf_phase_" + name)
 
     # readback
+    def launch_config(self) -> UpfLaunchConfig:
+        c = UpfLaunchConfig()
+        check(lib().upf_get_launch_config(self._h, C.byref(c)), "upf_get_launch_config")
+        return c
+
+    def set_launch_config(self, cfg: UpfLaunchConfig):
+        check(lib().upf_set_launch_config(self._h, C.byref(cfg)), "upf_set_launch_config")
+
+    def autotune(self, repeats: int = 3) -> UpfLaunchConfig:
+        """Times every launch shape of the tunable passes on the current state
+        and keeps the fastest (the state is left unchanged)."""
+        c = UpfLaunchConfig()
+        check(lib().upf_autotune(self._h, int(repeats), C.byref(c)), "upf_autotune")
+        return c
+
     def particles(self):
         n = self.n_dynamic
         pos = np.zeros((n, 4), np.float32)
@@ -404,6 +425,19 @@ class ParticleBatch:
 
     def restore(self, slot: int = 0):
         check(lib().upf_batch_restore(self._h, int(slot)), "upf_batch_restore")
+
+    def launch_config(self) -> UpfLaunchConfig:
+        c = UpfLaunchConfig()
+        check(lib().upf_batch_get_launch_config(self._h, C.byref(c)), "upf_batch_get_launch_config")
+        return c
+
+    def set_launch_config(self, cfg: UpfLaunchConfig):
+        check(lib().upf_batch_set_launch_config(self._h, C.byref(cfg)), "upf_batch_set_launch_config")
+
+    def autotune(self, repeats: int = 3) -> UpfLaunchConfig:
+        c = UpfLaunchConfig()
+        check(lib().upf_batch_autotune(self._h, int(repeats), C.byref(c)), "upf_batch_autotune")
+        return c
 
     def profile_step(self):
         """(phase times of one step, particles processed by the loop passes)."""

@@ -127,3 +127,22 @@ class UpfPhaseTimes(C.Structure):
         ("iterations", C.c_int32),
         ("launches", C.c_int32),
     ]
+
+
+class UpfLaunchConfig(C.Structure):
+    """upf_launch_config (include/upf.h): launch shapes of the tunable passes."""
+    _fields_ = [
+        ("nlist_threads", C.c_int32),
+        ("external_threads", C.c_int32),
+        ("density_threads", C.c_int32),
+        ("density_rows", C.c_int32),
+        ("pforce_threads", C.c_int32),
+        ("pforce_rows", C.c_int32),
+        ("measured_ms", C.c_float * 4),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "measured_ms"}
+        d["measured_ms"] = list(self.measured_ms)
+        return d
+

@@ -129,7 +129,7 @@ namespace {
 // 2D tensor map over a column-major neighbour array [rows][cols] for the
 // TMA list stream: box = 32 columns (one warp) x kListRows rows.
 upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint32_t elem_bytes, uint64_t cols,
-                           uint64_t rows) {
+                           uint64_t rows, uint32_t box_rows) {
   typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -146,7 +146,7 @@ upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt,
   }
   const cuuint64_t dims[2] = {cols, rows};
   const cuuint64_t strides[1] = {cols * elem_bytes};
-  const cuuint32_t box[2] = {32, (cuuint32_t)kListRows};
+  const cuuint32_t box[2] = {32, (cuuint32_t)box_rows};
   const cuuint32_t estride[2] = {1, 1};
   CUresult r = encode(map, dt, 2, base, dims, strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -154,6 +154,156 @@ upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt,
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
     return UPF_ERR_CUDA;
+  }
+  return UPF_OK;
+}
+
+upf_status encode_list_maps(CUtensorMap* cmaps, CUtensorMap* bmaps, uint32_t* nbr, uint16_t* bins, uint64_t cols,
+                            uint64_t rows) {
+  const uint32_t box_rows[kListRowVariants] = {4, 8, 16};
+  for (int k = 0; k < kListRowVariants; ++k) {
+    upf_status st = encode_list_map(&cmaps[k], nbr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, cols, rows, box_rows[k]);
+    if (st != UPF_OK) return st;
+    st = encode_list_map(&bmaps[k], bins, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cols, rows, box_rows[k]);
+    if (st != UPF_OK) return st;
+  }
+  return UPF_OK;
+}
+
+bool shape_valid(const LaunchShape& s, bool batched, const char** why) {
+  auto bad = [&](const char* w) {
+    if (why) *why = w;
+    return false;
+  };
+  auto pair_ok = [&](int t, int r) {
+    return (t == 128 && (r == 8 || r == 16)) || (t == 256 && (r == 4 || r == 8)) || (t == 512 && r == 4);
+  };
+  if (s.nlist_threads != 64 && s.nlist_threads != 128 && s.nlist_threads != 256)
+    return bad("nlist_threads must be 64, 128 or 256");
+  if (s.external_threads != 128 && s.external_threads != 256) return bad("external_threads must be 128 or 256");
+  if (!pair_ok(s.density_threads, s.density_rows) || !pair_ok(s.pforce_threads, s.pforce_rows))
+    return bad("(threads, rows) of a loop pass must be (128,8), (128,16), (256,4), (256,8) or (512,4)");
+  if (batched && (s.density_threads > 256 || s.pforce_threads > 256))
+    return bad("batched scenes: at most 256 threads per CTA (a CTA must stay within one scene's segment)");
+  return true;
+}
+
+void shape_to_config(const LaunchShape& s, upf_launch_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->nlist_threads = s.nlist_threads;
+  c->external_threads = s.external_threads;
+  c->density_threads = s.density_threads;
+  c->density_rows = s.density_rows;
+  c->pforce_threads = s.pforce_threads;
+  c->pforce_rows = s.pforce_rows;
+}
+
+LaunchShape config_to_shape(const upf_launch_config& c) {
+  LaunchShape s;
+  s.nlist_threads = c.nlist_threads;
+  s.external_threads = c.external_threads;
+  s.density_threads = c.density_threads;
+  s.density_rows = c.density_rows;
+  s.pforce_threads = c.pforce_threads;
+  s.pforce_rows = c.pforce_rows;
+  return s;
+}
+
+upf_status autotune_shapes(const TuneOps& ops, int repeats, upf_launch_config* out) {
+  if (repeats < 1) repeats = 1;
+  cudaStream_t st = ops.stream;
+  LaunchShape& sh = *ops.shape;
+  cudaEvent_t e0, e1;
+  UPF_CUDA(cudaEventCreate(&e0));
+  UPF_CUDA(cudaEventCreate(&e1));
+  float chosen_ms[4] = {0, 0, 0, 0};
+  upf_status rc = UPF_OK;
+  // ms per launch of `launch` at the current shape (one untimed launch first)
+  auto time_pass = [&](cudaError_t (*launch)(void*, cudaStream_t), float* ms) -> upf_status {
+    UPF_CUDA(launch(ops.ctx, st));
+    UPF_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < repeats; ++r) UPF_CUDA(launch(ops.ctx, st));
+    UPF_CUDA(cudaEventRecord(e1, st));
+    UPF_CUDA(cudaEventSynchronize(e1));
+    float t = 0;
+    UPF_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / repeats;
+    return UPF_OK;
+  };
+  do {
+    if ((rc = ops.save(ops.ctx)) != UPF_OK) break;
+    if (ops.prepare) {
+      cudaError_t e = ops.prepare(ops.ctx, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        set_error("autotune: prepare: %s", cudaGetErrorString(e));
+        rc = UPF_ERR_CUDA;
+        break;
+      }
+    }
+    // one pass at a time, the others at their current shapes
+    if (ops.nlist) {
+      const int cand[] = {64, 128, 256};
+      int best = sh.nlist_threads;
+      float best_ms = 1e30f;
+      for (int t : cand) {
+        sh.nlist_threads = t;
+        float ms;
+        if ((rc = time_pass(ops.nlist, &ms)) != UPF_OK) break;
+        if (ms < best_ms) best_ms = ms, best = t;
+      }
+      if (rc != UPF_OK) break;
+      sh.nlist_threads = best;
+      chosen_ms[0] = best_ms;
+      // the lists of the chosen shape (identical for every shape)
+      if (cudaSuccess != ops.nlist(ops.ctx, st)) {
+        rc = UPF_ERR_CUDA;
+        break;
+      }
+    }
+    if (ops.external) {
+      const int cand[] = {128, 256};
+      int best = sh.external_threads;
+      float best_ms = 1e30f;
+      for (int t : cand) {
+        sh.external_threads = t;
+        float ms;
+        if ((rc = time_pass(ops.external, &ms)) != UPF_OK) break;
+        if (ms < best_ms) best_ms = ms, best = t;
+      }
+      if (rc != UPF_OK) break;
+      sh.external_threads = best;
+      chosen_ms[1] = best_ms;
+    }
+    const int pairs[5][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {512, 4}};
+    for (int pass = 0; pass < 2 && rc == UPF_OK; ++pass) {
+      cudaError_t (*launch)(void*, cudaStream_t) = pass == 0 ? ops.density : ops.pforce;
+      if (!launch) continue;
+      int& threads = pass == 0 ? sh.density_threads : sh.pforce_threads;
+      int& rows = pass == 0 ? sh.density_rows : sh.pforce_rows;
+      int bt = threads, br = rows;
+      float best_ms = 1e30f;
+      for (const auto& pr : pairs) {
+        if (ops.batched && pr[0] > 256) continue;
+        threads = pr[0];
+        rows = pr[1];
+        float ms;
+        if ((rc = time_pass(launch, &ms)) != UPF_OK) break;
+        if (ms < best_ms) best_ms = ms, bt = pr[0], br = pr[1];
+      }
+      threads = bt;
+      rows = br;
+      chosen_ms[2 + pass] = best_ms;
+    }
+  } while (0);
+  const upf_status rr = ops.restore(ops.ctx);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != UPF_OK) return rc;
+  if (rr != UPF_OK) return rr;
+  if (out) {
+    shape_to_config(sh, out);
+    for (int k = 0; k < 4; ++k) out->measured_ms[k] = chosen_ms[k];
   }
   return UPF_OK;
 }
@@ -452,11 +602,7 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   ALLOC(s->luts, 5 * UPF_LUT_ENTRIES + kThresholds);
   ALLOC(s->st, 1);
 #undef ALLOC
-  if ((st = encode_list_map(&s->nbr_map, s->nbr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, s->nstride,
-                            p->max_neighbors)) != UPF_OK)
-    return bail(st);
-  if ((st = encode_list_map(&s->bins_map, s->bins, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, s->nstride,
-                            p->max_neighbors)) != UPF_OK)
+  if ((st = encode_list_maps(s->nbr_maps, s->bins_maps, s->nbr, s->bins, s->nstride, p->max_neighbors)) != UPF_OK)
     return bail(st);
   e = cudaMallocHost((void**)&s->st_host, sizeof(DevState));
   if (e != cudaSuccess) {
@@ -1023,6 +1169,86 @@ upf_status upf_state_load(upf_system* s, const void* host, size_t bytes) {
   UPF_TRY(state_copy(*s, (char*)const_cast<void*>(host), false, cudaMemcpyHostToDevice));
   UPF_CUDA(cudaStreamSynchronize(s->stream));
   return UPF_OK;
+}
+
+upf_status upf_get_launch_config(upf_system* s, upf_launch_config* out) {
+  if (!s || !out) {
+    set_error("upf_get_launch_config: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  shape_to_config(s->shape, out);
+  return UPF_OK;
+}
+
+upf_status upf_set_launch_config(upf_system* s, const upf_launch_config* cfg) {
+  if (!s || !cfg) {
+    set_error("upf_set_launch_config: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  const LaunchShape sh = config_to_shape(*cfg);
+  const char* why = nullptr;
+  if (!shape_valid(sh, false, &why)) {
+    set_error("upf_set_launch_config: %s", why);
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  s->shape = sh;
+  return s->have_particles ? build_step_graph(*s) : UPF_OK;
+}
+
+namespace {
+struct SysTune {
+  System* s;
+  void* buf;
+};
+}  // namespace
+
+upf_status upf_autotune(upf_system* s, int32_t repeats, upf_launch_config* chosen) {
+  UPF_TRY(phase_guard(s));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  SysTune t{s, nullptr};
+  TuneOps ops;
+  ops.ctx = &t;
+  ops.shape = &s->shape;
+  ops.batched = false;
+  ops.stream = s->stream;
+  ops.save = [](void* c) -> upf_status {
+    SysTune& T = *static_cast<SysTune*>(c);
+    cudaError_t e = cudaMalloc(&T.buf, state_total(*T.s));
+    if (e != cudaSuccess) {
+      T.buf = nullptr;
+      set_error("upf_autotune: cudaMalloc: %s", cudaGetErrorString(e));
+      return UPF_ERR_ALLOC;
+    }
+    return state_copy(*T.s, (char*)T.buf, true, cudaMemcpyDeviceToDevice);
+  };
+  ops.restore = [](void* c) -> upf_status {
+    SysTune& T = *static_cast<SysTune*>(c);
+    if (!T.buf) return UPF_OK;
+    upf_status rc = state_copy(*T.s, (char*)T.buf, false, cudaMemcpyDeviceToDevice);
+    cudaStreamSynchronize(T.s->stream);
+    cudaFree(T.buf);
+    T.buf = nullptr;
+    return rc;
+  };
+  const bool pcisph = s->prm.method == UPF_METHOD_PCISPH;
+  ops.prepare = [](void* c, cudaStream_t st) {
+    System& S = *static_cast<SysTune*>(c)->s;
+    cudaError_t e = launch_sort_phase(S, st);
+    if (e == cudaSuccess) e = launch_neighbor_phase(S, st);
+    if (e == cudaSuccess) e = launch_force_phase(S, st);
+    if (e == cudaSuccess && S.prm.method == UPF_METHOD_PCISPH) e = launch_loop_init(S, st);
+    return e;
+  };
+  ops.nlist = [](void* c, cudaStream_t st) { return launch_neighbor_phase(*static_cast<SysTune*>(c)->s, st); };
+  if (pcisph) {
+    ops.external = [](void* c, cudaStream_t st) { return launch_force_phase(*static_cast<SysTune*>(c)->s, st); };
+    ops.density = [](void* c, cudaStream_t st) { return launch_loop_density(*static_cast<SysTune*>(c)->s, st); };
+    ops.pforce = [](void* c, cudaStream_t st) { return launch_loop_pforce(*static_cast<SysTune*>(c)->s, st); };
+  }
+  UPF_TRY(autotune_shapes(ops, repeats, chosen));
+  UPF_TRY(check_device_errors(*s));
+  return build_step_graph(*s);
 }
 
 upf_status upf_profile_step(upf_system* s, upf_phase_times* out) {

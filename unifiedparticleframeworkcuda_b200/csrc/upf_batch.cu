@@ -260,10 +260,7 @@ upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, ui
   ALLOC(b->x.comp_begin_d, num_scenes); ALLOC(b->x.stage_a, std::max<size_t>(total, 1));
   ALLOC(b->x.stage_b, std::max<size_t>(total, 1));
 #undef ALLOC
-  if ((st = encode_list_map(&b->nbr_map, b->nbr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, n, rows)) != UPF_OK)
-    return bail(st);
-  if ((st = encode_list_map(&b->bins_map, b->bins, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, n, rows)) != UPF_OK)
-    return bail(st);
+  if ((st = encode_list_maps(b->nbr_maps, b->bins_maps, b->nbr, b->bins, n, rows)) != UPF_OK) return bail(st);
   e = cudaMallocHost((void**)&b->st_h, sizeof(DevState) * num_scenes);
   if (e != cudaSuccess) {
     b->st_h = nullptr;
@@ -538,6 +535,83 @@ upf_status upf_batch_download_state(upf_batch* b, float* pos4, float* vel4) {
   UPF_CUDA(cudaMemcpyAsync(vel4, b->x.stage_b, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
   UPF_CUDA(cudaStreamSynchronize(st));
   return UPF_OK;
+}
+
+upf_status upf_batch_get_launch_config(upf_batch* b, upf_launch_config* out) {
+  if (!b || !out) {
+    set_error("upf_batch_get_launch_config: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  shape_to_config(b->shape, out);
+  return UPF_OK;
+}
+
+upf_status upf_batch_set_launch_config(upf_batch* b, const upf_launch_config* cfg) {
+  if (!b || !cfg) {
+    set_error("upf_batch_set_launch_config: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  const LaunchShape sh = config_to_shape(*cfg);
+  const char* why = nullptr;
+  if (!shape_valid(sh, true, &why)) {
+    set_error("upf_batch_set_launch_config: %s", why);
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaStreamSynchronize(b->stream));
+  b->shape = sh;
+  return b->have_particles ? build_batch_graph(b) : UPF_OK;
+}
+
+namespace {
+struct BatchTune {
+  upf_batch* b;
+  void* buf;
+};
+}  // namespace
+
+upf_status upf_batch_autotune(upf_batch* b, int32_t repeats, upf_launch_config* chosen) {
+  UPF_TRY(batch_guard(b, "upf_batch_autotune"));
+  UPF_CUDA(cudaStreamSynchronize(b->stream));
+  BatchTune t{b, nullptr};
+  TuneOps ops;
+  ops.ctx = &t;
+  ops.shape = &b->shape;
+  ops.batched = true;
+  ops.stream = b->stream;
+  ops.save = [](void* c) -> upf_status {
+    BatchTune& T = *static_cast<BatchTune*>(c);
+    cudaError_t e = cudaMalloc(&T.buf, batch_state_bytes(T.b));
+    if (e != cudaSuccess) {
+      T.buf = nullptr;
+      set_error("upf_batch_autotune: cudaMalloc: %s", cudaGetErrorString(e));
+      return UPF_ERR_ALLOC;
+    }
+    return batch_state_copy(T.b, (char*)T.buf, true);
+  };
+  ops.restore = [](void* c) -> upf_status {
+    BatchTune& T = *static_cast<BatchTune*>(c);
+    if (!T.buf) return UPF_OK;
+    upf_status rc = batch_state_copy(T.b, (char*)T.buf, false);
+    cudaStreamSynchronize(T.b->stream);
+    cudaFree(T.buf);
+    T.buf = nullptr;
+    return rc;
+  };
+  ops.prepare = [](void* c, cudaStream_t st) {
+    BatchSystem& B = *static_cast<BatchTune*>(c)->b;
+    cudaError_t e = batch_launch_sort(B, st);
+    if (e == cudaSuccess) e = batch_launch_neighbors(B, st);
+    if (e == cudaSuccess) e = batch_launch_forces(B, st);
+    if (e == cudaSuccess) e = batch_launch_loop_init(B, st);
+    return e;
+  };
+  ops.nlist = [](void* c, cudaStream_t st) { return batch_launch_neighbors(*static_cast<BatchTune*>(c)->b, st); };
+  ops.external = [](void* c, cudaStream_t st) { return batch_launch_forces(*static_cast<BatchTune*>(c)->b, st); };
+  ops.density = [](void* c, cudaStream_t st) { return batch_launch_loop_density(*static_cast<BatchTune*>(c)->b, st); };
+  ops.pforce = [](void* c, cudaStream_t st) { return batch_launch_loop_pforce(*static_cast<BatchTune*>(c)->b, st); };
+  UPF_TRY(autotune_shapes(ops, repeats, chosen));
+  UPF_TRY(batch_check_errors(b));
+  return build_batch_graph(b);
 }
 
 upf_status upf_batch_profile_step(upf_batch* b, upf_phase_times* out, uint64_t* active_particle_iterations) {

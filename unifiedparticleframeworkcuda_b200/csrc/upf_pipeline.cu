@@ -189,8 +189,8 @@ __device__ __forceinline__ float dist2(float4 a, float4 b) {
 // and |x_i - x_j| < h in float. Candidate positions are gathered kUnroll at
 // a time. Each entry also records its kernel-table bin at the current
 // positions (used by every pass that evaluates at current positions).
-template <bool kBatch>
-__global__ void __launch_bounds__(kBlock) k_build_nlist(
+template <bool kBatch, int kThreads>
+__global__ void __launch_bounds__(kThreads) k_build_nlist(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const float4* __restrict__ pos,
     const uint32_t* __restrict__ keys, const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend,
     uint32_t ns, const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
@@ -726,8 +726,8 @@ __device__ __forceinline__ float3 solid_external(const DevParams& P, uint32_t i,
 // CalculateExternalForcesVersatilCouplingPCISPH (UnifiedPhysics.cpp:5252-5365):
 // liquid particles (then the first prediction of the loop), rigid and
 // granular particles (solid_external).
-template <bool kBatch>
-__global__ void __launch_bounds__(kBlock) k_pcisph_external(
+template <bool kBatch, int kThreads>
+__global__ void __launch_bounds__(kThreads) k_pcisph_external(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
     const float* __restrict__ wvol, const int32_t* __restrict__ id_body, const uint32_t* __restrict__ nbr,
     const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, float4* __restrict__ force,
@@ -831,10 +831,10 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_external(
 // maximum for the loop test reduced in the same pass.
 //
 // The warp's list rows stream through shared memory by TMA (upf_tma.cuh);
-// each lane then gathers kListRows neighbours' predicted positions at once
+// each lane then gathers kRows neighbours' predicted positions at once
 // and accumulates them in list order.
-template <bool kBatch>
-__global__ void __launch_bounds__(kBlock) k_pcisph_density(
+template <bool kBatch, int kThreads, int kRows>
+__global__ void __launch_bounds__(kThreads) k_pcisph_density(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const int32_t* __restrict__ type,
     const float4* __restrict__ xs, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
     const float* __restrict__ luts_plain, float* __restrict__ rho, float* __restrict__ press,
@@ -842,8 +842,8 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
   __shared__ DevParams sP;
   __shared__ float m4[UPF_LUT_ENTRIES];
   __shared__ float thr[kThresholds];
-  __shared__ uint32_t wmax[kBlock / 32];
-  __shared__ WarpListRing<false> rings[kBlock / 32];
+  __shared__ uint32_t wmax[kThreads / 32];
+  __shared__ WarpListRing<false, kRows> rings[kThreads / 32];
   const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -861,17 +861,17 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
   const float4 xi = active ? xs[i] : make_float4(0, 0, 0, 0);
   const float m = P.mass;
   float den = P.kernel_self * m;
-  WarpListRing<false>& ring = rings[warp];
+  WarpListRing<false, kRows>& ring = rings[warp];
   const bool ok = ring_walk(ring, &cmap, &cmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
                             [&](int s, int k0) {
                               // predicted positions; boundary particles sit in the array's
                               // tail at their fixed positions
-                              float4 xj[kListRows];
+                              float4 xj[kRows];
 #pragma unroll
-                              for (int r = 0; r < kListRows; ++r)
+                              for (int r = 0; r < kRows; ++r)
                                 if (k0 + r < (int)cnt) xj[r] = __ldg(xs + ring.codes[s][r][lane]);
 #pragma unroll
-                              for (int r = 0; r < kListRows; ++r) {
+                              for (int r = 0; r < kRows; ++r) {
                                 if (k0 + r < (int)cnt) {
                                   // d < h and the table bin of d, from d^2 (exact)
                                   const float r2 = dist2(xi, xj[r]);
@@ -905,8 +905,8 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_density(
 
 // ComputeCorrectivePressureForce (UnifiedPhysics.cpp:5493-5522), then the
 // prediction of the next iteration (PredictPositionAndVelocity).
-template <bool kBatch>
-__global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
+template <bool kBatch, int kThreads, int kRows>
+__global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
     const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap bmap,
     const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, const float* __restrict__ pq,
@@ -914,7 +914,7 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
     DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float pg[UPF_LUT_ENTRIES];
-  __shared__ WarpListRing<true> rings[kBlock / 32];
+  __shared__ WarpListRing<true, kRows> rings[kThreads / 32];
   const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -936,14 +936,14 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
   const float4* __restrict__ pos = B.pos;
   // positions are those the list was built at: every entry passes |x_i - x_j| < h
   // and its kernel-table bin is stored with it
-  WarpListRing<true>& ring = rings[warp];
+  WarpListRing<true, kRows>& ring = rings[warp];
   const bool ok = ring_walk(ring, &cmap, &bmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
                             [&](int s, int k0) {
                               // boundary particles sit in the arrays' tails (pq = 0 there)
-                              float4 xj[kListRows];
-                              float qj[kListRows];
+                              float4 xj[kRows];
+                              float qj[kRows];
 #pragma unroll
-                              for (int r = 0; r < kListRows; ++r) {
+                              for (int r = 0; r < kRows; ++r) {
                                 if (k0 + r < (int)cnt) {
                                   const uint32_t code = ring.codes[s][r][lane];
                                   xj[r] = __ldg(pos + code);
@@ -951,7 +951,7 @@ __global__ void __launch_bounds__(kBlock) k_pcisph_pressure_force(
                                 }
                               }
 #pragma unroll
-                              for (int r = 0; r < kListRows; ++r) {
+                              for (int r = 0; r < kRows; ++r) {
                                 if (k0 + r < (int)cnt) {
                                   const float g = pg[ring.bins[s][r][lane]];
                                   const float kx = (xi.x - xj[r].x) * g, ky = (xi.y - xj[r].y) * g,
@@ -1227,6 +1227,79 @@ __global__ void __launch_bounds__(kBlock) k_static_wvol(DevParams P, uint32_t ns
 
 inline uint32_t grid_of(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 
+// ---- launches of the tunable passes at a LaunchShape
+template <bool kBatch>
+cudaError_t run_nlist(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
+                      const float4* pos, const uint32_t* keys, const uint32_t* cstart, const uint32_t* cend,
+                      uint32_t ns, const float4* spos, const uint32_t* skeys, const uint32_t* sstart,
+                      const uint32_t* send, uint32_t* nbr, uint16_t* bins, uint32_t* ncnt, const float* luts,
+                      DevState* stp) {
+#define UPF_NL(T)                                                                                          \
+  k_build_nlist<kBatch, T><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, pos, keys, cstart, cend, ns, spos, skeys, \
+                                                          sstart, send, nbr, bins, ncnt, luts, stp)
+  switch (sh.nlist_threads) {
+    case 64: UPF_NL(64); break;
+    case 128: UPF_NL(128); break;
+    case 256: UPF_NL(256); break;
+    default: return cudaErrorInvalidConfiguration;
+  }
+#undef UPF_NL
+  return cudaGetLastError();
+}
+
+template <bool kBatch>
+cudaError_t run_external(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
+                         const DynArrays& B, const float* wvol, const int32_t* id_body, const uint32_t* nbr,
+                         const uint32_t* ncnt, const float* luts, float4* force, float4* pforce, float4* xs,
+                         float* press, float* pq, DevState* stp) {
+#define UPF_EXT(T)                                                                                        \
+  k_pcisph_external<kBatch, T><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, B, wvol, id_body, nbr, ncnt, luts, \
+                                                              force, pforce, xs, press, pq, stp)
+  switch (sh.external_threads) {
+    case 128: UPF_EXT(128); break;
+    case 256: UPF_EXT(256); break;
+    default: return cudaErrorInvalidConfiguration;
+  }
+#undef UPF_EXT
+  return cudaGetLastError();
+}
+
+#define UPF_SHAPE_SWITCH(threads, rows, CALL) \
+  switch ((threads) * 100 + (rows)) {         \
+    case 12808: CALL(128, 8); break;          \
+    case 12816: CALL(128, 16); break;         \
+    case 25604: CALL(256, 4); break;          \
+    case 25608: CALL(256, 8); break;          \
+    case 51204: CALL(512, 4); break;          \
+    default: return cudaErrorInvalidConfiguration; \
+  }
+
+template <bool kBatch>
+cudaError_t run_density(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
+                        const int32_t* type, const float4* xs, const CUtensorMap* cmaps, const uint32_t* ncnt,
+                        const float* luts, float* rho, float* press, float* pq, DevState* stp) {
+#define UPF_DEN(T, R)                                                                                           \
+  k_pcisph_density<kBatch, T, R><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, type, xs, cmaps[rows_index(R)], ncnt, \
+                                                                luts, rho, press, pq, stp)
+  UPF_SHAPE_SWITCH(sh.density_threads, sh.density_rows, UPF_DEN)
+#undef UPF_DEN
+  return cudaGetLastError();
+}
+
+template <bool kBatch>
+cudaError_t run_pforce(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
+                       const DynArrays& B, const CUtensorMap* cmaps, const CUtensorMap* bmaps, const uint32_t* ncnt,
+                       const float* luts, const float* pq, const float4* force, float4* pforce, float4* xs,
+                       DevState* stp) {
+#define UPF_PF(T, R)                                                                                         \
+  k_pcisph_pressure_force<kBatch, T, R><<<(n + T - 1) / T, T, 0, st>>>(                                      \
+      P, bv, n, B, cmaps[rows_index(R)], bmaps[rows_index(R)], ncnt, luts, pq, force, pforce, xs, stp)
+  UPF_SHAPE_SWITCH(sh.pforce_threads, sh.pforce_rows, UPF_PF)
+#undef UPF_PF
+  return cudaGetLastError();
+}
+#undef UPF_SHAPE_SWITCH
+
 }  // namespace
 
 // ----------------------------------------------------------------- launchers
@@ -1248,9 +1321,8 @@ cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
   if (n == 0) return cudaGetLastError();
-  k_build_nlist<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
-                                                s.skeys, s.sstart, s.send, s.nbr, s.bins, s.ncnt, s.luts, s.st);
-  return cudaGetLastError();
+  return run_nlist<false>(s.shape, st, s.dp, BatchView{}, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
+                          s.skeys, s.sstart, s.send, s.nbr, s.bins, s.ncnt, s.luts, s.st);
 }
 
 cudaError_t launch_force_phase(System& s, cudaStream_t st) {
@@ -1260,8 +1332,8 @@ cudaError_t launch_force_phase(System& s, cudaStream_t st) {
     k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.bins, s.ncnt, s.luts, s.rho,
                                                    s.press);
   } else {
-    k_pcisph_external<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B, s.wvol, s.rb.id_body, s.nbr, s.ncnt, s.luts,
-                                                     s.force, s.pforce, s.xs, s.press, s.pq, s.st);
+    return run_external<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.wvol, s.rb.id_body, s.nbr, s.ncnt, s.luts,
+                               s.force, s.pforce, s.xs, s.press, s.pq, s.st);
   }
   return cudaGetLastError();
 }
@@ -1274,16 +1346,16 @@ cudaError_t launch_loop_init(System& s, cudaStream_t st) {
 cudaError_t launch_loop_density(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_density<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B.type, s.xs, s.nbr_map, s.ncnt, s.luts, s.rho,
-                                                    s.press, s.pq, s.st);
+    return run_density<false>(s.shape, st, s.dp, BatchView{}, n, s.B.type, s.xs, s.nbr_maps, s.ncnt, s.luts, s.rho,
+                              s.press, s.pq, s.st);
   return cudaGetLastError();
 }
 
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    k_pcisph_pressure_force<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B, s.nbr_map, s.bins_map, s.ncnt,
-                                                           s.luts, s.pq, s.force, s.pforce, s.xs, s.st);
+    return run_pforce<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.nbr_maps, s.bins_maps, s.ncnt, s.luts, s.pq,
+                             s.force, s.pforce, s.xs, s.st);
   return cudaGetLastError();
 }
 
@@ -1374,19 +1446,15 @@ cudaError_t batch_launch_neighbors(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
   k_step_init_batch<<<1, 256, 0, st>>>(b.st_d, b.n_scenes);
   if (!n) return cudaGetLastError();
-  k_build_nlist<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B.pos, b.keysA, b.cstart, b.cend, 0u,
-                                                     nullptr, nullptr, nullptr, nullptr, b.nbr, b.bins, b.ncnt,
-                                                     nullptr, nullptr);
-  return cudaGetLastError();
+  return run_nlist<true>(b.shape, st, DevParams{}, b.view, n, b.B.pos, b.keysA, b.cstart, b.cend, 0u, nullptr, nullptr,
+                         nullptr, nullptr, b.nbr, b.bins, b.ncnt, nullptr, nullptr);
 }
 
 cudaError_t batch_launch_forces(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
   if (!n) return cudaSuccess;
-  k_pcisph_external<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B, nullptr, nullptr, b.nbr,
-                                                         b.ncnt, nullptr, b.force, b.pforce, b.xs, b.press, b.pq,
-                                                         nullptr);
-  return cudaGetLastError();
+  return run_external<true>(b.shape, st, DevParams{}, b.view, n, b.B, nullptr, nullptr, b.nbr, b.ncnt, nullptr,
+                            b.force, b.pforce, b.xs, b.press, b.pq, nullptr);
 }
 
 cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st) {
@@ -1397,17 +1465,16 @@ cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st) {
 cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
   if (n)
-    k_pcisph_density<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B.type, b.xs, b.nbr_map, b.ncnt,
-                                                          nullptr, b.rho, b.press, b.pq, nullptr);
+    return run_density<true>(b.shape, st, DevParams{}, b.view, n, b.B.type, b.xs, b.nbr_maps, b.ncnt, nullptr, b.rho,
+                             b.press, b.pq, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
   if (n)
-    k_pcisph_pressure_force<true><<<grid_of(n), kBlock, 0, st>>>(DevParams{}, b.view, n, b.B, b.nbr_map, b.bins_map,
-                                                                 b.ncnt, nullptr, b.pq, b.force, b.pforce, b.xs,
-                                                                 nullptr);
+    return run_pforce<true>(b.shape, st, DevParams{}, b.view, n, b.B, b.nbr_maps, b.bins_maps, b.ncnt, nullptr, b.pq,
+                            b.force, b.pforce, b.xs, nullptr);
   return cudaGetLastError();
 }
 

@@ -51,6 +51,22 @@ struct RigidArrays {
   uint32_t* entry_slot = nullptr; // list entry -> current sorted index (set after each sort)
 };
 
+// Launch shapes of the tunable passes (upf_launch_config): CTA sizes, and
+// the list rows each TMA stage carries in the loop passes. The loop passes
+// are instantiated for the (threads, rows) pairs below, whose ring buffers
+// fit the 48 KB of static shared memory per CTA.
+struct LaunchShape {
+  int nlist_threads = 256;     // 64, 128, 256
+  int external_threads = 256;  // 128, 256
+  int density_threads = 256;   // with density_rows: (128,8) (128,16) (256,4) (256,8) (512,4)
+  int density_rows = 8;
+  int pforce_threads = 256;    // with pforce_rows: the same pairs
+  int pforce_rows = 8;
+};
+bool shape_valid(const LaunchShape& s, bool batched, const char** why);
+constexpr int kListRowVariants = 3;  // tensor maps for 4, 8 and 16 rows per box
+inline int rows_index(int rows) { return rows == 4 ? 0 : (rows == 8 ? 1 : 2); }
+
 // Batched scenes (upf_batch_*): independent scenes in one index space, each
 // in its own segment that starts on a kSegAlign boundary, so every CTA of a
 // kernel over that space (CTA sizes dividing kSegAlign) belongs to one scene.
@@ -99,9 +115,10 @@ struct System {
   uint32_t* nbr = nullptr;
   uint16_t* bins = nullptr;    // kernel-table bin of each list entry at current positions
   uint32_t* ncnt = nullptr;
-  CUtensorMap nbr_map;         // 2D [max_neighbors][nstride] uint32 view of nbr for TMA
-  CUtensorMap bins_map;        // same view of bins (uint16)
+  CUtensorMap nbr_maps[kListRowVariants];   // 2D [max_neighbors][nstride] uint32 views of nbr for TMA, box 32 x {4, 8, 16}
+  CUtensorMap bins_maps[kListRowVariants];  // same views of bins (uint16)
   uint32_t nstride = 0;
+  LaunchShape shape;
 
   // cells
   uint32_t ncells = 0;
@@ -167,10 +184,11 @@ struct BatchSystem {
   uint32_t* nbr = nullptr;
   uint16_t* bins = nullptr;
   uint32_t* ncnt = nullptr;
-  CUtensorMap nbr_map;
-  CUtensorMap bins_map;
+  CUtensorMap nbr_maps[kListRowVariants];
+  CUtensorMap bins_maps[kListRowVariants];
   uint32_t* cstart = nullptr;
   uint32_t* cend = nullptr;
+  LaunchShape shape;
 
   DevParams* params_d = nullptr;
   float* luts_d = nullptr;
@@ -214,7 +232,32 @@ struct GraphParts {
 upf_status capture_step_graph(const GraphParts& parts, cudaGraph_t* graph_out, cudaGraphExec_t* exec_out);
 DevParams make_dev_params(const upf_params& p, uint32_t nstride);
 upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint32_t elem_bytes,
-                           uint64_t cols, uint64_t rows);
+                           uint64_t cols, uint64_t rows, uint32_t box_rows);
+// the three box heights of each list (codes, bins)
+upf_status encode_list_maps(CUtensorMap* cmaps, CUtensorMap* bmaps, uint32_t* nbr, uint16_t* bins, uint64_t cols,
+                            uint64_t rows);
+
+// upf_api.cu: the launch-shape autotuner, over callbacks so that one
+// routine serves systems and batches. `prepare` runs a step's passes up to
+// the loop (lists, external forces, loop state); each pass callback launches
+// that pass once at the current *shape; save/restore bracket the tuning so
+// the simulation state is left unchanged. Null callbacks are not tuned.
+struct TuneOps {
+  void* ctx = nullptr;
+  LaunchShape* shape = nullptr;
+  bool batched = false;
+  cudaStream_t stream = nullptr;
+  cudaError_t (*prepare)(void* ctx, cudaStream_t st) = nullptr;
+  cudaError_t (*nlist)(void* ctx, cudaStream_t st) = nullptr;
+  cudaError_t (*external)(void* ctx, cudaStream_t st) = nullptr;
+  cudaError_t (*density)(void* ctx, cudaStream_t st) = nullptr;
+  cudaError_t (*pforce)(void* ctx, cudaStream_t st) = nullptr;
+  upf_status (*save)(void* ctx) = nullptr;
+  upf_status (*restore)(void* ctx) = nullptr;
+};
+upf_status autotune_shapes(const TuneOps& ops, int repeats, upf_launch_config* out);
+void shape_to_config(const LaunchShape& s, upf_launch_config* c);
+LaunchShape config_to_shape(const upf_launch_config& c);
 
 // upf_rigid.cu: list entry -> sorted index after a sort; body force/torque,
 // body integration and rigid particle sync after integration

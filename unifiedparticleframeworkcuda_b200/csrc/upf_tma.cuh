@@ -17,7 +17,7 @@
 
 namespace upf {
 
-constexpr int kListRows = 8;     // list rows per stage
+constexpr int kListRows = 8;     // default list rows per stage (a launch shape parameter)
 constexpr int kListStages = 3;   // ring depth
 constexpr uint32_t kWaitSpins = 1u << 22;  // bounded wait (~seconds at worst)
 
@@ -65,11 +65,11 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 
 // One warp's ring of list stages. Stage s holds rows [c*R, c*R+R) of chunk c
 // (c % kListStages == s) for the warp's 32 columns: codes (uint32) and,
-// when kWithBins, bins (uint16).
-template <bool kWithBins>
+// when kWithBins, bins (uint16). R = kRows, the box height of the tensor map.
+template <bool kWithBins, int kRows = kListRows>
 struct __align__(128) WarpListRing {
-  uint32_t codes[kListStages][kListRows][32];                   // 1 KB per stage
-  uint16_t bins[kWithBins ? kListStages : 1][kListRows][32];     // 512 B per stage
+  uint32_t codes[kListStages][kRows][32];                   // 128 B per row
+  uint16_t bins[kWithBins ? kListStages : 1][kRows][32];     // 64 B per row
   uint64_t full[kListStages];
 };
 
@@ -77,25 +77,25 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <bool kWithBins>
-__device__ __forceinline__ void ring_issue(WarpListRing<kWithBins>& r, const CUtensorMap* cmap,
+template <bool kWithBins, int kRows>
+__device__ __forceinline__ void ring_issue(WarpListRing<kWithBins, kRows>& r, const CUtensorMap* cmap,
                                            const CUtensorMap* bmap, int chunk, int col0) {
   const int s = chunk % kListStages;
-  const uint32_t bytes = kListRows * 32 * (4 + (kWithBins ? 2 : 0));
+  const uint32_t bytes = kRows * 32 * (4 + (kWithBins ? 2 : 0));
   fence_proxy_async_smem();  // the stage's previous contents were read through the generic proxy
   mbar_arrive_expect_tx(&r.full[s], bytes);
-  tma_load_2d(&r.codes[s][0][0], cmap, &r.full[s], col0, chunk * kListRows);
-  if (kWithBins) tma_load_2d(&r.bins[s][0][0], bmap, &r.full[s], col0, chunk * kListRows);
+  tma_load_2d(&r.codes[s][0][0], cmap, &r.full[s], col0, chunk * kRows);
+  if (kWithBins) tma_load_2d(&r.bins[s][0][0], bmap, &r.full[s], col0, chunk * kRows);
 }
 
 // Walks the warp's lists chunk by chunk. `body(s, rows)` consumes stage s
 // (rows valid rows); lanes index their own column. Returns false if a wait
 // ran out.
-template <bool kWithBins, class Body>
-__device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins>& r, const CUtensorMap* cmap,
+template <bool kWithBins, int kRows, class Body>
+__device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins, kRows>& r, const CUtensorMap* cmap,
                                           const CUtensorMap* bmap, int col0, uint32_t warp_max_cnt, Body&& body) {
   const int lane = threadIdx.x & 31;
-  const int nchunks = (int)((warp_max_cnt + kListRows - 1) / kListRows);
+  const int nchunks = (int)((warp_max_cnt + kRows - 1) / kRows);
   if (lane == 0) {
     for (int c = 0; c < kListStages && c < nchunks; ++c) ring_issue(r, cmap, bmap, c, col0);
   }
@@ -104,15 +104,15 @@ __device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins>& r, const CUte
     const int s = c % kListStages;
     const uint32_t parity = (uint32_t)(c / kListStages) & 1u;
     ok = mbar_wait(&r.full[s], parity) && ok;
-    body(s, c * kListRows);
+    body(s, c * kRows);
     __syncwarp();
     if (lane == 0 && c + kListStages < nchunks) ring_issue(r, cmap, bmap, c + kListStages, col0);
   }
   return ok;
 }
 
-template <bool kWithBins>
-__device__ __forceinline__ void ring_init(WarpListRing<kWithBins>& r) {
+template <bool kWithBins, int kRows>
+__device__ __forceinline__ void ring_init(WarpListRing<kWithBins, kRows>& r) {
   if ((threadIdx.x & 31) == 0) {
     for (int s = 0; s < kListStages; ++s) mbar_init(&r.full[s], 1);
     fence_barrier_init();
