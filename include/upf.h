@@ -304,8 +304,9 @@ upf_status upf_profile_step(upf_system* s, upf_phase_times* out);
  * whose kernels run at fixed block sizes) --------------------------------
  * CTA sizes of the neighbour-list and external-force passes, and CTA size x
  * list rows per TMA stage of the two predict-correct passes. Valid loop-pass
- * pairs: (128,8) (128,16) (256,4) (256,8) (512,4); batches allow up to 256
- * threads. Shapes change timing only: every shape gives the same results. */
+ * pairs: (128,4) (128,8) (128,16) (256,2) (256,4) (256,8) (512,2) (512,4)
+ * (1024,2); batches allow up to 256 threads. Shapes change timing only:
+ * every shape gives the same results. */
 typedef struct upf_launch_config {
   int32_t nlist_threads;      /* 64, 128, 256 */
   int32_t external_threads;   /* 128, 256 */

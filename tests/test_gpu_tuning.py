@@ -9,7 +9,7 @@ from unifiedparticleframeworkcuda_b200 import UpfError, UpfLaunchConfig, scenes
 
 pytestmark = pytest.mark.gpu
 
-LOOP_PAIRS = [(128, 8), (128, 16), (256, 4), (256, 8), (512, 4)]
+LOOP_PAIRS = [(128, 4), (128, 8), (128, 16), (256, 2), (256, 4), (256, 8), (512, 2), (512, 4), (1024, 2)]
 
 
 def shape(nl, ext, dens, pf):
@@ -100,3 +100,4 @@ def test_invalid_shapes_rejected(upf_lib):
     with upf_lib.ParticleBatch.from_scenes(scs) as b:
         with pytest.raises(UpfError):
             b.set_launch_config(shape(256, 256, (512, 4), (256, 8)))  # a CTA across two scenes
+        b.set_launch_config(shape(128, 128, (256, 2), (128, 4)))

@@ -160,7 +160,7 @@ upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt,
 
 upf_status encode_list_maps(CUtensorMap* cmaps, CUtensorMap* bmaps, uint32_t* nbr, uint16_t* bins, uint64_t cols,
                             uint64_t rows) {
-  const uint32_t box_rows[kListRowVariants] = {4, 8, 16};
+  const uint32_t box_rows[kListRowVariants] = {2, 4, 8, 16};
   for (int k = 0; k < kListRowVariants; ++k) {
     upf_status st = encode_list_map(&cmaps[k], nbr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, cols, rows, box_rows[k]);
     if (st != UPF_OK) return st;
@@ -176,13 +176,16 @@ bool shape_valid(const LaunchShape& s, bool batched, const char** why) {
     return false;
   };
   auto pair_ok = [&](int t, int r) {
-    return (t == 128 && (r == 8 || r == 16)) || (t == 256 && (r == 4 || r == 8)) || (t == 512 && r == 4);
+    for (const auto& p : kLoopShapes)
+      if (p[0] == t && p[1] == r) return true;
+    return false;
   };
   if (s.nlist_threads != 64 && s.nlist_threads != 128 && s.nlist_threads != 256)
     return bad("nlist_threads must be 64, 128 or 256");
   if (s.external_threads != 128 && s.external_threads != 256) return bad("external_threads must be 128 or 256");
   if (!pair_ok(s.density_threads, s.density_rows) || !pair_ok(s.pforce_threads, s.pforce_rows))
-    return bad("(threads, rows) of a loop pass must be (128,8), (128,16), (256,4), (256,8) or (512,4)");
+    return bad("(threads, rows) of a loop pass must be one of (128,4) (128,8) (128,16) (256,2) (256,4) (256,8) "
+               "(512,2) (512,4) (1024,2)");
   if (batched && (s.density_threads > 256 || s.pforce_threads > 256))
     return bad("batched scenes: at most 256 threads per CTA (a CTA must stay within one scene's segment)");
   return true;
@@ -275,7 +278,7 @@ upf_status autotune_shapes(const TuneOps& ops, int repeats, upf_launch_config* o
       sh.external_threads = best;
       chosen_ms[1] = best_ms;
     }
-    const int pairs[5][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {512, 4}};
+    const auto& pairs = kLoopShapes;
     for (int pass = 0; pass < 2 && rc == UPF_OK; ++pass) {
       cudaError_t (*launch)(void*, cudaStream_t) = pass == 0 ? ops.density : ops.pforce;
       if (!launch) continue;

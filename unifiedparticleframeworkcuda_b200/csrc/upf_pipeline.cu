@@ -1264,13 +1264,17 @@ cudaError_t run_external(const LaunchShape& sh, cudaStream_t st, const DevParams
   return cudaGetLastError();
 }
 
-#define UPF_SHAPE_SWITCH(threads, rows, CALL) \
-  switch ((threads) * 100 + (rows)) {         \
-    case 12808: CALL(128, 8); break;          \
-    case 12816: CALL(128, 16); break;         \
-    case 25604: CALL(256, 4); break;          \
-    case 25608: CALL(256, 8); break;          \
-    case 51204: CALL(512, 4); break;          \
+#define UPF_SHAPE_SWITCH(threads, rows, CALL)     \
+  switch ((threads) * 100 + (rows)) {             \
+    case 12804: CALL(128, 4); break;              \
+    case 12808: CALL(128, 8); break;              \
+    case 12816: CALL(128, 16); break;             \
+    case 25602: CALL(256, 2); break;              \
+    case 25604: CALL(256, 4); break;              \
+    case 25608: CALL(256, 8); break;              \
+    case 51202: CALL(512, 2); break;              \
+    case 51204: CALL(512, 4); break;              \
+    case 102402: CALL(1024, 2); break;            \
     default: return cudaErrorInvalidConfiguration; \
   }
 

@@ -58,14 +58,18 @@ struct RigidArrays {
 struct LaunchShape {
   int nlist_threads = 256;     // 64, 128, 256
   int external_threads = 256;  // 128, 256
-  int density_threads = 256;   // with density_rows: (128,8) (128,16) (256,4) (256,8) (512,4)
+  int density_threads = 256;   // with density_rows: see kLoopShapes
   int density_rows = 8;
   int pforce_threads = 256;    // with pforce_rows: the same pairs
   int pforce_rows = 8;
 };
 bool shape_valid(const LaunchShape& s, bool batched, const char** why);
-constexpr int kListRowVariants = 3;  // tensor maps for 4, 8 and 16 rows per box
-inline int rows_index(int rows) { return rows == 4 ? 0 : (rows == 8 ? 1 : 2); }
+// (threads, rows) pairs of the loop passes
+constexpr int kLoopShapes[][2] = {{128, 4}, {128, 8}, {128, 16}, {256, 2}, {256, 4},
+                                  {256, 8}, {512, 2}, {512, 4}, {1024, 2}};
+constexpr int kNumLoopShapes = sizeof(kLoopShapes) / sizeof(kLoopShapes[0]);
+constexpr int kListRowVariants = 4;  // tensor maps for 2, 4, 8 and 16 rows per box
+inline int rows_index(int rows) { return rows == 2 ? 0 : (rows == 4 ? 1 : (rows == 8 ? 2 : 3)); }
 
 // Batched scenes (upf_batch_*): independent scenes in one index space, each
 // in its own segment that starts on a kSegAlign boundary, so every CTA of a
