@@ -391,6 +391,70 @@ def run_batch(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def run_adjoint(args, rank, world, local_rank):
+    """--scene c5: the differentiation form. 65,536 particles (32x32x64
+    lattice, initial velocities N(0, 0.1) m/s), 200 steps at dt = 1e-3, 3
+    predict-correct iterations per step, checkpoints every 20 steps; loss =
+    |x_com(T) - target|^2 + 1e-6 mean (rho - rho0)^2. Reports the forward and
+    backward device times and their ratio; the value is the backward's
+    particle-steps per second."""
+    import torch
+    import unifiedparticleframeworkcuda_b200 as upf
+    from unifiedparticleframeworkcuda_b200 import build as upfbuild
+    from unifiedparticleframeworkcuda_b200 import scenes
+
+    if rank == 0:
+        upfbuild.build()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sc = scenes.adjoint_scene(32, 32, 64, seed=77 + rank)
+    p = upf.derive_params(sc.params)
+    T = args.adjoint_steps
+    tgt = sc.pos[:, :3].astype(np.float64).mean(0) + np.array([0.1, 0.0, 0.0])
+    stream = torch.cuda.Stream(device=dev)
+    a = upf.Adjoint(p, sc.pos, sc.vel, T, checkpoint_interval=20, loop_iterations=3, target=tgt, derive=False,
+                    device=local_rank)
+    a.set_stream(stream.cuda_stream)
+    for _ in range(max(args.warmup, 1)):
+        a.forward()
+        a.backward()
+    fwd, bwd = [], []
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            loss = a.forward()
+            g, gm = a.backward()
+            f, b = a.times()
+            fwd.append(f)
+            bwd.append(b)
+    t = torch.tensor([float(np.median(fwd)), float(np.median(bwd))], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    f_ms, b_ms = float(t[0]), float(t[1])
+    a.close()
+    if rank != 0:
+        return
+    n = sc.n
+    out = {
+        "metric": "adjoint (backward) particle-steps/s, 65,536-particle PCISPH trajectory of 200 steps; bwd/fwd ratio",
+        "value": n * T * world / (b_ms / 1e3), "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": b_ms / T, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "adjoint_pcisph_65536x200", "particles": n, "trajectory_steps": T,
+                   "checkpoint_interval": 20, "loop_iterations": 3, "density_smoothing": 1e-2,
+                   "forward_ms": f_ms, "backward_ms": b_ms, "bwd_fwd_ratio": b_ms / f_ms, "loss": loss,
+                   "grad_norm": float(np.linalg.norm(g)), "dloss_dviscosity": gm,
+                   "timing": "median over the timed forward/backward pairs, CUDA events on the library stream",
+                   "l2": "per-interval lists and intermediates ~0.9 GB (larger than L2)"},
+        "e2e": {"value": n * T * world / ((f_ms + b_ms) / 1e3), "unit": "particle-steps/s (forward + backward)",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": n * 16 // T},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import unifiedparticleframeworkcuda_b200 as upf
@@ -581,7 +645,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3", "c4"])
+    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3", "c4", "c5"])
+    ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--block-size", type=int, default=0)
     ap.add_argument("--settle", type=int, default=0,
@@ -608,6 +673,8 @@ def main():
     try:
         if args.scene == "c4":
             run_batch(args, rank, world, local_rank)
+        elif args.scene == "c5":
+            run_adjoint(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

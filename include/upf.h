@@ -438,6 +438,52 @@ upf_status upf_batch_get_launch_config(upf_batch* b, upf_launch_config* out);
 upf_status upf_batch_set_launch_config(upf_batch* b, const upf_launch_config* cfg);
 upf_status upf_batch_autotune(upf_batch* b, int32_t repeats, upf_launch_config* chosen);
 
+/* ---- differentiation (adjoint) -------------------------------------------
+ * No counterpart in the reference. A differentiable PCISPH trajectory and its
+ * hand-written adjoint: LIQUID particles, the reference's kernel functions
+ * evaluated analytically (the 300-bin tables are piecewise constant, their
+ * derivative zero), a fixed number of predict-correct iterations per step (a
+ * data-dependent count would make the loss discontinuous), the pressure
+ * update's max(rho - rho0, 0) smoothed to 0.5 (d + sqrt(d^2 + eps^2)) with
+ * eps = density_smoothing * rho0 (at a hard kink the gradient of a 20-step
+ * trajectory changes by percent under float-rounding-sized perturbations of
+ * the input; smoothed over +-1% of rho0, the PCISPH tolerance's own scale, an
+ * FP32 adjoint of 20 steps agrees with FP64 to 1e-4), viscosity +
+ * gravity + PCISPH pressure, no surface tension or wall forces (collision-box
+ * clamping is applied forward and treated as inactive by the adjoint: keep
+ * the particles clear of the walls). Loss:
+ *   L = com_weight * |x_com(T) - target|^2
+ *     + density_weight * mean_i (rho_i(T) - rho0)^2,
+ * rho_i(T) the SPH density at the final positions. upf_adjoint_backward
+ * returns dL/dv(0) per particle and dL/d viscosity, recomputing each
+ * checkpoint interval forward from its checkpoint. */
+typedef struct upf_adjoint upf_adjoint;
+typedef struct upf_adjoint_options {
+  int32_t steps;                /* T */
+  int32_t checkpoint_interval;  /* steps between stored states (>= 1) */
+  int32_t loop_iterations;      /* predict-correct iterations per step (>= 1) */
+  float target[3];
+  float com_weight;
+  float density_weight;
+  float density_smoothing;      /* eps / rho0 of the smooth maximum (> 0; 1e-2: the 1% error scale) */
+} upf_adjoint_options;
+
+upf_status upf_adjoint_create(const upf_params* p, const upf_adjoint_options* opt, const float* pos4,
+                              const float* vel4, uint32_t n, int device, upf_adjoint** out);
+upf_status upf_adjoint_destroy(upf_adjoint* a);
+upf_status upf_adjoint_set_stream(upf_adjoint* a, void* stream);
+/* Runs the T steps from the initial positions with initial velocities vel4
+ * (n x 4 host floats; NULL keeps the last ones) and the given viscosity;
+ * *loss (may be NULL) receives L. */
+upf_status upf_adjoint_forward(upf_adjoint* a, const float* vel4, float viscosity, double* loss);
+/* Gradients of the last forward's loss: grad_vel4 (n x 4 host floats, w = 0)
+ * and *grad_viscosity (either may be NULL). */
+upf_status upf_adjoint_backward(upf_adjoint* a, float* grad_vel4, double* grad_viscosity);
+/* Final positions and velocities of the last forward (n x 4 host floats). */
+upf_status upf_adjoint_get_state(upf_adjoint* a, float* pos4, float* vel4);
+/* Device times of the last forward and backward (CUDA events). */
+upf_status upf_adjoint_times(upf_adjoint* a, float* forward_ms, float* backward_ms);
+
 /* ---- errors ------------------------------------------------------------- */
 const char* upf_last_error(void);
 const char* upf_status_string(upf_status st);

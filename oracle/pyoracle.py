@@ -88,6 +88,10 @@ def lib():
         L.orc_rigid_body_step.argtypes = [fp, fp, fp, C.c_float, C.c_float]
         L.orc_inverse3.argtypes = [fp, fp]
         L.orc_inverse3.restype = C.c_int
+        dp = C.POINTER(C.c_double)
+        L.orc_adjoint_run.argtypes = [P, dp, dp, C.c_uint32, C.c_int32, C.c_int32, dp, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, dp, dp, dp]
+        L.orc_adjoint_run.restype = C.c_int
         _lib = L
     return _lib
 
@@ -151,6 +155,26 @@ def inverse3(m9) -> np.ndarray:
     out = np.zeros(9, np.float32)
     lib().orc_inverse3(_ptr(a, C.c_float), _ptr(out, C.c_float))
     return out
+
+
+def adjoint_run(params, pos, vel, steps, iterations, target, com_weight, density_weight, viscosity, grad=True,
+                eps_rho=1e-2):
+    """FP64 differentiable PCISPH trajectory (the library's upf_adjoint model):
+    (loss, dL/dv0 (n,3), dL/dviscosity) or just the loss when grad is False."""
+    pos = np.ascontiguousarray(np.asarray(pos, np.float64)[:, :3])
+    vel = np.ascontiguousarray(np.asarray(vel, np.float64)[:, :3])
+    n = pos.shape[0]
+    tgt = np.ascontiguousarray(target, np.float64)
+    loss = C.c_double()
+    gv = np.zeros((n, 3), np.float64) if grad else None
+    gm = C.c_double()
+    rc = lib().orc_adjoint_run(C.byref(params), _ptr(pos, C.c_double), _ptr(vel, C.c_double), n, int(steps),
+                               int(iterations), _ptr(tgt, C.c_double), float(com_weight), float(density_weight),
+                               float(viscosity), float(eps_rho), C.byref(loss), _ptr(gv, C.c_double) if grad else None,
+                               C.byref(gm) if grad else None)
+    if rc != 0:
+        raise RuntimeError("orc_adjoint_run failed")
+    return (loss.value, gv, gm.value) if grad else loss.value
 
 
 def morton_table() -> np.ndarray:

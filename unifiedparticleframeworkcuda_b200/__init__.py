@@ -19,7 +19,7 @@ import numpy as np
 from ._abi import (FLAG_ADHESION, FLAG_BOUNDARY_PRESSURE, FLAG_PENALTY_WALLS,  # noqa: F401
                    FLAG_RECORD_ITERATIONS, FLAG_SURFACE_TENSION, FLAG_WALL_WEIGHT, FROZEN,
                    GRANULAR, LIQUID, METHOD_PCISPH, METHOD_WCSPH, RIGID, STATUS, UpfParams,
-                   UpfLaunchConfig, UpfPhaseTimes, UpfStepStats)
+                   UpfAdjointOptions, UpfLaunchConfig, UpfPhaseTimes, UpfStepStats)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libupf.so")
@@ -89,6 +89,13 @@ def lib():
             "upf_batch_get_launch_config": [vp, C.POINTER(UpfLaunchConfig)],
             "upf_batch_set_launch_config": [vp, C.POINTER(UpfLaunchConfig)],
             "upf_batch_autotune": [vp, C.c_int32, C.POINTER(UpfLaunchConfig)],
+            "upf_adjoint_create": [P, C.POINTER(UpfAdjointOptions), fp, fp, C.c_uint32, C.c_int, C.POINTER(vp)],
+            "upf_adjoint_destroy": [vp],
+            "upf_adjoint_set_stream": [vp, vp],
+            "upf_adjoint_forward": [vp, fp, C.c_float, C.POINTER(C.c_double)],
+            "upf_adjoint_backward": [vp, fp, C.POINTER(C.c_double)],
+            "upf_adjoint_get_state": [vp, fp, fp],
+            "upf_adjoint_times": [vp, fp, fp],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
             "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
             "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],
@@ -458,4 +465,79 @@ class ParticleBatch:
                                             _p(den, C.c_float), _p(pre, C.c_float), _p(ids, C.c_uint32),
                                             C.byref(cnt)), "upf_batch_get_particles")
         return dict(pos=pos, vel=vel, density=den, pressure=pre, id=ids)
+
+
+class Adjoint:
+    """A differentiable PCISPH trajectory and its adjoint (upf_adjoint_*):
+    forward() returns the loss, backward() its gradient with respect to the
+    initial velocities and the viscosity."""
+
+    def __init__(self, params, pos4, vel4, steps: int, checkpoint_interval: int = 20, loop_iterations: int = 3,
+                 target=(0.0, 0.0, 0.0), com_weight: float = 1.0, density_weight: float = 1e-6,
+                 density_smoothing: float = 1e-2, device: int = 0, derive: bool = True):
+        self.params = derive_params(params) if derive else params.copy()
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        vel4 = np.ascontiguousarray(vel4, np.float32)
+        self.n = pos4.shape[0]
+        if pos4.shape != (self.n, 4) or vel4.shape != (self.n, 4):
+            raise ValueError("pos4/vel4 must be (n, 4)")
+        o = UpfAdjointOptions()
+        o.steps, o.checkpoint_interval, o.loop_iterations = int(steps), int(checkpoint_interval), int(loop_iterations)
+        o.target[:] = [float(t) for t in target]
+        o.com_weight, o.density_weight = float(com_weight), float(density_weight)
+        o.density_smoothing = float(density_smoothing)
+        self.options = o
+        h = C.c_void_p()
+        check(lib().upf_adjoint_create(C.byref(self.params), C.byref(o), _p(pos4, C.c_float), _p(vel4, C.c_float),
+                                       self.n, int(device), C.byref(h)), "upf_adjoint_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().upf_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle: int | None):
+        check(lib().upf_adjoint_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None),
+              "upf_adjoint_set_stream")
+
+    def forward(self, vel4=None, viscosity: float | None = None) -> float:
+        v = None if vel4 is None else np.ascontiguousarray(vel4, np.float32)
+        if v is not None and v.shape != (self.n, 4):
+            raise ValueError("vel4 must be (n, 4)")
+        mu = self.params.viscosity if viscosity is None else float(viscosity)
+        loss = C.c_double()
+        check(lib().upf_adjoint_forward(self._h, _p(v, C.c_float), mu, C.byref(loss)), "upf_adjoint_forward")
+        return loss.value
+
+    def backward(self):
+        """(dL/dv0 as (n, 3), dL/dviscosity)."""
+        g = np.zeros((self.n, 4), np.float32)
+        gm = C.c_double()
+        check(lib().upf_adjoint_backward(self._h, _p(g, C.c_float), C.byref(gm)), "upf_adjoint_backward")
+        return g[:, :3].copy(), gm.value
+
+    def state(self):
+        pos = np.zeros((self.n, 4), np.float32)
+        vel = np.zeros((self.n, 4), np.float32)
+        check(lib().upf_adjoint_get_state(self._h, _p(pos, C.c_float), _p(vel, C.c_float)), "upf_adjoint_get_state")
+        return pos, vel
+
+    def times(self):
+        f = C.c_float()
+        b = C.c_float()
+        check(lib().upf_adjoint_times(self._h, C.byref(f), C.byref(b)), "upf_adjoint_times")
+        return f.value, b.value
 

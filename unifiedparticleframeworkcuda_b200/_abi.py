@@ -146,3 +146,16 @@ class UpfLaunchConfig(C.Structure):
         d["measured_ms"] = list(self.measured_ms)
         return d
 
+
+class UpfAdjointOptions(C.Structure):
+    """upf_adjoint_options (include/upf.h)."""
+    _fields_ = [
+        ("steps", C.c_int32),
+        ("checkpoint_interval", C.c_int32),
+        ("loop_iterations", C.c_int32),
+        ("target", C.c_float * 3),
+        ("com_weight", C.c_float),
+        ("density_weight", C.c_float),
+        ("density_smoothing", C.c_float),
+    ]
+

@@ -1410,6 +1410,16 @@ cudaError_t launch_static_setup(System& s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Neighbour lists of one sorted set with no boundary set (the adjoint's
+// per-step lists); P.nstride is the list stride, P.maxn its rows.
+cudaError_t launch_nlist_plain(const DevParams& P, uint32_t n, const float4* pos, const uint32_t* keys,
+                               const uint32_t* cstart, const uint32_t* cend, uint32_t* nbr, uint16_t* bins,
+                               uint32_t* ncnt, const float* luts, DevState* st, cudaStream_t stream) {
+  if (!n) return cudaSuccess;
+  return run_nlist<false>(LaunchShape{}, stream, P, BatchView{}, n, pos, keys, cstart, cend, 0u, nullptr, nullptr,
+                          nullptr, nullptr, nbr, bins, ncnt, luts, st);
+}
+
 // ----------------------------------------------------------- batched launchers
 cudaError_t batch_launch_init(BatchSystem& b, cudaStream_t st) {
   if (!b.n_slots) return cudaSuccess;

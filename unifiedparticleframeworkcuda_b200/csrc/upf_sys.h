@@ -211,6 +211,11 @@ struct BatchSystem {
   std::vector<void*> checkpoint_slots;
 };
 
+// upf_pipeline.cu: neighbour lists of one sorted set without boundary set
+cudaError_t launch_nlist_plain(const DevParams& P, uint32_t n, const float4* pos, const uint32_t* keys,
+                               const uint32_t* cstart, const uint32_t* cend, uint32_t* nbr, uint16_t* bins,
+                               uint32_t* ncnt, const float* luts, DevState* st, cudaStream_t stream);
+
 // upf_pipeline.cu: batched phase launchers (asynchronous on `st`)
 cudaError_t batch_launch_init(BatchSystem& b, cudaStream_t st);   // keys and lagged state after upload
 cudaError_t batch_launch_keys(BatchSystem& b, cudaStream_t st);   // keys only

@@ -365,6 +365,31 @@ def batch_scenes(num=256, seed=2024, counts=(2048, 65536), extents=(0.5, 2.0)) -
     return out
 
 
+def adjoint_scene(nx=32, ny=32, nz=64, seed=77, spacing=0.01, dt=1e-3, vel_sigma=0.1) -> Scene:
+    """The differentiation workload: an nx x ny x nz liquid block (default
+    65,536; jitter +-10% of the spacing) in the middle of a 2 m box it does
+    not reach within 200 steps, initial velocities N(0, vel_sigma) m/s per
+    component from the seed, h = 2 * spacing, dt, no surface tension or wall
+    forces (the trajectory the adjoint differentiates)."""
+    p = default_params()
+    p.method = METHOD_PCISPH
+    p.flags = 0
+    s = spacing
+    p.particle_spacing = s
+    p.support_radius = 2.0 * s
+    p.dt = dt
+    p.viscosity = 1.0
+    lo = np.array([0.02, 0.02, 0.02])
+    hi = lo + 2.0
+    _set_box(p, lo, hi)
+    p.zindex_extent[:] = (2.048, 2.048, 2.048)
+    block = np.array([nx, ny, nz], np.float64) * s
+    origin = lo + 1.0 - 0.5 * block + np.array([0.0, 0.5, 0.0])  # above the centre: it falls during the run
+    fluid = _lattice(nx, ny, nz, s, origin, 0.1 * s, seed)
+    vel = normal(seed, 3 * fluid.shape[0], stream=5).reshape(-1, 3) * vel_sigma
+    return _pack("adjoint_%dx%dx%d" % (nx, ny, nz), p, fluid, np.zeros((0, 3)), vel_fluid=vel)
+
+
 def small_coupling(seed=5) -> Scene:
     """A small coupling scene (oracle-sized): 12^3 fluid, an 8x4x8 pile and
     three small bodies."""
