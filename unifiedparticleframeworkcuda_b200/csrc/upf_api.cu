@@ -619,7 +619,7 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   e = cudaMemcpy(s->luts, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice);
   // boundary tails: zero velocity, pressure and pressure quotient
   if (e == cudaSuccess) e = cudaMemset(s->B.vel, 0, sizeof(float4) * ct);
-  if (e == cudaSuccess) e = cudaMemset(s->pq, 0, sizeof(float) * ct);
+  if (e == cudaSuccess) e = cudaMemset(s->pq, 0, sizeof(float4) * ct);
   if (e == cudaSuccess) e = cudaMemset(s->press, 0, sizeof(float) * ct);
   if (e == cudaSuccess) e = cudaMemset(s->rho, 0, sizeof(float) * ct);
   if (e == cudaSuccess) e = cudaMemset(s->st, 0, sizeof(DevState));
@@ -749,6 +749,7 @@ upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4
     const size_t tb = S.dp.static_base;
     UPF_CUDA(cudaMemcpyAsync(S.B.pos + tb, S.spos, sizeof(float4) * S.n_static, cudaMemcpyDeviceToDevice, st));
     UPF_CUDA(cudaMemcpyAsync(S.xs + tb, S.spos, sizeof(float4) * S.n_static, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.pq + tb, S.spos, sizeof(float4) * S.n_static, cudaMemcpyDeviceToDevice, st));
     std::vector<int32_t> frozen(S.n_static, UPF_FROZEN);
     UPF_CUDA(cudaMemcpyAsync(S.B.type + tb, frozen.data(), sizeof(int32_t) * S.n_static, cudaMemcpyHostToDevice, st));
   }

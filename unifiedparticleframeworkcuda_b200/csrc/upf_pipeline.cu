@@ -731,7 +731,7 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_external(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
     const float* __restrict__ wvol, const int32_t* __restrict__ id_body, const uint32_t* __restrict__ nbr,
     const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, float4* __restrict__ force,
-    float4* __restrict__ pforce, float4* __restrict__ xs, float* __restrict__ press, float* __restrict__ pq,
+    float4* __restrict__ pforce, float4* __restrict__ xs, float* __restrict__ press, float4* __restrict__ pq,
     DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float vl[UPF_LUT_ENTRIES], pg[UPF_LUT_ENTRIES], stl[UPF_LUT_ENTRIES], adl[UPF_LUT_ENTRIES];
@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_external(
   const int32_t ti = B.type[i];
   const float4 xi = B.pos[i];
   press[i] = 0.0f;
-  pq[i] = 0.0f;
+  pq[i] = make_float4(xi.x, xi.y, xi.z, 0.0f);  // position, p / rho0^2 (updated by the density pass)
   pforce[i] = f4(0, 0, 0);
   if (ti != UPF_LIQUID) {
     // predicted position of a non-liquid particle: its current position
@@ -838,7 +838,7 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const int32_t* __restrict__ type,
     const float4* __restrict__ xs, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
     const float* __restrict__ luts_plain, float* __restrict__ rho, float* __restrict__ press,
-    float* __restrict__ pq, DevState* __restrict__ st_plain) {
+    float4* __restrict__ pq, DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float m4[UPF_LUT_ENTRIES];
   __shared__ float thr[kThresholds];
@@ -889,7 +889,7 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
     press[i] = pnew;
     // p / (rho0 * rho0): the pressure-force pass divides every neighbour's
     // pressure by the same constant; dividing once here is bit-identical
-    pq[i] = pnew / (P.rho0 * P.rho0);
+    reinterpret_cast<float*>(pq + i)[3] = pnew / (P.rho0 * P.rho0);  // .w only: the position stays
     rho[i] = den;
     best = __float_as_uint(den);  // densities are positive: uint order == float order
   }
@@ -909,7 +909,7 @@ template <bool kBatch, int kThreads, int kRows>
 __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
     const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap bmap,
-    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, const float* __restrict__ pq,
+    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, const float4* __restrict__ pq,
     const float4* __restrict__ force, float4* __restrict__ pforce, float4* __restrict__ xs,
     DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
@@ -930,24 +930,25 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
   const float4 xi = active ? B.pos[i] : make_float4(0, 0, 0, 0);
   const float m = P.mass;
   // grad = p_i / rho0^2 + p_j / rho0^2, both quotients precomputed by the
-  // density pass (pq); boundary particles have p = 0, so 0 / rho0^2 = 0
-  const float qi = active ? pq[i] : 0.0f;
+  // density pass (pq.w); boundary particles have p = 0, so 0 / rho0^2 = 0
+  const float qi = active ? pq[i].w : 0.0f;
   float fx = 0, fy = 0, fz = 0;
-  const float4* __restrict__ pos = B.pos;
   // positions are those the list was built at: every entry passes |x_i - x_j| < h
   // and its kernel-table bin is stored with it
   WarpListRing<true, kRows>& ring = rings[warp];
   const bool ok = ring_walk(ring, &cmap, &bmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
                             [&](int s, int k0) {
-                              // boundary particles sit in the arrays' tails (pq = 0 there)
+                              // one gather per neighbour: position and p / rho0^2 packed in
+                              // pq (boundary particles sit in the tail, w = 0 there)
                               float4 xj[kRows];
                               float qj[kRows];
 #pragma unroll
                               for (int r = 0; r < kRows; ++r) {
                                 if (k0 + r < (int)cnt) {
                                   const uint32_t code = ring.codes[s][r][lane];
-                                  xj[r] = __ldg(pos + code);
-                                  qj[r] = __ldg(pq + code);
+                                  const float4 v = __ldg(pq + code);
+                                  xj[r] = v;
+                                  qj[r] = v.w;
                                 }
                               }
 #pragma unroll
@@ -1251,7 +1252,7 @@ template <bool kBatch>
 cudaError_t run_external(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
                          const DynArrays& B, const float* wvol, const int32_t* id_body, const uint32_t* nbr,
                          const uint32_t* ncnt, const float* luts, float4* force, float4* pforce, float4* xs,
-                         float* press, float* pq, DevState* stp) {
+                         float* press, float4* pq, DevState* stp) {
 #define UPF_EXT(T)                                                                                        \
   k_pcisph_external<kBatch, T><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, B, wvol, id_body, nbr, ncnt, luts, \
                                                               force, pforce, xs, press, pq, stp)
@@ -1281,7 +1282,7 @@ cudaError_t run_external(const LaunchShape& sh, cudaStream_t st, const DevParams
 template <bool kBatch>
 cudaError_t run_density(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
                         const int32_t* type, const float4* xs, const CUtensorMap* cmaps, const uint32_t* ncnt,
-                        const float* luts, float* rho, float* press, float* pq, DevState* stp) {
+                        const float* luts, float* rho, float* press, float4* pq, DevState* stp) {
 #define UPF_DEN(T, R)                                                                                           \
   k_pcisph_density<kBatch, T, R><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, type, xs, cmaps[rows_index(R)], ncnt, \
                                                                 luts, rho, press, pq, stp)
@@ -1293,7 +1294,7 @@ cudaError_t run_density(const LaunchShape& sh, cudaStream_t st, const DevParams&
 template <bool kBatch>
 cudaError_t run_pforce(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
                        const DynArrays& B, const CUtensorMap* cmaps, const CUtensorMap* bmaps, const uint32_t* ncnt,
-                       const float* luts, const float* pq, const float4* force, float4* pforce, float4* xs,
+                       const float* luts, const float4* pq, const float4* force, float4* pforce, float4* xs,
                        DevState* stp) {
 #define UPF_PF(T, R)                                                                                         \
   k_pcisph_pressure_force<kBatch, T, R><<<(n + T - 1) / T, T, 0, st>>>(                                      \

@@ -112,7 +112,7 @@ struct System {
   float4* xs = nullptr;
   float* rho = nullptr;
   float* press = nullptr;
-  float* pq = nullptr;         // press / rest_density^2 (PCISPH loop)
+  float4* pq = nullptr;        // (position, press / rest_density^2): the pressure-force pass's one gather
   float* wvol = nullptr;       // Akinci volume per neighbour index (dynamic, then boundary tail)
 
   // neighbour lists
@@ -184,7 +184,7 @@ struct BatchSystem {
   float4* xs = nullptr;
   float* rho = nullptr;
   float* press = nullptr;
-  float* pq = nullptr;
+  float4* pq = nullptr;
   uint32_t* nbr = nullptr;
   uint16_t* bins = nullptr;
   uint32_t* ncnt = nullptr;
