@@ -274,7 +274,11 @@ def run_batch(args, rank, world, local_rank):
     b.set_stream(stream.cuda_stream)
     b.step(args.warmup)
     b.synchronize()
-    tuned = b.autotune(3).as_dict() if not args.no_autotune else b.launch_config().as_dict()
+    if args.shape:
+        b.set_launch_config(parse_shape(args.shape))
+        tuned = b.launch_config().as_dict()
+    else:
+        tuned = b.autotune(3).as_dict() if not args.no_autotune else b.launch_config().as_dict()
     b.reset_counters()
     b.checkpoint(0)
 
@@ -455,6 +459,18 @@ def run_adjoint(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def parse_shape(text):
+    """'nlist,external,density_threads,density_rows,pforce_threads,pforce_rows'"""
+    from unifiedparticleframeworkcuda_b200 import UpfLaunchConfig
+    v = [int(t) for t in text.split(",")]
+    if len(v) != 6:
+        raise SystemExit("--shape needs six integers")
+    c = UpfLaunchConfig()
+    (c.nlist_threads, c.external_threads, c.density_threads, c.density_rows, c.pforce_threads,
+     c.pforce_rows) = v
+    return c
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import unifiedparticleframeworkcuda_b200 as upf
@@ -492,7 +508,11 @@ def run_ours(args, rank, world, local_rank):
     # it leaves the state unchanged)
     s.step(args.warmup)
     s.synchronize()
-    tuned = s.autotune(3).as_dict() if not args.no_autotune else s.launch_config().as_dict()
+    if args.shape:
+        s.set_launch_config(parse_shape(args.shape))
+        tuned = s.launch_config().as_dict()
+    else:
+        tuned = s.autotune(3).as_dict() if not args.no_autotune else s.launch_config().as_dict()
     s.reset_counters()
     # the end-to-end run below replays the same steps from this state
     s.checkpoint(0)
@@ -549,8 +569,10 @@ def run_ours(args, rank, world, local_rank):
     achieved = kbytes / (kms / 1e3) / 1e9
     step_bytes = algorithmic_bytes(nf, nb, args.steps, total_iters, method)
     # DRAM bytes per fluid particle per launch from one ncu capture of the same
-    # kernels (profiles/pcisph_loop_kernels_262k_ncu.md), scaled by fluid count
-    traffic_per_particle = {"k_pcisph_density": 158.0, "k_pcisph_pressure_force": 261.0}
+    # kernels at the tuned shapes (profiles/pcisph_loop_kernels_262k_tuned_ncu.md),
+    # scaled by the fluid count: the list length per particle does not depend
+    # on the scene size
+    traffic_per_particle = {"k_pcisph_density": 156.0, "k_pcisph_pressure_force": 276.0}
     traffic = traffic_per_particle[kname] * nf if kname in traffic_per_particle else None
 
     # end to end through the C ABI with host buffers, over the same steps as
@@ -654,6 +676,8 @@ def main():
                          "collapse (the CPU reference arm always times steps from rest)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--shape", default="", help="fixed launch shapes instead of the autotuner: "
+                                                "nlist,external,density_threads,density_rows,pforce_threads,pforce_rows")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
