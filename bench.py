@@ -34,6 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from unifiedparticleframeworkcuda_b200 import replicas  # noqa: E402
+
 METRIC = "particle-steps/s at 1M PCISPH (<1% density err)"
 UNIT = "particle-steps/s"
 RADIX_PASSES = 4  # 30-bit Morton keys, 8-bit digits
@@ -296,10 +298,7 @@ def run_batch(args, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(e0.elapsed_time(e1))[0]
 
     with ClockSampler(local_rank) as clk:
         batch_ms = timed(lambda: b.step(args.steps))
@@ -432,10 +431,7 @@ def run_adjoint(args, rank, world, local_rank):
             f, b = a.times()
             fwd.append(f)
             bwd.append(b)
-    t = torch.tensor([float(np.median(fwd)), float(np.median(bwd))], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    f_ms, b_ms = float(t[0]), float(t[1])
+    f_ms, b_ms = replicas.max_over_ranks(float(np.median(fwd)), float(np.median(bwd)))
     a.close()
     if rank != 0:
         return
@@ -535,10 +531,7 @@ def run_ours(args, rank, world, local_rank):
     elapsed_ms = start.elapsed_time(end)
     s.synchronize()
     stats = s.stats()
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = replicas.max_over_ranks(elapsed_ms)[0]
     total_iters = stats.total_iterations if method == "pcisph" else 0
     mean_k = total_iters / max(stats.total_steps, 1)
     value = nd * args.steps * world / (max_ms / 1e3)
@@ -614,10 +607,8 @@ def run_ours(args, rank, world, local_rank):
             readback()
         e1.record(stream)
         torch.cuda.synchronize()
-        t2 = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
-        e2e = {"value": nd * k_e2e * world / (float(t2.item()) / 1e3), "unit": UNIT,
+        e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1))[0]
+        e2e = {"value": nd * k_e2e * world / (e2e_ms / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * (16 + 16 + 4 + 4 + 4 + 4),
                "steps": k_e2e}
 
