@@ -484,6 +484,17 @@ upf_status upf_adjoint_get_state(upf_adjoint* a, float* pos4, float* vel4);
 /* Device times of the last forward and backward (CUDA events). */
 upf_status upf_adjoint_times(upf_adjoint* a, float* forward_ms, float* backward_ms);
 
+/* ---- failure-detection self-tests (no counterpart in the reference, which
+ * exits on API errors and only prints kernel errors) -----------------------
+ * upf_test_fail_allocation(nth): the nth library device allocation from now
+ * on (0 = the next) fails with UPF_ERR_ALLOC without calling cudaMalloc;
+ * nth < 0 disarms. Process-wide; for exercising error paths.
+ * upf_selftest_bounded_wait: one warp waits, with the bounded wait the list
+ * stream uses, on a barrier that never completes; the wait gives up after
+ * limit_us and the call returns UPF_ERR_TIMEOUT, with the context intact. */
+upf_status upf_test_fail_allocation(int32_t nth);
+upf_status upf_selftest_bounded_wait(int device, uint32_t limit_us);
+
 /* ---- errors ------------------------------------------------------------- */
 const char* upf_last_error(void);
 const char* upf_status_string(upf_status st);

@@ -466,6 +466,10 @@ struct upf_adjoint {
   template <class T>
   upf_status alloc(T** ptr, size_t count) {
     *ptr = nullptr;
+    if (inject_alloc_failure()) {
+      set_error("upf_adjoint: cudaMalloc failed: injected by upf_test_fail_allocation");
+      return UPF_ERR_ALLOC;
+    }
     cudaError_t e = cudaMalloc((void**)ptr, std::max<size_t>(count, 1) * sizeof(T));
     if (e != cudaSuccess) {
       *ptr = nullptr;
@@ -694,6 +698,7 @@ upf_status upf_adjoint_set_stream(upf_adjoint* a, void* stream) {
 }
 
 upf_status upf_adjoint_forward(upf_adjoint* a, const float* vel4, float viscosity, double* loss) {
+  NvtxRange nvtx("upf_adjoint_forward");
   if (!a) {
     set_error("upf_adjoint_forward: null");
     return UPF_ERR_INVALID_ARG;
@@ -752,6 +757,7 @@ upf_status upf_adjoint_forward(upf_adjoint* a, const float* vel4, float viscosit
 }
 
 upf_status upf_adjoint_backward(upf_adjoint* a, float* grad_vel4, double* grad_viscosity) {
+  NvtxRange nvtx("upf_adjoint_backward");
   if (!a || !a->have_forward) {
     set_error("upf_adjoint_backward: run upf_adjoint_forward first");
     return a ? UPF_ERR_STATE : UPF_ERR_INVALID_ARG;

@@ -10,8 +10,10 @@
 // 2139-2154). Here one step is a single CUDA graph and the loop is a
 // device-side conditional while-node fed by the loop-control kernel.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -26,6 +28,21 @@ namespace upf {
 namespace {
 thread_local char g_err[512] = "";
 }
+
+namespace {
+std::atomic<int64_t> g_fail_alloc_at{-1};  // allocations left before the injected failure; -1: none
+}  // namespace
+
+bool inject_alloc_failure() {
+  int64_t v = g_fail_alloc_at.load();
+  while (v >= 0) {
+    if (g_fail_alloc_at.compare_exchange_weak(v, v - 1)) return v == 0;
+  }
+  return false;
+}
+
+NvtxRange::NvtxRange(const char* name) { nvtxRangePushA(name); }
+NvtxRange::~NvtxRange() { nvtxRangePop(); }
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -49,6 +66,10 @@ template <class T>
 upf_status dalloc(System& s, T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
+  if (inject_alloc_failure()) {
+    set_error("cudaMalloc of %zu bytes failed: injected by upf_test_fail_allocation", count * sizeof(T));
+    return UPF_ERR_ALLOC;
+  }
   cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
   if (e != cudaSuccess) {
     set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
@@ -450,6 +471,20 @@ void clear_rigid(System& s) {
   s.rb = RigidArrays{};
 }
 
+// One warp waits, with the library's bounded wait, on an mbarrier that no
+// thread and no copy ever completes; the wait gives up after limit_ns and
+// records ERR_TIMEOUT like the list stream's waits do.
+__global__ void k_selftest_wait(uint64_t limit_ns, DevState* st) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+  const bool ok = mbar_wait(&bar, 0, limit_ns);
+  if (!ok && threadIdx.x == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
+}
+
 __global__ void k_init_dyn(uint32_t n, DynArrays A, float rho0) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -494,6 +529,44 @@ const char* upf_status_string(upf_status st) {
 }
 
 int32_t upf_abi_version(void) { return UPF_ABI_VERSION; }
+
+upf_status upf_test_fail_allocation(int32_t nth) {
+  g_fail_alloc_at.store(nth < 0 ? -1 : (int64_t)nth);
+  return UPF_OK;
+}
+
+upf_status upf_selftest_bounded_wait(int device, uint32_t limit_us) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("upf_selftest_bounded_wait: no CUDA device");
+    return UPF_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev || limit_us == 0 || limit_us > 1000000) {
+    set_error("upf_selftest_bounded_wait: bad device or limit (1..1e6 us)");
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaSetDevice(device));
+  DevState* st = nullptr;
+  UPF_CUDA(cudaMalloc(&st, sizeof(DevState)));
+  cudaError_t e = cudaMemset(st, 0, sizeof(DevState));
+  if (e == cudaSuccess) {
+    k_selftest_wait<<<1, 32>>>((uint64_t)limit_us * 1000ull, st);
+    e = cudaGetLastError();
+  }
+  DevState h{};
+  if (e == cudaSuccess) e = cudaMemcpy(&h, st, sizeof(DevState), cudaMemcpyDeviceToHost);
+  cudaFree(st);
+  if (e != cudaSuccess) {
+    set_error("upf_selftest_bounded_wait: %s", cudaGetErrorString(e));
+    return UPF_ERR_CUDA;
+  }
+  if (h.error_flags & ERR_TIMEOUT) {
+    set_error("a bounded device-side wait ran out (self-test)");
+    return UPF_ERR_TIMEOUT;
+  }
+  return UPF_OK;
+}
 
 upf_status upf_default_params(upf_params* p) {
   if (!p) {
@@ -673,6 +746,7 @@ upf_status upf_set_stream(upf_system* s, void* stream) {
 
 upf_status upf_set_particles(upf_system* s, const float* pos4, const float* vel4, const int32_t* type,
                              uint32_t n) {
+  NvtxRange nvtx("upf_set_particles");
   if (!s || (n && (!pos4 || !vel4 || !type))) {
     set_error("upf_set_particles: null argument");
     return UPF_ERR_INVALID_ARG;
@@ -947,6 +1021,7 @@ upf_status upf_get_rigid_bodies(upf_system* s, float* pos3, float* vel3, float* 
 }
 
 upf_status upf_step(upf_system* s, int32_t nsteps) {
+  NvtxRange nvtx("upf_step");
   if (!s || nsteps < 0) {
     set_error("upf_step: bad arguments");
     return UPF_ERR_INVALID_ARG;
@@ -1208,6 +1283,7 @@ struct SysTune {
 }  // namespace
 
 upf_status upf_autotune(upf_system* s, int32_t repeats, upf_launch_config* chosen) {
+  NvtxRange nvtx("upf_autotune");
   UPF_TRY(phase_guard(s));
   UPF_CUDA(cudaStreamSynchronize(s->stream));
   SysTune t{s, nullptr};
@@ -1256,6 +1332,7 @@ upf_status upf_autotune(upf_system* s, int32_t repeats, upf_launch_config* chose
 }
 
 upf_status upf_profile_step(upf_system* s, upf_phase_times* out) {
+  NvtxRange nvtx("upf_profile_step");
   UPF_TRY(phase_guard(s));
   s->stepped = true;
   if (!out) {

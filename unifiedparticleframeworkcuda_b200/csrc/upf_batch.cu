@@ -42,6 +42,10 @@ template <class T>
 upf_status balloc(BatchSystem& b, T** p, size_t count) {
   *p = nullptr;
   if (count == 0) count = 1;
+  if (inject_alloc_failure()) {
+    set_error("cudaMalloc of %zu bytes failed: injected by upf_test_fail_allocation", count * sizeof(T));
+    return UPF_ERR_ALLOC;
+  }
   cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
   if (e != cudaSuccess) {
     set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
@@ -158,6 +162,7 @@ extern "C" {
 
 upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, uint32_t num_scenes, int device,
                             upf_batch** out) {
+  NvtxRange nvtx("upf_batch_create");
   if (!out || !params || !counts || num_scenes == 0) {
     set_error("upf_batch_create: null argument or no scenes");
     return UPF_ERR_INVALID_ARG;
@@ -339,6 +344,7 @@ upf_status upf_batch_set_stream(upf_batch* b, void* stream) {
 }
 
 upf_status upf_batch_set_particles(upf_batch* b, const float* pos4, const float* vel4) {
+  NvtxRange nvtx("upf_batch_set_particles");
   if (!b || (b->n_particles && (!pos4 || !vel4))) {
     set_error("upf_batch_set_particles: null argument");
     return UPF_ERR_INVALID_ARG;
@@ -375,6 +381,7 @@ upf_status upf_batch_set_particles(upf_batch* b, const float* pos4, const float*
 }
 
 upf_status upf_batch_step(upf_batch* b, int32_t nsteps) {
+  NvtxRange nvtx("upf_batch_step");
   UPF_TRY(batch_guard(b, "upf_batch_step"));
   if (nsteps < 0) {
     set_error("upf_batch_step: negative step count");
@@ -570,6 +577,7 @@ struct BatchTune {
 }  // namespace
 
 upf_status upf_batch_autotune(upf_batch* b, int32_t repeats, upf_launch_config* chosen) {
+  NvtxRange nvtx("upf_batch_autotune");
   UPF_TRY(batch_guard(b, "upf_batch_autotune"));
   UPF_CUDA(cudaStreamSynchronize(b->stream));
   BatchTune t{b, nullptr};

@@ -24,6 +24,17 @@ uint32_t default_search_cell(const upf_params& p);
 uint32_t effective_search_cell(const upf_params& p);  // p.search_cell, or the default when 0
 double density_error_factor(const upf_params& p);
 
+// upf_api.cu: test hook for allocation failures (upf_test_fail_allocation):
+// true when the library's next device allocation is the one to fail
+bool inject_alloc_failure();
+
+// NVTX ranges around host entry points (header-only NVTX 3: a no-op unless a
+// tool is attached)
+struct NvtxRange {
+  explicit NvtxRange(const char* name);
+  ~NvtxRange();
+};
+
 // upf_sort.cu
 constexpr uint32_t kRadixTileKeys = 8192;  // keys per sort tile (16 warps x 512)
 constexpr uint32_t kRadixDigits = 256;     // 8-bit digits

@@ -19,7 +19,8 @@ namespace upf {
 
 constexpr int kListRows = 8;     // default list rows per stage (a launch shape parameter)
 constexpr int kListStages = 3;   // ring depth
-constexpr uint32_t kWaitSpins = 1u << 22;  // bounded wait (~seconds at worst)
+constexpr uint32_t kWaitSpins = 1u << 24;          // bounded wait: at most this many polls ...
+constexpr uint64_t kWaitLimitNs = 1000000000ull;    // ... and at most 1 s of device time
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -48,11 +49,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait; returns false (and the caller records a timeout) if the phase
-// did not complete
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t s = 0; s < kWaitSpins; ++s)
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait, by poll count and by device time; returns false (and the
+// caller records a timeout) if the phase did not complete
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t s = 0; s < kWaitSpins; ++s) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
+  }
   return false;
 }
 
