@@ -107,21 +107,20 @@ __device__ __forceinline__ float dist3(float4 a, float4 b) {
 __device__ __forceinline__ int lut_index(float d, float factor) {
   return (int)fmul(fmul(d, factor), (float)kLut);
 }
-// lut_index(sqrt_rn(r2)) from r2 without the correctly rounded square root:
-// an approximate root (relative error ~1e-7, so the scaled value is off by
-// far less than one bin) gives a guess g, and the exact thresholds `thr`
-// (kThresholds entries, see above) move it to the exact bin. Returns 300 for
-// r2 beyond the last bin (the tables' zero entry).
+// lut_index(sqrt_rn(r2)) from r2 without the correctly rounded square root.
+// rsqrtf is within 2 ulp, so r2 * rsqrtf(r2) is within 2^-21 of sqrt(r2);
+// scaled down by (1 - 2^-19) it is below the true root and within 2^-18 of
+// it. The reference's index, floor of sqrt_rn(r2) * factor * 300 with three
+// float roundings, lies within 2^-22 of the exact product, so the guess taken
+// from the scaled-down root is that index or one below it (the two differ by
+// under 300 * 2^-17.9 < 1): one exact threshold `thr` (kThresholds entries,
+// see above) decides. Returns 300 at or beyond the last bin (the tables' zero
+// entry); r2 == 0 gives bin 0 (0 * inf = NaN converts to 0).
 __device__ __forceinline__ int bin_of_r2(float r2, float factor, const float* thr) {
-  float d = r2 * rsqrtf(r2);             // approximate sqrt; r2 == 0 gives NaN -> guess 0
+  const float d = r2 * rsqrtf(r2) * 0.999998092651367188f;  // 1 - 2^-19
   int g = (int)(d * factor * (float)kLut);
-  g = g < 0 ? 0 : (g > kLut - 1 ? kLut - 1 : g);
-  if (thr[g + 1] <= r2) {
-    ++g;
-  } else if (g > 0 && thr[g] > r2) {
-    --g;
-  }
-  return g;
+  g = g > kLut - 1 ? kLut - 1 : g;
+  return g + (thr[g + 1] <= r2 ? 1 : 0);
 }
 
 // PCISPH dist_lut: uint(dist * 300 / h), clamped to 300

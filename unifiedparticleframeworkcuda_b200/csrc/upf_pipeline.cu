@@ -873,12 +873,11 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
 #pragma unroll
                               for (int r = 0; r < kRows; ++r) {
                                 if (k0 + r < (int)cnt) {
-                                  // d < h and the table bin of d, from d^2 (exact)
+                                  // the table bin of d from d^2 (exact); at or beyond h the
+                                  // bin is 300, whose entry 0 adds +0 exactly as the
+                                  // reference's skipped term does
                                   const float r2 = dist2(xi, xj[r]);
-                                  if (r2 < thr[kThresholds - 1]) {
-                                    const float kv = m4[bin_of_r2(r2, P.lut_factor, thr)];
-                                    den += kv * m;
-                                  }
+                                  den += m4[bin_of_r2(r2, P.lut_factor, thr)] * m;
                                 }
                               }
                             });
