@@ -456,14 +456,15 @@ def run_adjoint(args, rank, world, local_rank):
 
 
 def parse_shape(text):
-    """'nlist,external,density_threads,density_rows,pforce_threads,pforce_rows'"""
+    """'nlist,external,density_threads,density_rows,pforce_threads,pforce_rows[,density_mode,pforce_mode]'"""
     from unifiedparticleframeworkcuda_b200 import UpfLaunchConfig
     v = [int(t) for t in text.split(",")]
-    if len(v) != 6:
-        raise SystemExit("--shape needs six integers")
+    if len(v) not in (6, 8):
+        raise SystemExit("--shape needs six or eight integers")
+    v += [0, 0] if len(v) == 6 else []
     c = UpfLaunchConfig()
     (c.nlist_threads, c.external_threads, c.density_threads, c.density_rows, c.pforce_threads,
-     c.pforce_rows) = v
+     c.pforce_rows, c.density_mode, c.pforce_mode) = v
     return c
 
 
@@ -668,7 +669,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--shape", default="", help="fixed launch shapes instead of the autotuner: "
-                                                "nlist,external,density_threads,density_rows,pforce_threads,pforce_rows")
+                                                "nlist,external,density_threads,density_rows,pforce_threads,pforce_rows"
+                                                "[,density_mode,pforce_mode]")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()

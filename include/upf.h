@@ -303,10 +303,12 @@ upf_status upf_profile_step(upf_system* s, upf_phase_times* out);
 /* ---- launch shapes and the autotuner (no counterpart in the reference,
  * whose kernels run at fixed block sizes) --------------------------------
  * CTA sizes of the neighbour-list and external-force passes, and CTA size x
- * list rows per TMA stage of the two predict-correct passes. Valid loop-pass
- * pairs: (128,4) (128,8) (128,16) (256,2) (256,4) (256,8) (512,2) (512,4)
- * (1024,2); batches allow up to 256 threads. Shapes change timing only:
- * every shape gives the same results. */
+ * list rows per stage of the two predict-correct passes, whose list entries
+ * come either through a TMA ring in shared memory (mode 0; pairs (128,4)
+ * (128,8) (128,16) (256,2) (256,4) (256,8) (512,2) (512,4) (1024,2)) or by
+ * direct coalesced loads, rows entries at a time (mode 1; (128,4) (128,8)
+ * (256,4) (256,8) (512,4) (512,8)). Batches allow up to 256 threads. Shapes
+ * change timing only: every shape gives the same results. */
 typedef struct upf_launch_config {
   int32_t nlist_threads;      /* 64, 128, 256 */
   int32_t external_threads;   /* 128, 256 */
@@ -314,6 +316,8 @@ typedef struct upf_launch_config {
   int32_t density_rows;
   int32_t pforce_threads;
   int32_t pforce_rows;
+  int32_t density_mode;       /* list entries by 0: the TMA ring; 1: direct loads */
+  int32_t pforce_mode;
   float measured_ms[4];       /* autotune: per-launch ms of the chosen shapes
                                  (neighbour lists, external forces, predicted
                                  density, pressure force); 0 otherwise */

@@ -9,14 +9,20 @@ from unifiedparticleframeworkcuda_b200 import UpfError, UpfLaunchConfig, scenes
 
 pytestmark = pytest.mark.gpu
 
-LOOP_PAIRS = [(128, 4), (128, 8), (128, 16), (256, 2), (256, 4), (256, 8), (512, 2), (512, 4), (1024, 2)]
+# (threads, rows) with the TMA ring (mode 0) and with direct loads (mode 1)
+LOOP_PAIRS = [(0, 128, 4), (0, 128, 8), (0, 128, 16), (0, 256, 2), (0, 256, 4), (0, 256, 8), (0, 512, 2),
+              (0, 512, 4), (0, 1024, 2), (1, 128, 4), (1, 128, 8), (1, 256, 4), (1, 256, 8), (1, 512, 4),
+              (1, 512, 8)]
 
 
 def shape(nl, ext, dens, pf):
+    """dens, pf: (threads, rows) for the TMA ring or (mode, threads, rows)."""
+    dens = dens if len(dens) == 3 else (0,) + tuple(dens)
+    pf = pf if len(pf) == 3 else (0,) + tuple(pf)
     c = UpfLaunchConfig()
     c.nlist_threads, c.external_threads = nl, ext
-    c.density_threads, c.density_rows = dens
-    c.pforce_threads, c.pforce_rows = pf
+    c.density_mode, c.density_threads, c.density_rows = dens
+    c.pforce_mode, c.pforce_threads, c.pforce_rows = pf
     return c
 
 
@@ -58,8 +64,8 @@ def test_autotune_keeps_state_and_picks_a_valid_shape(upf_lib):
     got, _, chosen = run(upf_lib, sc, None, tune=True)
     for f in ("pos", "vel", "density", "pressure"):
         assert np.array_equal(got[f], ref[f]), f
-    assert (chosen.density_threads, chosen.density_rows) in LOOP_PAIRS
-    assert (chosen.pforce_threads, chosen.pforce_rows) in LOOP_PAIRS
+    assert (chosen.density_mode, chosen.density_threads, chosen.density_rows) in LOOP_PAIRS
+    assert (chosen.pforce_mode, chosen.pforce_threads, chosen.pforce_rows) in LOOP_PAIRS
     assert chosen.nlist_threads in (64, 128, 256) and chosen.external_threads in (128, 256)
     assert all(m > 0 for m in chosen.measured_ms)
 
@@ -77,7 +83,8 @@ def test_batch_shapes_and_autotune(upf_lib):
             return [b.particles(k) for k in range(len(scs))], chosen
 
     ref, _ = go(None, False)
-    for cfg in (shape(64, 128, (128, 16), (256, 4)), shape(128, 256, (256, 4), (128, 8))):
+    for cfg in (shape(64, 128, (128, 16), (256, 4)), shape(128, 256, (256, 4), (128, 8)),
+                shape(256, 256, (1, 256, 8), (1, 128, 4))):
         got, _ = go(cfg, False)
         for a, b in zip(got, ref):
             assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])
@@ -93,7 +100,8 @@ def test_invalid_shapes_rejected(upf_lib):
     with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
         s.set_particles(sc.pos, sc.vel, sc.type)
         for bad in (shape(96, 256, (256, 8), (256, 8)), shape(256, 256, (256, 16), (256, 8)),
-                    shape(256, 64, (256, 8), (256, 8))):
+                    shape(256, 64, (256, 8), (256, 8)), shape(256, 256, (1, 256, 2), (256, 8)),
+                    shape(256, 256, (256, 8), (2, 256, 8))):
             with pytest.raises(UpfError):
                 s.set_launch_config(bad)
     scs = scenes.batch_scenes(num=2, seed=3, counts=(2048, 4096))

@@ -138,6 +138,8 @@ class UpfLaunchConfig(C.Structure):
         ("density_rows", C.c_int32),
         ("pforce_threads", C.c_int32),
         ("pforce_rows", C.c_int32),
+        ("density_mode", C.c_int32),
+        ("pforce_mode", C.c_int32),
         ("measured_ms", C.c_float * 4),
     ]
 

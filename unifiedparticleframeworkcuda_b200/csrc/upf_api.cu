@@ -196,17 +196,19 @@ bool shape_valid(const LaunchShape& s, bool batched, const char** why) {
     if (why) *why = w;
     return false;
   };
-  auto pair_ok = [&](int t, int r) {
+  auto pair_ok = [&](int mode, int t, int r) {
     for (const auto& p : kLoopShapes)
-      if (p[0] == t && p[1] == r) return true;
+      if (p[0] == mode && p[1] == t && p[2] == r) return true;
     return false;
   };
   if (s.nlist_threads != 64 && s.nlist_threads != 128 && s.nlist_threads != 256)
     return bad("nlist_threads must be 64, 128 or 256");
   if (s.external_threads != 128 && s.external_threads != 256) return bad("external_threads must be 128 or 256");
-  if (!pair_ok(s.density_threads, s.density_rows) || !pair_ok(s.pforce_threads, s.pforce_rows))
+  if (!pair_ok(s.density_mode, s.density_threads, s.density_rows) ||
+      !pair_ok(s.pforce_mode, s.pforce_threads, s.pforce_rows))
     return bad("(threads, rows) of a loop pass must be one of (128,4) (128,8) (128,16) (256,2) (256,4) (256,8) "
-               "(512,2) (512,4) (1024,2)");
+               "(512,2) (512,4) (1024,2) with the TMA ring (mode 0), or (128,4) (128,8) (256,4) (256,8) (512,4) "
+               "(512,8) with direct loads (mode 1)");
   if (batched && (s.density_threads > 256 || s.pforce_threads > 256))
     return bad("batched scenes: at most 256 threads per CTA (a CTA must stay within one scene's segment)");
   return true;
@@ -220,6 +222,8 @@ void shape_to_config(const LaunchShape& s, upf_launch_config* c) {
   c->density_rows = s.density_rows;
   c->pforce_threads = s.pforce_threads;
   c->pforce_rows = s.pforce_rows;
+  c->density_mode = s.density_mode;
+  c->pforce_mode = s.pforce_mode;
 }
 
 LaunchShape config_to_shape(const upf_launch_config& c) {
@@ -230,6 +234,8 @@ LaunchShape config_to_shape(const upf_launch_config& c) {
   s.density_rows = c.density_rows;
   s.pforce_threads = c.pforce_threads;
   s.pforce_rows = c.pforce_rows;
+  s.density_mode = c.density_mode;
+  s.pforce_mode = c.pforce_mode;
   return s;
 }
 
@@ -303,18 +309,21 @@ upf_status autotune_shapes(const TuneOps& ops, int repeats, upf_launch_config* o
     for (int pass = 0; pass < 2 && rc == UPF_OK; ++pass) {
       cudaError_t (*launch)(void*, cudaStream_t) = pass == 0 ? ops.density : ops.pforce;
       if (!launch) continue;
+      int& mode = pass == 0 ? sh.density_mode : sh.pforce_mode;
       int& threads = pass == 0 ? sh.density_threads : sh.pforce_threads;
       int& rows = pass == 0 ? sh.density_rows : sh.pforce_rows;
-      int bt = threads, br = rows;
+      int bm = mode, bt = threads, br = rows;
       float best_ms = 1e30f;
       for (const auto& pr : pairs) {
-        if (ops.batched && pr[0] > 256) continue;
-        threads = pr[0];
-        rows = pr[1];
+        if (ops.batched && pr[1] > 256) continue;
+        mode = pr[0];
+        threads = pr[1];
+        rows = pr[2];
         float ms;
         if ((rc = time_pass(launch, &ms)) != UPF_OK) break;
-        if (ms < best_ms) best_ms = ms, bt = pr[0], br = pr[1];
+        if (ms < best_ms) best_ms = ms, bm = pr[0], bt = pr[1], br = pr[2];
       }
+      mode = bm;
       threads = bt;
       rows = br;
       chosen_ms[2 + pass] = best_ms;

@@ -154,6 +154,55 @@ __device__ __forceinline__ Scope enter_scope(const DevParams& Pk, const float* l
   }
 }
 
+// The list walk of the loop passes, in one of two modes:
+//  * TMA ring (kDirect = false): each warp streams its 32 columns' list rows
+//    through a shared-memory ring of kRows-row stages (upf_tma.cuh), waits on
+//    the stage's mbarrier, and hands the rows to `body`;
+//  * direct loads (kDirect = true): each thread loads its own list entries
+//    kRows at a time with coalesced global loads (consecutive threads read
+//    consecutive words of a row) and no barriers.
+// body(code, bin, k0) consumes entries k0 .. k0 + kRows - 1 (those below
+// the thread's count); code(r) / bin(r) give entry k0 + r (read from the
+// shared-memory stage when it is used, in the ring mode). Returns false if a
+// ring wait ran out.
+struct ListArgs {
+  const CUtensorMap* cmap;
+  const CUtensorMap* bmap;
+  const uint32_t* nbr;
+  const uint16_t* bins;
+  uint32_t stride;
+};
+
+template <bool kDirect, bool kWithBins, int kThreads, int kRows, class Body>
+__device__ __forceinline__ bool walk_lists(const ListArgs& L, uint32_t i, uint32_t cnt, Body&& body) {
+  if constexpr (kDirect) {
+    const uint32_t* __restrict__ col = L.nbr + i;
+    const uint16_t* __restrict__ bcol = L.bins + i;
+    for (uint32_t k0 = 0; k0 < cnt; k0 += kRows) {
+      uint32_t code[kRows], bin[kRows];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        if (k0 + r < cnt) {
+          code[r] = __ldg(col + (size_t)(k0 + r) * L.stride);
+          if (kWithBins) bin[r] = __ldg(bcol + (size_t)(k0 + r) * L.stride);
+        }
+      }
+      body([&](int r) { return code[r]; }, [&](int r) { return bin[r]; }, (int)k0);
+    }
+    return true;
+  } else {
+    __shared__ WarpListRing<kWithBins, kRows> rings[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpListRing<kWithBins, kRows>& ring = rings[warp];
+    ring_init(ring);
+    const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
+    return ring_walk(ring, L.cmap, L.bmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt, [&](int s, int k0) {
+      body([&](int r) { return ring.codes[s][r][lane]; }, [&](int r) { return (uint32_t)ring.bins[s][r][lane]; },
+           k0);
+    });
+  }
+}
+
 // ---------------------------------------------------------------- reorder
 // CopySortedParticleValuesKernel* (particles_kernel.cu:543-654): gather the
 // state into sorted order.
@@ -828,28 +877,24 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_external(
 }
 
 // ComputePredictedDensityAndPressure (UnifiedPhysics.cpp:5456-5491) with the
-// maximum for the loop test reduced in the same pass.
-//
-// The warp's list rows stream through shared memory by TMA (upf_tma.cuh);
-// each lane then gathers kRows neighbours' predicted positions at once
-// and accumulates them in list order.
-template <bool kBatch, int kThreads, int kRows>
+// maximum for the loop test reduced in the same pass. The list entries come
+// by the TMA ring or by direct loads (walk_lists); each lane gathers kRows
+// neighbours' predicted positions at once and accumulates them in list order.
+template <bool kBatch, bool kDirect, int kThreads, int kRows>
 __global__ void __launch_bounds__(kThreads) k_pcisph_density(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const int32_t* __restrict__ type,
-    const float4* __restrict__ xs, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ ncnt,
-    const float* __restrict__ luts_plain, float* __restrict__ rho, float* __restrict__ press,
-    float4* __restrict__ pq, DevState* __restrict__ st_plain) {
+    const float4* __restrict__ xs, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, float* __restrict__ rho,
+    float* __restrict__ press, float4* __restrict__ pq, DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float m4[UPF_LUT_ENTRIES];
   __shared__ float thr[kThresholds];
   __shared__ uint32_t wmax[kThreads / 32];
-  __shared__ WarpListRing<false, kRows> rings[kThreads / 32];
   const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   stage_lut(m4, sc.luts + LUT_M4 * UPF_LUT_ENTRIES);
   stage_thresholds(thr, sc.luts);
-  ring_init(rings[warp]);
   __syncthreads();
   const DevParams& P = *sc.P;
   DevState* st = sc.st;
@@ -857,30 +902,27 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
   uint32_t best = 0;
   const bool active = i < sc.end && type[i] == UPF_LIQUID;
   const uint32_t cnt = active ? ncnt[i] : 0u;
-  const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
   const float4 xi = active ? xs[i] : make_float4(0, 0, 0, 0);
   const float m = P.mass;
   float den = P.kernel_self * m;
-  WarpListRing<false, kRows>& ring = rings[warp];
-  const bool ok = ring_walk(ring, &cmap, &cmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
-                            [&](int s, int k0) {
-                              // predicted positions; boundary particles sit in the array's
-                              // tail at their fixed positions
-                              float4 xj[kRows];
+  const ListArgs L{&cmap, &cmap, nbr, nullptr, P.nstride};
+  const bool ok = walk_lists<kDirect, false, kThreads, kRows>(L, i, cnt, [&](auto code, auto, int k0) {
+    // predicted positions; boundary particles sit in the array's tail at
+    // their fixed positions
+    float4 xj[kRows];
 #pragma unroll
-                              for (int r = 0; r < kRows; ++r)
-                                if (k0 + r < (int)cnt) xj[r] = __ldg(xs + ring.codes[s][r][lane]);
+    for (int r = 0; r < kRows; ++r)
+      if (k0 + r < (int)cnt) xj[r] = __ldg(xs + code(r));
 #pragma unroll
-                              for (int r = 0; r < kRows; ++r) {
-                                if (k0 + r < (int)cnt) {
-                                  // the table bin of d from d^2 (exact); at or beyond h the
-                                  // bin is 300, whose entry 0 adds +0 exactly as the
-                                  // reference's skipped term does
-                                  const float r2 = dist2(xi, xj[r]);
-                                  den += m4[bin_of_r2(r2, P.lut_factor, thr)] * m;
-                                }
-                              }
-                            });
+    for (int r = 0; r < kRows; ++r) {
+      if (k0 + r < (int)cnt) {
+        // the table bin of d from d^2 (exact); at or beyond h the bin is 300,
+        // whose entry 0 adds +0 exactly as the reference's skipped term does
+        const float r2 = dist2(xi, xj[r]);
+        den += m4[bin_of_r2(r2, P.lut_factor, thr)] * m;
+      }
+    }
+  });
   if (!ok && lane == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
   if (active) {
     const float err = mx0(den - P.rho0, 0.0f);
@@ -903,29 +945,27 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
 }
 
 // ComputeCorrectivePressureForce (UnifiedPhysics.cpp:5493-5522), then the
-// prediction of the next iteration (PredictPositionAndVelocity).
-template <bool kBatch, int kThreads, int kRows>
+// prediction of the next iteration (PredictPositionAndVelocity). List entries
+// and their stored bins by the TMA ring or by direct loads (walk_lists).
+template <bool kBatch, bool kDirect, int kThreads, int kRows>
 __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
     const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap bmap,
-    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, const float4* __restrict__ pq,
-    const float4* __restrict__ force, float4* __restrict__ pforce, float4* __restrict__ xs,
-    DevState* __restrict__ st_plain) {
+    const uint32_t* __restrict__ nbr, const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt,
+    const float* __restrict__ luts_plain, const float4* __restrict__ pq, const float4* __restrict__ force,
+    float4* __restrict__ pforce, float4* __restrict__ xs, DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float pg[UPF_LUT_ENTRIES];
-  __shared__ WarpListRing<true, kRows> rings[kThreads / 32];
   const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   stage_lut(pg, sc.luts + LUT_PGRAD * UPF_LUT_ENTRIES);
-  ring_init(rings[warp]);
   __syncthreads();
   const DevParams& P = *sc.P;
   DevState* st = sc.st;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i < sc.end && B.type[i] == UPF_LIQUID;
   const uint32_t cnt = active ? ncnt[i] : 0u;
-  const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
   const float4 xi = active ? B.pos[i] : make_float4(0, 0, 0, 0);
   const float m = P.mass;
   // grad = p_i / rho0^2 + p_j / rho0^2, both quotients precomputed by the
@@ -934,35 +974,26 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
   float fx = 0, fy = 0, fz = 0;
   // positions are those the list was built at: every entry passes |x_i - x_j| < h
   // and its kernel-table bin is stored with it
-  WarpListRing<true, kRows>& ring = rings[warp];
-  const bool ok = ring_walk(ring, &cmap, &bmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt,
-                            [&](int s, int k0) {
-                              // one gather per neighbour: position and p / rho0^2 packed in
-                              // pq (boundary particles sit in the tail, w = 0 there)
-                              float4 xj[kRows];
-                              float qj[kRows];
+  const ListArgs L{&cmap, &bmap, nbr, bins, P.nstride};
+  const bool ok = walk_lists<kDirect, true, kThreads, kRows>(L, i, cnt, [&](auto code, auto bin, int k0) {
+    // one gather per neighbour: position and p / rho0^2 packed in pq
+    // (boundary particles sit in the tail, w = 0 there)
+    float4 xj[kRows];
 #pragma unroll
-                              for (int r = 0; r < kRows; ++r) {
-                                if (k0 + r < (int)cnt) {
-                                  const uint32_t code = ring.codes[s][r][lane];
-                                  const float4 v = __ldg(pq + code);
-                                  xj[r] = v;
-                                  qj[r] = v.w;
-                                }
-                              }
+    for (int r = 0; r < kRows; ++r)
+      if (k0 + r < (int)cnt) xj[r] = __ldg(pq + code(r));
 #pragma unroll
-                              for (int r = 0; r < kRows; ++r) {
-                                if (k0 + r < (int)cnt) {
-                                  const float g = pg[ring.bins[s][r][lane]];
-                                  const float kx = (xi.x - xj[r].x) * g, ky = (xi.y - xj[r].y) * g,
-                                              kz = (xi.z - xj[r].z) * g;
-                                  const float grad = qi + qj[r];
-                                  fx = fx - kx * grad * m * m;
-                                  fy = fy - ky * grad * m * m;
-                                  fz = fz - kz * grad * m * m;
-                                }
-                              }
-                            });
+    for (int r = 0; r < kRows; ++r) {
+      if (k0 + r < (int)cnt) {
+        const float g = pg[bin(r)];
+        const float kx = (xi.x - xj[r].x) * g, ky = (xi.y - xj[r].y) * g, kz = (xi.z - xj[r].z) * g;
+        const float grad = qi + xj[r].w;
+        fx = fx - kx * grad * m * m;
+        fy = fy - ky * grad * m * m;
+        fz = fz - kz * grad * m * m;
+      }
+    }
+  });
   if (!ok && lane == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
   if (!active) return;
   pforce[i] = f4(fx, fy, fz);
@@ -1264,41 +1295,49 @@ cudaError_t run_external(const LaunchShape& sh, cudaStream_t st, const DevParams
   return cudaGetLastError();
 }
 
-#define UPF_SHAPE_SWITCH(threads, rows, CALL)     \
-  switch ((threads) * 100 + (rows)) {             \
-    case 12804: CALL(128, 4); break;              \
-    case 12808: CALL(128, 8); break;              \
-    case 12816: CALL(128, 16); break;             \
-    case 25602: CALL(256, 2); break;              \
-    case 25604: CALL(256, 4); break;              \
-    case 25608: CALL(256, 8); break;              \
-    case 51202: CALL(512, 2); break;              \
-    case 51204: CALL(512, 4); break;              \
-    case 102402: CALL(1024, 2); break;            \
-    default: return cudaErrorInvalidConfiguration; \
+// (mode, threads, rows): TMA ring pairs and direct-load pairs (see kLoopShapes)
+#define UPF_SHAPE_SWITCH(mode, threads, rows, CALL)        \
+  switch ((mode) * 1000000 + (threads) * 100 + (rows)) {   \
+    case 12804: CALL(false, 128, 4); break;                \
+    case 12808: CALL(false, 128, 8); break;                \
+    case 12816: CALL(false, 128, 16); break;               \
+    case 25602: CALL(false, 256, 2); break;                \
+    case 25604: CALL(false, 256, 4); break;                \
+    case 25608: CALL(false, 256, 8); break;                \
+    case 51202: CALL(false, 512, 2); break;                \
+    case 51204: CALL(false, 512, 4); break;                \
+    case 102402: CALL(false, 1024, 2); break;              \
+    case 1012804: CALL(true, 128, 4); break;               \
+    case 1012808: CALL(true, 128, 8); break;               \
+    case 1025604: CALL(true, 256, 4); break;               \
+    case 1025608: CALL(true, 256, 8); break;               \
+    case 1051204: CALL(true, 512, 4); break;               \
+    case 1051208: CALL(true, 512, 8); break;               \
+    default: return cudaErrorInvalidConfiguration;          \
   }
 
 template <bool kBatch>
 cudaError_t run_density(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
-                        const int32_t* type, const float4* xs, const CUtensorMap* cmaps, const uint32_t* ncnt,
-                        const float* luts, float* rho, float* press, float4* pq, DevState* stp) {
-#define UPF_DEN(T, R)                                                                                           \
-  k_pcisph_density<kBatch, T, R><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, type, xs, cmaps[rows_index(R)], ncnt, \
-                                                                luts, rho, press, pq, stp)
-  UPF_SHAPE_SWITCH(sh.density_threads, sh.density_rows, UPF_DEN)
+                        const int32_t* type, const float4* xs, const CUtensorMap* cmaps, const uint32_t* nbr,
+                        const uint32_t* ncnt, const float* luts, float* rho, float* press, float4* pq,
+                        DevState* stp) {
+#define UPF_DEN(D, T, R)                                                                                   \
+  k_pcisph_density<kBatch, D, T, R><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, type, xs, cmaps[rows_index(R)], \
+                                                                   nbr, ncnt, luts, rho, press, pq, stp)
+  UPF_SHAPE_SWITCH(sh.density_mode, sh.density_threads, sh.density_rows, UPF_DEN)
 #undef UPF_DEN
   return cudaGetLastError();
 }
 
 template <bool kBatch>
 cudaError_t run_pforce(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
-                       const DynArrays& B, const CUtensorMap* cmaps, const CUtensorMap* bmaps, const uint32_t* ncnt,
-                       const float* luts, const float4* pq, const float4* force, float4* pforce, float4* xs,
-                       DevState* stp) {
-#define UPF_PF(T, R)                                                                                         \
-  k_pcisph_pressure_force<kBatch, T, R><<<(n + T - 1) / T, T, 0, st>>>(                                      \
-      P, bv, n, B, cmaps[rows_index(R)], bmaps[rows_index(R)], ncnt, luts, pq, force, pforce, xs, stp)
-  UPF_SHAPE_SWITCH(sh.pforce_threads, sh.pforce_rows, UPF_PF)
+                       const DynArrays& B, const CUtensorMap* cmaps, const CUtensorMap* bmaps, const uint32_t* nbr,
+                       const uint16_t* bins, const uint32_t* ncnt, const float* luts, const float4* pq,
+                       const float4* force, float4* pforce, float4* xs, DevState* stp) {
+#define UPF_PF(D, T, R)                                                                                            \
+  k_pcisph_pressure_force<kBatch, D, T, R><<<(n + T - 1) / T, T, 0, st>>>(                                         \
+      P, bv, n, B, cmaps[rows_index(R)], bmaps[rows_index(R)], nbr, bins, ncnt, luts, pq, force, pforce, xs, stp)
+  UPF_SHAPE_SWITCH(sh.pforce_mode, sh.pforce_threads, sh.pforce_rows, UPF_PF)
 #undef UPF_PF
   return cudaGetLastError();
 }
@@ -1350,7 +1389,7 @@ cudaError_t launch_loop_init(System& s, cudaStream_t st) {
 cudaError_t launch_loop_density(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    return run_density<false>(s.shape, st, s.dp, BatchView{}, n, s.B.type, s.xs, s.nbr_maps, s.ncnt, s.luts, s.rho,
+    return run_density<false>(s.shape, st, s.dp, BatchView{}, n, s.B.type, s.xs, s.nbr_maps, s.nbr, s.ncnt, s.luts, s.rho,
                               s.press, s.pq, s.st);
   return cudaGetLastError();
 }
@@ -1358,7 +1397,7 @@ cudaError_t launch_loop_density(System& s, cudaStream_t st) {
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    return run_pforce<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.nbr_maps, s.bins_maps, s.ncnt, s.luts, s.pq,
+    return run_pforce<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.nbr_maps, s.bins_maps, s.nbr, s.bins, s.ncnt, s.luts, s.pq,
                              s.force, s.pforce, s.xs, s.st);
   return cudaGetLastError();
 }
@@ -1479,7 +1518,7 @@ cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st) {
 cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
   if (n)
-    return run_density<true>(b.shape, st, DevParams{}, b.view, n, b.B.type, b.xs, b.nbr_maps, b.ncnt, nullptr, b.rho,
+    return run_density<true>(b.shape, st, DevParams{}, b.view, n, b.B.type, b.xs, b.nbr_maps, b.nbr, b.ncnt, nullptr, b.rho,
                              b.press, b.pq, nullptr);
   return cudaGetLastError();
 }
@@ -1487,7 +1526,7 @@ cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st) {
 cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
   if (n)
-    return run_pforce<true>(b.shape, st, DevParams{}, b.view, n, b.B, b.nbr_maps, b.bins_maps, b.ncnt, nullptr, b.pq,
+    return run_pforce<true>(b.shape, st, DevParams{}, b.view, n, b.B, b.nbr_maps, b.bins_maps, b.nbr, b.bins, b.ncnt, nullptr, b.pq,
                             b.force, b.pforce, b.xs, nullptr);
   return cudaGetLastError();
 }

@@ -62,11 +62,15 @@ struct LaunchShape {
   int density_rows = 8;
   int pforce_threads = 256;    // with pforce_rows: the same pairs
   int pforce_rows = 8;
+  int density_mode = 0;        // list entries by 0: the TMA ring, 1: direct loads (rows = entries per batch)
+  int pforce_mode = 0;
 };
 bool shape_valid(const LaunchShape& s, bool batched, const char** why);
-// (threads, rows) pairs of the loop passes
-constexpr int kLoopShapes[][2] = {{128, 4}, {128, 8}, {128, 16}, {256, 2}, {256, 4},
-                                  {256, 8}, {512, 2}, {512, 4}, {1024, 2}};
+// (mode, threads, rows) triples of the loop passes: TMA ring (mode 0) and
+// direct loads (mode 1)
+constexpr int kLoopShapes[][3] = {{0, 128, 4}, {0, 128, 8}, {0, 128, 16}, {0, 256, 2}, {0, 256, 4},
+                                  {0, 256, 8}, {0, 512, 2}, {0, 512, 4},  {0, 1024, 2}, {1, 128, 4},
+                                  {1, 128, 8}, {1, 256, 4}, {1, 256, 8},  {1, 512, 4},  {1, 512, 8}};
 constexpr int kNumLoopShapes = sizeof(kLoopShapes) / sizeof(kLoopShapes[0]);
 constexpr int kListRowVariants = 4;  // tensor maps for 2, 4, 8 and 16 rows per box
 inline int rows_index(int rows) { return rows == 2 ? 0 : (rows == 4 ? 1 : (rows == 8 ? 2 : 3)); }
