@@ -318,6 +318,7 @@ typedef struct upf_launch_config {
   int32_t pforce_rows;
   int32_t density_mode;       /* list entries by 0: the TMA ring; 1: direct loads */
   int32_t pforce_mode;
+  int32_t nlist_mode;         /* 0: each thread its own query box; 1: a warp walks the union of its boxes */
   float measured_ms[4];       /* autotune: per-launch ms of the chosen shapes
                                  (neighbour lists, external forces, predicted
                                  density, pressure force); 0 otherwise */

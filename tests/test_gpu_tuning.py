@@ -52,6 +52,7 @@ def test_every_shape_gives_identical_results(upf_lib):
     for k, dens in enumerate(LOOP_PAIRS):
         pf = LOOP_PAIRS[(k + 2) % len(LOOP_PAIRS)]
         cfg = shape(nls[k % 3], exts[k % 2], dens, pf)
+        cfg.nlist_mode = k % 2
         got, st, _ = run(upf_lib, sc, cfg)
         assert st.iterations == ref_st.iterations
         for f in ("pos", "vel", "density", "pressure"):
@@ -85,6 +86,7 @@ def test_batch_shapes_and_autotune(upf_lib):
     ref, _ = go(None, False)
     for cfg in (shape(64, 128, (128, 16), (256, 4)), shape(128, 256, (256, 4), (128, 8)),
                 shape(256, 256, (1, 256, 8), (1, 128, 4))):
+        cfg.nlist_mode = 1
         got, _ = go(cfg, False)
         for a, b in zip(got, ref):
             assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["vel"], b["vel"])

@@ -140,6 +140,7 @@ class UpfLaunchConfig(C.Structure):
         ("pforce_rows", C.c_int32),
         ("density_mode", C.c_int32),
         ("pforce_mode", C.c_int32),
+        ("nlist_mode", C.c_int32),
         ("measured_ms", C.c_float * 4),
     ]
 

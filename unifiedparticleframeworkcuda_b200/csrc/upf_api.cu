@@ -203,6 +203,7 @@ bool shape_valid(const LaunchShape& s, bool batched, const char** why) {
   };
   if (s.nlist_threads != 64 && s.nlist_threads != 128 && s.nlist_threads != 256)
     return bad("nlist_threads must be 64, 128 or 256");
+  if (s.nlist_mode != 0 && s.nlist_mode != 1) return bad("nlist_mode must be 0 (lane boxes) or 1 (warp union)");
   if (s.external_threads != 128 && s.external_threads != 256) return bad("external_threads must be 128 or 256");
   if (!pair_ok(s.density_mode, s.density_threads, s.density_rows) ||
       !pair_ok(s.pforce_mode, s.pforce_threads, s.pforce_rows))
@@ -224,6 +225,7 @@ void shape_to_config(const LaunchShape& s, upf_launch_config* c) {
   c->pforce_rows = s.pforce_rows;
   c->density_mode = s.density_mode;
   c->pforce_mode = s.pforce_mode;
+  c->nlist_mode = s.nlist_mode;
 }
 
 LaunchShape config_to_shape(const upf_launch_config& c) {
@@ -236,6 +238,7 @@ LaunchShape config_to_shape(const upf_launch_config& c) {
   s.pforce_rows = c.pforce_rows;
   s.density_mode = c.density_mode;
   s.pforce_mode = c.pforce_mode;
+  s.nlist_mode = c.nlist_mode;
   return s;
 }
 
@@ -274,16 +277,19 @@ upf_status autotune_shapes(const TuneOps& ops, int repeats, upf_launch_config* o
     // one pass at a time, the others at their current shapes
     if (ops.nlist) {
       const int cand[] = {64, 128, 256};
-      int best = sh.nlist_threads;
+      int best = sh.nlist_threads, best_mode = sh.nlist_mode;
       float best_ms = 1e30f;
-      for (int t : cand) {
-        sh.nlist_threads = t;
-        float ms;
-        if ((rc = time_pass(ops.nlist, &ms)) != UPF_OK) break;
-        if (ms < best_ms) best_ms = ms, best = t;
-      }
+      for (int mode = 0; mode < 2 && rc == UPF_OK; ++mode)
+        for (int t : cand) {
+          sh.nlist_threads = t;
+          sh.nlist_mode = mode;
+          float ms;
+          if ((rc = time_pass(ops.nlist, &ms)) != UPF_OK) break;
+          if (ms < best_ms) best_ms = ms, best = t, best_mode = mode;
+        }
       if (rc != UPF_OK) break;
       sh.nlist_threads = best;
+      sh.nlist_mode = best_mode;
       chosen_ms[0] = best_ms;
       // the lists of the chosen shape (identical for every shape)
       if (cudaSuccess != ops.nlist(ops.ctx, st)) {

@@ -238,7 +238,16 @@ __device__ __forceinline__ float dist2(float4 a, float4 b) {
 // and |x_i - x_j| < h in float. Candidate positions are gathered kUnroll at
 // a time. Each entry also records its kernel-table bin at the current
 // positions (used by every pass that evaluates at current positions).
-template <bool kBatch, int kThreads>
+//
+// kWarpUnion: the 32 lanes of a warp (32 consecutive Morton-sorted particles,
+// close together) walk the union of their query boxes, when it spans at
+// most 64 cells, instead of each lane its own box: every lane then visits
+// the same cells and candidates in the same order (no divergence; each
+// candidate position is one broadcast load) and keeps those within h of its
+// own particle. A lane's list is unchanged: all its neighbours lie in its own
+// box, a subset of the union, and the union's cells are still visited in
+// ascending Morton order.
+template <bool kBatch, int kThreads, bool kWarpUnion>
 __global__ void __launch_bounds__(kThreads) k_build_nlist(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const float4* __restrict__ pos,
     const uint32_t* __restrict__ keys, const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend,
@@ -259,8 +268,10 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
     cend += bv.cell_base[sc.scene];
   }
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= sc.end) return;
-  const float4 xi = pos[i];
+  const bool active = i < sc.end;
+  if (!kWarpUnion && !active) return;
+  if (kWarpUnion && !__any_sync(0xffffffffu, active)) return;  // uniform over the warp
+  const float4 xi = active ? pos[i] : make_float4(0, 0, 0, 0);
   const float h = P.h;
   int lo[3], hi[3];
   {
@@ -276,11 +287,27 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
       hi[a] = ui >> P.cell_shift;
     }
   }
+  if (kWarpUnion) {
+    int ulo[3], uhi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      ulo[a] = __reduce_min_sync(0xffffffffu, active ? lo[a] : 0x7fffffff);
+      uhi[a] = __reduce_max_sync(0xffffffffu, active ? hi[a] : -1);
+    }
+    if ((uhi[0] - ulo[0] + 1) * (uhi[1] - ulo[1] + 1) * (uhi[2] - ulo[2] + 1) <= 64) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = ulo[a];
+        hi[a] = uhi[a];
+      }
+    }
+  }
   const uint32_t maxn = P.maxn, stride = P.nstride;
   uint32_t cnt = 0;
   uint32_t* __restrict__ out = nbr + i;
   uint16_t* __restrict__ ob = bins + i;
   auto append = [&](uint32_t code, float r2) {
+    if (!active) return;
     if (cnt < maxn) {
       out[(size_t)cnt * stride] = code;
       ob[(size_t)cnt * stride] = (uint16_t)bin_of_r2(r2, P.lut_factor, thr);
@@ -356,6 +383,7 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
       for (int by = lo[1]; by <= hi[1]; ++by)
         for (int bx = lo[0]; bx <= hi[0]; ++bx) visit(morton3(bx, by, bz));
   }
+  if (!active) return;
   ncnt[i] = cnt < maxn ? cnt : maxn;
   if (cnt > maxn) atomicOr(&st->error_flags, (uint32_t)ERR_OVERFLOW);
   atomicMax(&st->max_neighbors, cnt);
@@ -1265,13 +1293,16 @@ cudaError_t run_nlist(const LaunchShape& sh, cudaStream_t st, const DevParams& P
                       uint32_t ns, const float4* spos, const uint32_t* skeys, const uint32_t* sstart,
                       const uint32_t* send, uint32_t* nbr, uint16_t* bins, uint32_t* ncnt, const float* luts,
                       DevState* stp) {
-#define UPF_NL(T)                                                                                          \
-  k_build_nlist<kBatch, T><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, pos, keys, cstart, cend, ns, spos, skeys, \
-                                                          sstart, send, nbr, bins, ncnt, luts, stp)
-  switch (sh.nlist_threads) {
-    case 64: UPF_NL(64); break;
-    case 128: UPF_NL(128); break;
-    case 256: UPF_NL(256); break;
+#define UPF_NL(T, W)                                                                                          \
+  k_build_nlist<kBatch, T, W><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, pos, keys, cstart, cend, ns, spos, skeys, \
+                                                             sstart, send, nbr, bins, ncnt, luts, stp)
+  switch (sh.nlist_threads * 10 + sh.nlist_mode) {
+    case 640: UPF_NL(64, false); break;
+    case 1280: UPF_NL(128, false); break;
+    case 2560: UPF_NL(256, false); break;
+    case 641: UPF_NL(64, true); break;
+    case 1281: UPF_NL(128, true); break;
+    case 2561: UPF_NL(256, true); break;
     default: return cudaErrorInvalidConfiguration;
   }
 #undef UPF_NL

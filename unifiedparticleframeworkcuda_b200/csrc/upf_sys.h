@@ -64,6 +64,7 @@ struct LaunchShape {
   int pforce_rows = 8;
   int density_mode = 0;        // list entries by 0: the TMA ring, 1: direct loads (rows = entries per batch)
   int pforce_mode = 0;
+  int nlist_mode = 0;          // 0: each lane its own query box; 1: the warp's union of boxes
 };
 bool shape_valid(const LaunchShape& s, bool batched, const char** why);
 // (mode, threads, rows) triples of the loop passes: TMA ring (mode 0) and
