@@ -118,6 +118,29 @@ def test_no_device_means_error_not_fallback(upf_lib):
     assert e.value.status == 9  # UPF_ERR_NO_DEVICE
 
 
+def test_bin_300_starts_no_later_than_the_support_edge(upf_lib):
+    """At these h, (int)(h * (float)(1/h) * 300) is 299, so the first r2 of
+    bin 300 would lie above h^2 and a pair just outside the support (which the
+    reference skips) would take bin 299; the table starts bin 300 at the
+    support's edge instead. Every other h keeps its exact bin-300 threshold.
+    (The GPU density-pass bins are checked against the reference rule at
+    these h in the GPU parity tests.)"""
+    for h in (0.021382991998565044, 0.02923523891741497, 0.05760840918395471):
+        p = upf_lib.default_params()
+        p.support_radius = h
+        thr = upf_lib.bin_thresholds(p)
+        hf = np.float32(h)
+        factor = np.float32(1.0 / np.float64(hf))
+        assert int(np.float32(np.float32(hf * factor) * np.float32(300))) == 299
+        assert thr[300] == thr[301]
+    rng = np.random.default_rng(5)
+    for h in rng.uniform(0.005, 0.2, 200):
+        p = upf_lib.default_params()
+        p.support_radius = float(h)
+        thr = upf_lib.bin_thresholds(p)
+        assert thr[300] <= thr[301]
+
+
 def test_bin_thresholds_reproduce_sqrt_binning(upf_lib):
     """The device derives table bins from r^2 with these thresholds; they must
     give exactly (int)(sqrtf(r2) * (float)(1/h) * 300) and sqrtf(r2) < h."""

@@ -198,3 +198,41 @@ def test_wcsph_multi_step_statistics(upf_lib, oracle_lib):
         assert abs(g.kinetic_energy - c.kinetic_energy) <= 1e-3 * c.kinetic_energy, s
     sysm.close()
     o.close()
+
+
+# support radii at which (int)(h * (float)(1/h) * 300) rounds to 299: the
+# thresholds cross there (the smallest r2 of bin 300 lies above h^2), so the
+# bin alone would let a pair just outside the support contribute
+CROSSING_H = (0.021382991998565044, 0.02923523891741497, 0.05760840918395471)
+
+
+def reference_bins(r2, h):
+    """(int)(sqrtf(r2) * (float)(1/h) * 300) where sqrtf(r2) < h, else 300
+    (the pair is skipped): ComputePredictedDensityAndPressure,
+    UnifiedPhysics.cpp:5468-5476, with kernelM4Lut (WeightingKernel.cpp:122-128)."""
+    hf = np.float32(h)
+    factor = np.float32(1.0 / np.float64(hf))
+    d = np.sqrt(r2.astype(np.float32), dtype=np.float32)
+    idx = ((d * factor).astype(np.float32) * np.float32(300)).astype(np.float32).astype(np.int64)
+    return np.where(d < hf, np.minimum(idx, 300), 300)
+
+
+@pytest.mark.parametrize("h", (0.02, 0.04) + CROSSING_H)
+def test_density_pass_bins_follow_the_reference_rule(upf_lib, h):
+    import ctypes as C
+    p = upf_lib.default_params()
+    p.support_radius = h
+    thr = upf_lib.bin_thresholds(p)
+    rng = np.random.default_rng(11)
+    hf = np.float32(h)
+    edges = thr[1:].astype(np.float32)
+    r2 = np.concatenate([rng.uniform(0, 1.2, 100000).astype(np.float32) * hf * hf, edges,
+                         np.nextafter(edges, np.float32(0)), np.nextafter(edges, np.float32(1)),
+                         np.array([0.0, hf * hf], np.float32)]).astype(np.float32)
+    out = np.zeros(r2.size, np.int32)
+    rc = upf_lib.lib().upf_selftest_support_bins(0, C.byref(p), r2.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 r2.size, out.ctypes.data_as(C.POINTER(C.c_int32)))
+    assert rc == 0, upf_lib.lib().upf_last_error()
+    want = reference_bins(r2, h)
+    bad = np.flatnonzero(out != want)
+    assert bad.size == 0, list(zip(r2[bad[:5]], out[bad[:5]], want[bad[:5]]))

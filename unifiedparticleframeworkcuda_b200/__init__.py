@@ -98,6 +98,7 @@ def lib():
             "upf_adjoint_times": [vp, fp, fp],
             "upf_test_fail_allocation": [C.c_int32],
             "upf_selftest_bounded_wait": [C.c_int, C.c_uint32],
+            "upf_selftest_support_bins": [C.c_int, P, fp, C.c_uint32, i32p],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],
             "upf_radix_sort_pairs": [vp, vp, C.c_uint32, C.c_int32, vp, C.c_size_t, vp],
             "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],

@@ -500,6 +500,17 @@ __global__ void k_selftest_wait(uint64_t limit_ns, DevState* st) {
   if (!ok && threadIdx.x == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
 }
 
+// The table bins the density pass takes for squared distances r2 (bin_of_r2
+// with the thresholds staged in shared memory, as in the pass).
+__global__ void k_selftest_support_bins(const float* __restrict__ thr_g, float factor, const float* __restrict__ r2,
+                                        uint32_t n, int32_t* __restrict__ out) {
+  __shared__ float thr[kThresholds];
+  for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) thr[k] = thr_g[k];
+  __syncthreads();
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = bin_of_r2(r2[i], factor, thr);
+}
+
 __global__ void k_init_dyn(uint32_t n, DynArrays A, float rho0) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -579,6 +590,47 @@ upf_status upf_selftest_bounded_wait(int device, uint32_t limit_us) {
   if (h.error_flags & ERR_TIMEOUT) {
     set_error("a bounded device-side wait ran out (self-test)");
     return UPF_ERR_TIMEOUT;
+  }
+  return UPF_OK;
+}
+
+upf_status upf_selftest_support_bins(int device, const upf_params* p, const float* r2, uint32_t n, int32_t* bins) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("upf_selftest_support_bins: no CUDA device");
+    return UPF_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev || !p || !(p->support_radius > 0.0f) || (n && (!r2 || !bins)) ||
+      n > (1u << 26)) {
+    set_error("upf_selftest_support_bins: bad arguments");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (n == 0) return UPF_OK;
+  UPF_CUDA(cudaSetDevice(device));
+  float thr_h[kThresholds];
+  build_bin_thresholds(*p, thr_h);
+  const float factor = (float)(1.0 / (double)p->support_radius);
+  float* d_thr = nullptr;
+  float* d_r2 = nullptr;
+  int32_t* d_out = nullptr;
+  cudaError_t e = cudaMalloc(&d_thr, sizeof(thr_h));
+  if (e == cudaSuccess) e = cudaMalloc(&d_r2, sizeof(float) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(int32_t) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(d_thr, thr_h, sizeof(thr_h), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_r2, r2, sizeof(float) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const uint32_t blocks = (n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184;
+    k_selftest_support_bins<<<blocks, 256>>>(d_thr, factor, d_r2, n, d_out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(bins, d_out, sizeof(int32_t) * n, cudaMemcpyDeviceToHost);
+  cudaFree(d_thr);
+  cudaFree(d_r2);
+  cudaFree(d_out);
+  if (e != cudaSuccess) {
+    set_error("upf_selftest_support_bins: %s", cudaGetErrorString(e));
+    return UPF_ERR_CUDA;
   }
   return UPF_OK;
 }

@@ -198,6 +198,15 @@ void build_bin_thresholds(const upf_params& p, float* out) {
   for (int b = 1; b <= UPF_LUT_SIZE; ++b)
     out[b] = first_true(top, [&](float r2) { return bin_exact(r2, factor) >= b; });
   out[UPF_LUT_SIZE + 1] = first_true(top, [&](float r2) { return sqrtf(r2) >= h; });
+  // Outside the support the reference adds nothing (it tests dist < h before
+  // the table, e.g. ComputePredictedDensityAndPressure, UnifiedPhysics.cpp:
+  // 5470). For some h, (int)(h * factor * 300) is 299, so the first r2 of
+  // bin 300 lies above h^2 and a pair just outside the support would still
+  // take bin 299. Starting bin 300 no later than the support's edge sends
+  // those pairs to the tables' zero entry; r2 inside the support is below
+  // both thresholds and keeps its bin. (bin_of_r2's guess near h^2 is 299,
+  // never lower, so the device then compares against this entry.)
+  if (out[UPF_LUT_SIZE] > out[UPF_LUT_SIZE + 1]) out[UPF_LUT_SIZE] = out[UPF_LUT_SIZE + 1];
 }
 
 void build_luts(const upf_params& p, float* out) {
