@@ -193,6 +193,9 @@ def run_reference(args, rank, world):
             "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
             flush=True)
         return
+    if args.scene == "io":
+        run_io_reference(args)
+        return
     from oracle import pyoracle
     pyoracle.build(with_ref=False)
     # bounded sample per step: a smaller block of the workload
@@ -455,6 +458,158 @@ def run_adjoint(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def run_io(args, rank, world, local_rank):
+    """State files of the 1M dam after one step: a "step" reads the state
+    back from the device and writes and re-reads it in each format, the
+    reference's liquid dump (UnifiedIO::SaveLiquidParticleInfoFull), the
+    PCISPH-format text file (ReadInFluidParticlesPCISPH's input) and the
+    binary snapshot file, in a temporary directory on the box's local disk.
+    The value is particle records per second through the liquid dump
+    (readback included); the reference writer, compiled from its sources
+    (oracle/_ref), formats a bounded sample of the same records for the
+    baseline."""
+    import tempfile
+
+    import torch
+    import unifiedparticleframeworkcuda_b200 as upf
+    from unifiedparticleframeworkcuda_b200 import build as upfbuild
+    from unifiedparticleframeworkcuda_b200 import particle_files as pf
+
+    if rank == 0:
+        upfbuild.build()
+    torch.cuda.set_device(local_rank)
+    sc = scene_for(argparse.Namespace(scene="c2"))
+    p = upf.derive_params(sc.params)
+    s = upf.ParticleSystem(p, capacity=sc.n, device=local_rank, derive=False)
+    s.set_particles(sc.pos, sc.vel, sc.type)
+    s.step(1)
+    s.synchronize()
+    nd = dynamic_count(sc)
+    phases = {"readback": 0.0, "liquid_dump": 0.0, "pcisph_text_write": 0.0, "pcisph_text_read": 0.0,
+              "snapshot_write": 0.0, "snapshot_read": 0.0}
+    sizes = {}
+    with tempfile.TemporaryDirectory(dir=os.environ.get("UPF_IO_DIR")) as d:
+        def one(timed):
+            t = {}
+            t0 = time.perf_counter()
+            st = s.particles()
+            t["readback"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            pf.save_liquid_info_full(os.path.join(d, "liquid.txt"), st["pos"], st["type"])
+            t["liquid_dump"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            pf.save_fluid_particles_pcisph(os.path.join(d, "fluid.txt"), st["pos"], st["vel"], st["type"],
+                                           st["pressure"], st["density"])
+            t["pcisph_text_write"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            back = pf.read_fluid_particles_pcisph(os.path.join(d, "fluid.txt"))
+            t["pcisph_text_read"] = time.perf_counter() - t0
+            assert back["type"].size == nd
+            t0 = time.perf_counter()
+            s.write_state_file(os.path.join(d, "state.upf"))
+            t["snapshot_write"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            s.read_state_file(os.path.join(d, "state.upf"))
+            t["snapshot_read"] = time.perf_counter() - t0
+            if timed:
+                for k, v in t.items():
+                    phases[k] += v
+            return st
+
+        for _ in range(args.warmup):
+            st = one(False)
+        for _ in range(args.steps):
+            st = one(True)
+        for name in ("liquid.txt", "fluid.txt", "state.upf"):
+            sizes[name] = os.path.getsize(os.path.join(d, name))
+        base = None
+        if not args.no_cpu_baseline:
+            base = io_reference_baseline(st, d)
+    s.close()
+    if rank != 0:
+        return
+    per = {k: v / args.steps for k, v in phases.items()}
+    dump_s = per["readback"] + per["liquid_dump"]
+    value = nd / dump_s
+    mbs = {"liquid_dump_MBps": sizes["liquid.txt"] / per["liquid_dump"] / 1e6,
+           "pcisph_text_write_MBps": sizes["fluid.txt"] / per["pcisph_text_write"] / 1e6,
+           "pcisph_text_read_MBps": sizes["fluid.txt"] / per["pcisph_text_read"] / 1e6,
+           "snapshot_write_MBps": sizes["state.upf"] / per["snapshot_write"] / 1e6,
+           "snapshot_read_MBps": sizes["state.upf"] / per["snapshot_read"] / 1e6}
+    out = {"metric": "particle records/s, reference-format liquid dump of the 1M dam state (readback included)",
+           "value": value, "unit": "records/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": sum(per.values()) * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "pcisph_dam_break_1M state files", "dynamic_particles": nd,
+                      "file_bytes": sizes, "host_threads": os.cpu_count()},
+           "phases_ms": {k: v * 1e3 for k, v in per.items()}, "throughput": mbs,
+           "e2e": {"value": value, "unit": "records/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": nd * (16 + 16 + 4 + 4 + 4 + 4)},
+           "gpu_launches": None, "note": "host-side file formatting and parsing; the device part is the readback"}
+    if base:
+        out["cpu_baseline"] = base
+    print(json.dumps(out))
+
+
+def run_io_reference(args):
+    """--impl reference --scene io: the reference's SaveLiquidParticleInfoFull
+    (compiled from src/cpu/UnifiedIO.cpp into oracle/_ref) on the 1M dam's
+    particles, one record stream; each step one full dump."""
+    from oracle import pyoracle
+    base = {"impl": "reference", "metric": "particle records/s, reference-format liquid dump of the 1M dam state "
+                                           "(readback included)", "unit": "records/s"}
+    if not pyoracle.ref_available():
+        print(json.dumps(dict(base, unavailable="oracle/_ref/libupfref.so (the compiled reference writer) is not "
+                                                "built")), flush=True)
+        return
+    sc = scene_for(argparse.Namespace(scene="c2"))
+    dyn = sc.type != 6
+    pos = np.ascontiguousarray(sc.pos[dyn], np.float32)
+    if pos.shape[1] == 3:
+        pos = np.ascontiguousarray(np.concatenate([pos, np.zeros((len(pos), 1), np.float32)], axis=1))
+    typ = np.ascontiguousarray(sc.type[dyn], np.int32)
+    nl = int(np.count_nonzero(typ == 2))
+    with tempfile.TemporaryDirectory(dir=os.environ.get("UPF_IO_DIR")) as d:
+        for _ in range(args.warmup):
+            pyoracle.ref_io_write("liquid", d, pos, typ, nl)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pyoracle.ref_io_write("liquid", d, pos, typ, nl)
+        dt = time.perf_counter() - t0
+    v = len(typ) * args.steps / dt
+    print(json.dumps(dict(base, value=v, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                          ms_per_step=1e3 * dt / args.steps, higher_is_better=True, scaling="weak",
+                          vs_baseline=None, dtype="f32", data="synthetic",
+                          config={"workload": "pcisph_dam_break_1M state files", "dynamic_particles": len(typ)},
+                          cpu_baseline={"value": v, "unit": "records/s", "cores": 1, "kind": "reference",
+                                        "sample": "SaveLiquidParticleInfoFull on all %d dynamic particles"
+                                                  % len(typ)},
+                          e2e={"value": v, "unit": "records/s", "h2d_bytes_per_step": 0,
+                               "d2h_bytes_per_step": 0})), flush=True)
+
+
+def io_reference_baseline(st, d, records=200_000):
+    """The reference's SaveLiquidParticleInfoFull and ReadInFluidParticlesPCISPH
+    (compiled from src/cpu/UnifiedIO.cpp into oracle/_ref) on the first
+    `records` particles of the same state, one thread."""
+    try:
+        from oracle import pyoracle
+        if not pyoracle.ref_available():
+            return None
+    except Exception:  # the pin library is not built
+        return None
+    pos = np.ascontiguousarray(st["pos"][:records])
+    typ = np.ascontiguousarray(st["type"][:records])
+    nl = int(np.count_nonzero(typ == 2))
+    work = os.path.join(d, "ref")
+    os.makedirs(work, exist_ok=True)
+    t0 = time.perf_counter()
+    pyoracle.ref_io_write("liquid", work, pos, typ, nl)
+    t_dump = time.perf_counter() - t0
+    return {"value": records / t_dump, "unit": "records/s", "cores": 1, "kind": "reference",
+            "sample": "SaveLiquidParticleInfoFull on the first %d particles of the same state" % records}
+
+
 def parse_shape(text):
     """'nlist,external,density_threads,density_rows,pforce_threads,pforce_rows[,density_mode,pforce_mode]'"""
     from unifiedparticleframeworkcuda_b200 import UpfLaunchConfig
@@ -659,7 +814,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3", "c4", "c5"])
+    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3", "c4", "c5", "io"])
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--block-size", type=int, default=0)
@@ -690,6 +845,8 @@ def main():
     try:
         if args.scene == "c4":
             run_batch(args, rank, world, local_rank)
+        elif args.scene == "io":
+            run_io(args, rank, world, local_rank)
         elif args.scene == "c5":
             run_adjoint(args, rank, world, local_rank)
         else:

@@ -49,7 +49,8 @@ typedef enum upf_status {
   UPF_ERR_TIMEOUT = 6,           /* a bounded device-side wait ran out */
   UPF_ERR_STATE = 7,             /* call out of order (e.g. step before set_particles) */
   UPF_ERR_UNSUPPORTED = 8,
-  UPF_ERR_NO_DEVICE = 9
+  UPF_ERR_NO_DEVICE = 9,
+  UPF_ERR_IO = 10                /* a file could not be opened, written, or parsed */
 } upf_status;
 
 /* Solver method, UnifiedConstants::setSimulationMethod
@@ -282,6 +283,69 @@ upf_status upf_restore(upf_system* s, int32_t slot);
 size_t upf_state_bytes(const upf_system* s);
 upf_status upf_state_save(upf_system* s, void* host, size_t bytes);
 upf_status upf_state_load(upf_system* s, const void* host, size_t bytes);
+
+/* Snapshot files: the upf_state_save bytes behind a header (format version,
+ * the saving system's upf_params, dynamic-particle and rigid-body counts,
+ * method, FNV-1a checksum). To resume in another process: create a system
+ * with the stored parameters (upf_state_file_info), set the same scene's
+ * particles, then upf_state_read_file; stepping on continues bit for bit.
+ * A file from a system of other counts or method is refused
+ * (UPF_ERR_INVALID_ARG); a damaged file gives UPF_ERR_IO. */
+upf_status upf_state_write_file(upf_system* s, const char* path);
+upf_status upf_state_read_file(upf_system* s, const char* path);
+upf_status upf_state_file_info(const char* path, upf_params* params, uint32_t* n_dynamic, uint32_t* num_bodies,
+                               uint64_t* state_bytes);
+
+/* ---- the reference's text formats (src/cpu/UnifiedIO.cpp,
+ * src/sceneConfigure/Scene.cpp) --------------------------------------------
+ * Host arrays in, files out (and back), byte for byte as the reference's
+ * stream formatting writes them; the reference writes to fixed paths with a
+ * per-function file counter, here the caller names the file. pos4: 4 floats
+ * per particle (x, y, z, unused), as the reference's device copies. Records
+ * are formatted on several host threads; the output does not depend on
+ * their number. Errors: UPF_ERR_IO (open/write/parse; upf_last_error says
+ * which record), UPF_ERR_INVALID_ARG. */
+/* UnifiedIO::SaveLiquidParticleInfoFull (UnifiedIO.cpp:60-105): the header
+ * count, then the liquid (type 2) particles among the first
+ * num_rounded_particles. */
+upf_status upf_io_save_liquid_info_full(const char* path, const float* pos4, const int32_t* type,
+                                        int32_t num_rounded_particles, int32_t num_liquid_particles);
+/* UnifiedIO::SaveRigidParticleInfoFull (UnifiedIO.cpp:107-152): rigid and
+ * frozen (types 0 and 6) particles; header_count is written as given (the
+ * reference's caller passes its rigid particle count). */
+upf_status upf_io_save_rigid_info_full(const char* path, const float* pos4, const int32_t* type,
+                                       int32_t num_rounded_particles, int32_t header_count);
+/* UnifiedIO::SaveParticlePositions (UnifiedIO.cpp:14-58). */
+upf_status upf_io_save_particle_positions(const char* path, const float* pos4, uint32_t n);
+/* Scene::saveParticles (Scene.cpp:247-279): position, rest density, mass,
+ * type; rest_density / mass may be NULL, then *_all is written for every
+ * particle. */
+upf_status upf_io_save_scene_particles(const char* path, const float* pos4, const float* rest_density,
+                                       const float* mass, const int32_t* type, uint32_t n, float rest_density_all,
+                                       float mass_all);
+/* The file UnifiedIO::ReadInFluidParticlesPCISPH reads: the count, then per
+ * particle position, type, velocity, correction pressure, predicted density
+ * (9 significant digits: floats read back exactly). corr_pressure /
+ * predicted_density may be NULL (written as 0). */
+upf_status upf_io_save_fluid_particles_pcisph(const char* path, const float* pos4, const float* vel4,
+                                              const int32_t* type, const float* corr_pressure,
+                                              const float* predicted_density, uint32_t n);
+/* UnifiedIO::ReadInFluidParticleNum (UnifiedIO.cpp:154-177). */
+upf_status upf_io_read_fluid_particle_num(const char* path, int32_t* count);
+/* UnifiedIO::ReadInFluidParticlesPCISPH (UnifiedIO.cpp:179-220); pos3 / vel3
+ * hold 3 floats per particle, as the reference's. *n_read: complete records
+ * read; a record that does not parse fully is an error (the reference keeps
+ * it half-read). More records than capacity: UPF_ERR_INVALID_ARG. */
+upf_status upf_io_read_fluid_particles_pcisph(const char* path, float* pos3, float* vel3, int32_t* type,
+                                              float* corr_pressure, float* predicted_density, int32_t capacity,
+                                              int32_t* n_read);
+/* Scene::readInParticles (Scene.cpp:218-243): position, density, mass, type
+ * records to the end of the file, granular (type 3) records skipped. All four
+ * arrays NULL: *n_out = the number of records kept. pos4 gets (x, y, z, 0).
+ * The reference repeats the last record at the end of the file; here it is
+ * read once. */
+upf_status upf_io_read_scene_particles(const char* path, float* pos4, float* density, float* mass, int32_t* type,
+                                       uint32_t capacity, uint32_t* n_out);
 
 /* Per-phase device timings of one step (the reference's SPH_PROFILING_VERBOSE
  * per-phase event timers, src/gpu/particles.cu:1460-1690). Runs one full

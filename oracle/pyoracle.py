@@ -115,6 +115,15 @@ def ref():
         L.ref_kernels.argtypes = [C.c_float, C.c_float, fp]
         L.ref_lut_lookup.argtypes = [C.c_float, fp, C.c_int, fp]
         L.ref_default_constants.argtypes = [fp]
+        ip = C.POINTER(C.c_int)
+        for name in ("ref_io_save_liquid", "ref_io_save_rigid"):
+            getattr(L, name).argtypes = [C.c_char_p, fp, ip, C.c_int, C.c_int, C.c_char_p, C.c_int]
+            getattr(L, name).restype = C.c_int
+        L.ref_io_save_positions.argtypes = [C.c_char_p, fp, C.c_int, C.c_char_p, C.c_int]
+        L.ref_io_save_positions.restype = C.c_int
+        L.ref_io_read_num.argtypes = [C.c_char_p]
+        L.ref_io_read_num.restype = C.c_int
+        L.ref_io_read_pcisph.argtypes = [C.c_char_p, fp, fp, ip, fp, fp]
         _ref = L
     return _ref
 
@@ -279,3 +288,36 @@ class OracleSim:
         ids = np.zeros(max(total, 1), np.uint32)
         lib().orc_neighbors(self._h, _ptr(off, C.c_uint32), _ptr(ids, C.c_uint32), total)
         return off, ids[:total]
+
+
+# ---------------------------------------------------------------- reference file I/O
+def ref_io_write(kind: str, workdir: str, pos4, type_=None, count: int = 0) -> bytes:
+    """The bytes the reference's UnifiedIO writer `kind` ("liquid", "rigid",
+    "positions") produces for these arrays (written under workdir)."""
+    R = ref()
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    name = C.create_string_buffer(512)
+    d = os.fsencode(workdir)
+    if kind == "positions":
+        rc = R.ref_io_save_positions(d, _ptr(pos4, C.c_float), len(pos4), name, 512)
+    else:
+        t = np.ascontiguousarray(type_, np.int32)
+        fn = R.ref_io_save_liquid if kind == "liquid" else R.ref_io_save_rigid
+        rc = fn(d, _ptr(pos4, C.c_float), _ptr(t, C.c_int), len(t), int(count), name, 512)
+    if rc != 0:
+        raise RuntimeError("reference writer failed")
+    with open(os.path.join(workdir, name.value.decode()), "rb") as f:
+        return f.read()
+
+
+def ref_io_read_pcisph(path: str) -> dict:
+    """UnifiedIO::ReadInFluidParticleNum + ReadInFluidParticlesPCISPH on path
+    (which must exist: the reference exits the process otherwise)."""
+    R = ref()
+    n = R.ref_io_read_num(os.fsencode(path))
+    out = {"pos": np.zeros((n, 3), np.float32), "vel": np.zeros((n, 3), np.float32), "type": np.zeros(n, np.int32),
+           "corr_pressure": np.zeros(n, np.float32), "predicted_density": np.zeros(n, np.float32)}
+    R.ref_io_read_pcisph(os.fsencode(path), _ptr(out["pos"], C.c_float), _ptr(out["vel"], C.c_float),
+                         _ptr(out["type"], C.c_int), _ptr(out["corr_pressure"], C.c_float),
+                         _ptr(out["predicted_density"], C.c_float))
+    return out

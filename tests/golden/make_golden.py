@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own CPU
 code (src/cpu/zIndex.cpp, src/cpu/WeightingKernel.cpp,
 src/sceneConfigure/UnifiedConstants.cpp, src/cpu/RigidBody.cpp,
-src/cpu/Matrix3x3.cpp), compiled by oracle/Makefile into
+src/cpu/Matrix3x3.cpp, src/cpu/UnifiedIO.cpp), compiled by oracle/Makefile into
 oracle/_ref/libupfref.so. Run in a checkout where the reference source tree
 is available:
 
@@ -91,6 +91,9 @@ def main():
     rigid = rigid_vectors(R)
     np.savez_compressed(os.path.join(HERE, "reference_rigid.npz"), **rigid)
     print("wrote", os.path.join(HERE, "reference_rigid.npz"))
+    io = io_vectors()
+    np.savez_compressed(os.path.join(HERE, "reference_io.npz"), **io)
+    print("wrote", os.path.join(HERE, "reference_io.npz"))
 
 
 def random_body_state(rng):
@@ -145,6 +148,86 @@ def rigid_vectors(R):
     return {"body_in": st_in, "body_force": force, "body_torque": torque, "body_dt": dt,
             "body_terminal_speed": terminal, "body_out": st_out, "inertia": mats, "inertia_inverse": inv,
             "inertia_ok": ok}
+
+
+def io_positions(rng, n):
+    """Positions spanning what the text writers must format: ordinary values,
+    lattice values, very small and very large exponents, integers, denormals,
+    signed zeros, the float extremes, infinities and NaNs."""
+    pos = rng.uniform(-1, 1, (n, 4)).astype(np.float32)
+    k = n // 8
+    pos[:k, :3] = rng.normal(size=(k, 3))
+    pos[k:2 * k, :3] = np.round(rng.uniform(0, 2, (k, 3)) / 0.01) * 0.01
+    pos[2 * k:3 * k, :3] = rng.normal(size=(k, 3)) * 10.0 ** rng.integers(-30, 30, (k, 3))
+    pos[3 * k:4 * k, :3] = rng.integers(-100000, 100000, (k, 3))
+    pos[4 * k:5 * k, :3] = rng.uniform(-1e-3, 1e-3, (k, 3))
+    special = np.array([0.0, -0.0, 1e-45, -3e-44, 1.17549435e-38, 3.4028235e38, -3.4028235e38, np.inf, -np.inf,
+                        np.nan, -np.nan, 0.1, 1.0 / 3.0, 123456789.0, 1e-7], np.float32)
+    rows = 5 * k + np.arange(special.size)
+    pos[rows, 0] = special
+    pos[rows, 1] = special[::-1]
+    pos[rows, 2] = -special
+    return pos.astype(np.float32)
+
+
+def io_reader_text(rng, n):
+    """A file in the format ReadInFluidParticlesPCISPH reads, written with
+    varied number spellings and white space."""
+    fmts = ["%.9g", "%e", "%+.3f", "%g", "%.2E", "%.0f.", "%.12g"]
+    seps = [" ", "  ", "\t", " \t ", "\n"]
+    vals = np.concatenate([rng.normal(size=(n, 8)) * 10.0 ** rng.integers(-8, 8, (n, 8)),
+                           rng.integers(-3, 8, (n, 1))], axis=1)
+    out = ["  %d\n" % n]
+    for i in range(n):
+        fields = []
+        for j, col in enumerate([0, 1, 2, 8, 3, 4, 5, 6, 7]):
+            if col == 8:
+                t = int(vals[i, 8])
+                fields.append(rng.choice(["%d", "+%d", "%03d"]) % t if t >= 0 else "%d" % t)
+            else:
+                fields.append(rng.choice(fmts) % float(vals[i, col]))
+        special = rng.integers(0, 12)
+        if special == 0:
+            fields[0] = "-0"
+        elif special == 1:
+            fields[4] = ".5"
+        elif special == 2:
+            fields[7] = "1e-45"
+        elif special == 3:
+            fields[8] = "5e3"
+        line = fields[0]
+        for f in fields[1:]:
+            line += rng.choice(seps) + f
+        out.append(line + "\n")
+    return "".join(out)
+
+
+def io_vectors():
+    """Inputs to the reference's text writers (UnifiedIO.cpp:14-152) and the
+    bytes it wrote; a reader file and the reference reader's values
+    (UnifiedIO.cpp:154-220)."""
+    import tempfile
+    rng = np.random.default_rng(20241203)
+    n = 400
+    pos = io_positions(rng, n)
+    types = rng.choice(np.array([0, 1, 2, 3, 6], np.int32), n, p=[0.15, 0.05, 0.6, 0.1, 0.1]).astype(np.int32)
+    nl = int(np.count_nonzero(types == 2))
+    nr = int(np.count_nonzero((types == 0) | (types == 6)))
+    text = io_reader_text(rng, 300)
+    with tempfile.TemporaryDirectory() as d:
+        liquid = pyoracle.ref_io_write("liquid", d, pos, types, nl)
+        rigid = pyoracle.ref_io_write("rigid", d, pos, types, nr)
+        positions = pyoracle.ref_io_write("positions", d, pos)
+        path = os.path.join(d, "fluid_in.txt")
+        with open(path, "w") as f:
+            f.write(text)
+        parsed = pyoracle.ref_io_read_pcisph(path)
+    out = {"pos": pos, "type": types, "num_liquid": np.int32(nl), "num_rigid": np.int32(nr),
+           "liquid_txt": np.frombuffer(liquid, np.uint8), "rigid_txt": np.frombuffer(rigid, np.uint8),
+           "positions_txt": np.frombuffer(positions, np.uint8),
+           "reader_txt": np.frombuffer(text.encode(), np.uint8)}
+    out.update({"read_" + k: v for k, v in parsed.items()})
+    return out
 
 
 if __name__ == "__main__":

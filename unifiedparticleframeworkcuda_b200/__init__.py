@@ -110,6 +110,17 @@ def lib():
             "upf_restore": [vp, C.c_int32],
             "upf_state_save": [vp, vp, C.c_size_t],
             "upf_state_load": [vp, vp, C.c_size_t],
+            "upf_state_write_file": [vp, C.c_char_p],
+            "upf_state_read_file": [vp, C.c_char_p],
+            "upf_state_file_info": [C.c_char_p, P, u32p, u32p, C.POINTER(C.c_uint64)],
+            "upf_io_save_liquid_info_full": [C.c_char_p, fp, i32p, C.c_int32, C.c_int32],
+            "upf_io_save_rigid_info_full": [C.c_char_p, fp, i32p, C.c_int32, C.c_int32],
+            "upf_io_save_particle_positions": [C.c_char_p, fp, C.c_uint32],
+            "upf_io_save_scene_particles": [C.c_char_p, fp, fp, fp, i32p, C.c_uint32, C.c_float, C.c_float],
+            "upf_io_save_fluid_particles_pcisph": [C.c_char_p, fp, fp, i32p, fp, fp, C.c_uint32],
+            "upf_io_read_fluid_particle_num": [C.c_char_p, i32p],
+            "upf_io_read_fluid_particles_pcisph": [C.c_char_p, fp, fp, i32p, fp, fp, C.c_int32, i32p],
+            "upf_io_read_scene_particles": [C.c_char_p, fp, fp, fp, i32p, C.c_uint32, u32p],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -263,6 +274,13 @@ class ParticleSystem:
     def load_state(self, data: bytes):
         buf = C.create_string_buffer(data, len(data))
         check(lib().upf_state_load(self._h, buf, len(data)), "upf_state_load")
+
+    def write_state_file(self, path: str):
+        """Snapshot file (upf_state_write_file): resume with read_state_file."""
+        check(lib().upf_state_write_file(self._h, os.fsencode(path)), "upf_state_write_file")
+
+    def read_state_file(self, path: str):
+        check(lib().upf_state_read_file(self._h, os.fsencode(path)), "upf_state_read_file")
 
     def reset_counters(self):
         check(lib().upf_reset_counters(self._h), "upf_reset_counters")

@@ -33,6 +33,7 @@ STATUS = {
     7: "UPF_ERR_STATE",
     8: "UPF_ERR_UNSUPPORTED",
     9: "UPF_ERR_NO_DEVICE",
+    10: "UPF_ERR_IO",
 }
 
 F3 = C.c_float * 3

@@ -23,7 +23,7 @@ LIB = os.path.join(HERE, "libupf.so")
 INCLUDE = os.path.abspath(os.path.join(HERE, "..", "include"))
 
 CU_SOURCES = ["upf_sort.cu", "upf_pipeline.cu", "upf_rigid.cu", "upf_api.cu", "upf_batch.cu", "upf_adjoint.cu", "upf_noalloc.cu"]
-CPP_SOURCES = ["upf_params.cpp"]
+CPP_SOURCES = ["upf_params.cpp", "upf_io.cpp"]
 HEADERS = ["upf_common.cuh", "upf_internal.h", "upf_sys.h", "upf_tma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -73,8 +73,8 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) 
     for f in CPP_SOURCES:
         obj = os.path.join(BUILD, f + ".o")
         objs.append(obj)
-        jobs.append([_cxx(), "-c", os.path.join(CSRC, f), "-o", obj, "-O2", "-std=c++17", "-fPIC",
-                     "-ffp-contract=off", "-I" + INCLUDE, "-I" + CSRC, "-I/usr/local/cuda/include"])
+        jobs.append([_cxx(), "-c", os.path.join(CSRC, f), "-o", obj, "-O2", "-std=c++17", "-fPIC", "-pthread",
+                     "-ffp-contract=off", "-Wall", "-I" + INCLUDE, "-I" + CSRC, "-I/usr/local/cuda/include"])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -88,7 +88,7 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) 
             if ptxas_verbose or not quiet:
                 sys.stderr.write(r.stderr)
     tmp = LIB + ".tmp"
-    link = [nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-ccbin", _cxx()]
+    link = [nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC,-pthread", "-ccbin", _cxx()]
     r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -550,6 +550,7 @@ const char* upf_status_string(upf_status st) {
     case UPF_ERR_STATE: return "UPF_ERR_STATE";
     case UPF_ERR_UNSUPPORTED: return "UPF_ERR_UNSUPPORTED";
     case UPF_ERR_NO_DEVICE: return "UPF_ERR_NO_DEVICE";
+    case UPF_ERR_IO: return "UPF_ERR_IO";
   }
   return "unknown";
 }
