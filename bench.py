@@ -196,6 +196,20 @@ def run_reference(args, rank, world):
     if args.scene == "io":
         run_io_reference(args)
         return
+    if args.scene == "mesh":
+        tri, _ = mesh_workload()
+        cb = mesh_reference_sample(tri)
+        base = {"impl": "reference", "metric": MESH_METRIC, "unit": "point-face tests/s"}
+        if cb is None:
+            print(json.dumps(dict(base, unavailable="oracle/_ref/libupfref.so (the compiled reference loader) is "
+                                                    "not built")), flush=True)
+            return
+        print(json.dumps(dict(base, value=cb["value"], n_gpus=args.gpus, steps=1, warmup=0, higher_is_better=True,
+                              scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+                              config={"workload": "icosphere_5120_faces_2mm"}, cpu_baseline=cb,
+                              e2e={"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
+                                   "d2h_bytes_per_step": 0})), flush=True)
+        return
     from oracle import pyoracle
     pyoracle.build(with_ref=False)
     # bounded sample per step: a smaller block of the workload
@@ -551,6 +565,79 @@ def run_io(args, rank, world, local_rank):
     print(json.dumps(out))
 
 
+MESH_METRIC = "lattice point-face tests/s, filling a 5120-face closed mesh (ObjectLoader::LoadParticles)"
+
+
+def mesh_workload():
+    """A 0.1 m sphere of 5,120 faces (about the reference's largest model,
+    banana.obj, 5,592 faces) centred on the origin, at 0.002 m spacing: a
+    101^3 lattice."""
+    from unifiedparticleframeworkcuda_b200 import scenes
+    return scenes.mesh_icosphere(0.1, 4), 0.002
+
+
+def run_mesh(args, rank, world, local_rank):
+    """Mesh filling on the GPU (upf_mesh_particles): each step is one call,
+    host face set-up, copies, the inside tests of every lattice point against
+    every face, compaction and the particles' readback included, timed by
+    the host clock around the synchronous call."""
+    import unifiedparticleframeworkcuda_b200 as upf
+    from unifiedparticleframeworkcuda_b200 import build as upfbuild
+    if rank == 0:
+        upfbuild.build()
+    tri, spacing = mesh_workload()
+    ext = tri.reshape(-1, 3)
+    lo = np.minimum(ext.min(0), 0.0)
+    hi = np.maximum(ext.max(0), 0.0)
+    pts = int(np.prod(np.floor((hi - lo) / spacing) + 1))
+    for _ in range(args.warmup):
+        out = upf.mesh_particles(tri, spacing, device=local_rank)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = upf.mesh_particles(tri, spacing, device=local_rank)
+    dt = (time.perf_counter() - t0) / args.steps
+    job = replicas.max_over_ranks(dt)[0]
+    if rank != 0:
+        return
+    tests = pts * len(tri)
+    line = {"metric": MESH_METRIC, "value": tests * world / job, "unit": "point-face tests/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": job * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "icosphere_5120_faces_2mm", "faces": len(tri), "lattice_points": pts,
+                       "particles": len(out)},
+            "e2e": {"value": tests * world / job, "unit": "point-face tests/s",
+                    "h2d_bytes_per_step": len(tri) * 72, "d2h_bytes_per_step": len(out) * 16},
+            "gpu_launches": args.steps * (4 if len(out) else 3)}
+    if world == 1 and not args.no_cpu_baseline:
+        cb = mesh_reference_sample(tri)
+        if cb:
+            line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+
+
+def mesh_reference_sample(tri, spacing=0.006):
+    """The reference's ObjectLoader::LoadParticles (compiled from its sources
+    into oracle/_ref) on the same mesh at a coarser spacing (a bounded
+    sample, about 43k lattice points), one thread."""
+    try:
+        from oracle import pyoracle
+        if not pyoracle.ref_available():
+            return None
+    except Exception:  # the pin library is not built
+        return None
+    from unifiedparticleframeworkcuda_b200 import scenes
+    ext = tri.reshape(-1, 3)
+    pts = int(np.prod(np.floor((np.maximum(ext.max(0), 0) - np.minimum(ext.min(0), 0)) / spacing) + 1))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "mesh.obj")
+        scenes.write_obj(path, tri)
+        t0 = time.perf_counter()
+        pyoracle.ref_obj_particles(path, (1.0, 1.0, 1.0), spacing)
+        dt = time.perf_counter() - t0
+    return {"value": pts * len(tri) / dt, "unit": "point-face tests/s", "cores": 1, "kind": "reference",
+            "sample": "the same mesh at %g m spacing (%d lattice points)" % (spacing, pts)}
+
+
 def run_io_reference(args):
     """--impl reference --scene io: the reference's SaveLiquidParticleInfoFull
     (compiled from src/cpu/UnifiedIO.cpp into oracle/_ref) on the 1M dam's
@@ -814,7 +901,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3", "c4", "c5", "io"])
+    ap.add_argument("--scene", default="c2", choices=["c2", "c2-small", "c1", "c3", "c4", "c5", "io", "mesh"])
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--block-size", type=int, default=0)
@@ -847,6 +934,8 @@ def main():
             run_batch(args, rank, world, local_rank)
         elif args.scene == "io":
             run_io(args, rank, world, local_rank)
+        elif args.scene == "mesh":
+            run_mesh(args, rank, world, local_rank)
         elif args.scene == "c5":
             run_adjoint(args, rank, world, local_rank)
         else:

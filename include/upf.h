@@ -347,6 +347,28 @@ upf_status upf_io_read_fluid_particles_pcisph(const char* path, float* pos3, flo
 upf_status upf_io_read_scene_particles(const char* path, float* pos4, float* density, float* mass, int32_t* type,
                                        uint32_t capacity, uint32_t* n_out);
 
+/* ---- scene construction --------------------------------------------------
+ * ObjLoader::Load + LoadFaces (src/cpu/ObjLoader.cpp:17-233): the triangles
+ * of a Wavefront OBJ file, 9 floats each (three corners x, y, z). tri9 NULL:
+ * *n_out = the number of triangles. "v" and "f" lines are read (faces as
+ * v/vt/vn corners like the reference, also a, a/b, a//c); a corner index
+ * outside the file's vertices is UPF_ERR_IO. As in the reference, a file
+ * that ends with a newline-terminated "f" line lists its last triangle
+ * twice (the reference's read loop handles its last line twice), which
+ * takes that face out of the filling's crossing count. */
+upf_status upf_obj_read_triangles(const char* path, float* tri9, uint32_t capacity, uint32_t* n_out);
+/* ObjectLoader::LoadParticles (src/cpu/ObjectLoader.cpp:8-97) on GPU `device`:
+ * the particles that fill the closed triangle mesh tri9 (n_tri triangles),
+ * scaled by scale_x/y/z, on the reference's staggered lattice of the given
+ * spacing, in the reference's order and bit for bit its positions
+ * ((p - box minimum) * scale, as the reference returns them; the caller
+ * adds an offset as Scene::CreateFullParticleObject does). pos4: x, y, z, 0
+ * per particle; pos4 NULL: *n_out = the count only. More particles than
+ * capacity: UPF_ERR_INVALID_ARG with *n_out = the count. The lattice may
+ * hold at most 2^31 points. Synchronous; allocates its working buffers. */
+upf_status upf_mesh_particles(int device, const float* tri9, uint32_t n_tri, float scale_x, float scale_y,
+                              float scale_z, float spacing, float* pos4, uint32_t capacity, uint32_t* n_out);
+
 /* Per-phase device timings of one step (the reference's SPH_PROFILING_VERBOSE
  * per-phase event timers, src/gpu/particles.cu:1460-1690). Runs one full
  * step through the phase entry points with CUDA events around each phase,

@@ -124,6 +124,8 @@ def ref():
         L.ref_io_read_num.argtypes = [C.c_char_p]
         L.ref_io_read_num.restype = C.c_int
         L.ref_io_read_pcisph.argtypes = [C.c_char_p, fp, fp, ip, fp, fp]
+        L.ref_obj_particles.argtypes = [C.c_char_p, C.c_float, C.c_float, C.c_float, C.c_float, fp, C.c_int]
+        L.ref_obj_particles.restype = C.c_int
         _ref = L
     return _ref
 
@@ -321,3 +323,18 @@ def ref_io_read_pcisph(path: str) -> dict:
                          _ptr(out["type"], C.c_int), _ptr(out["corr_pressure"], C.c_float),
                          _ptr(out["predicted_density"], C.c_float))
     return out
+
+
+# ---------------------------------------------------------------- reference mesh voxeliser
+def ref_obj_particles(path: str, scale, spacing: float) -> np.ndarray:
+    """ObjLoader::GetInstance().LoadParticles on an OBJ file: particle
+    positions (n x 3) in the reference's order."""
+    R = ref()
+    sx, sy, sz = (float(v) for v in scale)
+    cap = 1 << 16
+    while True:
+        buf = np.zeros((cap, 3), np.float32)
+        n = R.ref_obj_particles(os.fsencode(path), sx, sy, sz, float(spacing), _ptr(buf, C.c_float), cap)
+        if n <= cap:
+            return buf[:n].copy()
+        cap = n

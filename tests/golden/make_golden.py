@@ -94,6 +94,9 @@ def main():
     io = io_vectors()
     np.savez_compressed(os.path.join(HERE, "reference_io.npz"), **io)
     print("wrote", os.path.join(HERE, "reference_io.npz"))
+    mesh = mesh_vectors()
+    np.savez_compressed(os.path.join(HERE, "reference_mesh.npz"), **mesh)
+    print("wrote", os.path.join(HERE, "reference_mesh.npz"))
 
 
 def random_body_state(rng):
@@ -227,6 +230,42 @@ def io_vectors():
            "positions_txt": np.frombuffer(positions, np.uint8),
            "reader_txt": np.frombuffer(text.encode(), np.uint8)}
     out.update({"read_" + k: v for k, v in parsed.items()})
+    return out
+
+
+def mesh_cases():
+    """Closed procedural meshes (the library's own, written as OBJ files) with
+    the scale and spacing each is filled at: off the origin (the reference's
+    lattice box always contains the origin), at negative coordinates,
+    non-uniform scales, rotated, and an axis-aligned box whose faces lie on
+    lattice planes (points that touch a face)."""
+    from unifiedparticleframeworkcuda_b200 import scenes
+    return [
+        ("icosphere", scenes.mesh_icosphere(0.1, 2, (0.3, 0.2, 0.25)), (1.0, 1.0, 1.0), 0.012),
+        ("torus", scenes.mesh_torus(center=(-0.2, 0.1, -0.3)), (1.5, 2.0, 1.0), 0.015),
+        ("rotated_box", scenes.mesh_box(rotation_seed=5, center=(0.5, 0.4, 0.3)), (1.0, 1.0, 1.0), 0.013),
+        ("icosphere_fine_scaled", scenes.mesh_icosphere(0.08, 3), (2.5, 2.5, 2.5), 0.025),
+        ("torus_small", scenes.mesh_torus(0.05, 0.02, 32, 16, (0.02, 0.03, 0.01)), (0.5, 0.5, 0.5), 0.004),
+        ("aligned_box", scenes.mesh_box((0.1, 0.05, 0.08), center=(0.1, 0.05, 0.08)), (1.0, 1.0, 1.0), 0.01),
+    ]
+
+
+def mesh_vectors():
+    """The reference's ObjectLoader::LoadParticles (src/cpu/ObjectLoader.cpp,
+    with its OBJ parser and Polygon tests) on each case's OBJ file."""
+    import tempfile
+    from unifiedparticleframeworkcuda_b200 import scenes
+    R = pyoracle.ref()
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, tri, scale, spacing in mesh_cases():
+            path = os.path.join(d, name + ".obj")
+            scenes.write_obj(path, tri)
+            n = pyoracle.ref_obj_particles(path, scale, spacing)
+            out[name + "_tri"] = tri
+            out[name + "_scale"] = np.array(scale, np.float32)
+            out[name + "_spacing"] = np.float32(spacing)
+            out[name + "_pos"] = n
     return out
 
 

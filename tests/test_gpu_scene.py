@@ -1,0 +1,67 @@
+"""The device mesh voxeliser (upf_mesh_particles) against the reference's
+ObjectLoader::LoadParticles: on every golden mesh the particles, their
+positions and their order are bit-identical to what the compiled reference
+produced (tests/golden/reference_mesh.npz, from tests/golden/make_golden.py),
+reading the mesh through upf_obj_read_triangles as the reference reads it."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from unifiedparticleframeworkcuda_b200 import STATUS, UpfError, scenes
+
+pytestmark = pytest.mark.gpu
+CODE = {name: code for code, name in STATUS.items()}
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = np.load(os.path.join(HERE, "golden", "reference_mesh.npz"))
+CASES = sorted({k[: -len("_tri")] for k in GOLD.files if k.endswith("_tri")})
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mesh_particles_match_the_reference_voxeliser(upf_lib, tmp_path, name):
+    path = tmp_path / (name + ".obj")
+    scenes.write_obj(path, GOLD[name + "_tri"])
+    tri = upf_lib.obj_triangles(path)
+    got = upf_lib.mesh_particles(tri, float(GOLD[name + "_spacing"]), GOLD[name + "_scale"])
+    want = GOLD[name + "_pos"]
+    assert got.shape[0] == want.shape[0]
+    assert np.array_equal(got[:, :3].view(np.uint32), want.view(np.uint32))
+    assert np.all(got[:, 3] == 0)
+
+
+def _read_as_obj(upf, tmp_path, name):
+    path = tmp_path / (name + ".obj")
+    scenes.write_obj(path, GOLD[name + "_tri"])
+    return np.ascontiguousarray(upf.obj_triangles(path))
+
+
+def test_count_capacity_and_bad_arguments(upf_lib, tmp_path):
+    L = upf_lib.lib()
+    tri = _read_as_obj(upf_lib, tmp_path, "icosphere")
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    n = C.c_uint32()
+    assert L.upf_mesh_particles(0, fp(tri), len(tri), 1.0, 1.0, 1.0, 0.012, None, 0, C.byref(n)) == 0
+    assert n.value == len(GOLD["icosphere_pos"])
+    small = np.zeros((10, 4), np.float32)
+    rc = L.upf_mesh_particles(0, fp(tri), len(tri), 1.0, 1.0, 1.0, 0.012, fp(small), 10, C.byref(n))
+    assert rc == CODE["UPF_ERR_INVALID_ARG"] and n.value == len(GOLD["icosphere_pos"])
+    assert L.upf_mesh_particles(0, fp(tri), len(tri), 1.0, 1.0, 1.0, 0.0, None, 0, C.byref(n)) == 1
+    # a lattice beyond the 2^31-point limit is refused before any device work
+    rc = L.upf_mesh_particles(0, fp(tri), len(tri), 1.0, 1.0, 1.0, 1e-5, None, 0, C.byref(n))
+    assert rc == CODE["UPF_ERR_INVALID_ARG"] and "limit" in L.upf_last_error().decode()
+    # an empty mesh fills nothing, as in the reference
+    assert L.upf_mesh_particles(0, None, 0, 1.0, 1.0, 1.0, 0.01, None, 0, C.byref(n)) == 0 and n.value == 0
+
+
+def test_injected_allocation_failure_is_reported(upf_lib, tmp_path):
+    L = upf_lib.lib()
+    tri = _read_as_obj(upf_lib, tmp_path, "torus")
+    try:
+        L.upf_test_fail_allocation(2)
+        with pytest.raises(UpfError) as e:
+            upf_lib.mesh_particles(tri, 0.015, (1.5, 2.0, 1.0))
+        assert e.value.status == CODE["UPF_ERR_ALLOC"] and "injected" in str(e.value)
+    finally:
+        L.upf_test_fail_allocation(-1)
+    assert len(upf_lib.mesh_particles(tri, 0.015, (1.5, 2.0, 1.0))) == len(GOLD["torus_pos"])

@@ -121,6 +121,9 @@ def lib():
             "upf_io_read_fluid_particle_num": [C.c_char_p, i32p],
             "upf_io_read_fluid_particles_pcisph": [C.c_char_p, fp, fp, i32p, fp, fp, C.c_int32, i32p],
             "upf_io_read_scene_particles": [C.c_char_p, fp, fp, fp, i32p, C.c_uint32, u32p],
+            "upf_obj_read_triangles": [C.c_char_p, fp, C.c_uint32, u32p],
+            "upf_mesh_particles": [C.c_int, fp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, fp,
+                                   C.c_uint32, u32p],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -174,6 +177,42 @@ def build_luts(p: UpfParams) -> np.ndarray:
 def bin_thresholds(p: UpfParams) -> np.ndarray:
     out = np.zeros(302, np.float32)
     check(lib().upf_build_bin_thresholds(C.byref(p), _p(out, C.c_float)), "upf_build_bin_thresholds")
+    return out
+
+
+def obj_triangles(path) -> np.ndarray:
+    """The triangles of a Wavefront OBJ file (upf_obj_read_triangles), n x 9."""
+    n = C.c_uint32()
+    fs = os.fsencode(str(path))
+    check(lib().upf_obj_read_triangles(fs, None, 0, C.byref(n)), "upf_obj_read_triangles")
+    out = np.zeros((n.value, 9), np.float32)
+    check(lib().upf_obj_read_triangles(fs, _p(out, C.c_float), n.value, C.byref(n)), "upf_obj_read_triangles")
+    return out
+
+
+def mesh_particles(tri9, spacing: float, scale=(1.0, 1.0, 1.0), device: int = 0) -> np.ndarray:
+    """Particles filling a closed triangle mesh on the GPU (upf_mesh_particles,
+    the reference's ObjectLoader::LoadParticles), n x 4."""
+    t = np.ascontiguousarray(tri9, np.float32).reshape(-1, 9)
+    sx, sy, sz = (float(v) for v in scale)
+    n = C.c_uint32()
+    # at most one particle per lattice point: one pass when that bound is modest
+    if len(t):
+        v = t.reshape(-1, 3).astype(np.float64)
+        ext = (np.maximum(v.max(0), 0.0) - np.minimum(v.min(0), 0.0)) * np.array([sx, sy, sz])
+        bound = int(np.prod(np.floor(ext / float(spacing)) + 2))
+    else:
+        bound = 0
+    if 0 < bound <= (1 << 24):
+        out = np.zeros((bound, 4), np.float32)
+        check(lib().upf_mesh_particles(device, _p(t, C.c_float), len(t), sx, sy, sz, float(spacing),
+                                       _p(out, C.c_float), bound, C.byref(n)), "upf_mesh_particles")
+        return out[: n.value].copy()
+    check(lib().upf_mesh_particles(device, _p(t, C.c_float), len(t), sx, sy, sz, float(spacing), None, 0,
+                                   C.byref(n)), "upf_mesh_particles")
+    out = np.zeros((n.value, 4), np.float32)
+    check(lib().upf_mesh_particles(device, _p(t, C.c_float), len(t), sx, sy, sz, float(spacing), _p(out, C.c_float),
+                                   n.value, C.byref(n)), "upf_mesh_particles")
     return out
 
 

@@ -22,7 +22,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libupf.so")
 INCLUDE = os.path.abspath(os.path.join(HERE, "..", "include"))
 
-CU_SOURCES = ["upf_sort.cu", "upf_pipeline.cu", "upf_rigid.cu", "upf_api.cu", "upf_batch.cu", "upf_adjoint.cu", "upf_noalloc.cu"]
+CU_SOURCES = ["upf_sort.cu", "upf_pipeline.cu", "upf_rigid.cu", "upf_api.cu", "upf_batch.cu", "upf_adjoint.cu", "upf_noalloc.cu", "upf_scene.cu"]
 CPP_SOURCES = ["upf_params.cpp", "upf_io.cpp"]
 HEADERS = ["upf_common.cuh", "upf_internal.h", "upf_sys.h", "upf_tma.cuh"]
 

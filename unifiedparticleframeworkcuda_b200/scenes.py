@@ -211,6 +211,74 @@ def _random_rotation(u):
                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
 
 
+# ---------------------------------------------------------------- closed meshes
+# Triangle meshes (n x 9 float32: three corners per row, counter-clockwise
+# seen from outside) for the mesh voxeliser (upf_mesh_particles), which
+# fills a closed mesh the way the reference fills its OBJ models.
+
+def mesh_icosphere(radius=0.1, subdiv=2, center=(0.0, 0.0, 0.0)) -> np.ndarray:
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    v = [np.array(x, np.float64) / np.linalg.norm(x) for x in v]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        mid = {}
+
+        def m(a, b):
+            k = (min(a, b), max(a, b))
+            if k not in mid:
+                x = v[a] + v[b]
+                v.append(x / np.linalg.norm(x))
+                mid[k] = len(v) - 1
+            return mid[k]
+        f = [g for a, b, c in f for g in ((a, m(a, b), m(c, a)), (b, m(b, c), m(a, b)), (c, m(c, a), m(b, c)),
+                                          (m(a, b), m(b, c), m(c, a)))]
+    pts = np.array(v) * radius + np.asarray(center, np.float64)
+    return pts[np.array(f)].reshape(-1, 9).astype(np.float32)
+
+
+def mesh_torus(big=0.1, small=0.035, nu=24, nv=12, center=(0.0, 0.0, 0.0)) -> np.ndarray:
+    u = 2 * np.pi * np.arange(nu) / nu
+    w = 2 * np.pi * np.arange(nv) / nv
+    def p(i, j):
+        a, b = u[i % nu], w[j % nv]
+        return ((big + small * np.cos(b)) * np.cos(a), small * np.sin(b), (big + small * np.cos(b)) * np.sin(a))
+    tris = []
+    for i in range(nu):
+        for j in range(nv):
+            q00, q10, q11, q01 = p(i, j), p(i + 1, j), p(i + 1, j + 1), p(i, j + 1)
+            tris += [q00 + q01 + q11, q00 + q11 + q10]
+    return (np.array(tris) + np.tile(np.asarray(center, np.float64), 3)).astype(np.float32)
+
+
+def mesh_box(half=(0.1, 0.06, 0.08), rotation_seed=None, center=(0.0, 0.0, 0.0)) -> np.ndarray:
+    c = np.array([[x, y, z] for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)], np.float64) * np.asarray(half)
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    if rotation_seed is not None:
+        c = c @ _random_rotation(uniform(rotation_seed, 3)).T
+    c = c + np.asarray(center, np.float64)
+    tris = [c[[a, b, d]].ravel() for a, b, cc, d in quads] + [c[[b, cc, d]].ravel() for a, b, cc, d in quads]
+    return np.array(tris).astype(np.float32)
+
+
+def write_obj(path, tri9) -> None:
+    """A Wavefront OBJ file the reference's ObjLoader reads: one vertex line
+    per corner (9 significant digits: floats read back exactly), one texture
+    coordinate and one normal line (its face lines index both), faces as
+    v/vt/vn corners."""
+    t = np.asarray(tri9, np.float32).reshape(-1, 3)
+    with open(path, "w") as f:
+        f.write("# closed triangle mesh, %d faces\n" % (len(t) // 3))
+        for x, y, z in t:
+            f.write("v %.9g %.9g %.9g\n" % (x, y, z))
+        f.write("vt 0 0\nvn 0 0 1\n")
+        for k in range(len(t) // 3):
+            f.write("f %d/1/1 %d/1/1 %d/1/1\n" % (3 * k + 1, 3 * k + 2, 3 * k + 3))
+
+
 def sample_sphere(r, n):
     """n points on a sphere of radius r (Fibonacci lattice)."""
     k = np.arange(n) + 0.5
