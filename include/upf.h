@@ -271,6 +271,24 @@ upf_status upf_phase_integrate(upf_system* s);
  * host-driven caller (src/gpu/particles.cuh:437). */
 upf_status upf_upload_state(upf_system* s, const float* pos4, const float* vel4, uint32_t n);
 
+/* Asynchronous counterparts of the per-frame upload and readback, for a
+ * host-driven loop (upload, step, read back, every frame). No counterpart in
+ * the reference, which copies synchronously between steps. The host copies
+ * run on copy streams of the system's own (one per direction), against
+ * device staging buffers, so they overlap the steps and each other: an upload is copied while the previous step
+ * runs and enters the state in stream order before the next step; a
+ * readback is taken in stream order after the step and copied to the host
+ * while the next step runs. Each call returns at once; upf_wait_frames waits
+ * for the copies issued so far (after it, the upload's host arrays may be
+ * rewritten and the readback's host arrays hold their data). Until then
+ * neither may be touched. Use pinned host memory for the copies to overlap.
+ * The staging buffers (about 72 bytes per particle of capacity) are
+ * allocated on the first call. */
+upf_status upf_upload_state_async(upf_system* s, const float* pos4, const float* vel4, uint32_t n);
+upf_status upf_get_particles_async(upf_system* s, float* pos4, float* vel4, float* density, float* pressure,
+                                   int32_t* type, uint32_t* id, uint32_t* n_out);
+upf_status upf_wait_frames(upf_system* s);
+
 /* ---- checkpoint / resume ------------------------------------------------- */
 /* The reference only has text dumps and readers (src/cpu/UnifiedIO.cpp:14-220).
  * Here the dynamic state (positions, velocities, lagged PCISPH state, ids,

@@ -104,6 +104,9 @@ def lib():
             "upf_radix_sort_pairs_noalloc": [vp, vp, C.c_uint32, C.c_int32, vp],
             "upf_cell_ranges": [vp, C.c_uint32, C.c_int32, C.c_uint32, vp, vp, vp],
             "upf_upload_state": [vp, fp, fp, C.c_uint32],
+            "upf_upload_state_async": [vp, fp, fp, C.c_uint32],
+            "upf_get_particles_async": [vp, fp, fp, fp, fp, i32p, u32p, u32p],
+            "upf_wait_frames": [vp],
             "upf_profile_step": [vp, C.POINTER(UpfPhaseTimes)],
             "upf_reset_counters": [vp],
             "upf_checkpoint": [vp, C.c_int32],

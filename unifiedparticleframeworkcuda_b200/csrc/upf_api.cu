@@ -772,10 +772,13 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   return UPF_OK;
 }
 
+static void frames_release(System& s);  // below, with the asynchronous frame exchange
+
 upf_status upf_destroy(upf_system* s) {
   if (!s) return UPF_OK;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  frames_release(*s);
   destroy_graph(*s);
   for (void* p : s->allocations) cudaFree(p);
   free_list(s->rigid_allocations);
@@ -1485,6 +1488,110 @@ upf_status upf_get_particles(upf_system* s, float* pos4, float* vel4, float* den
   if (id && n) UPF_CUDA(cudaMemcpyAsync(id, s->A.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
   UPF_CUDA(cudaStreamSynchronize(st));
   if (n_out) *n_out = n;
+  return UPF_OK;
+}
+
+// ---- asynchronous per-frame exchange -----------------------------------------
+// A host-driven caller uploads its particles before a step and reads the
+// result after it (CopyParticleDataHostToDevice, CopyParticlesCUDA). Done
+// in stream order, those copies sit between the steps. Here they run on a
+// copy stream of each direction against device staging buffers: an upload
+// copies into staging while the previous step still runs, and enters the
+// state in stream order before the next step; a readback takes a device
+// copy of the result in stream order and copies it to the host while the
+// next step runs. With one stream per direction, a readback never holds up
+// the next upload. Events order the buffers' reuse.
+static upf_status frames_ready(System& s) {
+  System::FrameIO& io = s.io;
+  if (io.ready) return UPF_OK;
+  const uint32_t c = s.capacity;
+  UPF_TRY(dalloc(s, &io.in_pos, c));
+  UPF_TRY(dalloc(s, &io.in_vel, c));
+  UPF_TRY(dalloc(s, &io.out_pos, c));
+  UPF_TRY(dalloc(s, &io.out_vel, c));
+  UPF_TRY(dalloc(s, &io.out_rho, c));
+  UPF_TRY(dalloc(s, &io.out_press, c));
+  UPF_TRY(dalloc(s, &io.out_type, c));
+  UPF_TRY(dalloc(s, &io.out_id, c));
+  UPF_CUDA(cudaStreamCreateWithFlags(&io.up, cudaStreamNonBlocking));
+  UPF_CUDA(cudaStreamCreateWithFlags(&io.down, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&io.staged, &io.consumed, &io.snapped, &io.read_done})
+    UPF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  // all four start completed
+  for (cudaEvent_t e : {io.staged, io.consumed, io.snapped, io.read_done}) UPF_CUDA(cudaEventRecord(e, s.stream));
+  io.ready = true;
+  return UPF_OK;
+}
+
+static void frames_release(System& s) {
+  System::FrameIO& io = s.io;
+  for (cudaStream_t c : {io.up, io.down})
+    if (c) cudaStreamSynchronize(c);
+  for (cudaEvent_t e : {io.staged, io.consumed, io.snapped, io.read_done})
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t c : {io.up, io.down})
+    if (c) cudaStreamDestroy(c);
+  io = System::FrameIO{};  // the buffers are in s.allocations
+}
+
+upf_status upf_upload_state_async(upf_system* s, const float* pos4, const float* vel4, uint32_t n) {
+  UPF_TRY(phase_guard(s));
+  if (n != s->n_dyn || (n && (!pos4 || !vel4))) {
+    set_error("upf_upload_state_async: need %u dynamic particles and non-null arrays", s->n_dyn);
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (!n) return UPF_OK;
+  UPF_TRY(frames_ready(*s));
+  System::FrameIO& io = s->io;
+  UPF_CUDA(cudaStreamWaitEvent(io.up, io.consumed, 0));  // the last upload has left the staging buffers
+  UPF_CUDA(cudaMemcpyAsync(io.in_pos, pos4, sizeof(float4) * n, cudaMemcpyHostToDevice, io.up));
+  UPF_CUDA(cudaMemcpyAsync(io.in_vel, vel4, sizeof(float4) * n, cudaMemcpyHostToDevice, io.up));
+  UPF_CUDA(cudaEventRecord(io.staged, io.up));
+  UPF_CUDA(cudaStreamWaitEvent(s->stream, io.staged, 0));
+  UPF_CUDA(cudaMemcpyAsync(s->A.pos, io.in_pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, s->stream));
+  UPF_CUDA(cudaMemcpyAsync(s->A.vel, io.in_vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, s->stream));
+  UPF_CUDA(launch_upload_keys(*s, s->stream));
+  UPF_CUDA(cudaEventRecord(io.consumed, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_get_particles_async(upf_system* s, float* pos4, float* vel4, float* density, float* pressure,
+                                   int32_t* type, uint32_t* id, uint32_t* n_out) {
+  UPF_TRY(phase_guard(s));
+  const uint32_t n = s->n_dyn;
+  if (n_out) *n_out = n;
+  if (!n) return UPF_OK;
+  UPF_TRY(frames_ready(*s));
+  System::FrameIO& io = s->io;
+  cudaStream_t st = s->stream;
+  UPF_CUDA(cudaStreamWaitEvent(st, io.read_done, 0));  // the last readback has left the snapshot
+  struct Item {
+    void* host;
+    void* snap;
+    const void* src;
+    size_t bytes;
+  } items[] = {{pos4, io.out_pos, s->A.pos, sizeof(float4) * n},   {vel4, io.out_vel, s->A.vel, sizeof(float4) * n},
+               {density, io.out_rho, s->rho, sizeof(float) * n},   {pressure, io.out_press, s->press, sizeof(float) * n},
+               {type, io.out_type, s->A.type, sizeof(int32_t) * n}, {id, io.out_id, s->A.id, sizeof(uint32_t) * n}};
+  for (const Item& it : items)
+    if (it.host) UPF_CUDA(cudaMemcpyAsync(it.snap, it.src, it.bytes, cudaMemcpyDeviceToDevice, st));
+  UPF_CUDA(cudaEventRecord(io.snapped, st));
+  UPF_CUDA(cudaStreamWaitEvent(io.down, io.snapped, 0));
+  for (const Item& it : items)
+    if (it.host) UPF_CUDA(cudaMemcpyAsync(it.host, it.snap, it.bytes, cudaMemcpyDeviceToHost, io.down));
+  UPF_CUDA(cudaEventRecord(io.read_done, io.down));
+  return UPF_OK;
+}
+
+upf_status upf_wait_frames(upf_system* s) {
+  if (!s) {
+    set_error("upf_wait_frames: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (!s->io.ready) return UPF_OK;
+  UPF_CUDA(cudaStreamWaitEvent(s->stream, s->io.read_done, 0));  // later work on the stream comes after
+  UPF_CUDA(cudaEventSynchronize(s->io.staged));
+  UPF_CUDA(cudaEventSynchronize(s->io.read_done));
   return UPF_OK;
 }
 
