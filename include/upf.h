@@ -537,6 +537,14 @@ upf_status upf_batch_restore(upf_batch* b, int32_t slot);
  * batch's current device order per scene. */
 upf_status upf_batch_upload_state(upf_batch* b, const float* pos4, const float* vel4);
 upf_status upf_batch_download_state(upf_batch* b, float* pos4, float* vel4);
+/* Asynchronous counterparts (no counterpart in the reference; the scheme of
+ * upf_upload_state_async): the copies overlap the batch's steps;
+ * upf_batch_wait_frames waits for the copies issued so far, and until then
+ * the host arrays may not be touched. Pinned host memory; staging buffers
+ * (64 bytes per particle) are allocated on the first call. */
+upf_status upf_batch_upload_state_async(upf_batch* b, const float* pos4, const float* vel4);
+upf_status upf_batch_download_state_async(upf_batch* b, float* pos4, float* vel4);
+upf_status upf_batch_wait_frames(upf_batch* b);
 /* One batch step through its passes with CUDA events (as upf_profile_step);
  * iterations = the largest scene's count; *active_particle_iterations (may be
  * NULL) = the sum over loop iterations of the particles of the scenes still

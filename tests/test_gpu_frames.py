@@ -103,3 +103,43 @@ def test_partial_readback_and_idle_wait(upf_lib):
         assert L.upf_wait_frames(s.handle) == 0
         assert cnt.value == n
         assert np.array_equal(pos.numpy(), s.particles()["pos"])
+
+
+def test_batch_pipelined_frames_equal_synchronous_frames(upf_lib):
+    """upf_batch_upload_state_async / upf_batch_download_state_async against
+    upf_batch_upload_state / upf_batch_download_state, four frames."""
+    torch = pytest.importorskip("torch")
+    L = upf_lib.lib()
+    fp = C.POINTER(C.c_float)
+    scs = scenes.batch_scenes(num=6, seed=21, counts=(2048, 6000))
+    frames = 4
+    inputs, want = [], []
+    with upf_lib.ParticleBatch.from_scenes(scs) as a:
+        a.step(1)
+        n = int(a.offsets[-1])
+        pos = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        upf_lib.check(L.upf_batch_download_state(a.handle, pos.ctypes.data_as(fp), vel.ctypes.data_as(fp)), "dl")
+        for k in range(frames):
+            vel = (vel * np.float32(0.99)).astype(np.float32)
+            inputs.append((pos.copy(), vel.copy()))
+            upf_lib.check(L.upf_batch_upload_state(a.handle, pos.ctypes.data_as(fp), vel.ctypes.data_as(fp)), "ul")
+            a.step(1)
+            upf_lib.check(L.upf_batch_download_state(a.handle, pos.ctypes.data_as(fp), vel.ctypes.data_as(fp)), "dl")
+            want.append((pos.copy(), vel.copy()))
+    with upf_lib.ParticleBatch.from_scenes(scs) as b:
+        b.step(1)
+        ins = [(torch.from_numpy(p).pin_memory(), torch.from_numpy(v).pin_memory()) for p, v in inputs]
+        outs = [(torch.zeros((n, 4), dtype=torch.float32, pin_memory=True),
+                 torch.zeros((n, 4), dtype=torch.float32, pin_memory=True)) for _ in range(frames)]
+        for k in range(frames):
+            upf_lib.check(L.upf_batch_upload_state_async(b.handle, _ptr(ins[k][0], C.c_float),
+                                                         _ptr(ins[k][1], C.c_float)), "ul async")
+            b.step(1)
+            upf_lib.check(L.upf_batch_download_state_async(b.handle, _ptr(outs[k][0], C.c_float),
+                                                           _ptr(outs[k][1], C.c_float)), "dl async")
+        upf_lib.check(L.upf_batch_wait_frames(b.handle), "upf_batch_wait_frames")
+        b.synchronize()
+    for k in range(frames):
+        assert np.array_equal(outs[k][0].numpy().view(np.uint32), want[k][0].view(np.uint32)), k
+        assert np.array_equal(outs[k][1].numpy().view(np.uint32), want[k][1].view(np.uint32)), k

@@ -772,13 +772,11 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   return UPF_OK;
 }
 
-static void frames_release(System& s);  // below, with the asynchronous frame exchange
-
 upf_status upf_destroy(upf_system* s) {
   if (!s) return UPF_OK;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
-  frames_release(*s);
+  frame_streams_destroy(s->io);  // its buffers are in s->allocations
   destroy_graph(*s);
   for (void* p : s->allocations) cudaFree(p);
   free_list(s->rigid_allocations);
@@ -1501,8 +1499,31 @@ upf_status upf_get_particles(upf_system* s, float* pos4, float* vel4, float* den
 // copy of the result in stream order and copies it to the host while the
 // next step runs. With one stream per direction, a readback never holds up
 // the next upload. Events order the buffers' reuse.
+}  // extern "C"
+
+cudaError_t upf::frame_streams_create(FrameIO& io, cudaStream_t compute) {
+  cudaError_t e = cudaStreamCreateWithFlags(&io.up, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&io.down, cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&io.staged, &io.consumed, &io.snapped, &io.read_done})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  for (cudaEvent_t ev : {io.staged, io.consumed, io.snapped, io.read_done})  // all four start completed
+    if (e == cudaSuccess) e = cudaEventRecord(ev, compute);
+  return e;
+}
+
+void upf::frame_streams_destroy(FrameIO& io) {
+  for (cudaStream_t c : {io.up, io.down})
+    if (c) cudaStreamSynchronize(c);
+  for (cudaEvent_t e : {io.staged, io.consumed, io.snapped, io.read_done})
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t c : {io.up, io.down})
+    if (c) cudaStreamDestroy(c);
+  io = FrameIO{};
+}
+
+namespace upf {
 static upf_status frames_ready(System& s) {
-  System::FrameIO& io = s.io;
+  FrameIO& io = s.io;
   if (io.ready) return UPF_OK;
   const uint32_t c = s.capacity;
   UPF_TRY(dalloc(s, &io.in_pos, c));
@@ -1513,26 +1534,14 @@ static upf_status frames_ready(System& s) {
   UPF_TRY(dalloc(s, &io.out_press, c));
   UPF_TRY(dalloc(s, &io.out_type, c));
   UPF_TRY(dalloc(s, &io.out_id, c));
-  UPF_CUDA(cudaStreamCreateWithFlags(&io.up, cudaStreamNonBlocking));
-  UPF_CUDA(cudaStreamCreateWithFlags(&io.down, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&io.staged, &io.consumed, &io.snapped, &io.read_done})
-    UPF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-  // all four start completed
-  for (cudaEvent_t e : {io.staged, io.consumed, io.snapped, io.read_done}) UPF_CUDA(cudaEventRecord(e, s.stream));
+  UPF_CUDA(frame_streams_create(io, s.stream));
   io.ready = true;
   return UPF_OK;
 }
 
-static void frames_release(System& s) {
-  System::FrameIO& io = s.io;
-  for (cudaStream_t c : {io.up, io.down})
-    if (c) cudaStreamSynchronize(c);
-  for (cudaEvent_t e : {io.staged, io.consumed, io.snapped, io.read_done})
-    if (e) cudaEventDestroy(e);
-  for (cudaStream_t c : {io.up, io.down})
-    if (c) cudaStreamDestroy(c);
-  io = System::FrameIO{};  // the buffers are in s.allocations
-}
+}  // namespace upf
+
+extern "C" {
 
 upf_status upf_upload_state_async(upf_system* s, const float* pos4, const float* vel4, uint32_t n) {
   UPF_TRY(phase_guard(s));
@@ -1542,7 +1551,7 @@ upf_status upf_upload_state_async(upf_system* s, const float* pos4, const float*
   }
   if (!n) return UPF_OK;
   UPF_TRY(frames_ready(*s));
-  System::FrameIO& io = s->io;
+  FrameIO& io = s->io;
   UPF_CUDA(cudaStreamWaitEvent(io.up, io.consumed, 0));  // the last upload has left the staging buffers
   UPF_CUDA(cudaMemcpyAsync(io.in_pos, pos4, sizeof(float4) * n, cudaMemcpyHostToDevice, io.up));
   UPF_CUDA(cudaMemcpyAsync(io.in_vel, vel4, sizeof(float4) * n, cudaMemcpyHostToDevice, io.up));
@@ -1562,7 +1571,7 @@ upf_status upf_get_particles_async(upf_system* s, float* pos4, float* vel4, floa
   if (n_out) *n_out = n;
   if (!n) return UPF_OK;
   UPF_TRY(frames_ready(*s));
-  System::FrameIO& io = s->io;
+  FrameIO& io = s->io;
   cudaStream_t st = s->stream;
   UPF_CUDA(cudaStreamWaitEvent(st, io.read_done, 0));  // the last readback has left the snapshot
   struct Item {

@@ -316,6 +316,7 @@ upf_status upf_batch_destroy(upf_batch* b) {
   if (!b) return UPF_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  frame_streams_destroy(b->io);  // its buffers are in b->allocations
   destroy_batch_graph(b);
   for (void* p : b->allocations) cudaFree(p);
   for (void* p : b->checkpoint_slots)
@@ -541,6 +542,83 @@ upf_status upf_batch_download_state(upf_batch* b, float* pos4, float* vel4) {
   UPF_CUDA(cudaMemcpyAsync(pos4, b->x.stage_a, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
   UPF_CUDA(cudaMemcpyAsync(vel4, b->x.stage_b, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
   UPF_CUDA(cudaStreamSynchronize(st));
+  return UPF_OK;
+}
+
+// Asynchronous counterparts of the per-frame upload and download (the
+// single-system scheme of upf_upload_state_async): the host copies run on
+// the batch's copy streams against staging buffers in the caller's
+// scene-concatenated order; the scatter into the batch's slots (and back)
+// runs in stream order on the compute stream.
+static upf_status batch_frames_ready(BatchSystem& b) {
+  FrameIO& io = b.io;
+  if (io.ready) return UPF_OK;
+  const size_t n = b.n_particles;
+  UPF_TRY(balloc(b, &io.in_pos, n));
+  UPF_TRY(balloc(b, &io.in_vel, n));
+  UPF_TRY(balloc(b, &io.out_pos, n));
+  UPF_TRY(balloc(b, &io.out_vel, n));
+  UPF_CUDA(frame_streams_create(io, b.stream));
+  io.ready = true;
+  return UPF_OK;
+}
+
+upf_status upf_batch_upload_state_async(upf_batch* b, const float* pos4, const float* vel4) {
+  UPF_TRY(batch_guard(b, "upf_batch_upload_state_async"));
+  if (b->n_particles && (!pos4 || !vel4)) {
+    set_error("upf_batch_upload_state_async: null argument");
+    return UPF_ERR_INVALID_ARG;
+  }
+  const size_t n = b->n_particles;
+  if (!n) return UPF_OK;
+  UPF_TRY(batch_frames_ready(*b));
+  FrameIO& io = b->io;
+  cudaStream_t st = b->stream;
+  UPF_CUDA(cudaStreamWaitEvent(io.up, io.consumed, 0));  // the last upload has left the staging buffers
+  UPF_CUDA(cudaMemcpyAsync(io.in_pos, pos4, sizeof(float4) * n, cudaMemcpyHostToDevice, io.up));
+  UPF_CUDA(cudaMemcpyAsync(io.in_vel, vel4, sizeof(float4) * n, cudaMemcpyHostToDevice, io.up));
+  UPF_CUDA(cudaEventRecord(io.staged, io.up));
+  UPF_CUDA(cudaStreamWaitEvent(st, io.staged, 0));
+  k_batch_scatter<<<(b->n_slots + 255) / 256, 256, 0, st>>>(b->view, b->seg_begin_d, b->x.comp_begin_d, b->n_slots,
+                                                            io.in_pos, io.in_vel, b->A.pos, b->A.vel, 1);
+  UPF_CUDA(cudaGetLastError());
+  UPF_CUDA(batch_launch_keys(*b, st));
+  UPF_CUDA(cudaEventRecord(io.consumed, st));
+  return UPF_OK;
+}
+
+upf_status upf_batch_download_state_async(upf_batch* b, float* pos4, float* vel4) {
+  UPF_TRY(batch_guard(b, "upf_batch_download_state_async"));
+  if (b->n_particles && (!pos4 || !vel4)) {
+    set_error("upf_batch_download_state_async: null argument");
+    return UPF_ERR_INVALID_ARG;
+  }
+  const size_t n = b->n_particles;
+  if (!n) return UPF_OK;
+  UPF_TRY(batch_frames_ready(*b));
+  FrameIO& io = b->io;
+  cudaStream_t st = b->stream;
+  UPF_CUDA(cudaStreamWaitEvent(st, io.read_done, 0));  // the last download has left the snapshot
+  k_batch_scatter<<<(b->n_slots + 255) / 256, 256, 0, st>>>(b->view, b->seg_begin_d, b->x.comp_begin_d, b->n_slots,
+                                                            b->A.pos, b->A.vel, io.out_pos, io.out_vel, 0);
+  UPF_CUDA(cudaGetLastError());
+  UPF_CUDA(cudaEventRecord(io.snapped, st));
+  UPF_CUDA(cudaStreamWaitEvent(io.down, io.snapped, 0));
+  UPF_CUDA(cudaMemcpyAsync(pos4, io.out_pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, io.down));
+  UPF_CUDA(cudaMemcpyAsync(vel4, io.out_vel, sizeof(float4) * n, cudaMemcpyDeviceToHost, io.down));
+  UPF_CUDA(cudaEventRecord(io.read_done, io.down));
+  return UPF_OK;
+}
+
+upf_status upf_batch_wait_frames(upf_batch* b) {
+  if (!b) {
+    set_error("upf_batch_wait_frames: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (!b->io.ready) return UPF_OK;
+  UPF_CUDA(cudaStreamWaitEvent(b->stream, b->io.read_done, 0));
+  UPF_CUDA(cudaEventSynchronize(b->io.staged));
+  UPF_CUDA(cudaEventSynchronize(b->io.read_done));
   return UPF_OK;
 }
 

@@ -93,6 +93,31 @@ struct BatchView {
   const uint32_t* cell_base = nullptr;   // [scenes] offset of the scene's cell table
 };
 
+// Asynchronous per-frame exchange of a system or a batch: host copies run on
+// `up` (host to device) and `down` (device to host) against device staging
+// buffers, so that they overlap the steps on the compute stream and each
+// other. Created on first use.
+struct FrameIO {
+  cudaStream_t up = nullptr;
+  cudaStream_t down = nullptr;
+  cudaEvent_t staged = nullptr;     // upload copied into in_*
+  cudaEvent_t consumed = nullptr;   // in_* entered into the state
+  cudaEvent_t snapped = nullptr;    // result copied into out_*
+  cudaEvent_t read_done = nullptr;  // out_* copied to the host
+  float4* in_pos = nullptr;
+  float4* in_vel = nullptr;
+  float4* out_pos = nullptr;
+  float4* out_vel = nullptr;
+  float* out_rho = nullptr;
+  float* out_press = nullptr;
+  int32_t* out_type = nullptr;
+  uint32_t* out_id = nullptr;
+  bool ready = false;
+};
+// streams and events, all four events recorded once on `compute` (upf_api.cu)
+cudaError_t frame_streams_create(FrameIO& io, cudaStream_t compute);
+void frame_streams_destroy(FrameIO& io);  // waits for the copies; buffers stay with their owner
+
 struct System {
   upf_params prm{};
   DevParams dp{};
@@ -163,27 +188,7 @@ struct System {
   std::vector<void*> checkpoint_slots;  // device copies of the dynamic state (upf_checkpoint);
                                         // dropped when particles or bodies are set
 
-  // asynchronous per-frame exchange (upf_upload_state_async,
-  // upf_get_particles_async): host copies run on `up` (host to device) and
-  // `down` (device to host) against staging buffers, so that they overlap
-  // the steps on `stream` and each other; created on first use
-  struct FrameIO {
-    cudaStream_t up = nullptr;
-    cudaStream_t down = nullptr;
-    cudaEvent_t staged = nullptr;     // upload copied into in_*
-    cudaEvent_t consumed = nullptr;   // in_* entered into the state
-    cudaEvent_t snapped = nullptr;    // result copied into out_*
-    cudaEvent_t read_done = nullptr;  // out_* copied to the host
-    float4* in_pos = nullptr;
-    float4* in_vel = nullptr;
-    float4* out_pos = nullptr;
-    float4* out_vel = nullptr;
-    float* out_rho = nullptr;
-    float* out_press = nullptr;
-    int32_t* out_type = nullptr;
-    uint32_t* out_id = nullptr;
-    bool ready = false;
-  } io;
+  FrameIO io;  // asynchronous per-frame exchange (upf_upload_state_async, ...)
 };
 
 // The state behind one upf_batch handle: every array spans the batch's slot
@@ -234,6 +239,7 @@ struct BatchSystem {
 
   cudaGraphExec_t step_exec = nullptr;
   cudaGraph_t step_graph = nullptr;
+  FrameIO io;  // asynchronous per-frame exchange (upf_batch_upload_state_async, ...)
   std::vector<void*> allocations;
   std::vector<void*> checkpoint_slots;
 };
