@@ -387,6 +387,28 @@ upf_status upf_obj_read_triangles(const char* path, float* tri9, uint32_t capaci
 upf_status upf_mesh_particles(int device, const float* tri9, uint32_t n_tri, float scale_x, float scale_y,
                               float scale_z, float spacing, float* pos4, uint32_t capacity, uint32_t* n_out);
 
+/* Scene::createFluidObject (src/sceneConfigure/Scene.cpp:597-646) on GPU
+ * `device`: a lattice block filling [box_min, box_max) at `spacing`, in the
+ * reference's order (y, then x, then z) and bit for bit its positions
+ * (jitter + i * spacing, shifted by -0.5 * jitter and by offset in double:
+ * the reference's drand48() macro is an integer division that gives 0).
+ * pos4 NULL: *n_out = the count only. */
+upf_status upf_scene_fluid_block(int device, const float box_min[3], const float box_max[3], float spacing,
+                                 float jitter, const float offset[3], float* pos4, uint32_t capacity,
+                                 uint32_t* n_out);
+/* Scene::createBoxBoundaryFrozenParticles (layers = 1, Scene.cpp:890-1043)
+ * and ...MultiLayers (layers = 2, Scene.cpp:1045-1212; 1..8 allowed) on GPU
+ * `device`: wall particles around the container (widened by
+ * distance_frozen_to_boundary on each side), placed from zindex_start +
+ * (support_radius - distance_frozen_to_boundary), with each wall's inward
+ * normal in normal4, in the reference's order and bit for bit its
+ * positions. A particle at or below zindex_start in some coordinate is an
+ * error (the reference aborts). pos4 NULL: *n_out = the count only. */
+upf_status upf_scene_box_boundary(int device, const float container_min[3], const float container_max[3],
+                                  const float zindex_start[3], float spacing, float support_radius,
+                                  float distance_frozen_to_boundary, int32_t layers, float* pos4, float* normal4,
+                                  uint32_t capacity, uint32_t* n_out);
+
 /* Per-phase device timings of one step (the reference's SPH_PROFILING_VERBOSE
  * per-phase event timers, src/gpu/particles.cu:1460-1690). Runs one full
  * step through the phase entry points with CUDA events around each phase,

@@ -338,3 +338,39 @@ def ref_obj_particles(path: str, scale, spacing: float) -> np.ndarray:
         if n <= cap:
             return buf[:n].copy()
         cap = n
+
+
+# ---------------------------------------------------------------- scene generators (restated)
+def scene_fluid_block(box_min, box_max, spacing, jitter, offset) -> np.ndarray:
+    """Scene::createFluidObject restated (oracle/scene_oracle.cpp): n x 4."""
+    L = lib()
+    f3 = lambda v: np.ascontiguousarray(v, np.float32)  # noqa: E731
+    a, b, o = f3(box_min), f3(box_max), f3(offset)
+    L.orc_scene_fluid_block.restype = C.c_int64
+    L.orc_scene_fluid_block.argtypes = [C.POINTER(C.c_float)] * 2 + [C.c_float, C.c_float, C.POINTER(C.c_float),
+                                                                     C.POINTER(C.c_float), C.c_int64]
+    n = L.orc_scene_fluid_block(_ptr(a, C.c_float), _ptr(b, C.c_float), spacing, jitter, _ptr(o, C.c_float), None, 0)
+    out = np.zeros((max(n, 0), 4), np.float32)
+    L.orc_scene_fluid_block(_ptr(a, C.c_float), _ptr(b, C.c_float), spacing, jitter, _ptr(o, C.c_float),
+                            _ptr(out, C.c_float), n)
+    return out
+
+
+def scene_box_boundary(cmin, cmax, zstart, spacing, support_radius, dist_frozen, layers):
+    """Scene::createBoxBoundaryFrozenParticles(MultiLayers) restated: (pos n x 4,
+    normals n x 4), or None where the reference aborts."""
+    L = lib()
+    f3 = lambda v: np.ascontiguousarray(v, np.float32)  # noqa: E731
+    a, b, z = f3(cmin), f3(cmax), f3(zstart)
+    fp = C.POINTER(C.c_float)
+    L.orc_scene_box_boundary.restype = C.c_int64
+    L.orc_scene_box_boundary.argtypes = [fp, fp, fp, C.c_float, C.c_float, C.c_float, C.c_int, fp, fp, C.c_int64]
+    n = L.orc_scene_box_boundary(_ptr(a, C.c_float), _ptr(b, C.c_float), _ptr(z, C.c_float), spacing,
+                                 support_radius, dist_frozen, layers, None, None, 0)
+    if n < 0:
+        return None
+    pos = np.zeros((n, 4), np.float32)
+    nrm = np.zeros((n, 4), np.float32)
+    L.orc_scene_box_boundary(_ptr(a, C.c_float), _ptr(b, C.c_float), _ptr(z, C.c_float), spacing, support_radius,
+                             dist_frozen, layers, _ptr(pos, C.c_float), _ptr(nrm, C.c_float), n)
+    return pos, nrm

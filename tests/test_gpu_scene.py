@@ -65,3 +65,44 @@ def test_injected_allocation_failure_is_reported(upf_lib, tmp_path):
     finally:
         L.upf_test_fail_allocation(-1)
     assert len(upf_lib.mesh_particles(tri, 0.015, (1.5, 2.0, 1.0))) == len(GOLD["torus_pos"])
+
+
+FLUID_CASES = [
+    ((0.0, 0.0, 0.0), (0.13, 0.1, 0.07), 0.01, 0.0, (0.04, 0.035, 0.04)),
+    ((-0.5, 0.2, -0.1), (-0.41, 0.27, 0.0), 0.0125, 0.003, (0.1, -0.2, 0.3)),
+    ((0.02, 0.02, 0.02), (1.30, 1.30, 0.66), 0.01, 0.001, (0.03, 0.025, 0.03)),  # 128 x 128 x 64
+]
+
+
+@pytest.mark.parametrize("case", range(len(FLUID_CASES)))
+def test_fluid_block_matches_the_restated_reference(upf_lib, case):
+    from oracle import pyoracle
+    args = FLUID_CASES[case]
+    got = upf_lib.scene_fluid_block(*args)
+    want = pyoracle.scene_fluid_block(*args)
+    assert got.shape == want.shape and len(got) > 0
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("layers", [1, 2, 3])
+@pytest.mark.parametrize("h", [0.02, 0.04])
+def test_box_boundary_matches_the_restated_reference(upf_lib, layers, h):
+    from oracle import pyoracle
+    args = ((0.0, 0.0, 0.0), (2.0, 1.3, 1.3), (-0.05, -0.05, -0.05), 0.01, h, 0.005)
+    want = pyoracle.scene_box_boundary(*args, layers)
+    if want is None:  # an inner layer reaches the z-index origin: the reference aborts
+        with pytest.raises(UpfError) as e:
+            upf_lib.scene_box_boundary(*args, layers=layers)
+        assert e.value.status == CODE["UPF_ERR_INVALID_ARG"]
+        return
+    wpos, wnrm = want
+    pos, nrm = upf_lib.scene_box_boundary(*args, layers=layers)
+    assert pos.shape == wpos.shape
+    assert np.array_equal(pos.view(np.uint32), wpos.view(np.uint32))
+    assert np.array_equal(nrm, wnrm)
+
+
+def test_box_boundary_refuses_walls_at_the_origin(upf_lib):
+    with pytest.raises(UpfError) as e:
+        upf_lib.scene_box_boundary((0.0, 0.0, 0.0), (0.3, 0.2, 0.25), (0.0, 0.0, 0.0), 0.01, 0.005, 0.005, 1)
+    assert e.value.status == CODE["UPF_ERR_INVALID_ARG"] and "origin" in str(e.value)

@@ -59,6 +59,37 @@ def test_every_shape_gives_identical_results(upf_lib):
             assert np.array_equal(got[f], ref[f]), (cfg.as_dict(), f)
 
 
+@pytest.mark.parametrize("scene", ["small_pcisph", "small_coupling"])
+def test_every_list_mode_builds_the_same_lists(upf_lib, scene):
+    """Neighbour lists (ids, order, counts) of both list-building modes and
+    every CTA size equal those of the default shape; the scenes have boundary
+    particles, so cells with both sets (merged by key) are covered too."""
+    sc = getattr(scenes, scene)()
+    p = upf_lib.derive_params(sc.params)
+
+    def lists(nl, mode):
+        with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
+            s.set_particles(sc.pos, sc.vel, sc.type)
+            if getattr(sc, "num_bodies", 0):
+                s.set_rigid_bodies(sc.body, sc.num_bodies)
+            if nl:
+                c = s.launch_config()
+                c.nlist_threads, c.nlist_mode = nl, mode
+                s.set_launch_config(c)
+            s.phase("sort")
+            s.phase("neighbors")
+            return s.neighbors()
+
+    ref_cnt, ref_lists = lists(0, 0)
+    assert ref_cnt.max() > 0
+    for nl in (64, 128, 256):
+        for mode in (0, 1):
+            cnt, lst = lists(nl, mode)
+            assert np.array_equal(cnt, ref_cnt), (nl, mode)
+            for i in np.flatnonzero(cnt):
+                assert np.array_equal(lst[i, :cnt[i]], ref_lists[i, :cnt[i]]), (nl, mode, i)
+
+
 def test_autotune_keeps_state_and_picks_a_valid_shape(upf_lib):
     sc = scenes.small_pcisph()
     ref, _, _ = run(upf_lib, sc, None)
@@ -106,6 +137,10 @@ def test_invalid_shapes_rejected(upf_lib):
                     shape(256, 256, (256, 8), (2, 256, 8))):
             with pytest.raises(UpfError):
                 s.set_launch_config(bad)
+        bad = shape(256, 256, (256, 8), (256, 8))
+        bad.nlist_mode = 2
+        with pytest.raises(UpfError):
+            s.set_launch_config(bad)
     scs = scenes.batch_scenes(num=2, seed=3, counts=(2048, 4096))
     with upf_lib.ParticleBatch.from_scenes(scs) as b:
         with pytest.raises(UpfError):

@@ -101,3 +101,55 @@ def test_reference_voxeliser_reproduces_the_fixture(upf_lib, tmp_path):
         path = tmp_path / (name + ".obj")
         scenes.write_obj(path, tri)
         assert np.array_equal(pyoracle.ref_obj_particles(str(path), scale, spacing), gold[name + "_pos"]), name
+
+
+# ---------------------------------------------------------------- scene generators
+# The reference's Scene.cpp does not compile here, so the generators are
+# restated in the oracle (oracle/scene_oracle.cpp); the restatement is
+# checked here against an independent numpy reading of the same loops, and
+# the device generators against the restatement (tests/test_gpu_scene.py).
+
+def _numpy_fluid_block(box_min, box_max, spacing, jitter, offset):
+    f = np.float32
+    box_min, box_max, offset = (np.asarray(v, f) for v in (box_min, box_max, offset))
+    num = [int(f(f(box_max[a] - box_min[a]) / f(spacing))) for a in range(3)]
+    out = []
+    for iy in range(num[1]):
+        y = f(f(jitter) + f(f(iy) * f(spacing)))
+        for ix in range(num[0]):
+            x = f(f(jitter) + f(f(ix) * f(spacing)))
+            for iz in range(num[2]):
+                z = f(f(jitter) + f(f(iz) * f(spacing)))
+                sh = -0.5 * float(f(jitter))
+                out.append([f(float(c) + sh + float(o)) for c, o in zip((x, y, z), offset)] + [0.0])
+    return np.array(out, f).reshape(-1, 4)
+
+
+def test_fluid_block_restatement(upf_lib):
+    from oracle import pyoracle
+    for args in [((0.0, 0.0, 0.0), (0.13, 0.1, 0.07), 0.01, 0.0, (0.04, 0.035, 0.04)),
+                 ((-0.5, 0.2, -0.1), (-0.41, 0.27, 0.0), 0.0125, 0.003, (0.1, -0.2, 0.3))]:
+        got = pyoracle.scene_fluid_block(*args)
+        want = _numpy_fluid_block(*args)
+        assert got.shape == want.shape and np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_box_boundary_restatement_counts_and_order(upf_lib):
+    from oracle import pyoracle
+    cmin, cmax, zs = (0.0, 0.0, 0.0), (0.3, 0.2, 0.25), (-0.06, -0.06, -0.06)
+    sp, h, d = 0.01, 0.04, 0.005
+    for layers in (1, 2, 3):
+        pos, nrm = pyoracle.scene_box_boundary(cmin, cmax, zs, sp, h, d, layers)
+        num = [int(np.float32(np.float32(np.float32(cmax[a]) + np.float32(d)) -
+                              np.float32(np.float32(cmin[a]) - np.float32(d))) / np.float32(sp)) for a in range(3)]
+        nx, ny, nz = num
+        assert len(pos) == 2 * layers * ((nx + 2) * (nz + 2) + (nx + 2) * ny + ny * nz)
+        # the first pair: ground then ceiling at the first lattice column
+        assert nrm[0, 1] == 1 and nrm[1, 1] == -1 and pos[0, 0] == pos[1, 0] and pos[0, 2] == pos[1, 2]
+        f = np.float32
+        base = f(f(zs[0]) + f(f(h) - f(d)))
+        assert pos[0, 0] == base and pos[0, 1] == f(f(zs[1]) + f(f(h) - f(d)))
+        # every normal points into the box along one axis
+        assert np.all(np.abs(nrm[:, :3]).sum(1) == 1)
+    # a wall at the z-index origin: where the reference aborts
+    assert pyoracle.scene_box_boundary(cmin, cmax, (0.0, 0.0, 0.0), sp, 0.005, 0.005, 1) is None

@@ -128,6 +128,9 @@ def lib():
             "upf_io_read_fluid_particles_pcisph": [C.c_char_p, fp, fp, i32p, fp, fp, C.c_int32, i32p],
             "upf_io_read_scene_particles": [C.c_char_p, fp, fp, fp, i32p, C.c_uint32, u32p],
             "upf_obj_read_triangles": [C.c_char_p, fp, C.c_uint32, u32p],
+            "upf_scene_fluid_block": [C.c_int, fp, fp, C.c_float, C.c_float, fp, fp, C.c_uint32, u32p],
+            "upf_scene_box_boundary": [C.c_int, fp, fp, fp, C.c_float, C.c_float, C.c_float, C.c_int32, fp, fp,
+                                       C.c_uint32, u32p],
             "upf_mesh_particles": [C.c_int, fp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, fp,
                                    C.c_uint32, u32p],
         }
@@ -194,6 +197,39 @@ def obj_triangles(path) -> np.ndarray:
     out = np.zeros((n.value, 9), np.float32)
     check(lib().upf_obj_read_triangles(fs, _p(out, C.c_float), n.value, C.byref(n)), "upf_obj_read_triangles")
     return out
+
+
+def _f3(v):
+    return np.ascontiguousarray(v, np.float32).reshape(3)
+
+
+def scene_fluid_block(box_min, box_max, spacing: float, jitter: float = 0.0, offset=(0.0, 0.0, 0.0),
+                      device: int = 0) -> np.ndarray:
+    """The reference's Scene::createFluidObject lattice on the GPU
+    (upf_scene_fluid_block), n x 4."""
+    a, b, o = _f3(box_min), _f3(box_max), _f3(offset)
+    n = C.c_uint32()
+    args = (device, _p(a, C.c_float), _p(b, C.c_float), float(spacing), float(jitter), _p(o, C.c_float))
+    check(lib().upf_scene_fluid_block(*args, None, 0, C.byref(n)), "upf_scene_fluid_block")
+    out = np.zeros((n.value, 4), np.float32)
+    check(lib().upf_scene_fluid_block(*args, _p(out, C.c_float), n.value, C.byref(n)), "upf_scene_fluid_block")
+    return out
+
+
+def scene_box_boundary(container_min, container_max, zindex_start, spacing: float, support_radius: float,
+                       distance_frozen_to_boundary: float, layers: int = 2, device: int = 0):
+    """The reference's Scene::createBoxBoundaryFrozenParticles(MultiLayers)
+    walls on the GPU (upf_scene_box_boundary): (positions n x 4, normals n x 4)."""
+    a, b, z = _f3(container_min), _f3(container_max), _f3(zindex_start)
+    n = C.c_uint32()
+    args = (device, _p(a, C.c_float), _p(b, C.c_float), _p(z, C.c_float), float(spacing), float(support_radius),
+            float(distance_frozen_to_boundary), int(layers))
+    check(lib().upf_scene_box_boundary(*args, None, None, 0, C.byref(n)), "upf_scene_box_boundary")
+    pos = np.zeros((n.value, 4), np.float32)
+    nrm = np.zeros((n.value, 4), np.float32)
+    check(lib().upf_scene_box_boundary(*args, _p(pos, C.c_float), _p(nrm, C.c_float), n.value, C.byref(n)),
+          "upf_scene_box_boundary")
+    return pos, nrm
 
 
 def mesh_particles(tri9, spacing: float, scale=(1.0, 1.0, 1.0), device: int = 0) -> np.ndarray:

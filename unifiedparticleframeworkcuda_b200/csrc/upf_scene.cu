@@ -563,3 +563,236 @@ upf_status upf_obj_read_triangles(const char* path, float* tri9, uint32_t capaci
     for (int a = 0; a < 3; ++a) tri9[3 * k + a] = verts[3 * (size_t)(corners[k] - 1) + a];
   return UPF_OK;
 }
+
+// ---------------------------------------------------------------- lattice fluid and box walls
+namespace upf {
+namespace {
+
+struct FluidBlock {
+  int nx, ny, nz;
+  float spacing, jitter;
+  double off[3];
+};
+
+// Scene::createFluidObject (Scene.cpp:597-646), particle k of the iy, ix, iz
+// loops: x = jitter + ix * spacing in float, then x + (drand48() - 0.5) *
+// jitter + offset in double, stored as float; the reference's drand48() is
+// the macro rand() / RAND_MAX (global.h:12), integer division: 0.
+__global__ void k_fluid_block(const FluidBlock B, uint64_t n, float4* __restrict__ out) {
+  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int iz = (int)(k % (uint64_t)B.nz);
+  const uint64_t q = k / (uint64_t)B.nz;
+  const int ix = (int)(q % (uint64_t)B.nx);
+  const int iy = (int)(q / (uint64_t)B.nx);
+  const double shift = __dmul_rn(-0.5, (double)B.jitter);
+  const float f[3] = {fa(B.jitter, fm((float)ix, B.spacing)), fa(B.jitter, fm((float)iy, B.spacing)),
+                      fa(B.jitter, fm((float)iz, B.spacing))};
+  float p[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) p[a] = __double2float_rn(__dadd_rn(__dadd_rn((double)f[a], shift), B.off[a]));
+  out[k] = make_float4(p[0], p[1], p[2], 0.0f);
+}
+
+struct BoxWalls {
+  int nx, ny, nz, layers;
+  float spacing, distance;
+  float delta[3];
+  float start[3];
+  uint64_t s1, s2, s3;  // particles of the xz, xy and yz plane pairs
+};
+
+// Scene::createBoxBoundaryFrozenParticlesMultiLayers (Scene.cpp:1045-1212;
+// one layer: createBoxBoundaryFrozenParticles, 890-1043): particle k of the
+// reference's three loop nests, ground/ceiling, back/front, left/right,
+// each nest emitting the pair's two particles in turn. A particle not
+// strictly above the z-index origin in every coordinate sets *bad (where
+// the reference aborts).
+__global__ void k_box_walls(const BoxWalls W, float4* __restrict__ pos, float4* __restrict__ nrm,
+                            int* __restrict__ bad) {
+  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= W.s1 + W.s2 + W.s3) return;
+  const int g = (int)(k & 1u);  // first or second wall of the pair
+  const uint64_t t = k >> 1;
+  const int L = W.layers;
+  const float sp = W.spacing;
+  const float bx = fa(W.start[0], W.distance), by = fa(W.start[1], W.distance), bz = fa(W.start[2], W.distance);
+  float p[3], n[3] = {0.0f, 0.0f, 0.0f};
+  if (k < W.s1) {
+    const int y = (int)(t % L);
+    const uint64_t r = t / L;
+    const int z = (int)(r % (uint64_t)(W.nz + 2));
+    const int x = (int)(r / (uint64_t)(W.nz + 2));
+    p[0] = fa(bx, fm((float)x, sp));
+    p[1] = g == 0 ? fs(by, fm((float)y, sp)) : fa(fa(by, W.delta[1]), fm((float)y, sp));
+    p[2] = fa(bz, fm((float)z, sp));
+    n[1] = g == 0 ? 1.0f : -1.0f;
+  } else if (k < W.s1 + W.s2) {
+    const uint64_t u = t - (W.s1 >> 1);
+    const int zl = (int)(u % L);
+    const uint64_t r = u / L;
+    const int y = 1 + (int)(r % (uint64_t)W.ny);
+    const int x = (int)(r / (uint64_t)W.ny);
+    p[0] = fa(bx, fm((float)x, sp));
+    p[1] = fa(by, fm((float)y, sp));
+    p[2] = g == 0 ? fs(bz, fm((float)zl, sp)) : fa(fa(bz, W.delta[2]), fm((float)zl, sp));
+    n[2] = g == 0 ? 1.0f : -1.0f;
+  } else {
+    const uint64_t u = t - ((W.s1 + W.s2) >> 1);
+    const int xl = (int)(u % L);
+    const uint64_t r = u / L;
+    const int z = 1 + (int)(r % (uint64_t)W.nz);
+    const int y = 1 + (int)(r / (uint64_t)W.nz);
+    p[0] = g == 0 ? fs(bx, fm((float)xl, sp)) : fa(fa(bx, W.delta[0]), fm((float)xl, sp));
+    p[1] = fa(by, fm((float)y, sp));
+    p[2] = fa(bz, fm((float)z, sp));
+    n[0] = g == 0 ? 1.0f : -1.0f;
+  }
+  pos[k] = make_float4(p[0], p[1], p[2], 0.0f);
+  nrm[k] = make_float4(n[0], n[1], n[2], 0.0f);
+  if (!(fs(p[0], W.start[0]) > 0.0f && fs(p[1], W.start[1]) > 0.0f && fs(p[2], W.start[2]) > 0.0f)) *bad = 1;
+}
+
+// runs `launch` on a fresh stream of `device`, with its outputs in device
+// buffers copied to the host arrays
+upf_status generate(const char* who, int device, uint64_t n, float* pos4, float* nrm4,
+                    cudaError_t (*launch)(const void* args, uint64_t n, float4* pos, float4* nrm, int* bad,
+                                          cudaStream_t st),
+                    const void* args, bool* bad_out) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("%s: no CUDA device", who);
+    return UPF_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error("%s: bad device %d", who, device);
+    return UPF_ERR_INVALID_ARG;
+  }
+  cudaError_t e = cudaSetDevice(device);
+  cudaStream_t st = nullptr;
+  float4 *d_pos = nullptr, *d_nrm = nullptr;
+  int* d_bad = nullptr;
+  int bad = 0;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = dmalloc(&d_pos, n);
+  if (e == cudaSuccess && nrm4) e = dmalloc(&d_nrm, n);
+  if (e == cudaSuccess) e = dmalloc(&d_bad, 1);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = launch(args, n, d_pos, d_nrm, d_bad, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pos4, d_pos, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && nrm4) e = cudaMemcpyAsync(nrm4, d_nrm, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (st) cudaStreamSynchronize(st);
+  cudaFree(d_pos);
+  cudaFree(d_nrm);
+  cudaFree(d_bad);
+  if (st) cudaStreamDestroy(st);
+  if (e != cudaSuccess) {
+    if (e != cudaErrorMemoryAllocation || !std::strstr(upf_last_error(), "injected"))
+      set_error("%s: %s", who, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? UPF_ERR_ALLOC : UPF_ERR_CUDA;
+  }
+  if (bad_out) *bad_out = bad != 0;
+  return UPF_OK;
+}
+
+}  // namespace
+}  // namespace upf
+
+upf_status upf_scene_fluid_block(int device, const float box_min[3], const float box_max[3], float spacing,
+                                 float jitter, const float offset[3], float* pos4, uint32_t capacity,
+                                 uint32_t* n_out) {
+  const char* who = "upf_scene_fluid_block";
+  if (!box_min || !box_max || !offset || !n_out || !(spacing > 0.0f) || (capacity > 0 && !pos4)) {
+    set_error("%s: bad arguments", who);
+    return UPF_ERR_INVALID_ARG;
+  }
+  FluidBlock B{};
+  int64_t num[3];
+  for (int a = 0; a < 3; ++a) {
+    const float q = (box_max[a] - box_min[a]) / spacing;
+    if (!(q < 2147483647.0f)) {
+      set_error("%s: box / spacing too large", who);
+      return UPF_ERR_INVALID_ARG;
+    }
+    num[a] = q > 0.0f ? (int64_t)(int)q : 0;  // Vector3i(delta / Vector3f(spacing)); no particles below 1
+    B.off[a] = (double)offset[a];
+  }
+  B.nx = (int)num[0], B.ny = (int)num[1], B.nz = (int)num[2];
+  B.spacing = spacing;
+  B.jitter = jitter;
+  const uint64_t n = (uint64_t)num[0] * (uint64_t)num[1] * (uint64_t)num[2];
+  if (n > 0xffffffffu) {
+    set_error("%s: %llu particles exceed 2^32 - 1", who, (unsigned long long)n);
+    return UPF_ERR_INVALID_ARG;
+  }
+  *n_out = (uint32_t)n;
+  if (!pos4 || n == 0) return UPF_OK;
+  if (n > capacity) {
+    set_error("%s: the block holds %llu particles, capacity is %u", who, (unsigned long long)n, capacity);
+    return UPF_ERR_INVALID_ARG;
+  }
+  auto launch = [](const void* a, uint64_t n, float4* pos, float4*, int*, cudaStream_t st) {
+    k_fluid_block<<<(uint32_t)((n + 255) / 256), 256, 0, st>>>(*static_cast<const FluidBlock*>(a), n, pos);
+    return cudaGetLastError();
+  };
+  return generate(who, device, n, pos4, nullptr, launch, &B, nullptr);
+}
+
+upf_status upf_scene_box_boundary(int device, const float container_min[3], const float container_max[3],
+                                  const float zindex_start[3], float spacing, float support_radius,
+                                  float distance_frozen_to_boundary, int32_t layers, float* pos4, float* normal4,
+                                  uint32_t capacity, uint32_t* n_out) {
+  const char* who = "upf_scene_box_boundary";
+  if (!container_min || !container_max || !zindex_start || !n_out || !(spacing > 0.0f) || layers < 1 ||
+      layers > 8 || (capacity > 0 && (!pos4 || !normal4))) {
+    set_error("%s: bad arguments (layers 1..8)", who);
+    return UPF_ERR_INVALID_ARG;
+  }
+  BoxWalls W{};
+  int64_t num[3];
+  for (int a = 0; a < 3; ++a) {
+    const float mn = container_min[a] - distance_frozen_to_boundary;
+    const float mx = container_max[a] + distance_frozen_to_boundary;
+    W.delta[a] = mx - mn;
+    const float q = W.delta[a] / spacing;
+    if (!(q < 2147483647.0f) || !(q >= 0.0f)) {
+      set_error("%s: container / spacing out of range", who);
+      return UPF_ERR_INVALID_ARG;
+    }
+    num[a] = (int64_t)(int)q;
+    W.start[a] = zindex_start[a];
+  }
+  W.nx = (int)num[0], W.ny = (int)num[1], W.nz = (int)num[2], W.layers = layers;
+  W.spacing = spacing;
+  W.distance = support_radius - distance_frozen_to_boundary;
+  const uint64_t L2 = 2 * (uint64_t)layers;
+  W.s1 = L2 * (uint64_t)(num[0] + 2) * (uint64_t)(num[2] + 2);
+  W.s2 = L2 * (uint64_t)(num[0] + 2) * (uint64_t)num[1];
+  W.s3 = L2 * (uint64_t)num[1] * (uint64_t)num[2];
+  const uint64_t n = W.s1 + W.s2 + W.s3;
+  if (n > 0xffffffffu) {
+    set_error("%s: %llu particles exceed 2^32 - 1", who, (unsigned long long)n);
+    return UPF_ERR_INVALID_ARG;
+  }
+  *n_out = (uint32_t)n;
+  if (!pos4 || n == 0) return UPF_OK;
+  if (n > capacity) {
+    set_error("%s: the walls hold %llu particles, capacity is %u", who, (unsigned long long)n, capacity);
+    return UPF_ERR_INVALID_ARG;
+  }
+  auto launch = [](const void* a, uint64_t n, float4* pos, float4* nrm, int* bad, cudaStream_t st) {
+    k_box_walls<<<(uint32_t)((n + 255) / 256), 256, 0, st>>>(*static_cast<const BoxWalls*>(a), pos, nrm, bad);
+    return cudaGetLastError();
+  };
+  bool bad = false;
+  upf_status s = generate(who, device, n, pos4, normal4, launch, &W, &bad);
+  if (s == UPF_OK && bad) {
+    set_error("%s: a wall particle lies at or below the z-index origin (the reference aborts here); move "
+              "zindex_start below the container by more than support_radius", who);
+    return UPF_ERR_INVALID_ARG;
+  }
+  return s;
+}
