@@ -118,6 +118,44 @@ def _compare_step(sysm, o, method):
     return out
 
 
+FLAG_SETS = {
+    "none": 0,
+    "surface_tension": "FLAG_SURFACE_TENSION",
+    "adhesion": "FLAG_ADHESION",
+    "wall_weight": "FLAG_WALL_WEIGHT",
+    "penalty_walls": "FLAG_PENALTY_WALLS",
+    "all": ("FLAG_SURFACE_TENSION", "FLAG_ADHESION", "FLAG_WALL_WEIGHT", "FLAG_PENALTY_WALLS",
+            "FLAG_BOUNDARY_PRESSURE"),
+}
+
+
+@pytest.mark.parametrize("method", ["pcisph", "wcsph"])
+@pytest.mark.parametrize("flags", sorted(FLAG_SETS))
+def test_single_step_parity_per_optional_term(upf_lib, oracle_lib, method, flags):
+    """The optional force and density terms (UPF_FLAG_*; the reference's GPU
+    path switches several on where its CPU path does not) one at a time and
+    all together, one step against the oracle, within 1e-5."""
+    import unifiedparticleframeworkcuda_b200 as upf
+    sc = scenes.small_pcisph() if method == "pcisph" else scenes.small_wcsph()
+    spec = FLAG_SETS[flags]
+    names = (spec,) if isinstance(spec, str) else (spec or ())
+    value = 0
+    for name in names:
+        value |= getattr(upf, name)
+    sc.params.flags = value
+    p, sysm, o = make(upf_lib, oracle_lib, sc)
+    sysm.step(1)
+    stats = sysm.stats()
+    info = o.step()
+    if method == "pcisph":
+        assert stats.iterations == info.iterations
+    res = _compare_step(sysm, o, method)
+    bad = {k: v for k, v in res.items() if not v[0]}
+    assert not bad, "fields beyond %g relative: %s" % (RTOL, bad)
+    sysm.close()
+    o.close()
+
+
 def test_wcsph_single_step_parity(upf_lib, oracle_lib):
     sc = scenes.small_wcsph()
     p, sysm, o = make(upf_lib, oracle_lib, sc)
