@@ -110,6 +110,31 @@ __device__ __forceinline__ double block_sum(double v) {
   return t;
 }
 
+// The passes that walk neighbour lists give each particle kLanes lanes of
+// one warp: lane r takes list entries r, r + kLanes, ..., and the lanes'
+// partial sums are added over the group by xor shuffles, a fixed order, so
+// the results are deterministic (a recomputed forward step equals the
+// original bit for bit). At a few tens of thousands of particles a thread
+// per particle would leave most of the GPU idle.
+constexpr uint32_t kLanes = 4;
+struct Group {
+  uint32_t i;      // particle
+  uint32_t r;      // lane within the group
+  uint32_t mask;   // the group's lanes
+};
+__device__ __forceinline__ Group group_index() {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31u;
+  return Group{t / kLanes, t % kLanes, ((1u << kLanes) - 1u) << (lane - lane % kLanes)};
+}
+__device__ __forceinline__ float gsum(const Group& g, float v) {
+  for (uint32_t o = kLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(g.mask, v, o, kLanes);
+  return v;
+}
+__device__ __forceinline__ float3 gsum(const Group& g, float3 v) {
+  return make_float3(gsum(g, v.x), gsum(g, v.y), gsum(g, v.z));
+}
+
 // --------------------------------------------------------------- forward
 __global__ void k_af_gather(uint32_t n, const uint32_t* __restrict__ perm, const float4* __restrict__ x,
                             const float4* __restrict__ v, float4* __restrict__ xs, float4* __restrict__ vs) {
@@ -122,12 +147,13 @@ __global__ void k_af_gather(uint32_t n, const uint32_t* __restrict__ perm, const
 
 __global__ void k_af_external(uint32_t n, AK k, float a_visc, float mg, const float4* __restrict__ xs,
                               const float4* __restrict__ vs, Lists L, float4* __restrict__ F) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const Group gr = group_index();
+  const uint32_t i = gr.i;
+  if (i >= n) return;  // uniform over the group
   const float4 xi = xs[i], vi = vs[i];
   float3 f = make_float3(0, 0, 0);
   const uint32_t c = L.cnt[i];
-  for (uint32_t q = 0; q < c; ++q) {
+  for (uint32_t q = gr.r; q < c; q += kLanes) {
     const uint32_t j = L.nbr[(size_t)q * L.stride + i];
     const float r = len3(sub3(xi, xs[j]));
     const float w = a_visc * kL(k, r);
@@ -136,8 +162,9 @@ __global__ void k_af_external(uint32_t n, AK k, float a_visc, float mg, const fl
     f.y -= (vi.y - vj.y) * w;
     f.z -= (vi.z - vj.z) * w;
   }
+  f = gsum(gr, f);
   f.y -= mg;
-  F[i] = make_float4(f.x, f.y, f.z, 0.0f);
+  if (gr.r == 0) F[i] = make_float4(f.x, f.y, f.z, 0.0f);
 }
 
 __device__ __forceinline__ void clamp_pos(float4& x, float4& v, const float3& lo, const float3& hi, float damping) {
@@ -170,28 +197,32 @@ __device__ __forceinline__ float dsmax(float d, float eps) { return 0.5f * (1.0f
 __global__ void k_af_density(uint32_t n, AK k, float m, float rho0, float delta, float eps, const float4* __restrict__ xstar,
                              Lists L, const float* __restrict__ p_prev, float* __restrict__ rho,
                              float* __restrict__ p) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const Group gr = group_index();
+  const uint32_t i = gr.i;
+  if (i >= n) return;  // uniform over the group
   const float4 xi = xstar[i];
-  float d = m * kW(k, 0.0f);
+  float d = 0.0f;
   const uint32_t c = L.cnt[i];
-  for (uint32_t q = 0; q < c; ++q) {
+  for (uint32_t q = gr.r; q < c; q += kLanes) {
     const uint32_t j = L.nbr[(size_t)q * L.stride + i];
     d += m * kW(k, len3(sub3(xi, xstar[j])));
   }
+  d = m * kW(k, 0.0f) + gsum(gr, d);
+  if (gr.r != 0) return;
   rho[i] = d;
   p[i] = (p_prev ? p_prev[i] : 0.0f) + delta * smax(d - rho0, eps);
 }
 
 __global__ void k_af_pforce(uint32_t n, AK k, float c0, const float4* __restrict__ xs, const float* __restrict__ p,
                             Lists L, float4* __restrict__ Fp) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const Group gr = group_index();
+  const uint32_t i = gr.i;
+  if (i >= n) return;  // uniform over the group
   const float4 xi = xs[i];
   const float pi = p[i];
   float3 f = make_float3(0, 0, 0);
   const uint32_t c = L.cnt[i];
-  for (uint32_t q = 0; q < c; ++q) {
+  for (uint32_t q = gr.r; q < c; q += kLanes) {
     const uint32_t j = L.nbr[(size_t)q * L.stride + i];
     const float3 r = sub3(xi, xs[j]);
     const float w = -c0 * (pi + p[j]) * kG(k, len3(r));
@@ -199,7 +230,8 @@ __global__ void k_af_pforce(uint32_t n, AK k, float c0, const float4* __restrict
     f.y += r.y * w;
     f.z += r.z * w;
   }
-  Fp[i] = make_float4(f.x, f.y, f.z, 0.0f);
+  f = gsum(gr, f);
+  if (gr.r == 0) Fp[i] = make_float4(f.x, f.y, f.z, 0.0f);
 }
 
 __global__ void k_af_integrate(uint32_t n, float dt, float inv_m, float3 lo, float3 hi,
@@ -310,14 +342,15 @@ __global__ void k_ab_integrate(uint32_t n, float dt, float inv_m, float4* __rest
 __global__ void k_ab_pforce(uint32_t n, AK k, float c0, float delta, float rho0, float eps, const float4* __restrict__ xs,
                             const float* __restrict__ p, const float* __restrict__ rho, const float4* __restrict__ Fpb,
                             Lists L, float* __restrict__ pcarry, float* __restrict__ rhob, float4* __restrict__ xb) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const Group gr = group_index();
+  const uint32_t i = gr.i;
+  if (i >= n) return;  // uniform over the group
   const float4 xi = xs[i], fi = Fpb[i];
   const float pi = p[i];
   float pb = 0.0f;
   float3 g = make_float3(0, 0, 0);
   const uint32_t c = L.cnt[i];
-  for (uint32_t q = 0; q < c; ++q) {
+  for (uint32_t q = gr.r; q < c; q += kLanes) {
     const uint32_t j = L.nbr[(size_t)q * L.stride + i];
     const float3 r = sub3(xi, xs[j]);
     const float rl = len3(r);
@@ -333,6 +366,9 @@ __global__ void k_ab_pforce(uint32_t n, AK k, float c0, float delta, float rho0,
     g.y += cij * (G * d.y + t * r.y);
     g.z += cij * (G * d.z + t * r.z);
   }
+  pb = gsum(gr, pb);
+  g = gsum(gr, g);
+  if (gr.r != 0) return;
   const float ptot = pcarry[i] + pb;
   pcarry[i] = ptot;
   rhob[i] = delta * dsmax(rho[i] - rho0, eps) * ptot;
@@ -343,13 +379,14 @@ __global__ void k_ab_pforce(uint32_t n, AK k, float c0, float delta, float rho0,
 // adjoint of the predicted density of iteration k: dL/dx*
 __global__ void k_ab_density(uint32_t n, AK k, float m, const float4* __restrict__ xstar,
                              const float* __restrict__ rhob, Lists L, float4* __restrict__ xstarb) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const Group gr = group_index();
+  const uint32_t i = gr.i;
+  if (i >= n) return;  // uniform over the group
   const float4 xi = xstar[i];
   const float bi = rhob[i];
   float3 g = make_float3(0, 0, 0);
   const uint32_t c = L.cnt[i];
-  for (uint32_t q = 0; q < c; ++q) {
+  for (uint32_t q = gr.r; q < c; q += kLanes) {
     const uint32_t j = L.nbr[(size_t)q * L.stride + i];
     const float3 r = sub3(xi, xstar[j]);
     const float rl = len3(r);
@@ -359,7 +396,8 @@ __global__ void k_ab_density(uint32_t n, AK k, float m, const float4* __restrict
     g.y += r.y * w;
     g.z += r.z * w;
   }
-  xstarb[i] = make_float4(g.x, g.y, g.z, 0.0f);
+  g = gsum(gr, g);
+  if (gr.r == 0) xstarb[i] = make_float4(g.x, g.y, g.z, 0.0f);
 }
 
 // adjoint of the prediction of iteration k: x* = x + v* dt,
@@ -384,15 +422,16 @@ __global__ void __launch_bounds__(kT) k_ab_external(uint32_t n, AK k, float vol2
                                                     const float4* __restrict__ xs, const float4* __restrict__ vs,
                                                     const float4* __restrict__ Fb, Lists L, float4* __restrict__ xb,
                                                     float4* __restrict__ vb, double* __restrict__ mu_bar) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const Group gr = group_index();
+  const uint32_t i = gr.i;
   double mb = 0.0;
-  if (i < n) {
+  if (i < n) {  // uniform over the group; every thread reaches block_sum
     const float4 xi = xs[i], vi = vs[i], fi = Fb[i];
     float3 gx = make_float3(0, 0, 0), gv = make_float3(0, 0, 0);
     float m_acc = 0.0f;
     const uint32_t c = L.cnt[i];
     const float a = vol2 * mu;
-    for (uint32_t q = 0; q < c; ++q) {
+    for (uint32_t q = gr.r; q < c; q += kLanes) {
       const uint32_t j = L.nbr[(size_t)q * L.stride + i];
       const float3 r = sub3(xi, xs[j]);
       const float rl = len3(r);
@@ -411,16 +450,22 @@ __global__ void __launch_bounds__(kT) k_ab_external(uint32_t n, AK k, float vol2
       }
       m_acc += -vol2 * Lr * (dv.x * fi.x + dv.y * fi.y + dv.z * fi.z);
     }
-    const float4 x = xb[i], v = vb[i];
-    xb[i] = make_float4(x.x + gx.x, x.y + gx.y, x.z + gx.z, 0.0f);
-    vb[i] = make_float4(v.x + gv.x, v.y + gv.y, v.z + gv.z, 0.0f);
-    mb = m_acc;
+    gx = gsum(gr, gx);
+    gv = gsum(gr, gv);
+    m_acc = gsum(gr, m_acc);
+    if (gr.r == 0) {
+      const float4 x = xb[i], v = vb[i];
+      xb[i] = make_float4(x.x + gx.x, x.y + gx.y, x.z + gx.z, 0.0f);
+      vb[i] = make_float4(v.x + gv.x, v.y + gv.y, v.z + gv.z, 0.0f);
+      mb = m_acc;
+    }
   }
   mb = block_sum(mb);
   if (threadIdx.x == 0) atomicAdd(mu_bar, mb);
 }
 
 inline uint32_t grid(uint32_t n) { return (n + kT - 1) / kT; }
+inline uint32_t grid_lanes(uint32_t n) { return (uint32_t)(((uint64_t)n * kLanes + kT - 1) / kT); }
 
 }  // namespace
 }  // namespace upf
@@ -512,7 +557,7 @@ struct upf_adjoint {
     const float4* V = vs + slot(s);
     float4* Fs = F + slot(s);
     const float vol2 = dp.rest_volume * dp.rest_volume;
-    k_af_external<<<grid(n), kT, 0, q>>>(n, k, vol2 * visc, dp.mass * dp.gravity, X, V, L, Fs);
+    k_af_external<<<grid_lanes(n), kT, 0, q>>>(n, k, vol2 * visc, dp.mass * dp.gravity, X, V, L, Fs);
     const float3 lo = dp.cmin, hi = dp.cmax;
     const float c0 = dp.mass * dp.mass / (dp.rho0 * dp.rho0);
     for (int it = 0; it < K(); ++it) {
@@ -520,9 +565,9 @@ struct upf_adjoint {
       const float4* fp_prev = it ? Fp + (size_t)((it - 1) & 1) * n : nullptr;
       float4* fp_out = Fp + (size_t)(it & 1) * n;
       k_af_predict<<<grid(n), kT, 0, q>>>(n, dp.dt, dp.inv_mass, lo, hi, X, V, Fs, fp_prev, xstar + sk);
-      k_af_density<<<grid(n), kT, 0, q>>>(n, k, dp.mass, dp.rho0, dp.delta, eps_rho(), xstar + sk, L,
+      k_af_density<<<grid_lanes(n), kT, 0, q>>>(n, k, dp.mass, dp.rho0, dp.delta, eps_rho(), xstar + sk, L,
                                           it ? p + sk - n : nullptr, rho + sk, p + sk);
-      k_af_pforce<<<grid(n), kT, 0, q>>>(n, k, c0, X, p + sk, L, fp_out);
+      k_af_pforce<<<grid_lanes(n), kT, 0, q>>>(n, k, c0, X, p + sk, L, fp_out);
     }
     k_af_integrate<<<grid(n), kT, 0, q>>>(n, dp.dt, dp.inv_mass, lo, hi, perm + slot(s), X, V, Fs,
                                           Fp + (size_t)((K() - 1) & 1) * n, x, v);
@@ -542,13 +587,13 @@ struct upf_adjoint {
     k_ab_integrate<<<grid(n), kT, 0, q>>>(n, dp.dt, dp.inv_mass, xb, vb, Fb, Fpb, pcarry);
     for (int it = K() - 1; it >= 0; --it) {
       const size_t sk = ((size_t)s * K() + it) * n;
-      k_ab_pforce<<<grid(n), kT, 0, q>>>(n, k, c0, dp.delta, dp.rho0, eps_rho(), X, p + sk, rho + sk, Fpb, L, pcarry, rhob,
+      k_ab_pforce<<<grid_lanes(n), kT, 0, q>>>(n, k, c0, dp.delta, dp.rho0, eps_rho(), X, p + sk, rho + sk, Fpb, L, pcarry, rhob,
                                          xb);
-      k_ab_density<<<grid(n), kT, 0, q>>>(n, k, dp.mass, xstar + sk, rhob, L, xstarb);
+      k_ab_density<<<grid_lanes(n), kT, 0, q>>>(n, k, dp.mass, xstar + sk, rhob, L, xstarb);
       k_ab_predict<<<grid(n), kT, 0, q>>>(n, dp.dt, dp.inv_mass, xstarb, xb, vb, Fb, Fpb, it > 0 ? 1 : 0);
     }
     const float vol2 = dp.rest_volume * dp.rest_volume;
-    k_ab_external<<<grid(n), kT, 0, q>>>(n, k, vol2, visc, X, V, Fb, L, xb, vb, sums + 4);
+    k_ab_external<<<grid_lanes(n), kT, 0, q>>>(n, k, vol2, visc, X, V, Fb, L, xb, vb, sums + 4);
     k_ab_scatter<<<grid(n), kT, 0, q>>>(n, pm, xb, vb, xbar, vbar);
     UPF_CUDA(cudaGetLastError());
     return UPF_OK;
