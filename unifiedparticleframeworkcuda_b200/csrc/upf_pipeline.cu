@@ -274,6 +274,7 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
   const float4 xi = active ? pos[i] : make_float4(0, 0, 0, 0);
   const float h = P.h;
   int lo[3], hi[3];
+  float cg[3];  // the particle's grid position, clamped to the grid as keys are
   {
     const float c[3] = {(xi.x - P.origin.x) * P.scales.x, (xi.y - P.origin.y) * P.scales.y,
                         (xi.z - P.origin.z) * P.scales.z};
@@ -285,8 +286,31 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
       int ui = (u <= 0.0f) ? 0 : (u >= 1023.0f ? 1023 : (int)u);
       lo[a] = li >> P.cell_shift;
       hi[a] = ui >> P.cell_shift;
+      cg[a] = fminf(fmaxf(c[a], 0.0f), 1024.0f);
     }
   }
+  // Cells of the query box whose nearest point lies farther than h from the
+  // particle hold no neighbour and are skipped. A particle's key cell holds
+  // its clamped grid position to within float rounding, so the cell's box is
+  // widened by one grid unit; clamping shortens no distance, and h^2 gets
+  // a 1e-5 relative margin: the test only drops cells that cannot hold a
+  // particle within h. Lanes that walk the warp's union of boxes skip none.
+  const int cs = 1 << P.cell_shift;
+  const float cull_h2 = h * h * 1.00001f;
+  bool cull = !kWarpUnion;
+  auto may_hold = [&](int bx, int by, int bz) {
+    if (!cull) return true;
+    const int b[3] = {bx, by, bz};
+    const float sc[3] = {P.scales.x, P.scales.y, P.scales.z};
+    float s = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float blo = (float)(b[a] * cs) - 1.0f, bhi = (float)((b[a] + 1) * cs) + 1.0f;
+      const float d = fmaxf(0.0f, fmaxf(blo - cg[a], cg[a] - bhi)) / sc[a];
+      s += d * d;
+    }
+    return s <= cull_h2;
+  };
   if (kWarpUnion) {
     int ulo[3], uhi[3];
 #pragma unroll
@@ -369,6 +393,7 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
     for (int bz = lo[2]; bz <= hi[2]; ++bz)
       for (int by = lo[1]; by <= hi[1]; ++by)
         for (int bx = lo[0]; bx <= hi[0]; ++bx) {
+          if (!may_hold(bx, by, bz)) continue;
           uint32_t c = morton3(bx, by, bz);
           int q = m++;
           while (q > 0 && codes[q - 1] > c) {
@@ -381,7 +406,8 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
   } else {
     for (int bz = lo[2]; bz <= hi[2]; ++bz)
       for (int by = lo[1]; by <= hi[1]; ++by)
-        for (int bx = lo[0]; bx <= hi[0]; ++bx) visit(morton3(bx, by, bz));
+        for (int bx = lo[0]; bx <= hi[0]; ++bx)
+          if (may_hold(bx, by, bz)) visit(morton3(bx, by, bz));
   }
   if (!active) return;
   ncnt[i] = cnt < maxn ? cnt : maxn;
