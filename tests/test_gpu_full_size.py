@@ -1,0 +1,110 @@
+"""The benchmark workloads at full size against the CPU oracle.
+
+  * pcisph_dam_break_1M (128 x 128 x 64 = 1,048,576 fluid + 279,308
+    boundary particles): Morton keys, sort order, cell ranges and every
+    neighbour list bit-exact; one step with an equal iteration count and
+    every field within 1e-5 relative of its scale (the small-scene bars);
+  * rigid_fluid_granular_coupling_524k (524,288 fluid, 131,072 grains, 16
+    bodies): one step with an equal iteration count; particle fields, forces
+    and body states within 1e-5 relative of their scales.
+
+The oracle runs its OpenMP restatement on all host cores: a few seconds per
+step at these sizes."""
+import numpy as np
+import pytest
+
+from test_gpu_coupling import compare_bodies, compare_forces, compare_particles
+from test_gpu_parity import RTOL, _compare_step
+from unifiedparticleframeworkcuda_b200 import FROZEN, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _make(upf, oracle, sc, bodies=False):
+    p = upf.derive_params(sc.params)
+    sysm = upf.ParticleSystem(p, capacity=sc.n, derive=False)
+    sysm.set_particles(sc.pos, sc.vel, sc.type)
+    o = oracle.OracleSim(p, sc.pos, sc.vel, sc.type)
+    if bodies:
+        sysm.set_rigid_bodies(sc.body, sc.num_bodies)
+        o.set_rigid_bodies(sc.body, sc.num_bodies)
+    return p, sysm, o
+
+
+def test_full_size_keys_cells_and_lists_bit_exact(upf_lib, oracle_lib):
+    sc = scenes.pcisph_dam()
+    assert int(np.count_nonzero(sc.type != FROZEN)) == 1 << 20
+    p, sysm, o = _make(upf_lib, oracle_lib, sc)
+    sysm.phase("sort")
+    keys, ids = sysm.sorted_keys()
+    st = o.state()
+    dyn = st["type"] != FROZEN
+    assert np.array_equal(ids, st["id"][dyn]), "sort order differs"
+    assert np.array_equal(keys, st["key"][dyn]), "Morton keys differ"
+    assert np.all(np.diff(keys.astype(np.int64)) >= 0)
+
+    start, end = sysm.cell_ranges()
+    bs3 = int(p.search_cell) ** 3
+    k = st["key"][dyn].astype(np.int64)
+    occupied = np.unique(k // bs3)
+    assert np.array_equal(start[occupied], np.searchsorted(k, occupied * bs3, side="left"))
+    assert np.array_equal(end[occupied], np.searchsorted(k, (occupied + 1) * bs3, side="left"))
+    empty = np.ones(start.shape[0], bool)
+    empty[occupied] = False
+    assert not start[empty].any() and not end[empty].any()
+
+    sysm.phase("neighbors")
+    counts, lists = sysm.neighbors()
+    off, nb = o.neighbors()
+    # the oracle's row of each sorted particle
+    row = np.full(int(st["id"].max()) + 1, -1, np.int64)
+    row[st["id"]] = np.arange(st["id"].shape[0])
+    r = row[ids]
+    assert (r >= 0).all()
+    counts = counts.astype(np.int64)
+    want_counts = (off[r + 1] - off[r]).astype(np.int64)
+    bad = np.flatnonzero(counts != want_counts)
+    assert bad.size == 0, "neighbour counts differ at %d particles, first id %d" % (bad.size, ids[bad[0]])
+    total = int(counts.sum())
+    assert total > 20 * counts.shape[0]  # 28.6 entries per fluid particle on average
+    got = lists[np.arange(lists.shape[1])[None, :] < counts[:, None]].astype(np.int64)
+    first = np.cumsum(counts) - counts
+    want = np.asarray(nb, np.int64)[np.arange(total) + np.repeat(off[r] - first, counts)]
+    diff = np.flatnonzero(got != want)
+    assert diff.size == 0, "neighbour entries differ: %d of %d, first in the list of id %d" % (
+        diff.size, total, ids[np.searchsorted(first, diff[0], side="right") - 1])
+    sysm.close()
+    o.close()
+
+
+def test_full_size_pcisph_step(upf_lib, oracle_lib):
+    sc = scenes.pcisph_dam()
+    p, sysm, o = _make(upf_lib, oracle_lib, sc)
+    sysm.step(1)
+    stats = sysm.stats()
+    info = o.step()
+    assert stats.iterations == info.iterations
+    assert abs(stats.max_predicted_density - info.max_predicted_density) <= RTOL * info.max_predicted_density
+    res = _compare_step(sysm, o, "pcisph")
+    bad = {k: v for k, v in res.items() if not v[0]}
+    assert not bad, "fields beyond %g relative: %s" % (RTOL, bad)
+    sysm.close()
+    o.close()
+
+
+def test_full_size_coupling_step(upf_lib, oracle_lib):
+    sc = scenes.coupling_scene()
+    assert sc.num_bodies == 16
+    p, sysm, o = _make(upf_lib, oracle_lib, sc, bodies=True)
+    sysm.step(1)
+    stats = sysm.stats()
+    info = o.step()
+    assert stats.iterations == info.iterations
+    res = {}
+    res.update(compare_particles(sysm, o))
+    res.update(compare_forces(sysm, o))
+    res.update(compare_bodies(sysm, o))
+    bad = {k: v for k, v in res.items() if not v[0]}
+    assert not bad, "beyond %g relative: %s" % (RTOL, bad)
+    sysm.close()
+    o.close()
