@@ -6,7 +6,9 @@
     every field within 1e-5 relative of its scale (the small-scene bars);
   * rigid_fluid_granular_coupling_524k (524,288 fluid, 131,072 grains, 16
     bodies): one step with an equal iteration count; particle fields, forces
-    and body states within 1e-5 relative of their scales.
+    and body states within 1e-5 relative of their scales;
+  * batched_scenes_256: scenes of the full batch equal the same scenes run
+    alone, bit for bit, and the largest agrees with the oracle.
 
 The oracle runs its OpenMP restatement on all host cores: a few seconds per
 step at these sizes."""
@@ -106,5 +108,45 @@ def test_full_size_coupling_step(upf_lib, oracle_lib):
     res.update(compare_bodies(sysm, o))
     bad = {k: v for k, v in res.items() if not v[0]}
     assert not bad, "beyond %g relative: %s" % (RTOL, bad)
+    sysm.close()
+    o.close()
+
+
+def test_full_size_batch_scenes_equal_single_runs(upf_lib, oracle_lib):
+    """batched_scenes_256: all 256 scenes (counts log-uniform in [2048,
+    65536], about 4.7 M particles) step together; the smallest, the largest
+    and four seeded picks equal the same scenes run alone bit for bit, and
+    the largest agrees with the oracle after one step."""
+    from test_gpu_batch import run_single
+
+    scs = scenes.batch_scenes(256, seed=2024)
+    sizes = np.array([sc.n for sc in scs])
+    assert sizes.sum() > 4_000_000
+    picks = sorted({int(sizes.argmin()), int(sizes.argmax())}
+                   | set(np.random.default_rng(5).choice(len(scs), 4, replace=False).tolist()))
+    steps = 2
+    with upf_lib.ParticleBatch.from_scenes(scs) as b:
+        iters = []
+        for _ in range(steps):
+            b.step(1)
+            iters.append([st.iterations for st in b.stats()])
+        stats = b.stats()
+        got = {k: b.particles(k) for k in picks}
+    for k in picks:
+        want, want_iters, want_st = run_single(upf_lib, scs[k], steps)
+        g = {f: v[np.argsort(got[k]["id"], kind="stable")] for f, v in got[k].items()}
+        assert [it[k] for it in iters] == want_iters, "scene %d iterations" % k
+        for f in ("id", "pos", "vel", "density", "pressure"):
+            assert np.array_equal(g[f], want[f]), "scene %d field %s" % (k, f)
+        assert stats[k].max_predicted_density == want_st.max_predicted_density
+
+    big = scs[int(sizes.argmax())]
+    p, sysm, o = _make(upf_lib, oracle_lib, big)
+    sysm.step(1)
+    info = o.step()
+    assert sysm.stats().iterations == info.iterations
+    res = _compare_step(sysm, o, "pcisph")
+    bad = {k: v for k, v in res.items() if not v[0]}
+    assert not bad, "fields beyond %g relative: %s" % (RTOL, bad)
     sysm.close()
     o.close()
