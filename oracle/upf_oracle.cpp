@@ -379,10 +379,16 @@ struct Sim : SimBase {
     const R h = R(prm.support_radius);
     R mn[3] = {R(prm.scales[0]) * (p.x.x - h), R(prm.scales[1]) * (p.x.y - h), R(prm.scales[2]) * (p.x.z - h)};
     R mx[3] = {R(prm.scales[0]) * (p.x.x + h), R(prm.scales[1]) * (p.x.y + h), R(prm.scales[2]) * (p.x.z + h)};
+    // Both corners are clamped into [0, 1024]. The reference clamps only the
+    // lower one from below and the upper one from above. A particle outside
+    // the grid then converts a negative float (or one above 65535) to
+    // unsigned short, which is undefined, and an upper corner below the lower
+    // one makes an empty box of negative size. Particles inside the grid are
+    // unaffected.
     uint16_t a[3], b[3];
     for (int k = 0; k < 3; ++k) {
-      mn[k] = std::max(mn[k], R(0));
-      mx[k] = std::min(mx[k], R(UPF_GRID_RESOLUTION));
+      mn[k] = std::min(std::max(mn[k], R(0)), R(UPF_GRID_RESOLUTION));
+      mx[k] = std::min(std::max(mx[k], R(0)), R(UPF_GRID_RESOLUTION));
       a[k] = (unsigned short)mn[k];
       b[k] = (unsigned short)mx[k];
     }

@@ -1163,6 +1163,21 @@ upf_status upf_phase_sort(upf_system* s) {
   UPF_TRY(phase_guard(s));
   s->stepped = true;
   UPF_CUDA(launch_sort_phase(*s, s->stream));
+  // The sort leaves the keys sorted in place and the state sorted in B, while
+  // A keeps the previous order. In a step, integration rewrites A in sorted
+  // order, together with its keys. Called on its own, the phase copies the
+  // sorted state back into A instead. A and its keys then agree, and a
+  // repeated sort (this phase again, or a step) finds them in order and
+  // changes nothing, as re-sorting sorted arrays does in the reference.
+  const size_t n = s->n_dyn;
+  if (n) {
+    UPF_CUDA(cudaMemcpyAsync(s->A.pos, s->B.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, s->stream));
+    UPF_CUDA(cudaMemcpyAsync(s->A.vel, s->B.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, s->stream));
+    UPF_CUDA(cudaMemcpyAsync(s->A.id, s->B.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s->stream));
+    UPF_CUDA(cudaMemcpyAsync(s->A.type, s->B.type, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s->stream));
+    if (s->prm.method == UPF_METHOD_PCISPH)
+      UPF_CUDA(cudaMemcpyAsync(s->A.lag, s->B.lag, sizeof(float4) * n, cudaMemcpyDeviceToDevice, s->stream));
+  }
   return UPF_OK;
 }
 
