@@ -100,3 +100,24 @@ def test_batch_argument_checks(upf_lib):
     with pytest.raises(ValueError):
         b.set_particles(np.zeros((3, 4), np.float32), np.zeros((3, 4), np.float32))
     b.close()
+
+
+def test_batch_with_tiny_and_ragged_scenes(upf_lib):
+    """Scenes of 1, 2, 31, 33 and 257 particles beside a 6,000-particle
+    scene: each equals its single-scene run bit for bit. Every scene starts
+    its own segment, so scenes smaller than a warp or a CTA share no CTA."""
+    counts = [1, 2, 31, 33, 257, 6000]
+    scs = [scenes.batch_scene(n, (0.6, 0.8, 0.5), 100 + k, stream=k + 1) for k, n in enumerate(counts)]
+    assert [sc.n for sc in scs] == counts
+    steps = 3
+    with upf_lib.ParticleBatch.from_scenes(scs) as b:
+        iters = []
+        for _ in range(steps):
+            b.step(1)
+            iters.append([st.iterations for st in b.stats()])
+        got = [by_id(b.particles(k)) for k in range(len(scs))]
+    for k, sc in enumerate(scs):
+        want, want_iters, _ = run_single(upf_lib, sc, steps)
+        assert [it[k] for it in iters] == want_iters, "scene %d iterations" % k
+        for f in ("id", "pos", "vel", "density", "pressure"):
+            assert np.array_equal(got[k][f], want[f]), "scene %d field %s" % (k, f)
