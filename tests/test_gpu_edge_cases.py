@@ -127,3 +127,29 @@ def test_phase_entry_points_repeat_and_compose(upf_lib):
     for got in out[1:]:
         for f in ("id", "pos", "vel", "density", "pressure"):
             assert np.array_equal(got[f], out[0][f]), f
+
+
+def test_phases_in_order_make_one_step(upf_lib):
+    """sort, neighbors, forces, predict_correct and integrate, called in
+    order, advance the state exactly as one graph-launched step does."""
+    sc = scenes.small_pcisph()
+    p = upf_lib.derive_params(sc.params)
+    out = []
+    for by_phase in (False, True):
+        with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
+            s.set_particles(sc.pos, sc.vel, sc.type)
+            iters = []
+            for _ in range(2):
+                if by_phase:
+                    for ph in ("sort", "neighbors", "forces", "predict_correct", "integrate"):
+                        s.phase(ph)
+                else:
+                    s.step(1)
+                iters.append(s.stats().iterations)
+            g = s.particles()
+            o = np.argsort(g["id"], kind="stable")
+            out.append(({k: v[o] for k, v in g.items()}, iters))
+    (a, ia), (b, ib) = out
+    assert ia == ib
+    for f in ("id", "pos", "vel", "density", "pressure"):
+        assert np.array_equal(a[f], b[f]), f
