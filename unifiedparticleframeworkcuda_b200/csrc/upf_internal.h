@@ -36,9 +36,24 @@ struct NvtxRange {
 };
 
 // upf_sort.cu
-constexpr uint32_t kRadixTileKeys = 8192;  // keys per sort tile (16 warps x 512)
-constexpr uint32_t kRadixDigits = 256;     // 8-bit digits
-uint32_t radix_tiles(uint32_t n);
+// A sort pass runs one CTA per tile of keys. The tile is the smallest of
+// 512, 2048 and 8192 keys (16 warps x 32, 128 or 512) that needs at most
+// kRadixTileCap tiles: small inputs get more CTAs than 8192-key tiles would
+// give them, while the single-CTA digit scan (256 counts per tile) stays short.
+constexpr uint32_t kRadixDigits = 256;  // 8-bit digits
+constexpr uint32_t kRadixTileCap = 128;
+constexpr uint32_t radix_tile_keys(uint32_t n) {
+  return n <= kRadixTileCap * 512u ? 512u : (n <= kRadixTileCap * 2048u ? 2048u : 8192u);
+}
+constexpr uint32_t radix_tiles(uint32_t n) { return (n + radix_tile_keys(n) - 1) / radix_tile_keys(n); }
+// The most tiles of any count up to n: scratch sized for n serves every
+// smaller count (a system sorts any number of particles up to its capacity).
+constexpr uint32_t radix_tiles_upto(uint32_t n) {
+  const uint32_t a = radix_tiles(n);
+  const uint32_t b = radix_tiles(n < kRadixTileCap * 512u ? n : kRadixTileCap * 512u);
+  const uint32_t c = radix_tiles(n < kRadixTileCap * 2048u ? n : kRadixTileCap * 2048u);
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
 size_t radix_temp_words(uint32_t n);
 size_t radix_temp_bytes(uint32_t n);
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,

@@ -4,7 +4,8 @@
 // Replaces the reference's 2006 SDK sort (RadixSum / RadixPrefixSum /
 // RadixAddOffsetsAndShuffle, src/gpu/radixsort_kernel.cu:64-540, driver
 // src/gpu/particles.cu:31-60), which runs a fixed 48-CTA grid. Here each pass
-// is three launches sized to the input:
+// is three launches sized to the input, one CTA per tile of 512, 2048 or 8192
+// keys (radix_tile_keys: the smallest tile that needs at most 128 tiles):
 //   upsweep   per-tile digit histograms (shared-memory atomics)
 //   scan      exclusive scan of the digit-major [256][tiles] count matrix
 //   downsweep per-tile stable ranking with warp match/ballot (each warp owns
@@ -27,14 +28,15 @@ constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kThreads = 512;               // 16 warps
 constexpr int kWarps = kThreads / 32;
-constexpr int kItemsPerLane = 16;
-constexpr int kWarpItems = 32 * kItemsPerLane;   // 512
-constexpr int kTile = kWarps * kWarpItems;       // 8192 keys per tile
-static_assert(kTile == (int)kRadixTileKeys && kRadix == (int)kRadixDigits, "scratch layout constants");
+static_assert(kRadix == (int)kRadixDigits, "scratch layout constants");
 
+// kItems keys per lane: a warp ranks 32 * kItems consecutive keys, a tile is
+// kWarps warps' segments
+template <int kItems>
 __global__ void __launch_bounds__(kThreads) k_upsweep(const uint32_t* __restrict__ keys, uint32_t n,
                                                        int shift, uint32_t ntiles,
                                                        uint32_t* __restrict__ counts) {
+  constexpr int kTile = kWarps * 32 * kItems;
   __shared__ uint32_t hist[kRadix];
   for (int d = threadIdx.x; d < kRadix; d += kThreads) hist[d] = 0;
   __syncthreads();
@@ -95,13 +97,21 @@ __global__ void __launch_bounds__(1024) k_scan(uint32_t* __restrict__ counts, ui
   }
 }
 
-template <bool kIotaValues>
+template <int kItems>
+constexpr size_t down_smem() {
+  return sizeof(uint32_t) * (kWarps * kRadix + 2 * (kWarps * 32 * kItems) + 2 * kRadix);
+}
+
+template <bool kIotaValues, int kItems>
 __global__ void __launch_bounds__(kThreads) k_downsweep(const uint32_t* __restrict__ keys_in,
                                                          const uint32_t* __restrict__ vals_in,
                                                          uint32_t* __restrict__ keys_out,
                                                          uint32_t* __restrict__ vals_out, uint32_t n,
                                                          int shift, uint32_t ntiles,
                                                          const uint32_t* __restrict__ counts) {
+  constexpr int kItemsPerLane = kItems;
+  constexpr int kWarpItems = 32 * kItems;
+  constexpr int kTile = kWarps * kWarpItems;
   extern __shared__ uint32_t smem[];
   uint32_t* whist = smem;                                  // [kWarps][kRadix]
   uint32_t* skeys = whist + kWarps * kRadix;               // [kTile]
@@ -195,16 +205,12 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const uint32_t* __restri
   }
 }
 
-constexpr size_t kDownSmem = sizeof(uint32_t) * (kWarps * kRadix + 2 * kTile + 2 * kRadix);
-
 }  // namespace
-
-uint32_t radix_tiles(uint32_t n) { return (n + kTile - 1) / kTile; }
 
 // scratch layout: keys_alt[pad64(n)] | vals_alt[pad64(n)] | counts[256 * tiles]
 size_t radix_temp_words(uint32_t n) {
   size_t pad = ((size_t)n + 63) & ~size_t(63);
-  return 2 * pad + (size_t)kRadix * radix_tiles(n);
+  return 2 * pad + (size_t)kRadix * radix_tiles_upto(n);
 }
 
 size_t radix_temp_bytes(uint32_t n) { return radix_temp_words(n) * sizeof(uint32_t); }
@@ -220,9 +226,10 @@ cudaError_t radix_init() {
   if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(mu);
   if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
-  e = cudaFuncSetAttribute(k_downsweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDownSmem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_downsweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDownSmem);
+  e = cudaFuncSetAttribute(k_downsweep<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)down_smem<16>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_downsweep<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)down_smem<16>());
   if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
   return e;
 }
@@ -232,17 +239,28 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt,
                              cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const uint32_t ntiles = radix_tiles(n);
+  const uint32_t tile = radix_tile_keys(n);
   int passes = (key_bits + kRadixBits - 1) / kRadixBits;
   if (passes < 1) passes = 1;
   uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
   for (int p = 0; p < passes; ++p) {
     int shift = p * kRadixBits;
-    k_upsweep<<<ntiles, kThreads, 0, st>>>(ki, n, shift, ntiles, counts);
-    k_scan<<<1, 1024, 0, st>>>(counts, kRadix * ntiles);
-    if (p == 0 && iota_values)
-      k_downsweep<true><<<ntiles, kThreads, kDownSmem, st>>>(ki, vi, ko, vo, n, shift, ntiles, counts);
-    else
-      k_downsweep<false><<<ntiles, kThreads, kDownSmem, st>>>(ki, vi, ko, vo, n, shift, ntiles, counts);
+    const bool iota = p == 0 && iota_values;
+#define UPF_PASS(I)                                                                                          \
+  k_upsweep<I><<<ntiles, kThreads, 0, st>>>(ki, n, shift, ntiles, counts);                                   \
+  k_scan<<<1, 1024, 0, st>>>(counts, kRadix * ntiles);                                                       \
+  if (iota)                                                                                                  \
+    k_downsweep<true, I><<<ntiles, kThreads, down_smem<I>(), st>>>(ki, vi, ko, vo, n, shift, ntiles, counts); \
+  else                                                                                                       \
+    k_downsweep<false, I><<<ntiles, kThreads, down_smem<I>(), st>>>(ki, vi, ko, vo, n, shift, ntiles, counts);
+    if (tile == 8192u) {
+      UPF_PASS(16)
+    } else if (tile == 2048u) {
+      UPF_PASS(4)
+    } else {
+      UPF_PASS(1)
+    }
+#undef UPF_PASS
     uint32_t* t;
     t = ki; ki = ko; ko = t;
     t = vi; vi = vo; vo = t;
