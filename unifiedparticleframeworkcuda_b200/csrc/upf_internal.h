@@ -54,6 +54,9 @@ constexpr uint32_t radix_tiles_upto(uint32_t n) {
   const uint32_t c = radix_tiles(n < kRadixTileCap * 2048u ? n : kRadixTileCap * 2048u);
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
+// digit counts of a sort of up to n keys: [256][tiles] per tile, then the 256
+// digit totals
+constexpr size_t radix_count_words(uint32_t n) { return (size_t)kRadixDigits * (radix_tiles_upto(n) + 1); }
 size_t radix_temp_words(uint32_t n);
 size_t radix_temp_bytes(uint32_t n);
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,

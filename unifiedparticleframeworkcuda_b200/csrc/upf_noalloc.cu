@@ -18,7 +18,7 @@ namespace {
 
 constexpr uint32_t kNoAllocMaxPairs = UPF_NOALLOC_MAX_PAIRS;
 constexpr size_t kPad = ((size_t)kNoAllocMaxPairs + 63) & ~size_t(63);
-constexpr size_t kNoAllocWords = 2 * kPad + (size_t)kRadixDigits * radix_tiles_upto(kNoAllocMaxPairs);
+constexpr size_t kNoAllocWords = 2 * kPad + radix_count_words(kNoAllocMaxPairs);
 
 // keys_alt | vals_alt | digit counts, laid out as upf_radix_sort_pairs lays out
 // its caller's scratch (17 MB for the 2^21-pair maximum)

@@ -7,7 +7,8 @@
 // is three launches sized to the input, one CTA per tile of 512, 2048 or 8192
 // keys (radix_tile_keys: the smallest tile that needs at most 128 tiles):
 //   upsweep   per-tile digit histograms (shared-memory atomics)
-//   scan      exclusive scan of the digit-major [256][tiles] count matrix
+//   scan      per digit, exclusive scan of its row of tile counts (one CTA
+//             per digit) and the digit's total
 //   downsweep per-tile stable ranking with warp match/ballot (each warp owns
 //             a contiguous 512-key segment, rounds run in key order), a local
 //             sort through shared memory, and coalesced runs to global memory.
@@ -50,56 +51,62 @@ __global__ void __launch_bounds__(kThreads) k_upsweep(const uint32_t* __restrict
   for (int d = threadIdx.x; d < kRadix; d += kThreads) counts[(size_t)d * ntiles + blockIdx.x] = hist[d];
 }
 
-// Exclusive scan of `total` counts in place, one CTA of 1024 threads.
-__global__ void __launch_bounds__(1024) k_scan(uint32_t* __restrict__ counts, uint32_t total) {
-  __shared__ uint32_t warp_sums[32];
+// Exclusive scan of each digit's row of tile counts, one CTA of 256 threads
+// per digit: counts[d][t] becomes the number of keys with digit d in tiles
+// before t, and totals[d] the digit's count over all tiles. The downsweep
+// adds the digit's base (the exclusive scan of the totals).
+__global__ void __launch_bounds__(256) k_scan_rows(uint32_t* __restrict__ counts, uint32_t ntiles,
+                                                   uint32_t* __restrict__ totals) {
+  __shared__ uint32_t warp_sums[8];
   __shared__ uint32_t carry;
+  uint32_t* row = counts + (size_t)blockIdx.x * ntiles;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (uint32_t base = 0; base < total; base += 1024 * 4) {
+  for (uint32_t base = 0; base < ntiles; base += 256 * 4) {
     uint32_t v[4];
-    uint32_t idx0 = base + threadIdx.x * 4;
+    const uint32_t idx0 = base + threadIdx.x * 4;
     uint32_t s = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      v[k] = (idx0 + k < total) ? counts[idx0 + k] : 0u;
+      v[k] = (idx0 + k < ntiles) ? row[idx0 + k] : 0u;
       s += v[k];
     }
     uint32_t incl = s;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += t;
     }
     if (lane == 31) warp_sums[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-      uint32_t w = warp_sums[lane];
+      const uint32_t w = lane < 8 ? warp_sums[lane] : 0u;
       uint32_t wi = w;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+      for (int o = 1; o < 8; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
         if (lane >= o) wi += t;
       }
-      warp_sums[lane] = wi - w;  // exclusive
+      if (lane < 8) warp_sums[lane] = wi - w;  // exclusive
     }
     __syncthreads();
     uint32_t run = carry + warp_sums[warp] + (incl - s);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      if (idx0 + k < total) counts[idx0 + k] = run;
+      if (idx0 + k < ntiles) row[idx0 + k] = run;
       run += v[k];
     }
     __syncthreads();
-    if (threadIdx.x == 1023) carry = run;
+    if (threadIdx.x == 255) carry = run;
     __syncthreads();
   }
+  if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
 template <int kItems>
 constexpr size_t down_smem() {
-  return sizeof(uint32_t) * (kWarps * kRadix + 2 * (kWarps * 32 * kItems) + 2 * kRadix);
+  return sizeof(uint32_t) * (kWarps * kRadix + 2 * (kWarps * 32 * kItems) + 3 * kRadix);
 }
 
 template <bool kIotaValues, int kItems>
@@ -108,7 +115,8 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const uint32_t* __restri
                                                          uint32_t* __restrict__ keys_out,
                                                          uint32_t* __restrict__ vals_out, uint32_t n,
                                                          int shift, uint32_t ntiles,
-                                                         const uint32_t* __restrict__ counts) {
+                                                         const uint32_t* __restrict__ counts,
+                                                         const uint32_t* __restrict__ totals) {
   constexpr int kItemsPerLane = kItems;
   constexpr int kWarpItems = 32 * kItems;
   constexpr int kTile = kWarps * kWarpItems;
@@ -118,6 +126,7 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const uint32_t* __restri
   uint32_t* svals = skeys + kTile;                         // [kTile]
   uint32_t* digit_off = svals + kTile;                     // [kRadix] tile-local digit offsets
   uint32_t* gbase = digit_off + kRadix;                    // [kRadix] global bases
+  uint32_t* dbase = gbase + kRadix;                        // [kRadix] digit bases over all tiles
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int d = threadIdx.x; d < kWarps * kRadix; d += kThreads) whist[d] = 0;
@@ -160,9 +169,31 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const uint32_t* __restri
     }
     digit_off[d] = acc;  // total for now
     gbase[d] = counts[(size_t)d * ntiles + blockIdx.x];
+    dbase[d] = totals[d];
   }
   __syncthreads();
-  // exclusive scan of the 256 digit totals (one warp, 8 per lane)
+  // digit bases: exclusive scan of the 256 digit totals (warp 1, 8 per lane)
+  if (warp == 1) {
+    uint32_t t[8], s = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      t[q] = dbase[lane * 8 + q];
+      s += t[q];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    uint32_t run = incl - s;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      gbase[lane * 8 + q] += run;
+      run += t[q];
+    }
+  }
+  // the tile's digit offsets: exclusive scan of its 256 digit totals (warp 0)
   if (warp == 0) {
     uint32_t t[8], s = 0;
 #pragma unroll
@@ -210,7 +241,7 @@ __global__ void __launch_bounds__(kThreads) k_downsweep(const uint32_t* __restri
 // scratch layout: keys_alt[pad64(n)] | vals_alt[pad64(n)] | counts[256 * tiles]
 size_t radix_temp_words(uint32_t n) {
   size_t pad = ((size_t)n + 63) & ~size_t(63);
-  return 2 * pad + (size_t)kRadix * radix_tiles_upto(n);
+  return 2 * pad + radix_count_words(n);
 }
 
 size_t radix_temp_bytes(uint32_t n) { return radix_temp_words(n) * sizeof(uint32_t); }
@@ -240,6 +271,8 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt,
   if (n == 0) return cudaSuccess;
   const uint32_t ntiles = radix_tiles(n);
   const uint32_t tile = radix_tile_keys(n);
+  // the digit totals follow the [256][ntiles] counts
+  uint32_t* totals = counts + (size_t)kRadix * ntiles;
   int passes = (key_bits + kRadixBits - 1) / kRadixBits;
   if (passes < 1) passes = 1;
   uint32_t *ki = keys, *vi = vals, *ko = keys_alt, *vo = vals_alt;
@@ -248,11 +281,13 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt,
     const bool iota = p == 0 && iota_values;
 #define UPF_PASS(I)                                                                                          \
   k_upsweep<I><<<ntiles, kThreads, 0, st>>>(ki, n, shift, ntiles, counts);                                   \
-  k_scan<<<1, 1024, 0, st>>>(counts, kRadix * ntiles);                                                       \
+  k_scan_rows<<<kRadix, 256, 0, st>>>(counts, ntiles, totals);                                               \
   if (iota)                                                                                                  \
-    k_downsweep<true, I><<<ntiles, kThreads, down_smem<I>(), st>>>(ki, vi, ko, vo, n, shift, ntiles, counts); \
+    k_downsweep<true, I><<<ntiles, kThreads, down_smem<I>(), st>>>(ki, vi, ko, vo, n, shift, ntiles, counts,  \
+                                                                    totals);                                  \
   else                                                                                                       \
-    k_downsweep<false, I><<<ntiles, kThreads, down_smem<I>(), st>>>(ki, vi, ko, vo, n, shift, ntiles, counts);
+    k_downsweep<false, I><<<ntiles, kThreads, down_smem<I>(), st>>>(ki, vi, ko, vo, n, shift, ntiles, counts, \
+                                                                     totals);
     if (tile == 8192u) {
       UPF_PASS(16)
     } else if (tile == 2048u) {
