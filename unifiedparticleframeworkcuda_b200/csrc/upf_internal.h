@@ -41,7 +41,7 @@ struct NvtxRange {
 // kRadixTileCap tiles: small inputs get more CTAs than 8192-key tiles would
 // give them, while the single-CTA digit scan (256 counts per tile) stays short.
 constexpr uint32_t kRadixDigits = 256;  // 8-bit digits
-constexpr uint32_t kRadixTileCap = 128;
+constexpr uint32_t kRadixTileCap = 512;
 constexpr uint32_t radix_tile_keys(uint32_t n) {
   return n <= kRadixTileCap * 512u ? 512u : (n <= kRadixTileCap * 2048u ? 2048u : 8192u);
 }
