@@ -5,7 +5,8 @@
 // RadixAddOffsetsAndShuffle, src/gpu/radixsort_kernel.cu:64-540, driver
 // src/gpu/particles.cu:31-60), which runs a fixed 48-CTA grid. Here each pass
 // is three launches sized to the input, one CTA per tile of 512, 2048 or 8192
-// keys (radix_tile_keys: the smallest tile that needs at most 128 tiles):
+// keys (radix_tile_keys: the smallest tile that needs at most kRadixTileCap
+// tiles):
 //   upsweep   per-tile digit histograms (shared-memory atomics)
 //   scan      per digit, exclusive scan of its row of tile counts (one CTA
 //             per digit) and the digit's total
