@@ -11,7 +11,8 @@
 //   scan      per digit, exclusive scan of its row of tile counts (one CTA
 //             per digit) and the digit's total
 //   downsweep per-tile stable ranking with warp match/ballot (each warp owns
-//             a contiguous 512-key segment, rounds run in key order), a local
+//             a contiguous segment of 32, 128 or 512 keys, rounds run in key
+//             order), a local
 //             sort through shared memory, and coalesced runs to global memory.
 // Stability: warps own consecutive segments and rank in order, so equal
 // digits keep their input order; an LSD sort of stable passes is stable.
