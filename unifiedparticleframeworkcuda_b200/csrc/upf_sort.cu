@@ -12,8 +12,8 @@
 //             per digit) and the digit's total
 //   downsweep per-tile stable ranking with warp match/ballot (each warp owns
 //             a contiguous segment of 32, 128 or 512 keys, rounds run in key
-//             order), a local
-//             sort through shared memory, and coalesced runs to global memory.
+//             order), a local sort through shared memory, and coalesced runs
+//             to global memory.
 // Stability: warps own consecutive segments and rank in order, so equal
 // digits keep their input order; an LSD sort of stable passes is stable.
 #include <cuda_runtime.h>
