@@ -159,3 +159,15 @@ def test_bin_thresholds_reproduce_sqrt_binning(upf_lib):
         inside = d < hf
         assert np.array_equal(r2 < thr[301], inside)
         assert np.array_equal(np.minimum(exact, 300)[inside], got[inside])
+
+
+def test_scratch_for_a_capacity_serves_every_smaller_count(upf_lib):
+    """The radix sort's scratch size (host arithmetic): a system allocates it
+    for its capacity and sorts any count up to it, so it never shrinks as the
+    count grows, across the sizes where the sort's tile changes."""
+    f = upf_lib.lib().upf_radix_sort_temp_bytes
+    prev = 0
+    for n in list(range(0, 5000, 7)) + list(range(262_000, 263_000, 3)) + list(range(1_048_000, 1_049_500, 5)):
+        b = f(n)
+        assert b >= prev, n
+        prev = b
