@@ -9,8 +9,9 @@
  * a C++ `dataPointers&` (src/gpu/particles.cuh:430-586). Here the handle
  * `upf_system*` owns everything that struct held (device arrays, parameters,
  * lookup tables, ping-pong state), so several independent simulations may
- * live in one process. The reference-named entry points are declared in
- * upf_legacy.h on top of this header.
+ * live in one process. Each declaration below names the reference entry
+ * point it replaces (file:line); the reference's host facade calls these in
+ * place of its `dataPointers&` functions.
  */
 #ifndef UPF_H_
 #define UPF_H_
