@@ -8,7 +8,9 @@
     bodies): one step with an equal iteration count; particle fields, forces
     and body states within 1e-5 relative of their scales;
   * batched_scenes_256: scenes of the full batch equal the same scenes run
-    alone, bit for bit, and the largest agrees with the oracle.
+    alone, bit for bit, and the largest agrees with the oracle;
+  * wcsph_dam_break_32k: one step at the specified dt within 1e-5 of the
+    oracle, 20 steps at the timed dt on kinetic energy and momentum.
 
 The oracle runs its OpenMP restatement on all host cores: a few seconds per
 step at these sizes."""
@@ -148,5 +150,36 @@ def test_full_size_batch_scenes_equal_single_runs(upf_lib, oracle_lib):
     res = _compare_step(sysm, o, "pcisph")
     bad = {k: v for k, v in res.items() if not v[0]}
     assert not bad, "fields beyond %g relative: %s" % (RTOL, bad)
+    sysm.close()
+    o.close()
+
+
+def test_full_size_wcsph_dam(upf_lib, oracle_lib):
+    """wcsph_dam_break_32k (32,768 fluid + 15,002 boundary particles): one
+    step at the specified dt = 1e-3 within 1e-5 of the oracle; then 20 steps
+    at the timed dt = 5e-4 (the specified step diverges within 12 steps in
+    both), compared on kinetic energy and momentum within 1e-3."""
+    sc = scenes.wcsph_dam(32)
+    assert sc.n_fluid == 32_768
+    p, sysm, o = _make(upf_lib, oracle_lib, sc)
+    sysm.step(1)
+    sysm.synchronize()
+    o.step()
+    res = _compare_step(sysm, o, "wcsph")
+    bad = {k: v for k, v in res.items() if not v[0]}
+    assert not bad, "fields beyond %g relative: %s" % (RTOL, bad)
+    sysm.close()
+    o.close()
+
+    sc.params.dt = 5e-4
+    p, sysm, o = _make(upf_lib, oracle_lib, sc)
+    for s in range(20):
+        sysm.step(1)
+        g = sysm.stats()
+        c = o.step()
+        assert abs(g.kinetic_energy - c.kinetic_energy) <= 1e-3 * c.kinetic_energy, s
+        mg = np.array(g.momentum[:])
+        mc = np.array(c.momentum[:])
+        assert np.abs(mg - mc).max() <= 1e-3 * np.abs(mc).max(), s
     sysm.close()
     o.close()
