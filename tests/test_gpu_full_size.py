@@ -10,7 +10,9 @@
   * batched_scenes_256: scenes of the full batch equal the same scenes run
     alone, bit for bit, and the largest agrees with the oracle;
   * wcsph_dam_break_32k: one step at the specified dt within 1e-5 of the
-    oracle, 20 steps at the timed dt on kinetic energy and momentum.
+    oracle, 20 steps at the timed dt on kinetic energy and momentum;
+  * adjoint_pcisph at 65,536 particles over 20 steps: loss and gradients
+    against the FP64 oracle adjoint.
 
 The oracle runs its OpenMP restatement on all host cores: a few seconds per
 step at these sizes."""
@@ -183,3 +185,26 @@ def test_full_size_wcsph_dam(upf_lib, oracle_lib):
         assert np.abs(mg - mc).max() <= 1e-3 * np.abs(mc).max(), s
     sysm.close()
     o.close()
+
+
+def test_full_size_adjoint_particle_count(upf_lib, oracle_lib):
+    """adjoint_pcisph at its full particle count (32 x 32 x 64 = 65,536) over
+    20 steps, checkpoints every 5: the loss within 1e-4 and the gradients
+    (initial velocities, L2; viscosity) within 1e-3 of the FP64 oracle
+    adjoint. The trajectory length itself is covered by the small test of
+    checkpoint intervals, which shows that gradients do not depend on them."""
+    sc = scenes.adjoint_scene(32, 32, 64)
+    assert sc.n == 65_536
+    p = upf_lib.derive_params(sc.params)
+    tgt = sc.pos[:, :3].astype(np.float64).mean(0) + np.array([0.1, 0.0, 0.0])
+    with upf_lib.Adjoint(p, sc.pos, sc.vel, 20, checkpoint_interval=5, loop_iterations=3, target=tgt,
+                         com_weight=1.0, density_weight=1e-6, derive=False) as a:
+        loss = a.forward()
+        gv, gm = a.backward()
+    x = sc.pos[:, :3].astype(np.float64)
+    v = sc.vel[:, :3].astype(np.float64)
+    L64, gv64, gm64 = oracle_lib.adjoint_run(p, x, v, viscosity=p.viscosity, steps=20, iterations=3, target=tgt,
+                                             com_weight=1.0, density_weight=1e-6)
+    assert abs(loss - L64) <= 1e-4 * abs(L64)
+    assert np.linalg.norm(gv - gv64) <= 1e-3 * np.linalg.norm(gv64)
+    assert abs(gm - gm64) <= 1e-3 * abs(gm64)
