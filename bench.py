@@ -76,6 +76,54 @@ def cpu_sample_scene(args):
     return scenes.pcisph_dam(64, 64, 64), "pcisph_dam 64^3"
 
 
+# Steps from rest after which the dam's predict-correct loop meets the 1%
+# density error criterion. Measured on the 1M dam (per-step trace over 8,000
+# steps): steps 0-43 (the jittered lattice's start-up transient) end at the
+# 50-iteration cap with errors of 1-11%; steps 44-274 all end below 1%
+# (7-35 iterations) while the column collapses; from about step 275 the
+# surges against the walls send 20-60% of the steps back to the cap. The
+# timed steps (both arms) start from the state after these steps, so that a
+# default run (settle + warm-up + timed steps within 224 steps) times steps
+# that meet the criterion.
+SETTLE_DEFAULT = {"c2": 50, "c2-small": 50}
+
+
+def settle_steps(args):
+    return SETTLE_DEFAULT.get(args.scene, 0) if args.settle < 0 else args.settle
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def oracle_from_system(s, sc, threads):
+    """The oracle holding system `s`'s current state (the workload `sc`
+    advanced on the GPU): positions, velocities and the last step's pressure
+    and predicted density of the dynamic particles, the boundary as built."""
+    import unifiedparticleframeworkcuda_b200 as upf
+    from oracle import pyoracle
+    g = s.particles()
+    ids = g["id"].astype(np.int64)
+    pos = np.array(sc.pos, np.float32, copy=True)
+    vel = np.array(sc.vel, np.float32, copy=True)
+    p = upf.derive_params(sc.params)
+    pres = np.zeros(sc.n, np.float32)
+    dens = np.full(sc.n, np.float32(p.rest_density), np.float32)
+    pos[ids] = g["pos"]
+    vel[ids] = g["vel"]
+    pres[ids] = g["pressure"]
+    dens[ids] = g["density"]
+    o = pyoracle.OracleSim(p, pos, vel, sc.type, threads=threads, keep_fields=False)
+    o.set_lagged(pres, dens)
+    return o
+
+
 def workload_name(args):
     return {"c2": "pcisph_dam_break_1M", "c2-small": "pcisph_dam_break_262k",
             "c1": "wcsph_dam_break_32k", "c3": "rigid_fluid_granular_coupling_524k"}[args.scene]
@@ -162,17 +210,47 @@ def make_oracle(sc, threads):
     return o
 
 
-def cpu_baseline(args, seconds=15.0):
-    """The oracle (FP32 OpenMP restatement of the reference CPU path) on a
-    bounded sample of the same workload: the same spacing, h, dt and boundary
-    with fewer particles (particle-steps/s do not depend on the block's size
-    beyond cache effects)."""
+def full_config_oracle(args, threads):
+    """The dam workload at its full size for the reference arm: the oracle
+    advanced from rest by the workload's settle steps on the host cores (the
+    same procedure the GPU arm runs before its timed steps). Returns
+    (oracle, scene, label, settle info)."""
+    sc = scene_for(args)
+    settle = settle_steps(args)
+    o = make_oracle(sc, threads)
+    t0 = time.perf_counter()
+    its = [o.step().iterations for _ in range(settle)]
+    info = {"settle_steps": settle, "settle_seconds": time.perf_counter() - t0,
+            "settle_mean_iterations": float(np.mean(its)) if its else 0.0}
+    label = "%s after %d steps from rest" % (workload_name(args), settle) if settle else \
+        "%s from rest" % workload_name(args)
+    return o, sc, label, info
+
+
+def cpu_baseline(args, seconds=15.0, system=None):
+    """The oracle (FP32 OpenMP restatement of the reference CPU path). Given
+    the GPU arm's system (the dam workloads), it runs the full configuration
+    from that system's state: 2 warm-up steps, then steps until at least 5
+    and `seconds` have passed. The other workloads run a bounded sample of
+    the same scene (the same spacing, h, dt and boundary with fewer
+    particles)."""
     from oracle import pyoracle
     pyoracle.build(with_ref=False)
-    sc, label = cpu_sample_scene(args)
     threads = os.cpu_count() or 1
-    o = make_oracle(sc, threads)
-    o.step()  # warm-up
+    if system is not None:
+        # the full configuration from the GPU arm's own state at the start of
+        # its timed steps
+        sc = scene_for(args)
+        o = oracle_from_system(system, sc, threads)
+        label = "%s after %d steps from rest, the state the GPU arm times" % (workload_name(args),
+                                                                             settle_steps(args))
+        warm, min_steps = 2, 5
+    else:
+        sc, label = cpu_sample_scene(args)
+        o = make_oracle(sc, threads)
+        warm, min_steps = 1, 2
+    for _ in range(warm):
+        o.step()
     t0 = time.perf_counter()
     steps = 0
     iters = 0
@@ -180,14 +258,14 @@ def cpu_baseline(args, seconds=15.0):
         info = o.step()
         steps += 1
         iters += info.iterations
-        if time.perf_counter() - t0 >= seconds and steps >= 2:
+        if time.perf_counter() - t0 >= seconds and steps >= min_steps:
             break
     dt = time.perf_counter() - t0
     o.close()
     nd = dynamic_count(sc)
-    return {"value": nd * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "%d dynamic + %d boundary particles (%s), %d steps, mean %.1f iterations, %.1f s"
-                      % (nd, sc.n_boundary, label, steps, iters / steps, dt)}
+    return {"value": nd * steps / dt, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
+            "sample": "%d dynamic + %d boundary particles (%s), %d steps after %d warm-up, mean %.1f iterations, "
+                      "%.1f s" % (nd, sc.n_boundary, label, steps, warm, iters / steps, dt)}
 
 
 def run_reference(args, rank, world):
@@ -227,28 +305,46 @@ def run_reference(args, rank, world):
         return
     from oracle import pyoracle
     pyoracle.build(with_ref=False)
-    # bounded sample per step: a smaller block of the workload
-    sc, label = cpu_sample_scene(args)
     threads = os.cpu_count() or 1
-    o = make_oracle(sc, threads)
+    full = args.scene in ("c2", "c2-small")
+    if full:
+        # the full configuration, advanced by the same settle steps as the
+        # GPU arm before its timed steps
+        o, sc, label, settle_info = full_config_oracle(args, threads)
+    else:
+        # bounded sample per step: a smaller block of the workload
+        sc, label = cpu_sample_scene(args)
+        o = make_oracle(sc, threads)
     for _ in range(args.warmup):
         o.step()
     t0 = time.perf_counter()
     iters = 0
+    at_max = 0
+    max_err = 0.0
+    p = o.params
     for _ in range(args.steps):
-        iters += o.step().iterations
+        info = o.step()
+        iters += info.iterations
+        at_max += int(info.iterations >= p.max_loops)
+        max_err = max(max_err, float(info.density_error_percent))
     dt = time.perf_counter() - t0
     o.close()
     v = dynamic_count(sc) * args.steps / dt
+    cfg = {"workload": workload_name(args), "mean_iterations": iters / max(args.steps, 1),
+           **({"dt": C1_DT, "dt_note": C1_NOTE} if args.scene == "c1" else {})}
+    if full:
+        cfg.update({"fluid_particles": sc.n_fluid, "boundary_particles": sc.n_boundary, **settle_info,
+                    "state": label, "steps_at_max_loops": at_max,
+                    "max_step_density_error_percent": max_err, "same_config": True})
+    else:
+        cfg.update({"sample_fluid_particles": sc.n_fluid, "sample_boundary_particles": sc.n_boundary,
+                    "same_config": False})
     print(json.dumps({
         "impl": "reference", "metric": metric_for(args), "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": workload_name(args), "sample_fluid_particles": sc.n_fluid,
-                                        "sample_boundary_particles": sc.n_boundary,
-                                        "mean_iterations": iters / max(args.steps, 1),
-                                        **({"dt": C1_DT, "dt_note": C1_NOTE} if args.scene == "c1" else {})},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+        "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
                          "sample": "%s: %d dynamic + %d boundary per step" % (label, dynamic_count(sc),
                                                                               sc.n_boundary)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -758,12 +854,12 @@ def run_ours(args, rank, world, local_rank):
     nf, nb = sc.n_fluid, sc.n_boundary
     nd = dynamic_count(sc)
 
-    # optional settle: during the first ~150 steps (the dam's collapse) the
-    # loop runs into its 50-iteration cap with density errors above 1%;
-    # --settle N advances N untimed steps first so that the timed steps meet
-    # the 1% criterion (default 0: both arms time the same steps from rest)
-    if args.settle:
-        s.step(args.settle)
+    # the timed steps start from the state after the settle steps (the
+    # dam's collapse runs its loop into the 50-iteration cap above 1% density
+    # error); the reference arm times the same state
+    settle = settle_steps(args)
+    if settle:
+        s.step(settle)
         s.synchronize()
 
     # warm-up, then the launch-shape autotuner on the warmed state (untimed;
@@ -827,16 +923,21 @@ def run_ours(args, rank, world, local_rank):
         kname, kms, kbytes = "k_wcsph_force_integrate", pr.integrate_ms, (16 + 16 + 4 + 4 + 16 + 16 + 4) * nf
     achieved = kbytes / (kms / 1e3) / 1e9
     step_bytes = algorithmic_bytes(nf, nb, args.steps, total_iters, method)
-    # DRAM bytes per fluid particle per launch from one ncu capture of the same
-    # kernels at the tuned shapes (profiles/pcisph_loop_kernels_262k_tuned_ncu.md),
-    # scaled by the fluid count: the list length per particle does not depend
-    # on the scene size
+    # DRAM bytes per fluid particle per launch, measured by one ncu capture
+    # of the same kernels at the tuned shapes on the 262k-fluid dam and
+    # scaled here by the fluid count (the list length per particle does not
+    # depend on the scene size); not measured in this run
     traffic_per_particle = {"k_pcisph_density": 156.0, "k_pcisph_pressure_force": 276.0}
     traffic = traffic_per_particle[kname] * nf if kname in traffic_per_particle else None
+    traffic_source = ("ncu dram__bytes_read+write per fluid particle on the 262k-fluid dam, scaled to %d fluid "
+                      "particles" % nf) if traffic is not None else None
 
     # end to end through the C ABI with host buffers, over the same steps as
-    # the timed region (restored from the checkpoint): per step, upload the
-    # state from pinned host memory, step, read the result back
+    # the timed region (restored from the checkpoint): every step uploads its
+    # input positions and velocities from pinned host memory, steps, and
+    # reads its result back into pinned host memory; the next step's input
+    # is that readback, so the host carries the trajectory from frame to
+    # frame and the steps are the timed region's steps
     e2e = None
     if not args.no_e2e:
         s.restore(0)
@@ -852,13 +953,9 @@ def run_ours(args, rank, world, local_rank):
         fp = C.POINTER(C.c_float)
         cnt = C.c_uint32()
 
-        # every frame uploads an input frame from pinned host memory (the
-        # warmed state read back once before the timed region) and reads
-        # its result back into pinned host memory; upf_*_async run the
-        # copies on the library's copy streams, overlapping the steps
-        ipos = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
-        ivel = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
-
+        # upf_*_async run the copies on the library's copy streams; the
+        # host waits for each readback before it uploads it as the next
+        # step's input, so copies and steps alternate
         def readback():
             upf.check(L.upf_get_particles_async(s.handle, C.cast(hpos.data_ptr(), fp), C.cast(hvel.data_ptr(), fp),
                                                 C.cast(hden.data_ptr(), fp), C.cast(hpre.data_ptr(), fp),
@@ -866,10 +963,9 @@ def run_ours(args, rank, world, local_rank):
                                                 C.cast(hid.data_ptr(), C.POINTER(C.c_uint32)), C.byref(cnt)),
                       "upf_get_particles_async")
 
-        readback()
+        readback()  # the first step's input: the state at the checkpoint
         upf.check(L.upf_wait_frames(s.handle), "upf_wait_frames")
-        ipos.copy_(hpos)
-        ivel.copy_(hvel)
+        s.reset_counters()
         k_e2e = args.steps
         barrier()
         torch.cuda.synchronize()
@@ -877,17 +973,21 @@ def run_ours(args, rank, world, local_rank):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(k_e2e):
-            upf.check(L.upf_upload_state_async(s.handle, C.cast(ipos.data_ptr(), fp), C.cast(ivel.data_ptr(), fp), n),
+            upf.check(L.upf_upload_state_async(s.handle, C.cast(hpos.data_ptr(), fp), C.cast(hvel.data_ptr(), fp), n),
                       "upf_upload_state_async")
             s.step(1)
             readback()
-        upf.check(L.upf_wait_frames(s.handle), "upf_wait_frames")
+            upf.check(L.upf_wait_frames(s.handle), "upf_wait_frames")
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1))[0]
+        st_e2e = s.stats()
         e2e = {"value": nd * k_e2e * world / (e2e_ms / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * (16 + 16 + 4 + 4 + 4 + 4),
-               "steps": k_e2e}
+               "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e,
+               "input_of_each_step": "the previous step's readback (host round trip every step)",
+               "same_steps_as_value": bool(st_e2e.total_iterations == total_iters
+                                           and st_e2e.total_steps == stats.total_steps)}
 
     if rank != 0:
         s.close()
@@ -906,14 +1006,18 @@ def run_ours(args, rank, world, local_rank):
                    "dynamic_particles": nd, "rigid_bodies": int(sc.num_bodies),
                    "h": float(p.support_radius), "dt": float(p.dt),
                    **({"dt_note": C1_NOTE} if args.scene == "c1" else {}), "block_size": int(p.block_size),
-                   "settle_steps": args.settle, "mean_iterations": mean_k,
+                   "settle_steps": settle, "mean_iterations": mean_k,
                    "steps_at_max_loops": stats.steps_at_max_loops,
+                   "max_step_density_error_percent": float(stats.max_step_density_error_percent),
+                   "density_criterion_met_every_step": bool(method == "pcisph" and stats.steps_at_max_loops == 0
+                                                            and stats.max_step_density_error_percent < p.max_density_error),
                    "last_density_error_percent": float(stats.density_error_percent),
                    "parallelism": "replicas" if world > 1 else "single",
                    "launch_config": tuned,
                    "l2": "inputs larger than L2 (neighbour lists %.0f MB)" % (sc.n * p.max_neighbors * 4 / 1e6)},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                     "traffic_source": traffic_source,
                      "kernel_ms": kms, "algorithmic_bytes_per_launch": kbytes,
                      "step_achieved_gbs": step_bytes / (max_ms / 1e3) / 1e9 / world * world,
                      "step_frac": step_bytes / (max_ms / 1e3) / 1e9 / peak},
@@ -925,7 +1029,10 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
+        dam = args.scene in ("c2", "c2-small")
+        if dam:
+            s.restore(0)  # the state at the start of the timed steps
+        out["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds, system=s if dam else None)
     print(json.dumps(out), flush=True)
     s.close()
 
@@ -940,9 +1047,10 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--batch-scenes", type=int, default=256)
     ap.add_argument("--block-size", type=int, default=0)
-    ap.add_argument("--settle", type=int, default=0,
-                    help="untimed steps before the warm-up, e.g. 300 to time steps after the dam's initial "
-                         "collapse (the CPU reference arm always times steps from rest)")
+    ap.add_argument("--settle", type=int, default=-1,
+                    help="steps from rest before the warm-up (default: the workload's settle count, after which "
+                         "the dam's loop meets the 1%% criterion; 0 = time from rest); both arms time the state "
+                         "after them")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--shape", default="", help="fixed launch shapes instead of the autotuner: "

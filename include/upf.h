@@ -173,7 +173,7 @@ typedef struct upf_step_stats {
   int32_t total_steps;
   int32_t total_iterations;
   int32_t steps_at_max_loops;
-  int32_t reserved;
+  float max_step_density_error_percent;  /* largest density_error_percent of those steps (PCISPH) */
 } upf_step_stats;
 
 typedef struct upf_system upf_system;
@@ -308,8 +308,10 @@ upf_status upf_state_load(upf_system* s, const void* host, size_t bytes);
  * method, FNV-1a checksum). To resume in another process: create a system
  * with the stored parameters (upf_state_file_info), set the same scene's
  * particles, then upf_state_read_file; stepping on continues bit for bit.
- * A file from a system of other counts or method is refused
- * (UPF_ERR_INVALID_ARG); a damaged file gives UPF_ERR_IO. */
+ * A file from a system of other counts, method or parameters (any
+ * upf_params field but the reserved words) is refused (UPF_ERR_INVALID_ARG,
+ * the message names the first differing field); a damaged file gives
+ * UPF_ERR_IO. */
 upf_status upf_state_write_file(upf_system* s, const char* path);
 upf_status upf_state_read_file(upf_system* s, const char* path);
 upf_status upf_state_file_info(const char* path, upf_params* params, uint32_t* n_dynamic, uint32_t* num_bodies,
@@ -510,7 +512,10 @@ upf_status upf_radix_sort_pairs(uint32_t* keys_dev, uint32_t* vals_dev, uint32_t
  * device, with the device current); make that first call before any stream
  * capture. All calls share the one array and it keeps the last call's
  * contents: calls that overlap on the GPU (different streams or host threads
- * without ordering between them) race on it. */
+ * without ordering between them) race on it. The looked-up address is kept
+ * for the life of the process: do not call this after a cudaDeviceReset (or
+ * any teardown of the device's primary context) in the same process, since the
+ * array then lives at a new address the library does not know. */
 #define UPF_NOALLOC_MAX_PAIRS (1u << 21)
 upf_status upf_radix_sort_pairs_noalloc(uint32_t* keys_dev, uint32_t* vals_dev, uint32_t n,
                                         int32_t key_bits, void* stream);

@@ -17,17 +17,28 @@ from unifiedparticleframeworkcuda_b200._abi import UpfParams
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REFLIB = os.path.join(HERE, "_ref", "libupfref.so")
-REFERENCE_SRC = "/root/reference/src"
+
 
 _lib = None
 _ref = None
+
+
+def reference_dir() -> str:
+    """The reference tree oracle/Makefile compiles the pins from: the
+    environment's UPF_REFERENCE, else the recipe's default location."""
+    r = subprocess.run(["make", "-s", "-C", HERE, "refdir"], capture_output=True, text=True, check=True)
+    return r.stdout.strip()
+
+
+def reference_present() -> bool:
+    return os.path.isdir(os.path.join(reference_dir(), "src"))
 
 
 def build(with_ref: bool = True) -> None:
     """Compile the oracle (and the reference pins when the reference tree is
     present) with oracle/Makefile."""
     targets = ["all"]
-    if with_ref and os.path.isdir(REFERENCE_SRC):
+    if with_ref and reference_present():
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
@@ -77,6 +88,8 @@ def lib():
         L.orc_count.argtypes = [C.c_void_p]
         L.orc_count.restype = C.c_uint32
         L.orc_keep_fields.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_lagged.argtypes = [C.c_void_p, fp, fp]
+        L.orc_set_lagged.restype = None
         L.orc_get.argtypes = [C.c_void_p, fp, fp, fp, fp, i32p, u32p, u32p]
         L.orc_get_step_fields.argtypes = [C.c_void_p, fp, fp, fp, fp, fp, fp, u32p]
         L.orc_neighbors.argtypes = [C.c_void_p, u32p, u32p, C.c_uint32]
@@ -227,6 +240,14 @@ class OracleSim:
             self.close()
         except Exception:
             pass
+
+    def set_lagged(self, pressure, density):
+        """Continue from another run's state: its last step's correction
+        pressure and predicted density per particle, in creation order."""
+        pressure = np.ascontiguousarray(pressure, np.float32)
+        density = np.ascontiguousarray(density, np.float32)
+        assert pressure.shape == (self.n,) and density.shape == (self.n,)
+        lib().orc_set_lagged(self._h, _ptr(pressure, C.c_float), _ptr(density, C.c_float))
 
     def step(self) -> StepInfo:
         info = StepInfo()

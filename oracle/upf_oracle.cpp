@@ -290,6 +290,7 @@ struct SimBase {
   virtual int set_bodies(const int32_t*, uint32_t, uint32_t) = 0;
   virtual int get_rigid(float*, float*, float*, float*) const = 0;
   virtual void set_keep_fields(bool on) = 0;
+  virtual void set_lagged(const float*, const float*) = 0;
 };
 
 template <class R>
@@ -987,6 +988,16 @@ struct Sim : SimBase {
 
   uint32_t count() const override { return (uint32_t)ps.size(); }
 
+  // Resume a PCISPH run from another run's state: the correction pressure
+  // and predicted density of its last step, per particle in creation order
+  // (the lagged values of UnifiedPhysics.cpp:5360-5363 at the next step).
+  void set_lagged(const float* pressure, const float* density) override {
+    for (Particle<R>& p : ps) {
+      p.p_corr = p.p_prev = R(pressure[p.id]);
+      p.rho_star = p.rho_prev = R(density[p.id]);
+    }
+  }
+
   void get(float* pos4, float* vel4, float* density, float* pressure, int32_t* type, uint32_t* id,
            uint32_t* key) const override {
     for (size_t i = 0; i < ps.size(); ++i) {
@@ -1346,6 +1357,10 @@ int orc_step(orc_sim* s, orc_step_info* info) {
 uint32_t orc_count(const orc_sim* s) { return s->impl->count(); }
 
 void orc_keep_fields(orc_sim* s, int on) { s->impl->set_keep_fields(on != 0); }
+
+void orc_set_lagged(orc_sim* s, const float* pressure, const float* density) {
+  s->impl->set_lagged(pressure, density);
+}
 
 void orc_get(const orc_sim* s, float* pos4, float* vel4, float* density, float* pressure,
              int32_t* type, uint32_t* id, uint32_t* key) {

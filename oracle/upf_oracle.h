@@ -55,6 +55,9 @@ int orc_step(orc_sim* s, orc_step_info* info);
 uint32_t orc_count(const orc_sim* s);
 /* keep a copy of the step-start fields of every step (for orc_get_step_fields) */
 void orc_keep_fields(orc_sim* s, int on);
+/* continue from another run's state: last-step correction pressure and
+ * predicted density per particle, in creation order */
+void orc_set_lagged(orc_sim* s, const float* pressure, const float* density);
 /* current array order (sorted by key at the end of the last step) */
 void orc_get(const orc_sim* s, float* pos4, float* vel4, float* density, float* pressure,
              int32_t* type, uint32_t* id, uint32_t* key);

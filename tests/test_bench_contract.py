@@ -26,7 +26,10 @@ def _line(out):
 
 @pytest.mark.parametrize("scene", ["c1", "c2"])
 def test_reference_arm_line(scene):
-    r = _run(["--impl", "reference", "--scene", scene, "--steps", "2", "--warmup", "1"])
+    # c2 at its full size, advanced on the host cores by one settle step
+    # (the default settle count takes minutes on a small host)
+    extra = ["--settle", "1"] if scene == "c2" else []
+    r = _run(["--impl", "reference", "--scene", scene, "--steps", "2", "--warmup", "1"] + extra)
     assert r.returncode == 0, r.stderr[-2000:]
     d = _line(r.stdout)
     for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
@@ -40,8 +43,13 @@ def test_reference_arm_line(scene):
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    assert cb["cpu_model"]
     if scene == "c1":
         assert d["config"]["dt"] == 5e-4 and "dt_note" in d["config"]
+    if scene == "c2":
+        # the full configuration, not a sample, after the settle steps
+        assert d["config"]["same_config"] is True and d["config"]["fluid_particles"] == 1048576
+        assert d["config"]["settle_steps"] == 1
 
 
 def test_gpu_arm_fails_loudly_without_a_gpu():

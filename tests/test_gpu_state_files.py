@@ -78,6 +78,14 @@ def test_foreign_or_damaged_state_files_are_refused(upf_lib, tmp_path):
         with pytest.raises(UpfError) as e:
             c.read_state_file(path)
         assert e.value.status == CODE["UPF_ERR_INVALID_ARG"]
+    # the same scene under another time step: the snapshot would resume
+    # under the wrong physics, so it is refused and the field is named
+    changed = scenes.small_pcisph()
+    changed.params.dt = sc.params.dt * 0.5
+    with _system(upf_lib, changed) as d:
+        with pytest.raises(UpfError) as e:
+            d.read_state_file(path)
+        assert e.value.status == CODE["UPF_ERR_INVALID_ARG"] and "dt" in str(e.value)
 
 
 def test_text_dumps_of_a_device_state(upf_lib, tmp_path):

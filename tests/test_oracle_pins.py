@@ -10,6 +10,8 @@ import os
 import numpy as np
 import pytest
 
+from oracle import pyoracle
+
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_tables.npz")
 GOLDEN_RIGID = os.path.join(os.path.dirname(__file__), "golden", "reference_rigid.npz")
 
@@ -107,7 +109,7 @@ def test_morton_key_of_position(oracle_lib, golden):
         assert oracle_lib.lib().orc_morton(C.byref(p), *map(float, x)) == want
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src"), reason="reference tree not present")
+@pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
 def test_fixtures_regenerate_identically(oracle_lib, golden):
     """The committed fixtures are what the compiled reference produces now."""
     R = oracle_lib.ref()

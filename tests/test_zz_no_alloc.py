@@ -39,9 +39,11 @@ def _sort_noalloc(upf, torch, keys, vals, bits):
 def test_noalloc_sort_matches_scratch_sort_two_calls(upf_lib):
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(2024)
-    # two calls in a row: the second smaller and with other bits, so any
-    # stale contents of the shared scratch would show up
-    for n, bits in ((1_000_003, 30), (262_147, 24)):
+    # calls in a row: the second smaller and with other bits, so any stale
+    # contents of the shared scratch would show up; the third at exactly the
+    # maximum with full 32-bit keys, where the largest tiles run and the
+    # alternate buffers and digit counts end at the end of the fixed array
+    for n, bits in ((1_000_003, 30), (262_147, 24), (1 << 21, 32)):
         keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
         keys[: n // 10] = keys[0]  # many equal keys: stability matters
         vals = np.arange(n, dtype=np.uint32)

@@ -112,7 +112,7 @@ class UpfStepStats(C.Structure):
         ("total_steps", C.c_int32),
         ("total_iterations", C.c_int32),
         ("steps_at_max_loops", C.c_int32),
-        ("reserved", C.c_int32),
+        ("max_step_density_error_percent", C.c_float),
     ]
 
 

@@ -1133,6 +1133,7 @@ upf_status upf_get_step_stats(upf_system* s, upf_step_stats* out) {
   out->total_steps = d.total_steps;
   out->total_iterations = d.total_iterations;
   out->steps_at_max_loops = d.steps_at_max;
+  out->max_step_density_error_percent = d.max_step_err;
   return st;
 }
 

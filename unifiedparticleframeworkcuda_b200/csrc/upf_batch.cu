@@ -421,6 +421,7 @@ upf_status upf_batch_get_stats(upf_batch* b, upf_step_stats* out) {
     o.total_steps = d.total_steps;
     o.total_iterations = d.total_iterations;
     o.steps_at_max_loops = d.steps_at_max;
+    o.max_step_density_error_percent = d.max_step_err;
   }
   return rc;
 }
@@ -430,7 +431,10 @@ upf_status upf_batch_reset_counters(upf_batch* b) {
   std::vector<DevState> h(b->n_scenes);
   UPF_CUDA(cudaMemcpyAsync(h.data(), b->st_d, sizeof(DevState) * b->n_scenes, cudaMemcpyDeviceToHost, b->stream));
   UPF_CUDA(cudaStreamSynchronize(b->stream));
-  for (DevState& d : h) d.total_steps = d.total_iterations = d.steps_at_max = 0;
+  for (DevState& d : h) {
+    d.total_steps = d.total_iterations = d.steps_at_max = 0;
+    d.max_step_err = 0.0f;
+  }
   UPF_CUDA(cudaMemcpyAsync(b->st_d, h.data(), sizeof(DevState) * b->n_scenes, cudaMemcpyHostToDevice, b->stream));
   UPF_CUDA(cudaStreamSynchronize(b->stream));
   return UPF_OK;

@@ -89,6 +89,7 @@ struct DevState {
   int32_t total_steps;
   int32_t total_iterations;
   int32_t steps_at_max;
+  float max_step_err;      // largest final density error (percent) of the steps counted above
   int32_t loop_active;     // batched scenes: the scene's predict-correct loop still runs
 };
 

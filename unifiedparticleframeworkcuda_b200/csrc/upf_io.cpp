@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -736,6 +737,33 @@ upf_status upf_state_file_info(const char* path, upf_params* params, uint32_t* n
   return UPF_OK;
 }
 
+// The name of the first parameter whose stored bits differ between a and b
+// (the reserved words are not compared), or null if they all match.
+static const char* first_param_difference(const upf_params& a, const upf_params& b) {
+  static const struct {
+    size_t off, size;
+    const char* name;
+  } fields[] = {
+#define UPF_FIELD(f) {offsetof(upf_params, f), sizeof(((upf_params*)nullptr)->f), #f}
+      UPF_FIELD(method), UPF_FIELD(flags), UPF_FIELD(particle_spacing), UPF_FIELD(particle_radius),
+      UPF_FIELD(support_radius), UPF_FIELD(mass), UPF_FIELD(rest_density), UPF_FIELD(gas_constant),
+      UPF_FIELD(gamma), UPF_FIELD(viscosity), UPF_FIELD(gravity), UPF_FIELD(dt), UPF_FIELD(density_error_factor),
+      UPF_FIELD(density_error_fudge), UPF_FIELD(max_density_error), UPF_FIELD(min_loops), UPF_FIELD(max_loops),
+      UPF_FIELD(surface_tension_gamma), UPF_FIELD(surface_adhesion_beta), UPF_FIELD(force_distance),
+      UPF_FIELD(max_boundary_force), UPF_FIELD(spring_coefficient), UPF_FIELD(spring_coefficient_boundary),
+      UPF_FIELD(damping_coefficient), UPF_FIELD(terminal_speed), UPF_FIELD(granular_kr), UPF_FIELD(granular_kd),
+      UPF_FIELD(granular_kt), UPF_FIELD(granular_mu), UPF_FIELD(zindex_origin), UPF_FIELD(zindex_extent),
+      UPF_FIELD(scales), UPF_FIELD(block_size), UPF_FIELD(collision_min), UPF_FIELD(collision_max),
+      UPF_FIELD(container_min), UPF_FIELD(container_max), UPF_FIELD(max_neighbors), UPF_FIELD(search_cell),
+#undef UPF_FIELD
+  };
+  const char* pa = reinterpret_cast<const char*>(&a);
+  const char* pb = reinterpret_cast<const char*>(&b);
+  for (const auto& f : fields)
+    if (std::memcmp(pa + f.off, pb + f.off, f.size) != 0) return f.name;
+  return nullptr;
+}
+
 upf_status upf_state_read_file(upf_system* s, const char* path) {
   const char* who = "upf_state_read_file";
   if (!s || !path) {
@@ -780,6 +808,14 @@ upf_status upf_state_read_file(upf_system* s, const char* path) {
   if (fnv1a(state.data(), bytes, fnv1a(&prm, sizeof prm)) != h.checksum) {
     set_error("%s: %s fails its checksum (corrupted)", who, path);
     return UPF_ERR_IO;
+  }
+  // a snapshot resumes only under the physics it was saved with: every
+  // parameter word up to the reserved tail must match the system's own
+  const char* field = first_param_difference(prm, mine);
+  if (field) {
+    set_error("%s: %s was saved with different parameters (%s differs); create the system with the file's "
+              "parameters (upf_state_file_info returns them)", who, path, field);
+    return UPF_ERR_INVALID_ARG;
   }
   return upf_state_load(s, state.data(), bytes);
 }

@@ -1093,6 +1093,7 @@ __device__ __forceinline__ int loop_ctl(const DevParams& P, DevState* st) {
     st->total_steps += 1;
     st->total_iterations += it;
     if (it >= P.max_loops) st->steps_at_max += 1;
+    if (e > st->max_step_err) st->max_step_err = e;
   }
   return cont;
 }

@@ -5,8 +5,9 @@
 // k..k+R-1 of a warp's 32 consecutive particles form a 2D box of 32 x R
 // elements. Lane 0 of each warp issues one 2D tensor copy per box into a ring
 // of kStages shared-memory stages; every lane waits on the stage's mbarrier
-// (bounded: a wait that runs out records ERR_TIMEOUT and the pass goes on
-// without that data rather than hanging). Only loads from this GPU's own
+// (bounded: a wait that runs out records ERR_TIMEOUT, and the warp stops its
+// walk, drains the copies it issued and goes on without that data rather
+// than hanging). Only loads from this GPU's own
 // memory, no cluster multicast.
 #pragma once
 
@@ -101,7 +102,11 @@ __device__ __forceinline__ void ring_issue(WarpListRing<kWithBins, kRows>& r, co
 
 // Walks the warp's lists chunk by chunk. `body(s, rows)` consumes stage s
 // (rows valid rows); lanes index their own column. Returns false if a wait
-// ran out.
+// ran out: the warp then issues no further copy, skips the remaining chunks,
+// and waits (again bounded) for the copies it already issued, so that none
+// lands in the ring after the warp has moved on.
+constexpr uint64_t kDrainLimitNs = 100000000ull;  // 0.1 s per issued stage when draining after a timeout
+
 template <bool kWithBins, int kRows, class Body>
 __device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins, kRows>& r, const CUtensorMap* cmap,
                                           const CUtensorMap* bmap, int col0, uint32_t warp_max_cnt, Body&& body) {
@@ -110,16 +115,23 @@ __device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins, kRows>& r, con
   if (lane == 0) {
     for (int c = 0; c < kListStages && c < nchunks; ++c) ring_issue(r, cmap, bmap, c, col0);
   }
-  bool ok = true;
-  for (int c = 0; c < nchunks; ++c) {
+  int c = 0;
+  for (; c < nchunks; ++c) {
     const int s = c % kListStages;
     const uint32_t parity = (uint32_t)(c / kListStages) & 1u;
-    ok = mbar_wait(&r.full[s], parity) && ok;
+    // warp-uniform decision: every lane consumes the stage, or none does
+    if (!__all_sync(0xffffffffu, mbar_wait(&r.full[s], parity))) break;
     body(s, c * kRows);
     __syncwarp();
     if (lane == 0 && c + kListStages < nchunks) ring_issue(r, cmap, bmap, c + kListStages, col0);
   }
-  return ok;
+  if (c == nchunks) return true;
+  // chunks c .. issued-1 were issued and not consumed
+  const int issued = (c + kListStages < nchunks) ? c + kListStages : nchunks;
+  for (int d = c; d < issued; ++d)
+    (void)mbar_wait(&r.full[d % kListStages], (uint32_t)(d / kListStages) & 1u, kDrainLimitNs);
+  __syncwarp();
+  return false;
 }
 
 template <bool kWithBins, int kRows>
