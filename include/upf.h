@@ -465,6 +465,16 @@ upf_status upf_autotune(upf_system* s, int32_t repeats, upf_launch_config* chose
  * pos4/vel4/force4/pforce4: n x 4 floats. Returns count in *n_out. */
 upf_status upf_get_particles(upf_system* s, float* pos4, float* vel4, float* density,
                              float* pressure, int32_t* type, uint32_t* id, uint32_t* n_out);
+/* Every particle of the last upf_set_particles call (n = its count), at its
+ * input index: dynamic particles from the current state, boundary (FROZEN)
+ * particles at their fixed positions with zero velocity, rest density and
+ * zero pressure. pos4.w holds the particle's Morton key as a float (the
+ * reference keeps the z-index in pos.w). The permutation back to input order
+ * runs on the device. The readback of CopyParticlesCUDA
+ * (src/gpu/particles.cu:62-72) for a caller that indexes particles by the
+ * order it uploaded them in; any pointer may be NULL. */
+upf_status upf_get_particles_input_order(upf_system* s, float* pos4, float* vel4, float* density,
+                                        float* pressure, int32_t* type, uint32_t n);
 /* Per-particle step fields of the last step, in the sorted order of that step:
  * external force, correction pressure force, predicted density. */
 upf_status upf_get_step_fields(upf_system* s, float* force4, float* pforce4,

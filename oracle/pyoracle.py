@@ -43,6 +43,12 @@ def build(with_ref: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
+# the reference's own rule where the restatement deviates (orc_set_reference_literal)
+LITERAL_GRANULAR_TANGENTIAL_ONLY = 1
+LITERAL_OWN_BODY_SPRING = 2
+LITERAL_ZERO_INVERSE_INERTIA = 4
+
+
 class StepInfo(C.Structure):
     _fields_ = [
         ("iterations", C.c_int32),
@@ -88,6 +94,8 @@ def lib():
         L.orc_count.argtypes = [C.c_void_p]
         L.orc_count.restype = C.c_uint32
         L.orc_keep_fields.argtypes = [C.c_void_p, C.c_int]
+        L.orc_set_reference_literal.argtypes = [C.c_void_p, C.c_uint32]
+        L.orc_set_reference_literal.restype = None
         L.orc_set_lagged.argtypes = [C.c_void_p, fp, fp]
         L.orc_set_lagged.restype = None
         L.orc_get.argtypes = [C.c_void_p, fp, fp, fp, fp, i32p, u32p, u32p]
@@ -240,6 +248,11 @@ class OracleSim:
             self.close()
         except Exception:
             pass
+
+    def set_reference_literal(self, mask: int):
+        """Switch deviations back to the reference's literal rule (the
+        LITERAL_* bits; before set_rigid_bodies for the inertia bit)."""
+        lib().orc_set_reference_literal(self._h, int(mask))
 
     def set_lagged(self, pressure, density):
         """Continue from another run's state: its last step's correction

@@ -291,6 +291,7 @@ struct SimBase {
   virtual int get_rigid(float*, float*, float*, float*) const = 0;
   virtual void set_keep_fields(bool on) = 0;
   virtual void set_lagged(const float*, const float*) = 0;
+  virtual void set_literal(uint32_t mask) = 0;
 };
 
 template <class R>
@@ -304,6 +305,7 @@ struct Sim : SimBase {
   R lut_factor;                       // static float factor = 1.0 / h (WeightingKernel.cpp:124)
   int threads;
   bool keep_fields = false;           // snapshot step-start fields for parity tests
+  uint32_t literal = 0;               // ORC_LITERAL_*: the reference's own rule where this build deviates
 
   // ---- lookup tables (WeightingKernel::kernel*Lut, WeightingKernel.cpp:122-128 etc.)
   inline R lut(int k, R d) const {
@@ -751,7 +753,9 @@ struct Sim : SimBase {
       if (!(d < h)) continue;
       unsigned dl = dist_lut(d);
       if (q.type == UPF_RIGID) {
-        if (q.body == p.body) continue;
+        // literal: every rigid neighbour, the particle's own body included
+        // (UnifiedPhysics.cpp:5300-5311)
+        if (q.body == p.body && !(literal & ORC_LITERAL_OWN_BODY_SPRING)) continue;
         const R overlap = R(2.0f) * R(prm.particle_radius) - d;
         if (overlap > R(0.00001f)) {
           // CalculateSpringForceHost / CalculateDampingForceHost (UnifiedPhysics.cpp:2010-2030)
@@ -802,9 +806,16 @@ struct Sim : SimBase {
         const R fn = -R(prm.granular_kd) * ksiDot - R(prm.granular_kr) * ksi;
         const V3<R> Fn = N * fn;
         const R vtl = normalize(Vt);
-        const R t = std::min(R(prm.granular_mu) * std::fabs(fn), R(prm.granular_kt) * vtl);
-        const V3<R> Ft = Vt * (-t);
-        p.F = p.F + (Fn + Ft);
+        if (literal & ORC_LITERAL_GRANULAR_TANGENTIAL_ONLY) {
+          // literal (UnifiedPhysics.cpp:3276-3287): the friction bound uses
+          // the signed f_n and only F_t is added
+          const R t = std::min(R(prm.granular_mu) * fn, R(prm.granular_kt) * vtl);
+          p.F = p.F + Vt * (-t);
+        } else {
+          const R t = std::min(R(prm.granular_mu) * std::fabs(fn), R(prm.granular_kt) * vtl);
+          const V3<R> Ft = Vt * (-t);
+          p.F = p.F + (Fn + Ft);
+        }
       } else if (q.type == UPF_LIQUID) {
         if (prm.flags & UPF_FLAG_BOUNDARY_PRESSURE)
           p.F = p.F - boundary_pressure(d, q.x, p.x, q.rho_prev, q.p_prev, q.wvol);
@@ -1041,6 +1052,7 @@ struct Sim : SimBase {
   }
 
   void set_keep_fields(bool on) override { keep_fields = on; }
+  void set_literal(uint32_t mask) override { literal = mask; }
   // Rigid body assembly (AddToRigidBody UnifiedPhysics.cpp:825-885, inverse
   // Matrix3x3::CalculateInverse Matrix3x3.cpp:121-156, relative positions
   // UnifiedPhysics.cpp:150-158): mass, centre of mass, momenta and inertia are
@@ -1101,7 +1113,11 @@ struct Sim : SimBase {
       B.q[0] = 1;
       for (int i = 0; i < 3; ++i) {
         B.rot[i][i] = 1;
-        for (int j = 0; j < 3; ++j) B.inv_inertia_local[i][j] = R(inv[3 * i + j]);
+        // literal: CalculateInverse writes into the temporary that
+        // inverted_inertia_local() returns (UnifiedPhysics.cpp:150), so the
+        // body's local inverse inertia keeps its zero initial value
+        for (int j = 0; j < 3; ++j)
+          B.inv_inertia_local[i][j] = (literal & ORC_LITERAL_ZERO_INVERSE_INERTIA) ? R(0) : R(inv[3 * i + j]);
       }
     }
     for (uint32_t id = 0; id < n; ++id) {
@@ -1357,6 +1373,8 @@ int orc_step(orc_sim* s, orc_step_info* info) {
 uint32_t orc_count(const orc_sim* s) { return s->impl->count(); }
 
 void orc_keep_fields(orc_sim* s, int on) { s->impl->set_keep_fields(on != 0); }
+
+void orc_set_reference_literal(orc_sim* s, uint32_t mask) { s->impl->set_literal(mask); }
 
 void orc_set_lagged(orc_sim* s, const float* pressure, const float* density) {
   s->impl->set_lagged(pressure, density);

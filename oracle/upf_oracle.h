@@ -55,6 +55,19 @@ int orc_step(orc_sim* s, orc_step_info* info);
 uint32_t orc_count(const orc_sim* s);
 /* keep a copy of the step-start fields of every step (for orc_get_step_fields) */
 void orc_keep_fields(orc_sim* s, int on);
+/* The reference's own rule where the restatement deviates on purpose, one
+ * bit per deviation (set before orc_set_rigid_bodies for the inertia bit):
+ *   GRANULAR_TANGENTIAL_ONLY  grains add only F_t, friction bound mu * f_n
+ *                             with the signed f_n (UnifiedPhysics.cpp:3276-3287)
+ *   OWN_BODY_SPRING           the rigid spring-damper acts between particles
+ *                             of the same body too (UnifiedPhysics.cpp:5300-5311)
+ *   ZERO_INVERSE_INERTIA      the local inverse inertia stays zero, as the
+ *                             reference's inverse lands in a temporary
+ *                             (UnifiedPhysics.cpp:150) */
+#define ORC_LITERAL_GRANULAR_TANGENTIAL_ONLY 1u
+#define ORC_LITERAL_OWN_BODY_SPRING 2u
+#define ORC_LITERAL_ZERO_INVERSE_INERTIA 4u
+void orc_set_reference_literal(orc_sim* s, uint32_t mask);
 /* continue from another run's state: last-step correction pressure and
  * predicted density per particle, in creation order */
 void orc_set_lagged(orc_sim* s, const float* pressure, const float* density);

@@ -14,11 +14,9 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 INCLUDE = os.path.join(ROOT, "include")
 
 
-def declared_functions():
+def declared_functions(headers=("upf.h",)):
     names = set()
-    for f in sorted(os.listdir(INCLUDE)):
-        if not f.endswith(".h"):
-            continue
+    for f in headers:
         src = open(os.path.join(INCLUDE, f)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([a-zA-Z_]\w*)\s*\(", src, flags=re.M):
@@ -33,6 +31,18 @@ def test_library_exports_every_declared_function(upf_lib):
     lib = upf_lib.lib()
     names = declared_functions()
     assert "upf_create" in names and "upf_step" in names
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_compat_library_exports_every_declared_function(upf_lib):
+    """include/upf_compat.h (the reference's own entry points) against
+    libupf_compat.so; CopyParticleDataHostToDevice is compiled by the caller
+    (compat/upf_compat_particles.cpp reads the caller's particle class)."""
+    assert sorted(f for f in os.listdir(INCLUDE) if f.endswith(".h")) == ["upf.h", "upf_compat.h"]
+    lib = C.CDLL(os.path.join(os.path.dirname(upf_lib.LIBPATH), "libupf_compat.so"))
+    names = declared_functions(("upf_compat.h",)) - {"CopyParticleDataHostToDevice"}
+    assert {"ParticlePhysicsOnDevicePCISPH", "CopyParticlesCUDA", "FreeDeviceArrays", "RadixSort"} <= names
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
 

@@ -64,6 +64,7 @@ def lib():
             "upf_phase_predict_correct": [vp],
             "upf_phase_integrate": [vp],
             "upf_get_particles": [vp, fp, fp, fp, fp, i32p, u32p, u32p],
+            "upf_get_particles_input_order": [vp, fp, fp, fp, fp, i32p, C.c_uint32],
             "upf_get_step_fields": [vp, fp, fp, fp, u32p, u32p],
             "upf_get_neighbors": [vp, u32p, u32p, C.c_uint32, u32p],
             "upf_get_sorted_keys": [vp, u32p, u32p, u32p],
@@ -414,6 +415,21 @@ class ParticleSystem:
                                       _p(pre, C.c_float), _p(typ, C.c_int32), _p(ids, C.c_uint32), C.byref(cnt)),
               "upf_get_particles")
         return dict(pos=pos, vel=vel, density=den, pressure=pre, type=typ, id=ids)
+
+    def particles_input_order(self):
+        """Every particle of the last set_particles call at its input index
+        (boundary particles included; pos.w = the Morton key), permuted back
+        on the device."""
+        n = self.n_input
+        pos = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        den = np.zeros(n, np.float32)
+        pre = np.zeros(n, np.float32)
+        typ = np.zeros(n, np.int32)
+        check(lib().upf_get_particles_input_order(self._h, _p(pos, C.c_float), _p(vel, C.c_float),
+                                                  _p(den, C.c_float), _p(pre, C.c_float), _p(typ, C.c_int32), n),
+              "upf_get_particles_input_order")
+        return dict(pos=pos, vel=vel, density=den, pressure=pre, type=typ)
 
     def step_fields(self):
         n = self.n_dynamic

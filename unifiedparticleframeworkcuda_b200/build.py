@@ -1,4 +1,6 @@
-"""Build the in-tree CUDA library libupf.so for sm_100a.
+"""Build the in-tree CUDA libraries for sm_100a: libupf.so (the C ABI of
+include/upf.h) and libupf_compat.so (the reference's own entry points of
+include/upf_compat.h, over libupf.so).
 
     python -m unifiedparticleframeworkcuda_b200.build [--force] [--ptxas-v]
 
@@ -20,11 +22,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libupf.so")
+COMPAT_LIB = os.path.join(HERE, "libupf_compat.so")
 INCLUDE = os.path.abspath(os.path.join(HERE, "..", "include"))
 
 CU_SOURCES = ["upf_sort.cu", "upf_pipeline.cu", "upf_rigid.cu", "upf_api.cu", "upf_batch.cu", "upf_adjoint.cu", "upf_noalloc.cu", "upf_scene.cu"]
 CPP_SOURCES = ["upf_params.cpp", "upf_io.cpp"]
 HEADERS = ["upf_common.cuh", "upf_internal.h", "upf_sys.h", "upf_tma.cuh"]
+COMPAT_SOURCES = ["upf_compat.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -46,13 +50,16 @@ def _newest(paths):
 
 def _deps():
     srcs = [os.path.join(CSRC, f) for f in CU_SOURCES + CPP_SOURCES + HEADERS]
+    srcs += [os.path.join(CSRC, f) for f in COMPAT_SOURCES]
     srcs.append(os.path.join(INCLUDE, "upf.h"))
+    srcs.append(os.path.join(INCLUDE, "upf_compat.h"))
     srcs.append(os.path.abspath(__file__))
     return srcs
 
 
 def up_to_date() -> bool:
-    return os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest(_deps())
+    newest = _newest(_deps())
+    return all(os.path.exists(f) and os.path.getmtime(f) >= newest for f in (LIB, COMPAT_LIB))
 
 
 def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) -> str:
@@ -94,6 +101,24 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) 
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
     os.replace(tmp, LIB)
+    # the compatibility layer: its own objects, linked against libupf.so and
+    # finding it beside itself at run time
+    cobjs = []
+    for f in COMPAT_SOURCES:
+        obj = os.path.join(BUILD, f + ".o")
+        cobjs.append(obj)
+        r = subprocess.run([nvcc, "-c", os.path.join(CSRC, f), "-o", obj] + common, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("compile failed: " + f)
+    tmp = COMPAT_LIB + ".tmp"
+    link = [nvcc, "-shared", "-o", tmp] + cobjs + ARCH + ["-L" + HERE, "-lupf", "-Xlinker", "-rpath,$ORIGIN",
+                                                          "-Xcompiler", "-fPIC,-pthread", "-ccbin", _cxx()]
+    r = subprocess.run(link, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("link failed: libupf_compat.so")
+    os.replace(tmp, COMPAT_LIB)
     return LIB
 
 

@@ -517,6 +517,40 @@ __global__ void k_init_dyn(uint32_t n, DynArrays A, float rho0) {
   A.lag[i] = make_float4(0.0f, 0.0f, rho0, 0.0f);
 }
 
+// Every particle of the last upf_set_particles call at its input index: the
+// dynamic particles from the current state (position with its Morton key in
+// w, as the reference keeps the z-index in pos.w), the boundary particles from
+// the static set (at rest, rest density, zero pressure).
+__global__ void k_scatter_input_order(uint32_t nd, DynArrays A, const float* __restrict__ rho,
+                                      const float* __restrict__ press, uint32_t ns, const float4* __restrict__ spos,
+                                      const uint32_t* __restrict__ sid, float3 origin, float3 scales, float rho0,
+                                      uint32_t n_total, float4* __restrict__ opos, float4* __restrict__ ovel,
+                                      float* __restrict__ orho, float* __restrict__ opress, int32_t* __restrict__ otype) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd + ns) return;
+  if (i < nd) {
+    const uint32_t j = A.id[i];
+    if (j >= n_total) return;
+    const float4 x = A.pos[i];
+    const float4 v = A.vel[i];
+    opos[j] = make_float4(x.x, x.y, x.z, (float)morton_key(x, origin, scales));
+    ovel[j] = make_float4(v.x, v.y, v.z, 0.0f);
+    orho[j] = rho[i];
+    opress[j] = press[i];
+    otype[j] = A.type[i];
+  } else {
+    const uint32_t b = i - nd;
+    const uint32_t j = sid[b];
+    if (j >= n_total) return;
+    const float4 x = spos[b];
+    opos[j] = make_float4(x.x, x.y, x.z, (float)morton_key(x, origin, scales));
+    ovel[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    orho[j] = rho0;
+    opress[j] = 0.0f;
+    otype[j] = UPF_FROZEN;
+  }
+}
+
 __global__ void k_gather_static(uint32_t n, const uint32_t* __restrict__ perm, const float4* __restrict__ in,
                                 const uint32_t* __restrict__ in_id, float4* __restrict__ out,
                                 uint32_t* __restrict__ out_id) {
@@ -1502,6 +1536,46 @@ upf_status upf_get_particles(upf_system* s, float* pos4, float* vel4, float* den
   if (id && n) UPF_CUDA(cudaMemcpyAsync(id, s->A.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
   UPF_CUDA(cudaStreamSynchronize(st));
   if (n_out) *n_out = n;
+  return UPF_OK;
+}
+
+upf_status upf_get_particles_input_order(upf_system* s, float* pos4, float* vel4, float* density, float* pressure,
+                                        int32_t* type, uint32_t n) {
+  UPF_TRY(phase_guard(s));
+  const uint32_t total = s->n_dyn + s->n_static;
+  if (n != total) {
+    set_error("upf_get_particles_input_order: n = %u, but the last upf_set_particles call had %u particles", n,
+              total);
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (n == 0) return UPF_OK;
+  cudaStream_t st = s->stream;
+  // one stream-ordered block: positions, velocities, density, pressure, type
+  const size_t bytes = (size_t)n * (16 + 16 + 4 + 4 + 4);
+  char* buf = nullptr;
+  UPF_CUDA(cudaMallocAsync((void**)&buf, bytes, st));
+  float4* opos = (float4*)buf;
+  float4* ovel = opos + n;
+  float* orho = (float*)(ovel + n);
+  float* opress = orho + n;
+  int32_t* otype = (int32_t*)(opress + n);
+  k_scatter_input_order<<<(n + 255) / 256, 256, 0, st>>>(s->n_dyn, s->A, s->rho, s->press, s->n_static, s->spos,
+                                                         s->sid, s->dp.origin, s->dp.scales, s->prm.rest_density,
+                                                         n, opos, ovel, orho, opress, otype);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && pos4) e = cudaMemcpyAsync(pos4, opos, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && vel4) e = cudaMemcpyAsync(vel4, ovel, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && density) e = cudaMemcpyAsync(density, orho, sizeof(float) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && pressure)
+    e = cudaMemcpyAsync(pressure, opress, sizeof(float) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && type) e = cudaMemcpyAsync(type, otype, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+  const cudaError_t ef = cudaFreeAsync(buf, st);
+  if (e == cudaSuccess) e = ef;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    set_error("upf_get_particles_input_order: %s", cudaGetErrorString(e));
+    return UPF_ERR_CUDA;
+  }
   return UPF_OK;
 }
 
