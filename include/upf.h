@@ -651,7 +651,9 @@ upf_status upf_adjoint_times(upf_adjoint* a, float* forward_ms, float* backward_
  * takes for each squared distance r2[k] at p's support radius, computed on
  * the device (300 = outside the support: the pair adds nothing); for checking
  * the device's r2 -> bin rule against (int)(sqrtf(r2) * (1/h) * 300) and
- * sqrtf(r2) < h, UnifiedPhysics.cpp:5468-5476. n <= 2^26. */
+ * sqrtf(r2) < h, UnifiedPhysics.cpp:5468-5476. The neighbour-list build's
+ * table rule is computed beside it: -2 marks an r2 where the two differ.
+ * n <= 2^26. */
 upf_status upf_test_fail_allocation(int32_t nth);
 upf_status upf_selftest_bounded_wait(int device, uint32_t limit_us);
 upf_status upf_selftest_support_bins(int device, const upf_params* p, const float* r2, uint32_t n, int32_t* bins);

@@ -493,7 +493,7 @@ struct upf_adjoint {
   float4 *xbar = nullptr, *vbar = nullptr;
   // neighbour machinery (per step)
   uint32_t *keys = nullptr, *sort_tmp = nullptr, *cstart = nullptr, *cend = nullptr;
-  uint16_t* bins = nullptr;
+  uint32_t* lval = nullptr;
   float* luts = nullptr;
   DevState* st = nullptr;
   // per-step storage of one checkpoint interval: [C][...]
@@ -543,7 +543,7 @@ struct upf_adjoint {
     k_af_gather<<<grid(n), kT, 0, q>>>(n, pm, x, v, xs + slot(s), vs + slot(s));
     UPF_CUDA(cudaGetLastError());
     UPF_CUDA(cell_ranges(keys, n, 3 * (int)dp.cell_shift, ncells, cstart, cend, q));
-    UPF_CUDA(launch_nlist_plain(dp, n, xs + slot(s), keys, cstart, cend, nbr + (size_t)s * rows * stride, bins,
+    UPF_CUDA(launch_nlist_plain(dp, n, xs + slot(s), keys, cstart, cend, nbr + (size_t)s * rows * stride, lval,
                                 ncnt + slot(s), luts, st, q));
     return UPF_OK;
   }
@@ -687,7 +687,7 @@ upf_status upf_adjoint_create(const upf_params* p, const upf_adjoint_options* op
   ALLOC(a->ck_x, (size_t)a->nseg * N); ALLOC(a->ck_v, (size_t)a->nseg * N);
   ALLOC(a->xbar, N); ALLOC(a->vbar, N);
   ALLOC(a->keys, N); ALLOC(a->sort_tmp, radix_temp_words(n)); ALLOC(a->cstart, a->ncells); ALLOC(a->cend, a->ncells);
-  ALLOC(a->bins, (size_t)a->rows * a->stride); ALLOC(a->luts, kLutFloats); ALLOC(a->st, 1);
+  ALLOC(a->lval, (size_t)a->rows * a->stride); ALLOC(a->luts, kLutFloats); ALLOC(a->st, 1);
   ALLOC(a->perm, (size_t)C * N); ALLOC(a->nbr, (size_t)C * a->rows * a->stride); ALLOC(a->ncnt, (size_t)C * N);
   ALLOC(a->xs, (size_t)C * N); ALLOC(a->vs, (size_t)C * N); ALLOC(a->F, (size_t)C * N);
   ALLOC(a->xstar, (size_t)C * K * N); ALLOC(a->rho, (size_t)C * K * N); ALLOC(a->p, (size_t)C * K * N);

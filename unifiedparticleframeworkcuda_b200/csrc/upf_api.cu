@@ -140,6 +140,7 @@ DevParams make_dev_params(const upf_params& p, uint32_t nstride) {
   d.maxn = p.max_neighbors;
   d.nstride = nstride;
   d.static_base = nstride;
+  d.list_grad = p.method == UPF_METHOD_PCISPH ? 1u : 0u;
   return d;
 }
 
@@ -179,13 +180,13 @@ upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt,
   return UPF_OK;
 }
 
-upf_status encode_list_maps(CUtensorMap* cmaps, CUtensorMap* bmaps, uint32_t* nbr, uint16_t* bins, uint64_t cols,
+upf_status encode_list_maps(CUtensorMap* cmaps, CUtensorMap* vmaps, uint32_t* nbr, uint32_t* lval, uint64_t cols,
                             uint64_t rows) {
   const uint32_t box_rows[kListRowVariants] = {2, 4, 8, 16};
   for (int k = 0; k < kListRowVariants; ++k) {
     upf_status st = encode_list_map(&cmaps[k], nbr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, cols, rows, box_rows[k]);
     if (st != UPF_OK) return st;
-    st = encode_list_map(&bmaps[k], bins, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, cols, rows, box_rows[k]);
+    st = encode_list_map(&vmaps[k], lval, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, cols, rows, box_rows[k]);
     if (st != UPF_OK) return st;
   }
   return UPF_OK;
@@ -210,6 +211,9 @@ bool shape_valid(const LaunchShape& s, bool batched, const char** why) {
     return bad("(threads, rows) of a loop pass must be one of (128,4) (128,8) (128,16) (256,2) (256,4) (256,8) "
                "(512,2) (512,4) (1024,2) with the TMA ring (mode 0), or (128,4) (128,8) (256,4) (256,8) (512,4) "
                "(512,8) with direct loads (mode 1)");
+  if (!pforce_ring_fits(s.pforce_mode, s.pforce_threads, s.pforce_rows))
+    return bad("the pressure-force pass's TMA ring takes (128,4) (128,8) (256,2) (256,4) (512,2); its list values "
+               "leave the larger rings no room in shared memory");
   if (batched && (s.density_threads > 256 || s.pforce_threads > 256))
     return bad("batched scenes: at most 256 threads per CTA (a CTA must stay within one scene's segment)");
   return true;
@@ -322,6 +326,7 @@ upf_status autotune_shapes(const TuneOps& ops, int repeats, upf_launch_config* o
       float best_ms = 1e30f;
       for (const auto& pr : pairs) {
         if (ops.batched && pr[1] > 256) continue;
+        if (pass == 1 && !pforce_ring_fits(pr[0], pr[1], pr[2])) continue;
         mode = pr[0];
         threads = pr[1];
         rows = pr[2];
@@ -500,15 +505,18 @@ __global__ void k_selftest_wait(uint64_t limit_ns, DevState* st) {
   if (!ok && threadIdx.x == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
 }
 
-// The table bins the density pass takes for squared distances r2 (bin_of_r2
-// with the thresholds staged in shared memory, as in the pass).
+// The table bins the density pass takes for squared distances r2
+// (bin_of_r2_edge), checked against the list build's bin_of_r2 (thresholds
+// staged in shared memory, as in that pass): -2 where the two disagree.
 __global__ void k_selftest_support_bins(const float* __restrict__ thr_g, float factor, const float* __restrict__ r2,
                                         uint32_t n, int32_t* __restrict__ out) {
   __shared__ float thr[kThresholds];
   for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) thr[k] = thr_g[k];
   __syncthreads();
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = bin_of_r2(r2[i], factor, thr);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = bin_of_r2_edge(r2[i], factor, thr[kLut]);
+    out[i] = a == bin_of_r2(r2[i], factor, thr) ? a : -2;
+  }
 }
 
 __global__ void k_init_dyn(uint32_t n, DynArrays A, float rho0) {
@@ -772,7 +780,7 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   ALLOC(s->force, c); ALLOC(s->pforce, c); ALLOC(s->xs, ct);
   ALLOC(s->rho, ct); ALLOC(s->press, ct); ALLOC(s->pq, ct); ALLOC(s->wvol, ct);
   ALLOC(s->nbr, (size_t)s->nstride * p->max_neighbors);
-  ALLOC(s->bins, (size_t)s->nstride * p->max_neighbors);
+  ALLOC(s->lval, (size_t)s->nstride * p->max_neighbors);
   ALLOC(s->ncnt, c);
   ALLOC(s->cstart, s->ncells); ALLOC(s->cend, s->ncells);
   ALLOC(s->sstart, s->ncells); ALLOC(s->send, s->ncells);
@@ -780,7 +788,7 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   ALLOC(s->luts, 5 * UPF_LUT_ENTRIES + kThresholds);
   ALLOC(s->st, 1);
 #undef ALLOC
-  if ((st = encode_list_maps(s->nbr_maps, s->bins_maps, s->nbr, s->bins, s->nstride, p->max_neighbors)) != UPF_OK)
+  if ((st = encode_list_maps(s->nbr_maps, s->lval_maps, s->nbr, s->lval, s->nstride, p->max_neighbors)) != UPF_OK)
     return bail(st);
   e = cudaMallocHost((void**)&s->st_host, sizeof(DevState));
   if (e != cudaSuccess) {

@@ -256,7 +256,7 @@ upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, ui
   ALLOC(b->sort_tmp, radix_temp_words((uint32_t)n));
   ALLOC(b->force, n); ALLOC(b->pforce, n); ALLOC(b->xs, n);
   ALLOC(b->rho, n); ALLOC(b->press, n); ALLOC(b->pq, n);
-  ALLOC(b->nbr, n * rows); ALLOC(b->bins, n * rows); ALLOC(b->ncnt, n);
+  ALLOC(b->nbr, n * rows); ALLOC(b->lval, n * rows); ALLOC(b->ncnt, n);
   ALLOC(b->cstart, b->n_cells); ALLOC(b->cend, b->n_cells);
   ALLOC(b->params_d, num_scenes); ALLOC(b->luts_d, (size_t)num_scenes * kLutFloats);
   ALLOC(b->st_d, num_scenes);
@@ -265,7 +265,7 @@ upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, ui
   ALLOC(b->x.comp_begin_d, num_scenes); ALLOC(b->x.stage_a, std::max<size_t>(total, 1));
   ALLOC(b->x.stage_b, std::max<size_t>(total, 1));
 #undef ALLOC
-  if ((st = encode_list_maps(b->nbr_maps, b->bins_maps, b->nbr, b->bins, n, rows)) != UPF_OK) return bail(st);
+  if ((st = encode_list_maps(b->nbr_maps, b->lval_maps, b->nbr, b->lval, n, rows)) != UPF_OK) return bail(st);
   e = cudaMallocHost((void**)&b->st_h, sizeof(DevState) * num_scenes);
   if (e != cudaSuccess) {
     b->st_h = nullptr;

@@ -58,6 +58,7 @@ struct DevParams {
   uint32_t maxn;
   uint32_t nstride;        // neighbour-list column stride
   uint32_t static_base;    // neighbour index of boundary particle j is static_base + j
+  uint32_t list_grad;      // list values hold the pressure-gradient table value (PCISPH), else the bin
 };
 
 // One rigid body (RigidBody, src/cpu/RigidBody.h:105-134): float state as in
@@ -122,6 +123,24 @@ __device__ __forceinline__ int bin_of_r2(float r2, float factor, const float* th
   int g = (int)(d * factor * (float)kLut);
   g = g > kLut - 1 ? kLut - 1 : g;
   return g + (thr[g + 1] <= r2 ? 1 : 0);
+}
+
+// The same bin without reading the threshold table per pair. The bin
+// position x = r2 * rsqrtf(r2) * factor * 300 lies within 300 * (2^-21 +
+// 2^-22) < 2.2e-4 of the reference's sqrt_rn(r2) * factor * 300 (rsqrtf
+// within 2 ulp, two more roundings here, three there), so wherever x is at
+// least kBinEdge = 2^-10 from an integer both truncate to the same bin; only
+// within kBinEdge of a bin edge (about 0.2% of pairs, or a non-finite x)
+// does the correctly rounded root decide. r2_edge is thr[300], the first r2
+// that takes the zero entry: pairs from there on return 300 exactly as
+// bin_of_r2 does.
+constexpr float kBinEdge = 1.0f / 1024.0f;
+__device__ __forceinline__ int bin_of_r2_edge(float r2, float factor, float r2_edge) {
+  const float x = r2 * rsqrtf(r2) * factor * (float)kLut;
+  int g = (int)x;
+  if (!(fabsf(x - (float)g - 0.5f) <= 0.5f - kBinEdge)) g = lut_index(__fsqrt_rn(r2), factor);
+  g = g > kLut - 1 ? kLut - 1 : g;
+  return r2 < r2_edge ? g : kLut;
 }
 
 // PCISPH dist_lut: uint(dist * 300 / h), clamped to 300

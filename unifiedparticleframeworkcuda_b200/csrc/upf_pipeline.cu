@@ -91,9 +91,10 @@ __device__ __forceinline__ void for_neighbors(const uint32_t* __restrict__ col, 
   }
 }
 
-// The same, also handing each entry's stored kernel-table bin to `use`.
+// The same, also handing each entry's stored list value (the kernel-table
+// bin, in the WCSPH passes) to `use`.
 template <class Load, class Use>
-__device__ __forceinline__ void for_neighbors_bin(const uint32_t* __restrict__ col, const uint16_t* __restrict__ bcol,
+__device__ __forceinline__ void for_neighbors_bin(const uint32_t* __restrict__ col, const uint32_t* __restrict__ bcol,
                                                   uint32_t stride, uint32_t cnt, Load&& load, Use&& use) {
   using T = decltype(load(0u));
   uint32_t k = 0;
@@ -161,44 +162,43 @@ __device__ __forceinline__ Scope enter_scope(const DevParams& Pk, const float* l
 //  * direct loads (kDirect = true): each thread loads its own list entries
 //    kRows at a time with coalesced global loads (consecutive threads read
 //    consecutive words of a row) and no barriers.
-// body(code, bin, k0) consumes entries k0 .. k0 + kRows - 1 (those below
-// the thread's count); code(r) / bin(r) give entry k0 + r (read from the
-// shared-memory stage when it is used, in the ring mode). Returns false if a
-// ring wait ran out.
+// body(code, val, k0) consumes entries k0 .. k0 + kRows - 1 (those below
+// the thread's count); code(r) / val(r) give entry k0 + r and its list
+// value (read from the shared-memory stage when it is used, in the ring
+// mode). Returns false if a ring wait ran out.
 struct ListArgs {
   const CUtensorMap* cmap;
-  const CUtensorMap* bmap;
+  const CUtensorMap* vmap;
   const uint32_t* nbr;
-  const uint16_t* bins;
+  const uint32_t* vals;
   uint32_t stride;
 };
 
-template <bool kDirect, bool kWithBins, int kThreads, int kRows, class Body>
+template <bool kDirect, bool kWithVals, int kThreads, int kRows, class Body>
 __device__ __forceinline__ bool walk_lists(const ListArgs& L, uint32_t i, uint32_t cnt, Body&& body) {
   if constexpr (kDirect) {
     const uint32_t* __restrict__ col = L.nbr + i;
-    const uint16_t* __restrict__ bcol = L.bins + i;
+    const uint32_t* __restrict__ vcol = L.vals + i;
     for (uint32_t k0 = 0; k0 < cnt; k0 += kRows) {
-      uint32_t code[kRows], bin[kRows];
+      uint32_t code[kRows], val[kRows];
 #pragma unroll
       for (int r = 0; r < kRows; ++r) {
         if (k0 + r < cnt) {
           code[r] = __ldg(col + (size_t)(k0 + r) * L.stride);
-          if (kWithBins) bin[r] = __ldg(bcol + (size_t)(k0 + r) * L.stride);
+          if (kWithVals) val[r] = __ldg(vcol + (size_t)(k0 + r) * L.stride);
         }
       }
-      body([&](int r) { return code[r]; }, [&](int r) { return bin[r]; }, (int)k0);
+      body([&](int r) { return code[r]; }, [&](int r) { return val[r]; }, (int)k0);
     }
     return true;
   } else {
-    __shared__ WarpListRing<kWithBins, kRows> rings[kThreads / 32];
+    __shared__ WarpListRing<kWithVals, kRows> rings[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpListRing<kWithBins, kRows>& ring = rings[warp];
+    WarpListRing<kWithVals, kRows>& ring = rings[warp];
     ring_init(ring);
     const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
-    return ring_walk(ring, L.cmap, L.bmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt, [&](int s, int k0) {
-      body([&](int r) { return ring.codes[s][r][lane]; }, [&](int r) { return (uint32_t)ring.bins[s][r][lane]; },
-           k0);
+    return ring_walk(ring, L.cmap, L.vmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt, [&](int s, int k0) {
+      body([&](int r) { return ring.codes[s][r][lane]; }, [&](int r) { return ring.vals[s][r][lane]; }, k0);
     });
   }
 }
@@ -236,8 +236,11 @@ __device__ __forceinline__ float dist2(float4 a, float4 b) {
 // key. The list therefore comes out in the reference's ascending
 // sorted-index order, and membership is the reference's exact test: j != i
 // and |x_i - x_j| < h in float. Candidate positions are gathered kUnroll at
-// a time. Each entry also records its kernel-table bin at the current
-// positions (used by every pass that evaluates at current positions).
+// a time. Each entry also records a list value at the current positions:
+// its kernel-table bin (WCSPH: the density and force passes read their
+// tables by it), or the pressure-gradient table's value at that bin
+// (PCISPH: the pressure-force pass, which evaluates at the current
+// positions, then reads no table).
 //
 // kWarpUnion: the 32 lanes of a warp (32 consecutive Morton-sorted particles,
 // close together) walk the union of their query boxes, when it spans at
@@ -253,12 +256,14 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
     const uint32_t* __restrict__ keys, const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend,
     uint32_t ns, const float4* __restrict__ spos, const uint32_t* __restrict__ skeys,
     const uint32_t* __restrict__ sstart, const uint32_t* __restrict__ send, uint32_t* __restrict__ nbr,
-    uint16_t* __restrict__ bins, uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    uint32_t* __restrict__ lval, uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
     DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float thr[kThresholds];
+  __shared__ float pg[UPF_LUT_ENTRIES];
   const Scope sc = enter_scope<kBatch>(Pk, luts, st_plain, n, bv, &sP, false);
   for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) thr[k] = sc.luts[5 * UPF_LUT_ENTRIES + k];
+  stage_lut(pg, sc.luts + LUT_PGRAD * UPF_LUT_ENTRIES);
   __syncthreads();
   const DevParams& P = *sc.P;
   DevState* st = sc.st;
@@ -329,12 +334,14 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
   const uint32_t maxn = P.maxn, stride = P.nstride;
   uint32_t cnt = 0;
   uint32_t* __restrict__ out = nbr + i;
-  uint16_t* __restrict__ ob = bins + i;
+  uint32_t* __restrict__ ov = lval + i;
+  const bool grad = P.list_grad != 0;
   auto append = [&](uint32_t code, float r2) {
     if (!active) return;
     if (cnt < maxn) {
       out[(size_t)cnt * stride] = code;
-      ob[(size_t)cnt * stride] = (uint16_t)bin_of_r2(r2, P.lut_factor, thr);
+      const int bin = bin_of_r2(r2, P.lut_factor, thr);
+      ov[(size_t)cnt * stride] = grad ? __float_as_uint(pg[bin]) : (uint32_t)bin;
     }
     cnt++;
   };
@@ -446,7 +453,7 @@ __device__ float wall_weight(const DevParams& P, const float* m4, float4 x) {
 // (UnifiedPhysics.cpp:2408-2501), liquid particles.
 __global__ void __launch_bounds__(kBlock) k_wcsph_density(
     DevParams P, uint32_t n, const float4* __restrict__ pos, const int32_t* __restrict__ type,
-    const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
+    const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts,
     float* __restrict__ rho, float* __restrict__ press) {
   __shared__ float m4[UPF_LUT_ENTRIES];
   stage_lut(m4, luts + LUT_M4 * UPF_LUT_ENTRIES);
@@ -458,8 +465,8 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_density(
   const float m = P.mass;
   float den = P.kernel_self * m;
   // densities at the positions the list was built at: every entry is within
-  // h and carries its kernel-table bin, so only the bins are read
-  const uint16_t* __restrict__ b = bins + i;
+  // h and carries its kernel-table bin, so only the bins are read (list values)
+  const uint32_t* __restrict__ b = lval + i;
   const uint32_t c = ncnt[i];
   uint32_t k = 0;
   for (; k + kUnroll <= c; k += kUnroll) {
@@ -554,7 +561,7 @@ __device__ __forceinline__ void integrate_store(const DevParams& P, uint32_t i, 
 // CalculateForcesInBlocksKernelWCSPH particles_kernel.cu:2399-2653).
 __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
     DevParams P, uint32_t n, DynArrays B, DynArrays A, uint32_t* __restrict__ keysA,
-    const uint32_t* __restrict__ nbr, const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt,
     const float* __restrict__ luts, const float* __restrict__ rho, const float* __restrict__ press,
     float4* __restrict__ force, DevState* __restrict__ st) {
   __shared__ float pg[UPF_LUT_ENTRIES], vl[UPF_LUT_ENTRIES];
@@ -583,7 +590,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_integrate(
       // positions are those the list was built at: entries are within h and
       // carry their kernel-table bin
       for_neighbors_bin(
-          nbr + i, bins + i, P.nstride, ncnt[i],
+          nbr + i, lval + i, P.nstride, ncnt[i],
           [&](uint32_t code) {
             WNb s;
             // boundary particles (array tails) are FROZEN and skipped below
@@ -942,13 +949,13 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
     float* __restrict__ press, float4* __restrict__ pq, DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float m4[UPF_LUT_ENTRIES];
-  __shared__ float thr[kThresholds];
   __shared__ uint32_t wmax[kThreads / 32];
   const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31;
   stage_lut(m4, sc.luts + LUT_M4 * UPF_LUT_ENTRIES);
-  stage_thresholds(thr, sc.luts);
+  // the first r2 of the zero entry (thresholds follow the five tables)
+  const float r2_edge = __ldg(sc.luts + 5 * UPF_LUT_ENTRIES + kLut);
   __syncthreads();
   const DevParams& P = *sc.P;
   DevState* st = sc.st;
@@ -973,7 +980,7 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
         // the table bin of d from d^2 (exact); at or beyond h the bin is 300,
         // whose entry 0 adds +0 exactly as the reference's skipped term does
         const float r2 = dist2(xi, xj[r]);
-        den += m4[bin_of_r2(r2, P.lut_factor, thr)] * m;
+        den += m4[bin_of_r2_edge(r2, P.lut_factor, r2_edge)] * m;
       }
     }
   });
@@ -999,22 +1006,23 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
 }
 
 // ComputeCorrectivePressureForce (UnifiedPhysics.cpp:5493-5522), then the
-// prediction of the next iteration (PredictPositionAndVelocity). List entries
-// and their stored bins by the TMA ring or by direct loads (walk_lists).
+// prediction of the next iteration (PredictPositionAndVelocity). The
+// positions are the step's, at which the list was built: every entry lies
+// within h and carries the pressure-gradient table's value at its bin as its
+// list value, so the pass reads no table. List entries and values come by
+// the TMA ring or by direct loads (walk_lists).
 template <bool kBatch, bool kDirect, int kThreads, int kRows>
 __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
-    const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap bmap,
-    const uint32_t* __restrict__ nbr, const uint16_t* __restrict__ bins, const uint32_t* __restrict__ ncnt,
+    const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap vmap,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt,
     const float* __restrict__ luts_plain, const float4* __restrict__ pq, const float4* __restrict__ force,
     float4* __restrict__ pforce, float4* __restrict__ xs, DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
-  __shared__ float pg[UPF_LUT_ENTRIES];
   const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31;
-  stage_lut(pg, sc.luts + LUT_PGRAD * UPF_LUT_ENTRIES);
-  __syncthreads();
+  if (kBatch) __syncthreads();  // the scene's parameters in shared memory
   const DevParams& P = *sc.P;
   DevState* st = sc.st;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1026,10 +1034,8 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
   // density pass (pq.w); boundary particles have p = 0, so 0 / rho0^2 = 0
   const float qi = active ? pq[i].w : 0.0f;
   float fx = 0, fy = 0, fz = 0;
-  // positions are those the list was built at: every entry passes |x_i - x_j| < h
-  // and its kernel-table bin is stored with it
-  const ListArgs L{&cmap, &bmap, nbr, bins, P.nstride};
-  const bool ok = walk_lists<kDirect, true, kThreads, kRows>(L, i, cnt, [&](auto code, auto bin, int k0) {
+  const ListArgs L{&cmap, &vmap, nbr, lval, P.nstride};
+  const bool ok = walk_lists<kDirect, true, kThreads, kRows>(L, i, cnt, [&](auto code, auto val, int k0) {
     // one gather per neighbour: position and p / rho0^2 packed in pq
     // (boundary particles sit in the tail, w = 0 there)
     float4 xj[kRows];
@@ -1039,7 +1045,7 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
       if (k0 + r < (int)cnt) {
-        const float g = pg[bin(r)];
+        const float g = __uint_as_float(val(r));  // kernelPressureGradLut at the entry's bin
         const float kx = (xi.x - xj[r].x) * g, ky = (xi.y - xj[r].y) * g, kz = (xi.z - xj[r].z) * g;
         const float grad = qi + xj[r].w;
         fx = fx - kx * grad * m * m;
@@ -1318,11 +1324,11 @@ template <bool kBatch>
 cudaError_t run_nlist(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
                       const float4* pos, const uint32_t* keys, const uint32_t* cstart, const uint32_t* cend,
                       uint32_t ns, const float4* spos, const uint32_t* skeys, const uint32_t* sstart,
-                      const uint32_t* send, uint32_t* nbr, uint16_t* bins, uint32_t* ncnt, const float* luts,
+                      const uint32_t* send, uint32_t* nbr, uint32_t* lval, uint32_t* ncnt, const float* luts,
                       DevState* stp) {
 #define UPF_NL(T, W)                                                                                          \
   k_build_nlist<kBatch, T, W><<<(n + T - 1) / T, T, 0, st>>>(P, bv, n, pos, keys, cstart, cend, ns, spos, skeys, \
-                                                             sstart, send, nbr, bins, ncnt, luts, stp)
+                                                             sstart, send, nbr, lval, ncnt, luts, stp)
   switch (sh.nlist_threads * 10 + sh.nlist_mode) {
     case 640: UPF_NL(64, false); break;
     case 1280: UPF_NL(128, false); break;
@@ -1389,12 +1395,17 @@ cudaError_t run_density(const LaunchShape& sh, cudaStream_t st, const DevParams&
 
 template <bool kBatch>
 cudaError_t run_pforce(const LaunchShape& sh, cudaStream_t st, const DevParams& P, const BatchView& bv, uint32_t n,
-                       const DynArrays& B, const CUtensorMap* cmaps, const CUtensorMap* bmaps, const uint32_t* nbr,
-                       const uint16_t* bins, const uint32_t* ncnt, const float* luts, const float4* pq,
+                       const DynArrays& B, const CUtensorMap* cmaps, const CUtensorMap* vmaps, const uint32_t* nbr,
+                       const uint32_t* lval, const uint32_t* ncnt, const float* luts, const float4* pq,
                        const float4* force, float4* pforce, float4* xs, DevState* stp) {
-#define UPF_PF(D, T, R)                                                                                            \
-  k_pcisph_pressure_force<kBatch, D, T, R><<<(n + T - 1) / T, T, 0, st>>>(                                         \
-      P, bv, n, B, cmaps[rows_index(R)], bmaps[rows_index(R)], nbr, bins, ncnt, luts, pq, force, pforce, xs, stp)
+  // shapes whose ring does not fit are neither built nor launched
+#define UPF_PF(D, T, R)                                                                                             \
+  if constexpr (pforce_ring_fits(D ? 1 : 0, T, R)) {                                                                \
+    k_pcisph_pressure_force<kBatch, D, T, R><<<(n + T - 1) / T, T, 0, st>>>(                                        \
+        P, bv, n, B, cmaps[rows_index(R)], vmaps[rows_index(R)], nbr, lval, ncnt, luts, pq, force, pforce, xs, stp); \
+  } else {                                                                                                          \
+    return cudaErrorInvalidConfiguration;                                                                          \
+  }
   UPF_SHAPE_SWITCH(sh.pforce_mode, sh.pforce_threads, sh.pforce_rows, UPF_PF)
 #undef UPF_PF
   return cudaGetLastError();
@@ -1423,14 +1434,14 @@ cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
   k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
   if (n == 0) return cudaGetLastError();
   return run_nlist<false>(s.shape, st, s.dp, BatchView{}, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
-                          s.skeys, s.sstart, s.send, s.nbr, s.bins, s.ncnt, s.luts, s.st);
+                          s.skeys, s.sstart, s.send, s.nbr, s.lval, s.ncnt, s.luts, s.st);
 }
 
 cudaError_t launch_force_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n == 0) return cudaSuccess;
   if (s.prm.method == UPF_METHOD_WCSPH) {
-    k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.bins, s.ncnt, s.luts, s.rho,
+    k_wcsph_density<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B.pos, s.B.type, s.lval, s.ncnt, s.luts, s.rho,
                                                    s.press);
   } else {
     return run_external<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.wvol, s.rb.id_body, s.nbr, s.ncnt, s.luts,
@@ -1455,7 +1466,7 @@ cudaError_t launch_loop_density(System& s, cudaStream_t st) {
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n)
-    return run_pforce<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.nbr_maps, s.bins_maps, s.nbr, s.bins, s.ncnt, s.luts, s.pq,
+    return run_pforce<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.nbr_maps, s.lval_maps, s.nbr, s.lval, s.ncnt, s.luts, s.pq,
                              s.force, s.pforce, s.xs, s.st);
   return cudaGetLastError();
 }
@@ -1480,7 +1491,7 @@ cudaError_t launch_integrate_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   if (n == 0) return cudaSuccess;
   if (s.prm.method == UPF_METHOD_WCSPH) {
-    k_wcsph_force_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.nbr, s.bins, s.ncnt,
+    k_wcsph_force_integrate<<<grid_of(n), kBlock, 0, st>>>(s.dp, n, s.B, s.A, s.keysA, s.nbr, s.lval, s.ncnt,
                                                            s.luts, s.rho, s.press, s.force, s.st);
   } else {
     k_pcisph_integrate<false><<<grid_of(n), kBlock, 0, st>>>(s.dp, BatchView{}, n, s.B, s.A, s.keysA, s.force, s.pforce, s.rho, s.press,
@@ -1510,11 +1521,11 @@ cudaError_t launch_static_setup(System& s, cudaStream_t st) {
 // Neighbour lists of one sorted set with no boundary set (the adjoint's
 // per-step lists); P.nstride is the list stride, P.maxn its rows.
 cudaError_t launch_nlist_plain(const DevParams& P, uint32_t n, const float4* pos, const uint32_t* keys,
-                               const uint32_t* cstart, const uint32_t* cend, uint32_t* nbr, uint16_t* bins,
+                               const uint32_t* cstart, const uint32_t* cend, uint32_t* nbr, uint32_t* lval,
                                uint32_t* ncnt, const float* luts, DevState* st, cudaStream_t stream) {
   if (!n) return cudaSuccess;
   return run_nlist<false>(LaunchShape{}, stream, P, BatchView{}, n, pos, keys, cstart, cend, 0u, nullptr, nullptr,
-                          nullptr, nullptr, nbr, bins, ncnt, luts, st);
+                          nullptr, nullptr, nbr, lval, ncnt, luts, st);
 }
 
 // ----------------------------------------------------------- batched launchers
@@ -1558,7 +1569,7 @@ cudaError_t batch_launch_neighbors(BatchSystem& b, cudaStream_t st) {
   k_step_init_batch<<<1, 256, 0, st>>>(b.st_d, b.n_scenes);
   if (!n) return cudaGetLastError();
   return run_nlist<true>(b.shape, st, DevParams{}, b.view, n, b.B.pos, b.keysA, b.cstart, b.cend, 0u, nullptr, nullptr,
-                         nullptr, nullptr, b.nbr, b.bins, b.ncnt, nullptr, nullptr);
+                         nullptr, nullptr, b.nbr, b.lval, b.ncnt, nullptr, nullptr);
 }
 
 cudaError_t batch_launch_forces(BatchSystem& b, cudaStream_t st) {
@@ -1584,7 +1595,7 @@ cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st) {
 cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st) {
   const uint32_t n = b.n_slots;
   if (n)
-    return run_pforce<true>(b.shape, st, DevParams{}, b.view, n, b.B, b.nbr_maps, b.bins_maps, b.nbr, b.bins, b.ncnt, nullptr, b.pq,
+    return run_pforce<true>(b.shape, st, DevParams{}, b.view, n, b.B, b.nbr_maps, b.lval_maps, b.nbr, b.lval, b.ncnt, nullptr, b.pq,
                             b.force, b.pforce, b.xs, nullptr);
   return cudaGetLastError();
 }

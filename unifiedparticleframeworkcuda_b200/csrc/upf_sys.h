@@ -73,6 +73,12 @@ constexpr int kLoopShapes[][3] = {{0, 128, 4}, {0, 128, 8}, {0, 128, 16}, {0, 25
                                   {0, 256, 8}, {0, 512, 2}, {0, 512, 4},  {0, 1024, 2}, {1, 128, 4},
                                   {1, 128, 8}, {1, 256, 4}, {1, 256, 8},  {1, 512, 4},  {1, 512, 8}};
 constexpr int kNumLoopShapes = sizeof(kLoopShapes) / sizeof(kLoopShapes[0]);
+// The pressure-force pass's TMA ring carries a 32-bit value per list entry
+// beside its code: shapes whose rings (three stages a warp) leave no room
+// within the 48 KB of static shared memory are not built for that pass.
+constexpr bool pforce_ring_fits(int mode, int threads, int rows) {
+  return mode != 0 || (threads / 32) * ((3 * rows * 32 * 8 + 3 * 8 + 127) / 128 * 128) + 1024 <= 48 * 1024;
+}
 constexpr int kListRowVariants = 4;  // tensor maps for 2, 4, 8 and 16 rows per box
 inline int rows_index(int rows) { return rows == 2 ? 0 : (rows == 4 ? 1 : (rows == 8 ? 2 : 3)); }
 
@@ -147,10 +153,13 @@ struct System {
 
   // neighbour lists
   uint32_t* nbr = nullptr;
-  uint16_t* bins = nullptr;    // kernel-table bin of each list entry at current positions
+  // per list entry, at the step's positions: the kernel-table bin (WCSPH),
+  // or the bits of the pressure-gradient table value at that bin (PCISPH,
+  // the one table the pressure-force pass reads)
+  uint32_t* lval = nullptr;
   uint32_t* ncnt = nullptr;
   CUtensorMap nbr_maps[kListRowVariants];   // 2D [max_neighbors][nstride] uint32 views of nbr for TMA, box 32 x {4, 8, 16}
-  CUtensorMap bins_maps[kListRowVariants];  // same views of bins (uint16)
+  CUtensorMap lval_maps[kListRowVariants];  // same views of lval (uint32)
   uint32_t nstride = 0;
   LaunchShape shape;
 
@@ -218,10 +227,10 @@ struct BatchSystem {
   float* press = nullptr;
   float4* pq = nullptr;
   uint32_t* nbr = nullptr;
-  uint16_t* bins = nullptr;
+  uint32_t* lval = nullptr;     // pressure-gradient table value bits per list entry
   uint32_t* ncnt = nullptr;
   CUtensorMap nbr_maps[kListRowVariants];
-  CUtensorMap bins_maps[kListRowVariants];
+  CUtensorMap lval_maps[kListRowVariants];
   uint32_t* cstart = nullptr;
   uint32_t* cend = nullptr;
   LaunchShape shape;
@@ -246,7 +255,7 @@ struct BatchSystem {
 
 // upf_pipeline.cu: neighbour lists of one sorted set without boundary set
 cudaError_t launch_nlist_plain(const DevParams& P, uint32_t n, const float4* pos, const uint32_t* keys,
-                               const uint32_t* cstart, const uint32_t* cend, uint32_t* nbr, uint16_t* bins,
+                               const uint32_t* cstart, const uint32_t* cend, uint32_t* nbr, uint32_t* lval,
                                uint32_t* ncnt, const float* luts, DevState* st, cudaStream_t stream);
 
 // upf_pipeline.cu: batched phase launchers (asynchronous on `st`)
@@ -275,8 +284,8 @@ upf_status capture_step_graph(const GraphParts& parts, cudaGraph_t* graph_out, c
 DevParams make_dev_params(const upf_params& p, uint32_t nstride);
 upf_status encode_list_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint32_t elem_bytes,
                            uint64_t cols, uint64_t rows, uint32_t box_rows);
-// the three box heights of each list (codes, bins)
-upf_status encode_list_maps(CUtensorMap* cmaps, CUtensorMap* bmaps, uint32_t* nbr, uint16_t* bins, uint64_t cols,
+// the box heights of each list (codes, list values)
+upf_status encode_list_maps(CUtensorMap* cmaps, CUtensorMap* vmaps, uint32_t* nbr, uint32_t* lval, uint64_t cols,
                             uint64_t rows);
 
 // upf_api.cu: the launch-shape autotuner, over callbacks so that one

@@ -77,11 +77,12 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 
 // One warp's ring of list stages. Stage s holds rows [c*R, c*R+R) of chunk c
 // (c % kListStages == s) for the warp's 32 columns: codes (uint32) and,
-// when kWithBins, bins (uint16). R = kRows, the box height of the tensor map.
-template <bool kWithBins, int kRows = kListRows>
+// when kWithVals, the entries' list values (uint32). R = kRows, the box
+// height of the tensor map.
+template <bool kWithVals, int kRows = kListRows>
 struct __align__(128) WarpListRing {
   uint32_t codes[kListStages][kRows][32];                   // 128 B per row
-  uint16_t bins[kWithBins ? kListStages : 1][kRows][32];     // 64 B per row
+  uint32_t vals[kWithVals ? kListStages : 1][kRows][32];     // 128 B per row
   uint64_t full[kListStages];
 };
 
@@ -89,15 +90,15 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <bool kWithBins, int kRows>
-__device__ __forceinline__ void ring_issue(WarpListRing<kWithBins, kRows>& r, const CUtensorMap* cmap,
-                                           const CUtensorMap* bmap, int chunk, int col0) {
+template <bool kWithVals, int kRows>
+__device__ __forceinline__ void ring_issue(WarpListRing<kWithVals, kRows>& r, const CUtensorMap* cmap,
+                                           const CUtensorMap* vmap, int chunk, int col0) {
   const int s = chunk % kListStages;
-  const uint32_t bytes = kRows * 32 * (4 + (kWithBins ? 2 : 0));
+  const uint32_t bytes = kRows * 32 * (4 + (kWithVals ? 4 : 0));
   fence_proxy_async_smem();  // the stage's previous contents were read through the generic proxy
   mbar_arrive_expect_tx(&r.full[s], bytes);
   tma_load_2d(&r.codes[s][0][0], cmap, &r.full[s], col0, chunk * kRows);
-  if (kWithBins) tma_load_2d(&r.bins[s][0][0], bmap, &r.full[s], col0, chunk * kRows);
+  if (kWithVals) tma_load_2d(&r.vals[s][0][0], vmap, &r.full[s], col0, chunk * kRows);
 }
 
 // Walks the warp's lists chunk by chunk. `body(s, rows)` consumes stage s
@@ -107,13 +108,13 @@ __device__ __forceinline__ void ring_issue(WarpListRing<kWithBins, kRows>& r, co
 // lands in the ring after the warp has moved on.
 constexpr uint64_t kDrainLimitNs = 100000000ull;  // 0.1 s per issued stage when draining after a timeout
 
-template <bool kWithBins, int kRows, class Body>
-__device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins, kRows>& r, const CUtensorMap* cmap,
-                                          const CUtensorMap* bmap, int col0, uint32_t warp_max_cnt, Body&& body) {
+template <bool kWithVals, int kRows, class Body>
+__device__ __forceinline__ bool ring_walk(WarpListRing<kWithVals, kRows>& r, const CUtensorMap* cmap,
+                                          const CUtensorMap* vmap, int col0, uint32_t warp_max_cnt, Body&& body) {
   const int lane = threadIdx.x & 31;
   const int nchunks = (int)((warp_max_cnt + kRows - 1) / kRows);
   if (lane == 0) {
-    for (int c = 0; c < kListStages && c < nchunks; ++c) ring_issue(r, cmap, bmap, c, col0);
+    for (int c = 0; c < kListStages && c < nchunks; ++c) ring_issue(r, cmap, vmap, c, col0);
   }
   int c = 0;
   for (; c < nchunks; ++c) {
@@ -123,7 +124,7 @@ __device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins, kRows>& r, con
     if (!__all_sync(0xffffffffu, mbar_wait(&r.full[s], parity))) break;
     body(s, c * kRows);
     __syncwarp();
-    if (lane == 0 && c + kListStages < nchunks) ring_issue(r, cmap, bmap, c + kListStages, col0);
+    if (lane == 0 && c + kListStages < nchunks) ring_issue(r, cmap, vmap, c + kListStages, col0);
   }
   if (c == nchunks) return true;
   // chunks c .. issued-1 were issued and not consumed
@@ -134,8 +135,8 @@ __device__ __forceinline__ bool ring_walk(WarpListRing<kWithBins, kRows>& r, con
   return false;
 }
 
-template <bool kWithBins, int kRows>
-__device__ __forceinline__ void ring_init(WarpListRing<kWithBins, kRows>& r) {
+template <bool kWithVals, int kRows>
+__device__ __forceinline__ void ring_init(WarpListRing<kWithVals, kRows>& r) {
   if ((threadIdx.x & 31) == 0) {
     for (int s = 0; s < kListStages; ++s) mbar_init(&r.full[s], 1);
     fence_barrier_init();
