@@ -102,10 +102,11 @@ def cpu_model():
     return "unknown"
 
 
-def oracle_from_system(s, sc, threads):
-    """The oracle holding system `s`'s current state (the workload `sc`
-    advanced on the GPU): positions, velocities and the last step's pressure
-    and predicted density of the dynamic particles, the boundary as built."""
+def oracle_from_system(s, sc, threads, fp64=False):
+    """The oracle (FP32, or its FP64 twin) holding system `s`'s current state
+    (the workload `sc` advanced on the GPU): positions, velocities and the
+    last step's pressure and predicted density of the dynamic particles, the
+    boundary as built."""
     import unifiedparticleframeworkcuda_b200 as upf
     from oracle import pyoracle
     g = s.particles()
@@ -119,9 +120,39 @@ def oracle_from_system(s, sc, threads):
     vel[ids] = g["vel"]
     pres[ids] = g["pressure"]
     dens[ids] = g["density"]
-    o = pyoracle.OracleSim(p, pos, vel, sc.type, threads=threads, keep_fields=False)
+    o = pyoracle.OracleSim(p, pos, vel, sc.type, threads=threads, keep_fields=False, fp64=fp64)
     o.set_lagged(pres, dens)
     return o
+
+
+def fp64_error(s, sc, threads):
+    """One step of system `s` from its checkpoint 0 against the FP64 oracle
+    from the same state: the largest differences of the liquid particles'
+    fields (positions absolute in m, the rest relative to the field's largest
+    magnitude) and both iteration counts."""
+    import unifiedparticleframeworkcuda_b200 as upf
+    s.restore(0)
+    o = oracle_from_system(s, sc, threads, fp64=True)
+    s.step(1)
+    s.synchronize()
+    gi = s.stats().iterations
+    g = s.particles()
+    info = o.step()
+    c = o.state()
+    o.close()
+    liq = np.sort(g["id"][g["type"] == upf.LIQUID])
+    out = {"iterations_gpu": int(gi), "iterations_fp64": int(info.iterations)}
+    go, co = np.argsort(g["id"]), np.argsort(c["id"])
+    gs = go[np.searchsorted(g["id"][go], liq)]
+    cs = co[np.searchsorted(c["id"][co], liq)]
+    for k in ("pos", "vel", "density", "pressure"):
+        a = g[k][gs].astype(np.float64)
+        b = c[k][cs].astype(np.float64)
+        if a.ndim == 2:
+            a, b = a[:, :3], b[:, :3]
+        scale = 1.0 if k == "pos" else max(np.abs(b).max(), 1e-30)
+        out[("pos_max_abs_m" if k == "pos" else k + "_max_rel")] = float(np.abs(a - b).max() / scale)
+    return out
 
 
 def workload_name(args):
@@ -1033,6 +1064,8 @@ def run_ours(args, rank, world, local_rank):
         if dam:
             s.restore(0)  # the state at the start of the timed steps
         out["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds, system=s if dam else None)
+        if dam:
+            out["config"]["fp64_err"] = fp64_error(s, sc, os.cpu_count() or 1)
     print(json.dumps(out), flush=True)
     s.close()
 
