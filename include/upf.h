@@ -265,6 +265,63 @@ upf_status upf_phase_predict_correct(upf_system* s);
 /* Time integration + clamp + next key (UpdateLiquidParticlePosVel*, CalculateZindex). */
 upf_status upf_phase_integrate(upf_system* s);
 
+/* The predict-correct loop pass by pass (PCISPH), for a caller that
+ * exchanges fields between the passes, e.g. the halos of a scene split into
+ * slabs over several GPUs. After upf_phase_forces: upf_phase_loop_begin, then
+ * per iteration upf_phase_density (predicted density, pressure update, the
+ * running maximum for the loop test), upf_phase_pressure_force (pressure
+ * force, next prediction) and upf_phase_loop_control, which runs the loop
+ * test of PredictionCorrectionStep (UnifiedPhysics.cpp:5376-5420) on the
+ * maximum found in loop_max_density_bits (which the caller may replace, e.g.
+ * by a maximum over all slabs) and returns in *cont whether to iterate again;
+ * then upf_phase_integrate. The reference reads its maximum back every
+ * iteration as well (GetMaxPredictedDensityCUDA, particles.cu:2139-2154). */
+upf_status upf_phase_loop_begin(upf_system* s);
+upf_status upf_phase_density(upf_system* s);
+upf_status upf_phase_pressure_force(upf_system* s);
+upf_status upf_phase_loop_control(upf_system* s, int32_t* cont);
+
+/* Device arrays of a system (no copies), for callers that move particles
+ * between systems on the device. The dynamic state (after integration, or
+ * as set): pos4/vel4/lag4 n x 4 floats (lag4: previous correction pressure,
+ * last correction pressure, last predicted density, -), type, id. The
+ * current step's sorted working set (valid after upf_phase_sort): positions,
+ * ids, predicted positions, correction pressure, pq4 (position, pressure /
+ * rest_density^2: what the pressure-force pass gathers), predicted density.
+ * loop_max_density_bits: the loop test's running maximum (float bits).
+ * stream: the system's stream; work on these arrays belongs on it. */
+typedef struct upf_device_state {
+  float* pos4;
+  float* vel4;
+  float* lag4;
+  int32_t* type;
+  uint32_t* id;
+  uint32_t n;
+  uint32_t capacity_dynamic;
+  float* sorted_pos4;
+  uint32_t* sorted_id;
+  float* predicted_pos4;
+  float* pressure;
+  float* pq4;
+  float* density;
+  uint32_t* loop_max_density_bits;
+  void* stream;
+} upf_device_state;
+upf_status upf_get_device_state(upf_system* s, upf_device_state* out);
+/* Replace the dynamic particles (device arrays, n of them; the boundary set
+ * stays) in stream order on the system's stream; the inputs may be the
+ * system's own arrays. Ids are the caller's (carried through every step).
+ * Not for systems with rigid bodies. */
+upf_status upf_set_dynamic_device(upf_system* s, const float* pos4, const float* vel4, const float* lag4,
+                                  const int32_t* type, const uint32_t* id, uint32_t n);
+/* dst[k] = src[idx[k]] (gather) and dst[idx[k]] = src[k] (scatter) for k < n,
+ * rows of row_bytes = 4 or 16, device pointers: the pack and unpack of a
+ * halo exchange. */
+upf_status upf_gather_rows(const void* src, uint32_t row_bytes, const uint32_t* idx, uint32_t n, void* dst,
+                           void* stream);
+upf_status upf_scatter_rows(const void* src, uint32_t row_bytes, const uint32_t* idx, uint32_t n, void* dst,
+                            void* stream);
+
 /* Replace the dynamic particles' positions and velocities from host arrays in
  * the current device order (the order upf_get_particles returns), keeping the
  * rest of the state; the next step re-sorts them. n must equal the dynamic

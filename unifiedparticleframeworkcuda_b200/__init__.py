@@ -19,7 +19,7 @@ import numpy as np
 from ._abi import (FLAG_ADHESION, FLAG_BOUNDARY_PRESSURE, FLAG_PENALTY_WALLS,  # noqa: F401
                    FLAG_RECORD_ITERATIONS, FLAG_SURFACE_TENSION, FLAG_WALL_WEIGHT, FROZEN,
                    GRANULAR, LIQUID, METHOD_PCISPH, METHOD_WCSPH, RIGID, STATUS, UpfParams,
-                   UpfAdjointOptions, UpfLaunchConfig, UpfPhaseTimes, UpfStepStats)
+                   UpfAdjointOptions, UpfDeviceState, UpfLaunchConfig, UpfPhaseTimes, UpfStepStats)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libupf.so")
@@ -63,6 +63,14 @@ def lib():
             "upf_phase_forces": [vp],
             "upf_phase_predict_correct": [vp],
             "upf_phase_integrate": [vp],
+            "upf_phase_loop_begin": [vp],
+            "upf_phase_density": [vp],
+            "upf_phase_pressure_force": [vp],
+            "upf_phase_loop_control": [vp, i32p],
+            "upf_get_device_state": [vp, C.POINTER(UpfDeviceState)],
+            "upf_set_dynamic_device": [vp, fp, fp, fp, i32p, u32p, C.c_uint32],
+            "upf_gather_rows": [vp, C.c_uint32, vp, C.c_uint32, vp, vp],
+            "upf_scatter_rows": [vp, C.c_uint32, vp, C.c_uint32, vp, vp],
             "upf_get_particles": [vp, fp, fp, fp, fp, i32p, u32p, u32p],
             "upf_get_particles_input_order": [vp, fp, fp, fp, fp, i32p, C.c_uint32],
             "upf_get_step_fields": [vp, fp, fp, fp, u32p, u32p],

@@ -116,6 +116,17 @@ class UpfStepStats(C.Structure):
     ]
 
 
+class UpfDeviceState(C.Structure):
+    """upf_device_state: device pointers of a system's arrays."""
+    _fields_ = [
+        ("pos4", C.c_void_p), ("vel4", C.c_void_p), ("lag4", C.c_void_p), ("type", C.c_void_p), ("id", C.c_void_p),
+        ("n", C.c_uint32), ("capacity_dynamic", C.c_uint32),
+        ("sorted_pos4", C.c_void_p), ("sorted_id", C.c_void_p), ("predicted_pos4", C.c_void_p),
+        ("pressure", C.c_void_p), ("pq4", C.c_void_p), ("density", C.c_void_p),
+        ("loop_max_density_bits", C.c_void_p), ("stream", C.c_void_p),
+    ]
+
+
 class UpfPhaseTimes(C.Structure):
     _fields_ = [
         ("sort_ms", C.c_float),

@@ -559,6 +559,29 @@ __global__ void k_scatter_input_order(uint32_t nd, DynArrays A, const float* __r
   }
 }
 
+// dst[k] = src[idx[k]] (gather) or dst[idx[k]] = src[k] (scatter), rows of
+// one float or one float4: the halo exchange packs and unpacks with these
+template <class T>
+__global__ void k_rows(const T* __restrict__ src, const uint32_t* __restrict__ idx, uint32_t n, T* __restrict__ dst,
+                       bool scatter) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  if (scatter)
+    dst[idx[k]] = src[k];
+  else
+    dst[k] = src[idx[k]];
+}
+
+cudaError_t launch_rows(const void* src, uint32_t row_bytes, const uint32_t* idx, uint32_t n, void* dst,
+                        bool scatter, cudaStream_t st) {
+  const uint32_t grid = (n + 255) / 256;
+  if (row_bytes == 16)
+    k_rows<float4><<<grid, 256, 0, st>>>((const float4*)src, idx, n, (float4*)dst, scatter);
+  else
+    k_rows<uint32_t><<<grid, 256, 0, st>>>((const uint32_t*)src, idx, n, (uint32_t*)dst, scatter);
+  return cudaGetLastError();
+}
+
 __global__ void k_gather_static(uint32_t n, const uint32_t* __restrict__ perm, const float4* __restrict__ in,
                                 const uint32_t* __restrict__ in_id, float4* __restrict__ out,
                                 uint32_t* __restrict__ out_id) {
@@ -1141,6 +1164,10 @@ upf_status upf_step(upf_system* s, int32_t nsteps) {
     set_error("upf_step: call upf_set_particles first");
     return UPF_ERR_STATE;
   }
+  if (s->graph_stale) {
+    UPF_TRY(build_step_graph(*s));
+    s->graph_stale = false;
+  }
   s->stepped = true;
   for (int32_t k = 0; k < nsteps; ++k) UPF_CUDA(cudaGraphLaunch(s->step_exec, s->stream));
   return UPF_OK;
@@ -1260,6 +1287,140 @@ upf_status upf_phase_integrate(upf_system* s) {
   UPF_TRY(phase_guard(s));
   s->stepped = true;
   UPF_CUDA(launch_integrate_phase(*s, s->stream));
+  return UPF_OK;
+}
+
+// ---- the predict-correct loop pass by pass, and device access for a
+// caller that exchanges fields between the passes (slab decomposition) -----
+static upf_status pcisph_guard(upf_system* s, const char* who) {
+  UPF_TRY(phase_guard(s));
+  if (s->prm.method != UPF_METHOD_PCISPH) {
+    set_error("%s: PCISPH systems only", who);
+    return UPF_ERR_UNSUPPORTED;
+  }
+  return UPF_OK;
+}
+
+upf_status upf_phase_loop_begin(upf_system* s) {
+  UPF_TRY(pcisph_guard(s, "upf_phase_loop_begin"));
+  s->stepped = true;
+  UPF_CUDA(launch_loop_init(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_phase_density(upf_system* s) {
+  UPF_TRY(pcisph_guard(s, "upf_phase_density"));
+  UPF_CUDA(launch_loop_density(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_phase_pressure_force(upf_system* s) {
+  UPF_TRY(pcisph_guard(s, "upf_phase_pressure_force"));
+  UPF_CUDA(launch_loop_pforce(*s, s->stream));
+  return UPF_OK;
+}
+
+upf_status upf_phase_loop_control(upf_system* s, int32_t* cont) {
+  UPF_TRY(pcisph_guard(s, "upf_phase_loop_control"));
+  if (!cont) {
+    set_error("upf_phase_loop_control: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(launch_loop_ctl(*s, s->stream, 0, false));
+  UPF_CUDA(cudaMemcpyAsync(s->st_host, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  const DevState& d = *s->st_host;
+  *cont = (d.final_iterations < s->prm.min_loops) ||
+          (d.too_large && d.final_iterations < s->prm.max_loops);
+  if (d.error_flags & ERR_NAN) *cont = 0;
+  return UPF_OK;
+}
+
+upf_status upf_get_device_state(upf_system* s, upf_device_state* out) {
+  UPF_TRY(phase_guard(s));
+  if (!out) {
+    set_error("upf_get_device_state: null");
+    return UPF_ERR_INVALID_ARG;
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->pos4 = (float*)s->A.pos;
+  out->vel4 = (float*)s->A.vel;
+  out->lag4 = (float*)s->A.lag;
+  out->type = s->A.type;
+  out->id = s->A.id;
+  out->n = s->n_dyn;
+  out->capacity_dynamic = s->capacity - s->n_static;
+  out->sorted_pos4 = (float*)s->B.pos;
+  out->sorted_id = s->B.id;
+  out->predicted_pos4 = (float*)s->xs;
+  out->pressure = s->press;
+  out->pq4 = (float*)s->pq;
+  out->density = s->rho;
+  out->loop_max_density_bits = &s->st->max_rho_bits;
+  out->stream = (void*)s->stream;
+  return UPF_OK;
+}
+
+upf_status upf_set_dynamic_device(upf_system* s, const float* pos4, const float* vel4, const float* lag4,
+                                  const int32_t* type, const uint32_t* id, uint32_t n) {
+  UPF_TRY(phase_guard(s));
+  System& S = *s;
+  if (n && (!pos4 || !vel4 || !lag4 || !type || !id)) {
+    set_error("upf_set_dynamic_device: null argument");
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (n + S.n_static > S.capacity) {
+    set_error("upf_set_dynamic_device: %u dynamic + %u boundary particles exceed capacity %u", n, S.n_static,
+              S.capacity);
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (S.rb.n_bodies) {
+    set_error("upf_set_dynamic_device: systems with rigid bodies keep their particle set");
+    return UPF_ERR_UNSUPPORTED;
+  }
+  cudaStream_t st = S.stream;
+  const float4* p4 = (const float4*)pos4;
+  const float4* v4 = (const float4*)vel4;
+  const float4* l4 = (const float4*)lag4;
+  // the inputs may alias the system's own arrays: copy through B first
+  if (n) {
+    UPF_CUDA(cudaMemcpyAsync(S.B.pos, p4, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.B.vel, v4, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.B.lag, l4, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.B.type, type, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.B.id, id, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.pos, S.B.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.vel, S.B.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.lag, S.B.lag, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.type, S.B.type, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(S.A.id, S.B.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+    UPF_CUDA(launch_upload_keys(S, st));
+  }
+  S.n_dyn = n;
+  drop_checkpoints(S);
+  S.graph_stale = true;
+  return UPF_OK;
+}
+
+upf_status upf_gather_rows(const void* src, uint32_t row_bytes, const uint32_t* idx, uint32_t n, void* dst,
+                           void* stream) {
+  if (n == 0) return UPF_OK;
+  if (!src || !idx || !dst || (row_bytes != 4 && row_bytes != 16)) {
+    set_error("upf_gather_rows: null pointer or row size %u (4 or 16)", row_bytes);
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(launch_rows(src, row_bytes, idx, n, dst, false, (cudaStream_t)stream));
+  return UPF_OK;
+}
+
+upf_status upf_scatter_rows(const void* src, uint32_t row_bytes, const uint32_t* idx, uint32_t n, void* dst,
+                            void* stream) {
+  if (n == 0) return UPF_OK;
+  if (!src || !idx || !dst || (row_bytes != 4 && row_bytes != 16)) {
+    set_error("upf_scatter_rows: null pointer or row size %u (4 or 16)", row_bytes);
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(launch_rows(src, row_bytes, idx, n, dst, true, (cudaStream_t)stream));
   return UPF_OK;
 }
 

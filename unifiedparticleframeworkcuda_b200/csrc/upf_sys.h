@@ -60,8 +60,8 @@ struct LaunchShape {
   int external_threads = 256;  // 128, 256
   int density_threads = 256;   // with density_rows: see kLoopShapes
   int density_rows = 8;
-  int pforce_threads = 256;    // with pforce_rows: the same pairs
-  int pforce_rows = 8;
+  int pforce_threads = 256;    // with pforce_rows: the same pairs, where the ring fits
+  int pforce_rows = 4;
   int density_mode = 0;        // list entries by 0: the TMA ring, 1: direct loads (rows = entries per batch)
   int pforce_mode = 0;
   int nlist_mode = 0;          // 0: each lane its own query box; 1: the warp's union of boxes
@@ -79,6 +79,8 @@ constexpr int kNumLoopShapes = sizeof(kLoopShapes) / sizeof(kLoopShapes[0]);
 constexpr bool pforce_ring_fits(int mode, int threads, int rows) {
   return mode != 0 || (threads / 32) * ((3 * rows * 32 * 8 + 3 * 8 + 127) / 128 * 128) + 1024 <= 48 * 1024;
 }
+static_assert(pforce_ring_fits(LaunchShape{}.pforce_mode, LaunchShape{}.pforce_threads, LaunchShape{}.pforce_rows),
+              "the default pressure-force shape must be one that is built");
 constexpr int kListRowVariants = 4;  // tensor maps for 2, 4, 8 and 16 rows per box
 inline int rows_index(int rows) { return rows == 2 ? 0 : (rows == 4 ? 1 : (rows == 8 ? 2 : 3)); }
 
@@ -135,6 +137,7 @@ struct System {
   uint32_t n_dyn = 0, n_static = 0;
   bool have_particles = false;
   bool stepped = false;          // a step or phase ran since the last upf_set_particles
+  bool graph_stale = false;      // the dynamic count changed (upf_set_dynamic_device): rebuild the step graph
 
   DynArrays A, B;
   uint32_t* keysA = nullptr;   // keys of A (sorted in place by the sort)
