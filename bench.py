@@ -110,18 +110,21 @@ def oracle_from_system(s, sc, threads, fp64=False):
     import unifiedparticleframeworkcuda_b200 as upf
     from oracle import pyoracle
     g = s.particles()
+    lag = s.lagged_state()  # (previous correction pressure, last one, last predicted density), same order
     ids = g["id"].astype(np.int64)
     pos = np.array(sc.pos, np.float32, copy=True)
     vel = np.array(sc.vel, np.float32, copy=True)
     p = upf.derive_params(sc.params)
+    prev = np.zeros(sc.n, np.float32)
     pres = np.zeros(sc.n, np.float32)
     dens = np.full(sc.n, np.float32(p.rest_density), np.float32)
     pos[ids] = g["pos"]
     vel[ids] = g["vel"]
-    pres[ids] = g["pressure"]
-    dens[ids] = g["density"]
+    prev[ids] = lag[:, 0]
+    pres[ids] = lag[:, 1]
+    dens[ids] = lag[:, 2]
     o = pyoracle.OracleSim(p, pos, vel, sc.type, threads=threads, keep_fields=False, fp64=fp64)
-    o.set_lagged(pres, dens)
+    o.set_lagged(prev, pres, dens)
     return o
 
 

@@ -532,6 +532,12 @@ upf_status upf_get_particles(upf_system* s, float* pos4, float* vel4, float* den
  * order it uploaded them in; any pointer may be NULL. */
 upf_status upf_get_particles_input_order(upf_system* s, float* pos4, float* vel4, float* density,
                                         float* pressure, int32_t* type, uint32_t n);
+/* The dynamic particles' lagged PCISPH state in current device order (the
+ * order of upf_get_particles), n x 4 floats: the final correction pressure
+ * of the step before last (what the next step's external forces read as
+ * previous_correction_pressure_, UnifiedPhysics.cpp:5360-5363), that of the
+ * last step, the last step's predicted density, 0. n = the dynamic count. */
+upf_status upf_get_lagged_state(upf_system* s, float* lag4, uint32_t n);
 /* Per-particle step fields of the last step, in the sorted order of that step:
  * external force, correction pressure force, predicted density. */
 upf_status upf_get_step_fields(upf_system* s, float* force4, float* pforce4,

@@ -96,7 +96,7 @@ def lib():
         L.orc_keep_fields.argtypes = [C.c_void_p, C.c_int]
         L.orc_set_reference_literal.argtypes = [C.c_void_p, C.c_uint32]
         L.orc_set_reference_literal.restype = None
-        L.orc_set_lagged.argtypes = [C.c_void_p, fp, fp]
+        L.orc_set_lagged.argtypes = [C.c_void_p, fp, fp, fp]
         L.orc_set_lagged.restype = None
         L.orc_get.argtypes = [C.c_void_p, fp, fp, fp, fp, i32p, u32p, u32p]
         L.orc_get_step_fields.argtypes = [C.c_void_p, fp, fp, fp, fp, fp, fp, u32p]
@@ -254,13 +254,13 @@ class OracleSim:
         LITERAL_* bits; before set_rigid_bodies for the inertia bit)."""
         lib().orc_set_reference_literal(self._h, int(mask))
 
-    def set_lagged(self, pressure, density):
-        """Continue from another run's state: its last step's correction
-        pressure and predicted density per particle, in creation order."""
-        pressure = np.ascontiguousarray(pressure, np.float32)
-        density = np.ascontiguousarray(density, np.float32)
-        assert pressure.shape == (self.n,) and density.shape == (self.n,)
-        lib().orc_set_lagged(self._h, _ptr(pressure, C.c_float), _ptr(density, C.c_float))
+    def set_lagged(self, pressure_prev, pressure, density):
+        """Continue from another run's state, per particle in creation order:
+        the final correction pressure of the step before last and of the last
+        step, and the last step's predicted density."""
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (pressure_prev, pressure, density)]
+        assert all(a.shape == (self.n,) for a in arrs)
+        lib().orc_set_lagged(self._h, *[_ptr(a, C.c_float) for a in arrs])
 
     def step(self) -> StepInfo:
         info = StepInfo()

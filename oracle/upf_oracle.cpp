@@ -290,7 +290,7 @@ struct SimBase {
   virtual int set_bodies(const int32_t*, uint32_t, uint32_t) = 0;
   virtual int get_rigid(float*, float*, float*, float*) const = 0;
   virtual void set_keep_fields(bool on) = 0;
-  virtual void set_lagged(const float*, const float*) = 0;
+  virtual void set_lagged(const float*, const float*, const float*) = 0;
   virtual void set_literal(uint32_t mask) = 0;
 };
 
@@ -999,12 +999,15 @@ struct Sim : SimBase {
 
   uint32_t count() const override { return (uint32_t)ps.size(); }
 
-  // Resume a PCISPH run from another run's state: the correction pressure
-  // and predicted density of its last step, per particle in creation order
-  // (the lagged values of UnifiedPhysics.cpp:5360-5363 at the next step).
-  void set_lagged(const float* pressure, const float* density) override {
+  // Resume a PCISPH run from another run's state, per particle in creation
+  // order: the final correction pressure of the step before last (what the
+  // next step's external forces read as previous_correction_pressure_), of
+  // the last step (which becomes it after them, UnifiedPhysics.cpp:5360-5363),
+  // and the last step's predicted density.
+  void set_lagged(const float* pressure_prev, const float* pressure, const float* density) override {
     for (Particle<R>& p : ps) {
-      p.p_corr = p.p_prev = R(pressure[p.id]);
+      p.p_prev = R(pressure_prev[p.id]);
+      p.p_corr = R(pressure[p.id]);
       p.rho_star = p.rho_prev = R(density[p.id]);
     }
   }
@@ -1376,8 +1379,8 @@ void orc_keep_fields(orc_sim* s, int on) { s->impl->set_keep_fields(on != 0); }
 
 void orc_set_reference_literal(orc_sim* s, uint32_t mask) { s->impl->set_literal(mask); }
 
-void orc_set_lagged(orc_sim* s, const float* pressure, const float* density) {
-  s->impl->set_lagged(pressure, density);
+void orc_set_lagged(orc_sim* s, const float* pressure_prev, const float* pressure, const float* density) {
+  s->impl->set_lagged(pressure_prev, pressure, density);
 }
 
 void orc_get(const orc_sim* s, float* pos4, float* vel4, float* density, float* pressure,

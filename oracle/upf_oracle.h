@@ -68,9 +68,10 @@ void orc_keep_fields(orc_sim* s, int on);
 #define ORC_LITERAL_OWN_BODY_SPRING 2u
 #define ORC_LITERAL_ZERO_INVERSE_INERTIA 4u
 void orc_set_reference_literal(orc_sim* s, uint32_t mask);
-/* continue from another run's state: last-step correction pressure and
- * predicted density per particle, in creation order */
-void orc_set_lagged(orc_sim* s, const float* pressure, const float* density);
+/* continue from another run's state, per particle in creation order: the
+ * final correction pressure of the step before last and of the last step,
+ * and the last step's predicted density */
+void orc_set_lagged(orc_sim* s, const float* pressure_prev, const float* pressure, const float* density);
 /* current array order (sorted by key at the end of the last step) */
 void orc_get(const orc_sim* s, float* pos4, float* vel4, float* density, float* pressure,
              int32_t* type, uint32_t* id, uint32_t* key);

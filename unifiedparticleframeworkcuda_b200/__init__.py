@@ -73,6 +73,7 @@ def lib():
             "upf_scatter_rows": [vp, C.c_uint32, vp, C.c_uint32, vp, vp],
             "upf_get_particles": [vp, fp, fp, fp, fp, i32p, u32p, u32p],
             "upf_get_particles_input_order": [vp, fp, fp, fp, fp, i32p, C.c_uint32],
+            "upf_get_lagged_state": [vp, fp, C.c_uint32],
             "upf_get_step_fields": [vp, fp, fp, fp, u32p, u32p],
             "upf_get_neighbors": [vp, u32p, u32p, C.c_uint32, u32p],
             "upf_get_sorted_keys": [vp, u32p, u32p, u32p],
@@ -423,6 +424,14 @@ class ParticleSystem:
                                       _p(pre, C.c_float), _p(typ, C.c_int32), _p(ids, C.c_uint32), C.byref(cnt)),
               "upf_get_particles")
         return dict(pos=pos, vel=vel, density=den, pressure=pre, type=typ, id=ids)
+
+    def lagged_state(self):
+        """The dynamic particles' lagged PCISPH state, in the order of
+        particles(): (final correction pressure of the step before last, of
+        the last step, last predicted density, 0) per particle."""
+        out = np.zeros((self.n_dynamic, 4), np.float32)
+        check(lib().upf_get_lagged_state(self._h, _p(out, C.c_float), self.n_dynamic), "upf_get_lagged_state")
+        return out
 
     def particles_input_order(self):
         """Every particle of the last set_particles call at its input index

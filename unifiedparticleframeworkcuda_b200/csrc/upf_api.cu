@@ -1394,9 +1394,9 @@ upf_status upf_set_dynamic_device(upf_system* s, const float* pos4, const float*
     UPF_CUDA(cudaMemcpyAsync(S.A.lag, S.B.lag, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
     UPF_CUDA(cudaMemcpyAsync(S.A.type, S.B.type, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
     UPF_CUDA(cudaMemcpyAsync(S.A.id, S.B.id, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
-    UPF_CUDA(launch_upload_keys(S, st));
   }
-  S.n_dyn = n;
+  S.n_dyn = n;  // the keys below cover the new count
+  if (n) UPF_CUDA(launch_upload_keys(S, st));
   drop_checkpoints(S);
   S.graph_stale = true;
   return UPF_OK;
@@ -1745,6 +1745,17 @@ upf_status upf_get_particles_input_order(upf_system* s, float* pos4, float* vel4
     set_error("upf_get_particles_input_order: %s", cudaGetErrorString(e));
     return UPF_ERR_CUDA;
   }
+  return UPF_OK;
+}
+
+upf_status upf_get_lagged_state(upf_system* s, float* lag4, uint32_t n) {
+  UPF_TRY(phase_guard(s));
+  if (n != s->n_dyn || (n && !lag4)) {
+    set_error("upf_get_lagged_state: n = %u, the system has %u dynamic particles", n, s->n_dyn);
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (n) UPF_CUDA(cudaMemcpyAsync(lag4, s->A.lag, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
   return UPF_OK;
 }
 

@@ -8,7 +8,8 @@ lies in its range and holds, besides them:
 
   * ghosts: copies of the neighbouring slabs' particles within `width` (the
     support radius and a margin) of its faces, refreshed every step;
-  * the boundary particles within `width` of its range (static, set once).
+  * the boundary particles within two `width`s of its range (static, set
+    once), so that those within one width have complete Akinci volumes.
 
 Each slab is an ordinary upf_system. A step runs the library's phases on
 every slab, with exchanges between neighbouring slabs:
@@ -266,7 +267,10 @@ class SlabScene:
         x = pos[:, 0]
         for lo, hi in self.bounds:
             own = dyn & (x >= lo) & (x < hi)
-            bnd = (~dyn) & (x >= lo - self.width) & (x < hi + self.width)
+            # boundary particles within two widths: those within one width
+            # (the neighbours of owned particles and ghosts) then have their
+            # complete boundary neighbourhood for the Akinci volume
+            bnd = (~dyn) & (x >= lo - 2 * self.width) & (x < hi + 2 * self.width)
             near = dyn & (x >= lo - self.width) & (x < hi + self.width)
             # room for the owned particles growing by migration, and the ghosts
             cap = int(capacity_factor * near.sum()) + int(bnd.sum()) + 1024
