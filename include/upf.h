@@ -447,6 +447,20 @@ upf_status upf_obj_read_triangles(const char* path, float* tri9, uint32_t capaci
 upf_status upf_mesh_particles(int device, const float* tri9, uint32_t n_tri, float scale_x, float scale_y,
                               float scale_z, float spacing, float* pos4, uint32_t capacity, uint32_t* n_out);
 
+/* A rigid body's surface particles on GPU `device`, for the coupling
+ * scenes' procedural bodies (in place of voxelising an OBJ model with
+ * ObjectLoader::LoadParticles, src/cpu/ObjectLoader.cpp:8-97): shape 0 a
+ * Fibonacci lattice of n_target points on a sphere of the given radius;
+ * 1 a k x k grid of cell centres on each face of a cube of half-edge radius,
+ * k = max(2, round(sqrt(n_target / 6))); 2 an nu x nv grid on a torus of
+ * major radius `radius` and minor radius radius / 3, nu = max(8,
+ * round(sqrt(3 n_target))), nv = max(4, round(n_target / nu)). Each point p
+ * becomes rot9 (row-major) p + center, computed in double and stored as
+ * float (w = 0). pos4 NULL: *n_out = the count only. Feed the result to
+ * upf_set_particles as RIGID particles of one body. */
+upf_status upf_scene_rigid_surface(int device, int32_t shape, float radius, uint32_t n_target, const float rot9[9],
+                                   const float center[3], float* pos4, uint32_t capacity, uint32_t* n_out);
+
 /* Scene::createFluidObject (src/sceneConfigure/Scene.cpp:597-646) on GPU
  * `device`: a lattice block filling [box_min, box_max) at `spacing`, in the
  * reference's order (y, then x, then z) and bit for bit its positions

@@ -106,3 +106,25 @@ def test_box_boundary_refuses_walls_at_the_origin(upf_lib):
     with pytest.raises(UpfError) as e:
         upf_lib.scene_box_boundary((0.0, 0.0, 0.0), (0.3, 0.2, 0.25), (0.0, 0.0, 0.0), 0.01, 0.005, 0.005, 1)
     assert e.value.status == CODE["UPF_ERR_INVALID_ARG"] and "origin" in str(e.value)
+
+
+@pytest.mark.parametrize("shape", [0, 1, 2])
+def test_rigid_surface_on_gpu_equals_the_host_sampler(upf_lib, shape):
+    """upf_scene_rigid_surface against the host samplers of the coupling
+    scenes (scenes.sample_sphere / sample_box / sample_torus, rotated and
+    moved in double): the same count, and every point within 1e-6 m (the two
+    evaluate cos, sin and acos in different double libraries before rounding
+    to float)."""
+    rng = np.random.default_rng(shape)
+    for r, n in ((0.05, 2000), (0.13, 7777)):
+        R = scenes._random_rotation(rng.uniform(size=3))
+        c = rng.uniform(0.2, 1.0, 3)
+        want = (scenes.sample_sphere, scenes.sample_box, scenes.sample_torus)[shape](r, n) @ R.T + c
+        got = upf_lib.scene_rigid_surface(shape, r, n, R.astype(np.float32), c.astype(np.float32))
+        assert got.shape[0] == want.shape[0]
+        # the host sampler works from the double radius and rotation; the
+        # device takes them as float, so compare at float input precision
+        want32 = (scenes.sample_sphere, scenes.sample_box, scenes.sample_torus)[shape](
+            float(np.float32(r)), n) @ R.astype(np.float32).astype(np.float64).T + c.astype(np.float32)
+        assert np.abs(got[:, :3] - want32).max() <= 1e-6
+        assert np.abs(got[:, :3] - want).max() <= 1e-5 and np.all(got[:, 3] == 0)

@@ -139,6 +139,7 @@ def lib():
             "upf_io_read_scene_particles": [C.c_char_p, fp, fp, fp, i32p, C.c_uint32, u32p],
             "upf_obj_read_triangles": [C.c_char_p, fp, C.c_uint32, u32p],
             "upf_scene_fluid_block": [C.c_int, fp, fp, C.c_float, C.c_float, fp, fp, C.c_uint32, u32p],
+            "upf_scene_rigid_surface": [C.c_int, C.c_int32, C.c_float, C.c_uint32, fp, fp, fp, C.c_uint32, u32p],
             "upf_scene_box_boundary": [C.c_int, fp, fp, fp, C.c_float, C.c_float, C.c_float, C.c_int32, fp, fp,
                                        C.c_uint32, u32p],
             "upf_mesh_particles": [C.c_int, fp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, fp,
@@ -223,6 +224,20 @@ def scene_fluid_block(box_min, box_max, spacing: float, jitter: float = 0.0, off
     check(lib().upf_scene_fluid_block(*args, None, 0, C.byref(n)), "upf_scene_fluid_block")
     out = np.zeros((n.value, 4), np.float32)
     check(lib().upf_scene_fluid_block(*args, _p(out, C.c_float), n.value, C.byref(n)), "upf_scene_fluid_block")
+    return out
+
+
+def scene_rigid_surface(shape: int, radius: float, n_target: int, rotation=None, center=(0.0, 0.0, 0.0),
+                        device: int = 0) -> np.ndarray:
+    """A procedural rigid body's surface particles on the GPU
+    (upf_scene_rigid_surface; shape 0 sphere, 1 cube, 2 torus), n x 4."""
+    R = np.ascontiguousarray(np.eye(3) if rotation is None else rotation, np.float32).reshape(9)
+    c = _f3(center)
+    n = C.c_uint32()
+    args = (device, int(shape), float(radius), int(n_target), _p(R, C.c_float), _p(c, C.c_float))
+    check(lib().upf_scene_rigid_surface(*args, None, 0, C.byref(n)), "upf_scene_rigid_surface")
+    out = np.zeros((n.value, 4), np.float32)
+    check(lib().upf_scene_rigid_surface(*args, _p(out, C.c_float), n.value, C.byref(n)), "upf_scene_rigid_surface")
     return out
 
 

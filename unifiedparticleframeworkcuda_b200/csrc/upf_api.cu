@@ -995,13 +995,10 @@ upf_status upf_set_rigid_bodies(upf_system* s, const int32_t* body_of_particle, 
     return UPF_ERR_INVALID_ARG;
   }
   const int32_t* bop = body_of_particle;
-  // AddToRigidBody (UnifiedPhysics.cpp:825-885): mass, centre of mass and
-  // momentum, then inertia and angular momentum about the centre, summed in
-  // FP64 in input order; the inertia is inverted in FP64 by the adjugate
-  // (Matrix3x3::CalculateInverse, Matrix3x3.cpp:121-156).
-  const double m = S.prm.mass;
-  std::vector<double> M(n_bodies, 0.0), C(3 * n_bodies, 0.0), Pm(3 * n_bodies, 0.0), I(9 * n_bodies, 0.0),
-      L(3 * n_bodies, 0.0);
+  // The rigid list: bodies in index order, each body's particles in input
+  // order (a counting sort on the host, O(particles)); the bodies' mass,
+  // centre, momenta and inertia (AddToRigidBody, UnifiedPhysics.cpp:825-885)
+  // are summed on the device in FP64 (k_rigid_assemble).
   std::vector<uint32_t> start(n_bodies + 1, 0);
   for (uint32_t id = 0; id < n; ++id) {
     const int32_t b = bop[id];
@@ -1010,80 +1007,25 @@ upf_status upf_set_rigid_bodies(upf_system* s, const int32_t* body_of_particle, 
       set_error("upf_set_rigid_bodies: particle %u: body %d is out of range or the particle is not RIGID", id, b);
       return UPF_ERR_INVALID_ARG;
     }
-    const float4 x = S.host_pos[id], v = S.host_vel[id];
-    M[b] += m;
-    C[3 * b] += m * (double)x.x;
-    C[3 * b + 1] += m * (double)x.y;
-    C[3 * b + 2] += m * (double)x.z;
-    Pm[3 * b] += m * (double)v.x;
-    Pm[3 * b + 1] += m * (double)v.y;
-    Pm[3 * b + 2] += m * (double)v.z;
     start[b + 1] += 1;
   }
   for (uint32_t b = 0; b < n_bodies; ++b) {
-    if (!(M[b] > 0)) {
+    if (start[b + 1] == 0) {
       set_error("upf_set_rigid_bodies: body %u has no particles", b);
       return UPF_ERR_INVALID_ARG;
     }
-    for (int a = 0; a < 3; ++a) C[3 * b + a] /= M[b];
+    start[b + 1] += start[b];
   }
-  for (uint32_t id = 0; id < n; ++id) {
-    const int32_t b = bop[id];
-    if (b < 0) continue;
-    const float4 x = S.host_pos[id], v4 = S.host_vel[id];
-    const double r[3] = {(double)x.x - C[3 * b], (double)x.y - C[3 * b + 1], (double)x.z - C[3 * b + 2]};
-    const double v[3] = {m * (double)v4.x, m * (double)v4.y, m * (double)v4.z};
-    const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) I[9 * b + 3 * i + j] += m * ((i == j ? rr : 0.0) - r[i] * r[j]);
-    L[3 * b] += r[1] * v[2] - r[2] * v[1];
-    L[3 * b + 1] += r[2] * v[0] - r[0] * v[2];
-    L[3 * b + 2] += r[0] * v[1] - r[1] * v[0];
-  }
-  std::vector<DevBody> bodies(n_bodies);
-  for (uint32_t b = 0; b < n_bodies; ++b) {
-    DevBody& B = bodies[b];
-    std::memset(&B, 0, sizeof(B));
-    const double* A = &I[9 * b];
-    double inv[9] = {0};
-    const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
-                       A[2] * (A[3] * A[7] - A[4] * A[6]);
-    if (det != 0.0) {
-      inv[0] = (A[4] * A[8] - A[5] * A[7]) / det;
-      inv[1] = (A[2] * A[7] - A[1] * A[8]) / det;
-      inv[2] = (A[1] * A[5] - A[2] * A[4]) / det;
-      inv[3] = (A[5] * A[6] - A[3] * A[8]) / det;
-      inv[4] = (A[0] * A[8] - A[2] * A[6]) / det;
-      inv[5] = (A[2] * A[3] - A[0] * A[5]) / det;
-      inv[6] = (A[3] * A[7] - A[4] * A[6]) / det;
-      inv[7] = (A[1] * A[6] - A[0] * A[7]) / det;
-      inv[8] = (A[0] * A[4] - A[1] * A[3]) / det;
-    }
-    B.mass = (float)M[b];
-    B.pos = make_float3((float)C[3 * b], (float)C[3 * b + 1], (float)C[3 * b + 2]);
-    B.P = make_float3((float)Pm[3 * b], (float)Pm[3 * b + 1], (float)Pm[3 * b + 2]);
-    B.vel = make_float3((float)(Pm[3 * b] / M[b]), (float)(Pm[3 * b + 1] / M[b]), (float)(Pm[3 * b + 2] / M[b]));
-    B.L = make_float3((float)L[3 * b], (float)L[3 * b + 1], (float)L[3 * b + 2]);
-    B.q[0] = 1.0f;
-    for (int i = 0; i < 3; ++i) {
-      B.rot[i][i] = 1.0f;
-      for (int j = 0; j < 3; ++j) B.iinv_local[i][j] = (float)inv[3 * i + j];
-    }
-  }
-  // the rigid list: bodies in index order, each body's particles in input order;
-  // relative positions x - (float)centre, in float as the reference stores them
-  for (uint32_t b = 0; b < n_bodies; ++b) start[b + 1] += start[b];
   const uint32_t n_rigid = start[n_bodies];
   std::vector<uint32_t> fill(start.begin(), start.end() - 1), id_entry(n, 0xffffffffu);
   std::vector<int32_t> id_body(n, -1), entry_body(n_rigid);
-  std::vector<float4> entry_r0(n_rigid);
+  std::vector<float4> entry_pos(n_rigid), entry_vel(n_rigid);
   for (uint32_t id = 0; id < n; ++id) {
     const int32_t b = bop[id];
     if (b < 0) continue;
     const uint32_t k = fill[b]++;
-    const float4 x = S.host_pos[id];
-    const float3 c = bodies[b].pos;
-    entry_r0[k] = make_float4(x.x - c.x, x.y - c.y, x.z - c.z, 0.0f);
+    entry_pos[k] = S.host_pos[id];
+    entry_vel[k] = S.host_vel[id];
     entry_body[k] = b;
     id_entry[id] = k;
     id_body[id] = b;
@@ -1116,15 +1058,17 @@ upf_status upf_set_rigid_bodies(upf_system* s, const int32_t* body_of_particle, 
     r.n_rigid = n_rigid;
     r.n_ids = n;
     cudaStream_t st = S.stream;
-    UPF_CUDA(cudaMemcpyAsync(r.bodies, bodies.data(), sizeof(DevBody) * n_bodies, cudaMemcpyHostToDevice, st));
     UPF_CUDA(cudaMemcpyAsync(r.start, start.data(), sizeof(uint32_t) * (n_bodies + 1), cudaMemcpyHostToDevice, st));
     UPF_CUDA(cudaMemcpyAsync(r.id_body, id_body.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
     UPF_CUDA(cudaMemcpyAsync(r.id_entry, id_entry.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
-    if (n_rigid) {
-      UPF_CUDA(cudaMemcpyAsync(r.entry_r0, entry_r0.data(), sizeof(float4) * n_rigid, cudaMemcpyHostToDevice, st));
-      UPF_CUDA(
-          cudaMemcpyAsync(r.entry_body, entry_body.data(), sizeof(int32_t) * n_rigid, cudaMemcpyHostToDevice, st));
-    }
+    UPF_CUDA(cudaMemcpyAsync(r.entry_body, entry_body.data(), sizeof(int32_t) * n_rigid, cudaMemcpyHostToDevice, st));
+    // the entries' positions and velocities for the assembly, in scratch
+    // that is not live before the first step
+    float4* epos = S.xs;
+    float4* evel = S.pforce;
+    UPF_CUDA(cudaMemcpyAsync(epos, entry_pos.data(), sizeof(float4) * n_rigid, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(cudaMemcpyAsync(evel, entry_vel.data(), sizeof(float4) * n_rigid, cudaMemcpyHostToDevice, st));
+    UPF_CUDA(launch_rigid_assemble(S.prm.mass, r.bodies, n_bodies, r.start, epos, evel, r.entry_r0, st));
     UPF_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
     S.rb = r;
   }

@@ -116,7 +116,7 @@ upf_status build_batch_graph(upf_batch* b) {
     return e;
   };
   parts.loop = [](void* c, cudaStream_t st, cudaGraphConditionalHandle h) {
-    return batch_launch_loop_body(*static_cast<BatchSystem*>(c), st, h, true);
+    return batch_capture_loop_body(*static_cast<BatchSystem*>(c), st, h);
   };
   parts.post = [](void* c, cudaStream_t st) { return batch_launch_integrate(*static_cast<BatchSystem*>(c), st); };
   return capture_step_graph(parts, &b->step_graph, &b->step_exec);
@@ -262,6 +262,7 @@ upf_status upf_batch_create(const upf_params* params, const uint32_t* counts, ui
   ALLOC(b->st_d, num_scenes);
   ALLOC(b->group_scene_d, group_scene.size()); ALLOC(b->seg_begin_d, num_scenes); ALLOC(b->seg_end_d, num_scenes);
   ALLOC(b->cell_base_d, num_scenes); ALLOC(b->any_active_d, 1);
+  ALLOC(b->active_groups_d, n / kSegAlign + 1); ALLOC(b->n_active_groups_d, 1);
   ALLOC(b->x.comp_begin_d, num_scenes); ALLOC(b->x.stage_a, std::max<size_t>(total, 1));
   ALLOC(b->x.stage_b, std::max<size_t>(total, 1));
 #undef ALLOC

@@ -99,6 +99,30 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 
+// Packed pairs of floats (sm_100's f32x2 arithmetic): one instruction for two
+// lanes, each rounded exactly as the scalar operation (round to nearest, no
+// flush of subnormals), so results stay bit-identical to scalar code.
+__device__ __forceinline__ unsigned long long pk2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 up2(unsigned long long v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
 // |a - b| as vmml computes it: sqrtf((dx*dx + dy*dy) + dz*dz)
 __device__ __forceinline__ float dist3(float4 a, float4 b) {
   float dx = fsub(a.x, b.x), dy = fsub(a.y, b.y), dz = fsub(a.z, b.z);
@@ -135,8 +159,15 @@ __device__ __forceinline__ int bin_of_r2(float r2, float factor, const float* th
 // that takes the zero entry: pairs from there on return 300 exactly as
 // bin_of_r2 does.
 constexpr float kBinEdge = 1.0f / 1024.0f;
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));  // within 2 ulp
+  return r;
+}
 __device__ __forceinline__ int bin_of_r2_edge(float r2, float factor, float r2_edge) {
-  const float x = r2 * rsqrtf(r2) * factor * (float)kLut;
+  // (a subnormal r2 flushes to 0 in the root: x is then NaN or infinite, and
+  // the exact root decides)
+  const float x = r2 * rsqrt_approx(r2) * factor * (float)kLut;
   int g = (int)x;
   if (!(fabsf(x - (float)g - 0.5f) <= 0.5f - kBinEdge)) g = lut_index(__fsqrt_rn(r2), factor);
   g = g > kLut - 1 ? kLut - 1 : g;

@@ -46,11 +46,6 @@ __device__ __forceinline__ void stage_lut(float* dst, const float* __restrict__ 
   for (int k = threadIdx.x; k < UPF_LUT_ENTRIES; k += blockDim.x) dst[k] = src[k];
 }
 
-// the bin thresholds follow the five tables in the device lookup buffer
-__device__ __forceinline__ void stage_thresholds(float* dst, const float* __restrict__ luts) {
-  for (int k = threadIdx.x; k < kThresholds; k += blockDim.x) dst[k] = luts[5 * UPF_LUT_ENTRIES + k];
-}
-
 __device__ __forceinline__ float4 f4(float x, float y, float z) { return make_float4(x, y, z, 0.0f); }
 
 // Neighbour loop with memory-level parallelism: the list entries of a batch
@@ -139,13 +134,15 @@ struct Scope {
 // batched scenes: the key of a padding slot (above every 30-bit Morton key)
 constexpr uint32_t kPadKeyBatch = 1u << 30;
 
+// The scope of virtual block `block` (blockIdx.x, or a group taken from a
+// list of work by a resident grid).
 template <bool kBatch>
-__device__ __forceinline__ Scope enter_scope(const DevParams& Pk, const float* luts, DevState* st, uint32_t n,
-                                             const BatchView& bv, DevParams* sP, bool loop_pass) {
+__device__ __forceinline__ Scope enter_scope_at(uint32_t block, const DevParams& Pk, const float* luts, DevState* st,
+                                                uint32_t n, const BatchView& bv, DevParams* sP, bool loop_pass) {
   if constexpr (!kBatch) {
     return Scope{&Pk, luts, st, n, 0u, false};
   } else {
-    const uint32_t s = bv.group_scene[(blockIdx.x * blockDim.x) / kSegAlign];
+    const uint32_t s = bv.group_scene[(block * blockDim.x) / kSegAlign];
     const uint32_t* src = reinterpret_cast<const uint32_t*>(bv.params + s);
     for (uint32_t k = threadIdx.x; k < sizeof(DevParams) / 4; k += blockDim.x)
       reinterpret_cast<uint32_t*>(sP)[k] = src[k];
@@ -153,6 +150,12 @@ __device__ __forceinline__ Scope enter_scope(const DevParams& Pk, const float* l
     const bool skip = loop_pass && !*reinterpret_cast<volatile int32_t*>(&sst->loop_active);
     return Scope{sP, bv.luts + (size_t)s * kLutFloats, sst, bv.seg_end[s], s, skip};
   }
+}
+
+template <bool kBatch>
+__device__ __forceinline__ Scope enter_scope(const DevParams& Pk, const float* luts, DevState* st, uint32_t n,
+                                             const BatchView& bv, DevParams* sP, bool loop_pass) {
+  return enter_scope_at<kBatch>(blockIdx.x, Pk, luts, st, n, bv, sP, loop_pass);
 }
 
 // The list walk of the loop passes, in one of two modes:
@@ -175,7 +178,7 @@ struct ListArgs {
 };
 
 template <bool kDirect, bool kWithVals, int kThreads, int kRows, class Body>
-__device__ __forceinline__ bool walk_lists(const ListArgs& L, uint32_t i, uint32_t cnt, Body&& body) {
+__device__ __forceinline__ bool walk_lists(const ListArgs& L, uint32_t block, uint32_t i, uint32_t cnt, Body&& body) {
   if constexpr (kDirect) {
     const uint32_t* __restrict__ col = L.nbr + i;
     const uint32_t* __restrict__ vcol = L.vals + i;
@@ -197,7 +200,7 @@ __device__ __forceinline__ bool walk_lists(const ListArgs& L, uint32_t i, uint32
     WarpListRing<kWithVals, kRows>& ring = rings[warp];
     ring_init(ring);
     const uint32_t wcnt = __reduce_max_sync(0xffffffffu, cnt);
-    return ring_walk(ring, L.cmap, L.vmap, (int)(blockIdx.x * blockDim.x + warp * 32), wcnt, [&](int s, int k0) {
+    return ring_walk(ring, L.cmap, L.vmap, (int)(block * blockDim.x + warp * 32), wcnt, [&](int s, int k0) {
       body([&](int r) { return ring.codes[s][r][lane]; }, [&](int r) { return ring.vals[s][r][lane]; }, k0);
     });
   }
@@ -223,6 +226,13 @@ __global__ void __launch_bounds__(kBlock) k_reorder(uint32_t n, const uint32_t* 
 __device__ __forceinline__ float dist2(float4 a, float4 b) {
   float dx = fsub(a.x, b.x), dy = fsub(a.y, b.y), dz = fsub(a.z, b.z);
   return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+}
+// The same with x and y as one packed pair (axy = pk2(a.x, a.y)): the same
+// operations, the same roundings.
+__device__ __forceinline__ float dist2_xy(unsigned long long axy, float az, float4 b) {
+  const float2 s = up2(mul2(sub2(axy, pk2(b.x, b.y)), sub2(axy, pk2(b.x, b.y))));
+  const float dz = fsub(az, b.z);
+  return fadd(fadd(s.x, s.y), fmul(dz, dz));
 }
 
 // GetNeighbors (UnifiedPhysics.cpp:2242-2280) with ZIndex::BoxQuery
@@ -942,32 +952,37 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_external(
 // by the TMA ring or by direct loads (walk_lists); each lane gathers kRows
 // neighbours' predicted positions at once and accumulates them in list order.
 template <bool kBatch, bool kDirect, int kThreads, int kRows>
-__global__ void __launch_bounds__(kThreads) k_pcisph_density(
-    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const int32_t* __restrict__ type,
-    const float4* __restrict__ xs, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ nbr,
+__device__ __forceinline__ void density_block(
+    uint32_t block, const DevParams& Pk, const BatchView& bv, uint32_t n, const int32_t* __restrict__ type,
+    const float4* __restrict__ xs, const CUtensorMap& cmap, const uint32_t* __restrict__ nbr,
     const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, float* __restrict__ rho,
     float* __restrict__ press, float4* __restrict__ pq, DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
   __shared__ float m4[UPF_LUT_ENTRIES];
   __shared__ uint32_t wmax[kThreads / 32];
-  const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
+  const Scope sc = enter_scope_at<kBatch>(block, Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31;
-  stage_lut(m4, sc.luts + LUT_M4 * UPF_LUT_ENTRIES);
+  // the table times the mass: each pair adds the same rounded product
+  // m4[bin] * m as the reference's kernelM4Lut(d) * mass
+  const float mass = kBatch ? __ldg(&bv.params[sc.scene].mass) : Pk.mass;
+  for (int k = threadIdx.x; k < UPF_LUT_ENTRIES; k += blockDim.x)
+    m4[k] = fmul(__ldg(sc.luts + LUT_M4 * UPF_LUT_ENTRIES + k), mass);
   // the first r2 of the zero entry (thresholds follow the five tables)
   const float r2_edge = __ldg(sc.luts + 5 * UPF_LUT_ENTRIES + kLut);
   __syncthreads();
   const DevParams& P = *sc.P;
   DevState* st = sc.st;
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t i = block * blockDim.x + threadIdx.x;
   uint32_t best = 0;
   const bool active = i < sc.end && type[i] == UPF_LIQUID;
   const uint32_t cnt = active ? ncnt[i] : 0u;
   const float4 xi = active ? xs[i] : make_float4(0, 0, 0, 0);
+  const unsigned long long xiy = pk2(xi.x, xi.y);
   const float m = P.mass;
   float den = P.kernel_self * m;
   const ListArgs L{&cmap, &cmap, nbr, nullptr, P.nstride};
-  const bool ok = walk_lists<kDirect, false, kThreads, kRows>(L, i, cnt, [&](auto code, auto, int k0) {
+  const bool ok = walk_lists<kDirect, false, kThreads, kRows>(L, block, i, cnt, [&](auto code, auto, int k0) {
     // predicted positions; boundary particles sit in the array's tail at
     // their fixed positions
     float4 xj[kRows];
@@ -979,8 +994,8 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
       if (k0 + r < (int)cnt) {
         // the table bin of d from d^2 (exact); at or beyond h the bin is 300,
         // whose entry 0 adds +0 exactly as the reference's skipped term does
-        const float r2 = dist2(xi, xj[r]);
-        den += m4[bin_of_r2_edge(r2, P.lut_factor, r2_edge)] * m;
+        const float r2 = dist2_xy(xiy, xi.z, xj[r]);
+        den += m4[bin_of_r2_edge(r2, P.lut_factor, r2_edge)];  // table times mass
       }
     }
   });
@@ -1005,27 +1020,62 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_density(
   }
 }
 
+template <bool kBatch, bool kDirect, int kThreads, int kRows>
+__global__ void __launch_bounds__(kThreads) k_pcisph_density(
+    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, const int32_t* __restrict__ type,
+    const float4* __restrict__ xs, const __grid_constant__ CUtensorMap cmap, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, float* __restrict__ rho,
+    float* __restrict__ press, float4* __restrict__ pq, DevState* __restrict__ st_plain) {
+  density_block<kBatch, kDirect, kThreads, kRows>(blockIdx.x, Pk, bv, n, type, xs, cmap, nbr, ncnt, luts_plain, rho,
+                                                  press, pq, st_plain);
+}
+
+// Batched scenes once most have finished their loop: a resident grid takes
+// the 256-slot groups of the scenes still iterating from the list the loop
+// control wrote (direct list loads: the TMA ring's barriers belong to one
+// walk), instead of a CTA for every group of every scene.
+template <int kRows>
+__global__ void __launch_bounds__(kSegAlign) k_pcisph_density_active(
+    const BatchView bv, uint32_t n, const uint32_t* __restrict__ groups, const uint32_t* __restrict__ ngroups,
+    const int32_t* __restrict__ type, const float4* __restrict__ xs, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, float* __restrict__ rho, float* __restrict__ press,
+    float4* __restrict__ pq) {
+  const uint32_t count = *ngroups;
+  for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
+    density_block<true, true, kSegAlign, kRows>(groups[g], DevParams{}, bv, n, type, xs, CUtensorMap{}, nbr, ncnt,
+                                                 nullptr, rho, press, pq, nullptr);
+    __syncthreads();  // the next group reuses the shared scope and table
+  }
+}
+
 // ComputeCorrectivePressureForce (UnifiedPhysics.cpp:5493-5522), then the
 // prediction of the next iteration (PredictPositionAndVelocity). The
 // positions are the step's, at which the list was built: every entry lies
 // within h and carries the pressure-gradient table's value at its bin as its
 // list value, so the pass reads no table. List entries and values come by
 // the TMA ring or by direct loads (walk_lists).
+// Short TMA rings (at most 4 rows a stage) are held to 40 registers a thread
+// (six 256-thread CTAs an SM, no spills): occupancy hides the gathers'
+// latency.
+constexpr int pforce_min_blocks(bool direct, int threads, int rows) {
+  return (!direct && rows <= 4) ? 1536 / threads : 1;
+}
+
 template <bool kBatch, bool kDirect, int kThreads, int kRows>
-__global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
-    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
-    const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap vmap,
-    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt,
-    const float* __restrict__ luts_plain, const float4* __restrict__ pq, const float4* __restrict__ force,
-    float4* __restrict__ pforce, float4* __restrict__ xs, DevState* __restrict__ st_plain) {
+__device__ __forceinline__ void pforce_block(
+    uint32_t block, const DevParams& Pk, const BatchView& bv, uint32_t n, const DynArrays& B,
+    const CUtensorMap& cmap, const CUtensorMap& vmap, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain,
+    const float4* __restrict__ pq, const float4* __restrict__ force, float4* __restrict__ pforce,
+    float4* __restrict__ xs, DevState* __restrict__ st_plain) {
   __shared__ DevParams sP;
-  const Scope sc = enter_scope<kBatch>(Pk, luts_plain, st_plain, n, bv, &sP, true);
+  const Scope sc = enter_scope_at<kBatch>(block, Pk, luts_plain, st_plain, n, bv, &sP, true);
   if (sc.skip) return;  // uniform over the CTA: the scene's loop has finished
   const int lane = threadIdx.x & 31;
   if (kBatch) __syncthreads();  // the scene's parameters in shared memory
   const DevParams& P = *sc.P;
   DevState* st = sc.st;
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t i = block * blockDim.x + threadIdx.x;
   const bool active = i < sc.end && B.type[i] == UPF_LIQUID;
   const uint32_t cnt = active ? ncnt[i] : 0u;
   const float4 xi = active ? B.pos[i] : make_float4(0, 0, 0, 0);
@@ -1033,9 +1083,12 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
   // grad = p_i / rho0^2 + p_j / rho0^2, both quotients precomputed by the
   // density pass (pq.w); boundary particles have p = 0, so 0 / rho0^2 = 0
   const float qi = active ? pq[i].w : 0.0f;
-  float fx = 0, fy = 0, fz = 0;
+  // x and y as packed pairs: the same operations and roundings as scalar code
+  const unsigned long long xiy = pk2(xi.x, xi.y), mm = pk2(m, m);
+  unsigned long long fxy = pk2(0.0f, 0.0f);
+  float fz = 0;
   const ListArgs L{&cmap, &vmap, nbr, lval, P.nstride};
-  const bool ok = walk_lists<kDirect, true, kThreads, kRows>(L, i, cnt, [&](auto code, auto val, int k0) {
+  const bool ok = walk_lists<kDirect, true, kThreads, kRows>(L, block, i, cnt, [&](auto code, auto val, int k0) {
     // one gather per neighbour: position and p / rho0^2 packed in pq
     // (boundary particles sit in the tail, w = 0 there)
     float4 xj[kRows];
@@ -1046,21 +1099,49 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_pressure_force(
     for (int r = 0; r < kRows; ++r) {
       if (k0 + r < (int)cnt) {
         const float g = __uint_as_float(val(r));  // kernelPressureGradLut at the entry's bin
-        const float kx = (xi.x - xj[r].x) * g, ky = (xi.y - xj[r].y) * g, kz = (xi.z - xj[r].z) * g;
+        // k = (x_i - x_j) * g; f -= ((k * grad) * m) * m, per component
+        const unsigned long long kxy = mul2(sub2(xiy, pk2(xj[r].x, xj[r].y)), pk2(g, g));
+        const float kz = (xi.z - xj[r].z) * g;
         const float grad = qi + xj[r].w;
-        fx = fx - kx * grad * m * m;
-        fy = fy - ky * grad * m * m;
+        fxy = sub2(fxy, mul2(mul2(mul2(kxy, pk2(grad, grad)), mm), mm));
         fz = fz - kz * grad * m * m;
       }
     }
   });
   if (!ok && lane == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
   if (!active) return;
-  pforce[i] = f4(fx, fy, fz);
+  const float2 fp = up2(fxy);
+  pforce[i] = f4(fp.x, fp.y, fz);
   const float4 F = force[i];
   bool bad;
-  xs[i] = predict(P, xi, B.vel[i], make_float3(F.x, F.y, F.z), make_float3(fx, fy, fz), bad);
+  xs[i] = predict(P, xi, B.vel[i], make_float3(F.x, F.y, F.z), make_float3(fp.x, fp.y, fz), bad);
   if (bad) atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
+}
+
+template <bool kBatch, bool kDirect, int kThreads, int kRows>
+__global__ void __launch_bounds__(kThreads, pforce_min_blocks(kDirect, kThreads, kRows)) k_pcisph_pressure_force(
+    const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
+    const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap vmap,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt,
+    const float* __restrict__ luts_plain, const float4* __restrict__ pq, const float4* __restrict__ force,
+    float4* __restrict__ pforce, float4* __restrict__ xs, DevState* __restrict__ st_plain) {
+  pforce_block<kBatch, kDirect, kThreads, kRows>(blockIdx.x, Pk, bv, n, B, cmap, vmap, nbr, lval, ncnt, luts_plain,
+                                                 pq, force, pforce, xs, st_plain);
+}
+
+// The pressure-force pass over the active groups (k_pcisph_density_active).
+template <int kRows>
+__global__ void __launch_bounds__(kSegAlign) k_pcisph_pressure_force_active(
+    const BatchView bv, uint32_t n, const uint32_t* __restrict__ groups, const uint32_t* __restrict__ ngroups,
+    DynArrays B, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ lval,
+    const uint32_t* __restrict__ ncnt, const float4* __restrict__ pq, const float4* __restrict__ force,
+    float4* __restrict__ pforce, float4* __restrict__ xs) {
+  const uint32_t count = *ngroups;
+  for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
+    pforce_block<true, true, kSegAlign, kRows>(groups[g], DevParams{}, bv, n, B, CUtensorMap{}, CUtensorMap{}, nbr,
+                                                lval, ncnt, nullptr, pq, force, pforce, xs, nullptr);
+    __syncthreads();  // the next group reuses the shared scope
+  }
 }
 
 __global__ void k_loop_init(DevState* st) {
@@ -1193,20 +1274,66 @@ __global__ void k_loop_init_batch(DevState* st, uint32_t nscenes, int32_t* any_a
 
 // Loop control of every scene still iterating (each exactly as k_loop_ctl);
 // the while-node continues while any scene does.
-__global__ void k_loop_ctl_batch(const BatchView bv, uint32_t nscenes, int32_t* any_active,
-                                 cudaGraphConditionalHandle h, int use_handle) {
+// Loop control of the batch: the loop test of every scene still iterating;
+// the 256-slot groups of the scenes that go on, listed in scene order for
+// the resident passes; and for the next iteration, whether the passes run
+// over the full grid (while at least half of the groups iterate) or over the
+// list. One CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) k_loop_ctl_batch(const BatchView bv, uint32_t nscenes, int32_t* any_active,
+                                                         const uint32_t* __restrict__ seg_begin, uint32_t total_groups,
+                                                         uint32_t* __restrict__ groups, uint32_t* __restrict__ ngroups,
+                                                         cudaGraphConditionalHandle h,
+                                                         cudaGraphConditionalHandle h_full,
+                                                         cudaGraphConditionalHandle h_list, int use_handle) {
+  __shared__ uint32_t warp_sums[32];
   int any = 0;
+  uint32_t mine = 0;  // groups of this thread's active scenes
   for (uint32_t s = threadIdx.x; s < nscenes; s += blockDim.x) {
     DevState* st = bv.st + s;
     if (!st->loop_active) continue;
     const int cont = loop_ctl(bv.params[s], st);
     st->loop_active = cont;
     any |= cont;
+    if (cont) mine += (bv.seg_end[s] - seg_begin[s] + kSegAlign - 1) / kSegAlign;
   }
   any = __syncthreads_or(any);
+  // exclusive scan of the threads' group counts
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = mine;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += v;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += v;
+    }
+    warp_sums[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  uint32_t at = (warp ? warp_sums[warp - 1] : 0u) + incl - mine;
+  for (uint32_t s = threadIdx.x; s < nscenes; s += blockDim.x) {
+    if (!bv.st[s].loop_active) continue;
+    const uint32_t g0 = seg_begin[s] / kSegAlign;
+    const uint32_t ng = (bv.seg_end[s] - seg_begin[s] + kSegAlign - 1) / kSegAlign;
+    for (uint32_t k = 0; k < ng; ++k) groups[at++] = g0 + k;
+  }
   if (threadIdx.x == 0) {
+    const uint32_t total = warp_sums[(blockDim.x >> 5) - 1];
+    *ngroups = total;
     *any_active = any;
-    if (use_handle) cudaGraphSetConditional(h, any ? 1u : 0u);
+    if (use_handle) {
+      const bool full = 2 * total >= total_groups;
+      cudaGraphSetConditional(h, any ? 1u : 0u);
+      cudaGraphSetConditional(h_full, (any && full) ? 1u : 0u);
+      cudaGraphSetConditional(h_list, (any && !full) ? 1u : 0u);
+    }
   }
 }
 
@@ -1601,7 +1728,83 @@ cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st) {
 }
 
 cudaError_t batch_launch_loop_ctl(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle) {
-  k_loop_ctl_batch<<<1, 1024, 0, st>>>(b.view, b.n_scenes, b.any_active_d, h, use_handle ? 1 : 0);
+  k_loop_ctl_batch<<<1, 1024, 0, st>>>(b.view, b.n_scenes, b.any_active_d, b.seg_begin_d, b.n_slots / kSegAlign,
+                                       b.active_groups_d, b.n_active_groups_d, h, 0, 0, 0);
+  (void)use_handle;  // the host-driven loop reads any_active
+  return cudaGetLastError();
+}
+
+// The loop passes over the active groups only, on a resident grid.
+cudaError_t batch_launch_loop_active(BatchSystem& b, cudaStream_t st) {
+  constexpr int kR = 4;
+  if (!b.active_grid) {
+    int dev = 0, sms = 0, per_sm_d = 0, per_sm_p = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_d, k_pcisph_density_active<kR>, kSegAlign, 0);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p, k_pcisph_pressure_force_active<kR>, kSegAlign, 0);
+    if (e != cudaSuccess) return e;
+    b.active_grid = (uint32_t)(sms * std::max(1, std::min(per_sm_d, per_sm_p)));
+  }
+  const uint32_t n = b.n_slots;
+  k_pcisph_density_active<kR><<<b.active_grid, kSegAlign, 0, st>>>(b.view, n, b.active_groups_d, b.n_active_groups_d,
+                                                                   b.B.type, b.xs, b.nbr, b.ncnt, b.rho, b.press,
+                                                                   b.pq);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_pcisph_pressure_force_active<kR><<<b.active_grid, kSegAlign, 0, st>>>(
+      b.view, n, b.active_groups_d, b.n_active_groups_d, b.B, b.nbr, b.lval, b.ncnt, b.pq, b.force, b.pforce, b.xs);
+  return cudaGetLastError();
+}
+
+// An IF node at the capture point of `st` (capturing into a graph) whose
+// body `fn` captures; the capture goes on after the node.
+template <class Fn>
+cudaError_t capture_if(cudaStream_t st, unsigned int default_value, cudaGraphConditionalHandle* h, Fn&& fn) {
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(st, &cst, nullptr, &g, &deps, &ndeps);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaGraphConditionalHandleCreate(h, g, default_value, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = *h;
+  np.conditional.type = cudaGraphCondTypeIf;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, g, deps, ndeps, &np)) != cudaSuccess) return e;
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  if ((e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+    return e;
+  cudaStream_t bs = nullptr;
+  if ((e = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking)) != cudaSuccess) return e;
+  e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const cudaError_t eb = fn(bs);
+    cudaGraph_t out = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(bs, &out);
+    e = eb != cudaSuccess ? eb : ee;
+  }
+  cudaStreamDestroy(bs);
+  return e;
+}
+
+cudaError_t batch_capture_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h) {
+  // every scene iterates in the first iteration: the full grid by default
+  cudaGraphConditionalHandle h_full = 0, h_list = 0;
+  cudaError_t e = capture_if(st, 1u, &h_full, [&](cudaStream_t bs) {
+    cudaError_t r = batch_launch_loop_density(b, bs);
+    return r == cudaSuccess ? batch_launch_loop_pforce(b, bs) : r;
+  });
+  if (e != cudaSuccess) return e;
+  e = capture_if(st, 0u, &h_list, [&](cudaStream_t bs) { return batch_launch_loop_active(b, bs); });
+  if (e != cudaSuccess) return e;
+  k_loop_ctl_batch<<<1, 1024, 0, st>>>(b.view, b.n_scenes, b.any_active_d, b.seg_begin_d, b.n_slots / kSegAlign,
+                                       b.active_groups_d, b.n_active_groups_d, h, h_full, h_list, 1);
   return cudaGetLastError();
 }
 

@@ -69,6 +69,107 @@ __global__ void __launch_bounds__(kReduceThreads) k_rigid_reduce(DevParams P, De
   }
 }
 
+// AddToRigidBody (UnifiedPhysics.cpp:825-885) and
+// ComputeLocalInertiaTensorRigidBody (:1143-1176), one CTA per body: mass,
+// centre of mass and momentum, then the inertia tensor and angular momentum
+// about the centre, each an FP64 tree sum over the body's particles (entries
+// in the body's input order); the FP64 adjugate inverse of the inertia
+// (Matrix3x3::CalculateInverse, Matrix3x3.cpp:121-156); the body at rest
+// orientation; and every particle's position relative to the centre, in
+// float as the reference stores it.
+__device__ __forceinline__ void tree_sum(double (*red)[kReduceThreads], int nvals) {
+  __syncthreads();
+  for (int w = kReduceThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int a = 0; a < nvals; ++a) red[a][threadIdx.x] += red[a][threadIdx.x + w];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_rigid_assemble(float mass, DevBody* __restrict__ bodies,
+                                                                   const uint32_t* __restrict__ body_start,
+                                                                   const float4* __restrict__ epos,
+                                                                   const float4* __restrict__ evel,
+                                                                   float4* __restrict__ entry_r0) {
+  __shared__ double red[9][kReduceThreads];
+  __shared__ double centre[3];
+  const int b = blockIdx.x;
+  const uint32_t k0 = body_start[b], k1 = body_start[b + 1];
+  const double m = mass;
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t k = k0 + threadIdx.x; k < k1; k += kReduceThreads) {
+    const float4 x = epos[k], v = evel[k];
+    acc[0] += m * (double)x.x;
+    acc[1] += m * (double)x.y;
+    acc[2] += m * (double)x.z;
+    acc[3] += m * (double)v.x;
+    acc[4] += m * (double)v.y;
+    acc[5] += m * (double)v.z;
+  }
+  for (int a = 0; a < 6; ++a) red[a][threadIdx.x] = acc[a];
+  tree_sum(red, 6);
+  const double M = m * (double)(k1 - k0);
+  double P[3];
+  for (int a = 0; a < 3; ++a) P[a] = red[3 + a][0];
+  if (threadIdx.x < 3) centre[threadIdx.x] = red[threadIdx.x][0] / M;
+  __syncthreads();
+  const double c[3] = {centre[0], centre[1], centre[2]};
+  for (int a = 0; a < 9; ++a) acc[a] = 0.0;
+  for (uint32_t k = k0 + threadIdx.x; k < k1; k += kReduceThreads) {
+    const float4 x = epos[k], v4 = evel[k];
+    const double r[3] = {(double)x.x - c[0], (double)x.y - c[1], (double)x.z - c[2]};
+    const double v[3] = {m * (double)v4.x, m * (double)v4.y, m * (double)v4.z};
+    const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    acc[0] += m * (rr - r[0] * r[0]);  // xx
+    acc[1] += m * (-r[0] * r[1]);      // xy
+    acc[2] += m * (-r[0] * r[2]);      // xz
+    acc[3] += m * (rr - r[1] * r[1]);  // yy
+    acc[4] += m * (-r[1] * r[2]);      // yz
+    acc[5] += m * (rr - r[2] * r[2]);  // zz
+    acc[6] += r[1] * v[2] - r[2] * v[1];
+    acc[7] += r[2] * v[0] - r[0] * v[2];
+    acc[8] += r[0] * v[1] - r[1] * v[0];
+  }
+  for (int a = 0; a < 9; ++a) red[a][threadIdx.x] = acc[a];
+  tree_sum(red, 9);
+  const float3 cf = make_float3((float)c[0], (float)c[1], (float)c[2]);
+  if (threadIdx.x == 0) {
+    const double A[9] = {red[0][0], red[1][0], red[2][0], red[1][0], red[3][0], red[4][0],
+                         red[2][0], red[4][0], red[5][0]};
+    double inv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                       A[2] * (A[3] * A[7] - A[4] * A[6]);
+    if (det != 0.0) {
+      inv[0] = (A[4] * A[8] - A[5] * A[7]) / det;
+      inv[1] = (A[2] * A[7] - A[1] * A[8]) / det;
+      inv[2] = (A[1] * A[5] - A[2] * A[4]) / det;
+      inv[3] = (A[5] * A[6] - A[3] * A[8]) / det;
+      inv[4] = (A[0] * A[8] - A[2] * A[6]) / det;
+      inv[5] = (A[2] * A[3] - A[0] * A[5]) / det;
+      inv[6] = (A[3] * A[7] - A[4] * A[6]) / det;
+      inv[7] = (A[1] * A[6] - A[0] * A[7]) / det;
+      inv[8] = (A[0] * A[4] - A[1] * A[3]) / det;
+    }
+    DevBody B;
+    memset(&B, 0, sizeof(B));
+    B.mass = (float)M;
+    B.pos = cf;
+    B.P = make_float3((float)P[0], (float)P[1], (float)P[2]);
+    B.vel = make_float3((float)(P[0] / M), (float)(P[1] / M), (float)(P[2] / M));
+    B.L = make_float3((float)red[6][0], (float)red[7][0], (float)red[8][0]);
+    B.q[0] = 1.0f;
+    for (int i = 0; i < 3; ++i) {
+      B.rot[i][i] = 1.0f;
+      for (int j = 0; j < 3; ++j) B.iinv_local[i][j] = (float)inv[3 * i + j];
+    }
+    bodies[b] = B;
+  }
+  for (uint32_t k = k0 + threadIdx.x; k < k1; k += kReduceThreads) {
+    const float4 x = epos[k];
+    entry_r0[k] = make_float4(x.x - cf.x, x.y - cf.y, x.z - cf.z, 0.0f);
+  }
+}
+
 // the reference's MIN / MAX macros (global.h:4-5)
 __device__ __forceinline__ float min_ref(float a, float b) { return (a <= b) ? a : b; }
 __device__ __forceinline__ float max_ref(float a, float b) { return (a >= b) ? a : b; }
@@ -177,6 +278,13 @@ cudaError_t launch_rigid_slots(System& s, cudaStream_t st) {
   const RigidArrays& r = s.rb;
   if (!r.n_rigid || !s.n_dyn) return cudaSuccess;
   k_rigid_slots<<<(s.n_dyn + 255) / 256, 256, 0, st>>>(s.n_dyn, s.B.id, r.id_entry, r.entry_slot);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rigid_assemble(float mass, DevBody* bodies, uint32_t n_bodies, const uint32_t* start,
+                                  const float4* epos, const float4* evel, float4* entry_r0, cudaStream_t st) {
+  if (!n_bodies) return cudaSuccess;
+  k_rigid_assemble<<<n_bodies, kReduceThreads, 0, st>>>(mass, bodies, start, epos, evel, entry_r0);
   return cudaGetLastError();
 }
 

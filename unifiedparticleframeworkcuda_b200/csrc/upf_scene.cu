@@ -574,6 +574,57 @@ struct FluidBlock {
   double off[3];
 };
 
+// A rigid body's surface particles (the procedural shapes of the coupling
+// workload, in place of voxelising an OBJ model): point k in the body frame,
+// then rotated and moved, x = R p + c, in double and stored as float.
+//   sphere (shape 0): a Fibonacci lattice of n points on radius r;
+//   cube (1): a k x k grid of cell centres on each face of half-edge r, faces
+//     in the order -x, +x, -y, +y, -z, +z (the grid's first index runs along
+//     the next axis after the face's normal);
+//   torus (2): an nu x nv grid of (u, v) cell centres, major radius r, minor
+//     radius r / 3.
+struct RigidSurface {
+  int shape;
+  double r;
+  uint32_t n, k, nu, nv;
+  double R[9], c[3];
+};
+
+__global__ void k_rigid_surface(const RigidSurface S, float4* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S.n) return;
+  const double pi = 3.141592653589793;
+  double p[3];
+  if (S.shape == 0) {
+    const double t = (double)i + 0.5;
+    const double phi = acos(1.0 - 2.0 * t / (double)S.n);
+    const double theta = pi * (1.0 + sqrt(5.0)) * t;
+    p[0] = S.r * (cos(theta) * sin(phi));
+    p[1] = S.r * (sin(theta) * sin(phi));
+    p[2] = S.r * cos(phi);
+  } else if (S.shape == 1) {
+    const uint32_t kk = S.k * S.k, face = i / kk, j = i % kk;
+    const uint32_t ia = j / S.k, ib = j % S.k;
+    const double a = ((double)ia + 0.5) / (double)S.k * 2.0 * S.r - S.r;
+    const double b = ((double)ib + 0.5) / (double)S.k * 2.0 * S.r - S.r;
+    const int axis = (int)(face / 2);
+    p[axis] = (face & 1) ? S.r : -S.r;
+    p[(axis + 1) % 3] = a;
+    p[(axis + 2) % 3] = b;
+  } else {
+    const uint32_t iu = i / S.nv, iv = i % S.nv;
+    const double u = ((double)iu + 0.5) / (double)S.nu * 2.0 * pi;
+    const double v = ((double)iv + 0.5) / (double)S.nv * 2.0 * pi;
+    const double a = S.r / 3.0;
+    p[0] = (S.r + a * cos(v)) * cos(u);
+    p[1] = (S.r + a * cos(v)) * sin(u);
+    p[2] = a * sin(v);
+  }
+  double x[3];
+  for (int r = 0; r < 3; ++r) x[r] = S.R[3 * r] * p[0] + S.R[3 * r + 1] * p[1] + S.R[3 * r + 2] * p[2] + S.c[r];
+  out[i] = make_float4((float)x[0], (float)x[1], (float)x[2], 0.0f);
+}
+
 // Scene::createFluidObject (Scene.cpp:597-646), particle k of the iy, ix, iz
 // loops: x = jitter + ix * spacing in float, then x + (drand48() - 0.5) *
 // jitter + offset in double, stored as float; the reference's drand48() is
@@ -795,4 +846,45 @@ upf_status upf_scene_box_boundary(int device, const float container_min[3], cons
     return UPF_ERR_INVALID_ARG;
   }
   return s;
+}
+
+upf_status upf_scene_rigid_surface(int device, int32_t shape, float radius, uint32_t n_target, const float rot9[9],
+                                   const float center[3], float* pos4, uint32_t capacity, uint32_t* n_out) {
+  const char* who = "upf_scene_rigid_surface";
+  if (shape < 0 || shape > 2 || !(radius > 0.0f) || n_target == 0 || !rot9 || !center || !n_out ||
+      (capacity > 0 && !pos4)) {
+    set_error("%s: bad arguments (shape 0 sphere, 1 cube, 2 torus; radius > 0; n_target > 0)", who);
+    return UPF_ERR_INVALID_ARG;
+  }
+  RigidSurface S{};
+  S.shape = shape;
+  S.r = (double)radius;
+  uint64_t n = n_target;
+  if (shape == 1) {
+    S.k = (uint32_t)std::max(2.0, std::nearbyint(std::sqrt((double)n_target / 6.0)));
+    n = 6ull * S.k * S.k;
+  } else if (shape == 2) {
+    // nu around the major circle, nv around the minor one, near-square cells
+    S.nu = (uint32_t)std::max(8.0, std::nearbyint(std::sqrt((double)n_target * 3.0)));
+    S.nv = (uint32_t)std::max(4.0, std::nearbyint((double)n_target / (double)S.nu));
+    n = (uint64_t)S.nu * S.nv;
+  }
+  if (n > 0xffffffffu) {
+    set_error("%s: too many points", who);
+    return UPF_ERR_INVALID_ARG;
+  }
+  S.n = (uint32_t)n;
+  for (int k = 0; k < 9; ++k) S.R[k] = (double)rot9[k];
+  for (int a = 0; a < 3; ++a) S.c[a] = (double)center[a];
+  *n_out = S.n;
+  if (!pos4) return UPF_OK;
+  if (n > capacity) {
+    set_error("%s: the surface holds %llu particles, capacity is %u", who, (unsigned long long)n, capacity);
+    return UPF_ERR_INVALID_ARG;
+  }
+  auto launch = [](const void* a, uint64_t n, float4* pos, float4*, int*, cudaStream_t st) {
+    k_rigid_surface<<<(uint32_t)((n + 255) / 256), 256, 0, st>>>(*static_cast<const RigidSurface*>(a), pos);
+    return cudaGetLastError();
+  };
+  return generate(who, device, n, pos4, nullptr, launch, &S, nullptr);
 }

@@ -247,6 +247,9 @@ struct BatchSystem {
   uint32_t* seg_end_d = nullptr;
   uint32_t* cell_base_d = nullptr;
   int32_t* any_active_d = nullptr; // host-driven loop: any scene still iterating
+  uint32_t* active_groups_d = nullptr;  // [n_slots / kSegAlign] groups of the scenes still iterating
+  uint32_t* n_active_groups_d = nullptr;
+  uint32_t active_grid = 0;             // resident CTAs of the active-group passes
   BatchView view;
 
   cudaGraphExec_t step_exec = nullptr;
@@ -271,6 +274,9 @@ cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st);
 cudaError_t batch_launch_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle);
 cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st);
 cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st);
+// the graph's loop body: [if most groups iterate: full-grid passes] [else:
+// resident passes over the active groups] loop control (sets all three)
+cudaError_t batch_capture_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h);
 cudaError_t batch_launch_loop_ctl(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h = 0,
                                   bool use_handle = false);
 cudaError_t batch_launch_integrate(BatchSystem& b, cudaStream_t st);
@@ -316,6 +322,10 @@ LaunchShape config_to_shape(const upf_launch_config& c);
 // upf_rigid.cu: list entry -> sorted index after a sort; body force/torque,
 // body integration and rigid particle sync after integration
 cudaError_t launch_rigid_slots(System& s, cudaStream_t st);
+// body mass, centre, momenta and inverse inertia, and the particles' relative
+// positions, from the bodies' particles in entry order (upf_rigid.cu)
+cudaError_t launch_rigid_assemble(float mass, DevBody* bodies, uint32_t n_bodies, const uint32_t* start,
+                                  const float4* epos, const float4* evel, float4* entry_r0, cudaStream_t st);
 cudaError_t launch_rigid_phase(System& s, cudaStream_t st);
 int rigid_launches_per_step(const System& s);
 
