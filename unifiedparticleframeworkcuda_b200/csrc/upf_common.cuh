@@ -100,8 +100,10 @@ __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 
 // Packed pairs of floats (sm_100's f32x2 arithmetic): one instruction for two
-// lanes, each rounded exactly as the scalar operation (round to nearest, no
-// flush of subnormals), so results stay bit-identical to scalar code.
+// lanes, each rounded as the scalar operation (round to nearest, no flush of
+// subnormals). Used only where a packed product is unpacked before the next
+// operation (the density pass's squared distance): a packed product feeding a
+// packed add or subtract was measured not to reproduce the scalar results.
 __device__ __forceinline__ unsigned long long pk2(float a, float b) {
   unsigned long long r;
   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));

@@ -1083,10 +1083,12 @@ __device__ __forceinline__ void pforce_block(
   // grad = p_i / rho0^2 + p_j / rho0^2, both quotients precomputed by the
   // density pass (pq.w); boundary particles have p = 0, so 0 / rho0^2 = 0
   const float qi = active ? pq[i].w : 0.0f;
-  // x and y as packed pairs: the same operations and roundings as scalar code
-  const unsigned long long xiy = pk2(xi.x, xi.y), mm = pk2(m, m);
-  unsigned long long fxy = pk2(0.0f, 0.0f);
-  float fz = 0;
+  // Scalar arithmetic on purpose: a packed (f32x2) multiply whose product
+  // feeds a packed subtract did not reproduce the scalar roundings on the
+  // device (measured: the pass drifted from the oracle by an ulp in rare
+  // pairs, then the loop by whole iterations), and the packed form was no
+  // faster.
+  float fx = 0, fy = 0, fz = 0;
   const ListArgs L{&cmap, &vmap, nbr, lval, P.nstride};
   const bool ok = walk_lists<kDirect, true, kThreads, kRows>(L, block, i, cnt, [&](auto code, auto val, int k0) {
     // one gather per neighbour: position and p / rho0^2 packed in pq
@@ -1100,21 +1102,20 @@ __device__ __forceinline__ void pforce_block(
       if (k0 + r < (int)cnt) {
         const float g = __uint_as_float(val(r));  // kernelPressureGradLut at the entry's bin
         // k = (x_i - x_j) * g; f -= ((k * grad) * m) * m, per component
-        const unsigned long long kxy = mul2(sub2(xiy, pk2(xj[r].x, xj[r].y)), pk2(g, g));
-        const float kz = (xi.z - xj[r].z) * g;
+        const float kx = (xi.x - xj[r].x) * g, ky = (xi.y - xj[r].y) * g, kz = (xi.z - xj[r].z) * g;
         const float grad = qi + xj[r].w;
-        fxy = sub2(fxy, mul2(mul2(mul2(kxy, pk2(grad, grad)), mm), mm));
+        fx = fx - kx * grad * m * m;
+        fy = fy - ky * grad * m * m;
         fz = fz - kz * grad * m * m;
       }
     }
   });
   if (!ok && lane == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
   if (!active) return;
-  const float2 fp = up2(fxy);
-  pforce[i] = f4(fp.x, fp.y, fz);
+  pforce[i] = f4(fx, fy, fz);
   const float4 F = force[i];
   bool bad;
-  xs[i] = predict(P, xi, B.vel[i], make_float3(F.x, F.y, F.z), make_float3(fp.x, fp.y, fz), bad);
+  xs[i] = predict(P, xi, B.vel[i], make_float3(F.x, F.y, F.z), make_float3(fx, fy, fz), bad);
   if (bad) atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
 }
 
