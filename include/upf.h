@@ -507,8 +507,13 @@ upf_status upf_profile_step(upf_system* s, upf_phase_times* out);
  * come either through a TMA ring in shared memory (mode 0; pairs (128,4)
  * (128,8) (128,16) (256,2) (256,4) (256,8) (512,2) (512,4) (1024,2)) or by
  * direct coalesced loads, rows entries at a time (mode 1; (128,4) (128,8)
- * (256,4) (256,8) (512,4) (512,8)). Batches allow up to 256 threads. Shapes
- * change timing only: every shape gives the same results. */
+ * (256,4) (256,8) (512,4) (512,8)), or from staged neighbourhoods (mode 2;
+ * (256,4) (256,8); single PCISPH systems): each 256-particle CTA copies the
+ * distinct neighbours of its particles into shared memory once per pass and
+ * walks lists rewritten as 16-bit positions in that set (the rewrite runs
+ * once per step, after the list build). Batches allow up to 256 threads and
+ * modes 0 and 1. Shapes change timing only: every shape gives the same
+ * results. */
 typedef struct upf_launch_config {
   int32_t nlist_threads;      /* 64, 128, 256 */
   int32_t external_threads;   /* 128, 256 */
@@ -516,7 +521,7 @@ typedef struct upf_launch_config {
   int32_t density_rows;
   int32_t pforce_threads;
   int32_t pforce_rows;
-  int32_t density_mode;       /* list entries by 0: the TMA ring; 1: direct loads */
+  int32_t density_mode;       /* list entries by 0: the TMA ring; 1: direct loads; 2: staged neighbourhoods */
   int32_t pforce_mode;
   int32_t nlist_mode;         /* 0: each thread its own query box; 1: a warp walks the union of its boxes */
   float measured_ms[4];       /* autotune: per-launch ms of the chosen shapes
@@ -730,8 +735,13 @@ upf_status upf_adjoint_times(upf_adjoint* a, float* forward_ms, float* backward_
  * the device's r2 -> bin rule against (int)(sqrtf(r2) * (1/h) * 300) and
  * sqrtf(r2) < h, UnifiedPhysics.cpp:5468-5476. The neighbour-list build's
  * table rule is computed beside it: -2 marks an r2 where the two differ.
- * n <= 2^26. */
+ * n <= 2^26.
+ * upf_test_stage_union_cap(s, cap): lowers the number of distinct neighbours
+ * a chunk of the staged loop passes (mode 2) may stage (at most 2048, the
+ * default); chunks whose union is larger read the plain lists. For reaching
+ * that fallback on small scenes. */
 upf_status upf_test_fail_allocation(int32_t nth);
+upf_status upf_test_stage_union_cap(upf_system* s, uint32_t cap);
 upf_status upf_selftest_bounded_wait(int device, uint32_t limit_us);
 upf_status upf_selftest_support_bins(int device, const upf_params* p, const float* r2, uint32_t n, int32_t* bins);
 

@@ -98,6 +98,34 @@ def test_full_size_pcisph_step(upf_lib, oracle_lib):
     o.close()
 
 
+def test_full_size_staged_modes_equal_the_default_shape(upf_lib):
+    """pcisph_dam_break_1M, three steps from rest (every iteration of the
+    loop, 150 launches of each pass): the staged-neighbourhood passes (mode 2,
+    both batch sizes) give results identical to the default shapes, which the
+    step test above holds to the oracle."""
+    from unifiedparticleframeworkcuda_b200 import UpfLaunchConfig
+    sc = scenes.pcisph_dam()
+    p = upf_lib.derive_params(sc.params)
+    out = []
+    for rows in (0, 4, 8):
+        with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
+            s.set_particles(sc.pos, sc.vel, sc.type)
+            if rows:
+                c = s.launch_config()
+                c.density_mode, c.density_threads, c.density_rows = 2, 256, rows
+                c.pforce_mode, c.pforce_threads, c.pforce_rows = 2, 256, rows
+                s.set_launch_config(c)
+            s.step(3)
+            g = s.particles()
+            o = np.argsort(g["id"], kind="stable")
+            out.append(({k: g[k][o] for k in ("pos", "vel", "density", "pressure")}, s.stats().iterations))
+    ref, it = out[0]
+    for got, it2 in out[1:]:
+        assert it2 == it
+        for f in ref:
+            assert np.array_equal(got[f], ref[f]), f
+
+
 def test_full_size_coupling_step(upf_lib, oracle_lib):
     sc = scenes.coupling_scene()
     assert sc.num_bodies == 16

@@ -9,13 +9,15 @@ from unifiedparticleframeworkcuda_b200 import UpfError, UpfLaunchConfig, scenes
 
 pytestmark = pytest.mark.gpu
 
-# (threads, rows) with the TMA ring (mode 0) and with direct loads (mode 1)
+# (mode, threads, rows) with the TMA ring (mode 0), direct loads (mode 1) and
+# staged neighbourhoods (mode 2, single scenes)
 LOOP_PAIRS = [(0, 128, 4), (0, 128, 8), (0, 128, 16), (0, 256, 2), (0, 256, 4), (0, 256, 8), (0, 512, 2),
               (0, 512, 4), (0, 1024, 2), (1, 128, 4), (1, 128, 8), (1, 256, 4), (1, 256, 8), (1, 512, 4),
-              (1, 512, 8)]
+              (1, 512, 8), (2, 256, 4), (2, 256, 8)]
 # the pressure-force pass also streams a 32-bit value per list entry: its
 # larger TMA rings do not fit in static shared memory and are not built
-PFORCE_PAIRS = [p for p in LOOP_PAIRS if p[0] == 1 or p[1:] in ((128, 4), (128, 8), (256, 2), (256, 4), (512, 2))]
+PFORCE_PAIRS = [p for p in LOOP_PAIRS if p[0] != 0 or p[1:] in ((128, 4), (128, 8), (256, 2), (256, 4), (512, 2))]
+STAGED = [p for p in LOOP_PAIRS if p[0] == 2]
 
 
 def shape(nl, ext, dens, pf):
@@ -60,6 +62,36 @@ def test_every_shape_gives_identical_results(upf_lib):
         assert st.iterations == ref_st.iterations
         for f in ("pos", "vel", "density", "pressure"):
             assert np.array_equal(got[f], ref[f]), (cfg.as_dict(), f)
+
+
+@pytest.mark.parametrize("cap", [2048, 600, 300, 0])
+def test_staged_passes_with_and_without_room_for_the_union(upf_lib, cap):
+    """Staged neighbourhoods (mode 2) in both passes, with the union capacity
+    lowered so that some chunks (600: a few, 300: most, 0: all) do not fit and
+    read the plain lists: identical results to the default shape either way.
+    The scene includes rigid bodies and grains, whose lists are not staged."""
+    for name in ("small_pcisph", "small_coupling"):
+        sc = getattr(scenes, name)()
+        p = upf_lib.derive_params(sc.params)
+        out = []
+        for cfg in (None, shape(128, 256, STAGED[0], STAGED[0]), shape(128, 256, STAGED[1], STAGED[1]),
+                    shape(128, 256, STAGED[0], (1, 256, 4)), shape(128, 256, (0, 256, 4), STAGED[1])):
+            with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
+                s.set_particles(sc.pos, sc.vel, sc.type)
+                if getattr(sc, "num_bodies", 0):
+                    s.set_rigid_bodies(sc.body, sc.num_bodies)
+                if cfg is not None:
+                    s.set_launch_config(cfg)
+                    upf_lib.check(upf_lib.lib().upf_test_stage_union_cap(s._h, cap), "upf_test_stage_union_cap")
+                s.step(3)
+                g = s.particles()
+                o = np.argsort(g["id"], kind="stable")
+                out.append(({k: v[o] for k, v in g.items()}, s.stats().iterations))
+        ref, ref_it = out[0]
+        for got, it in out[1:]:
+            assert it == ref_it, name
+            for f in ("pos", "vel", "density", "pressure"):
+                assert np.array_equal(got[f], ref[f]), (name, cap, f)
 
 
 @pytest.mark.parametrize("scene", ["small_pcisph", "small_coupling"])
@@ -137,7 +169,8 @@ def test_invalid_shapes_rejected(upf_lib):
         s.set_particles(sc.pos, sc.vel, sc.type)
         for bad in (shape(96, 256, (256, 8), (256, 4)), shape(256, 256, (256, 16), (256, 4)),
                     shape(256, 64, (256, 8), (256, 4)), shape(256, 256, (1, 256, 2), (256, 4)),
-                    shape(256, 256, (256, 8), (2, 256, 8)), shape(256, 256, (256, 8), (128, 16)),
+                    shape(256, 256, (256, 8), (2, 128, 4)), shape(256, 256, (2, 256, 2), (256, 4)),
+                    shape(256, 256, (256, 8), (3, 256, 8)), shape(256, 256, (256, 8), (128, 16)),
                     shape(256, 256, (256, 8), (1024, 2))):
             with pytest.raises(UpfError):
                 s.set_launch_config(bad)
@@ -149,4 +182,6 @@ def test_invalid_shapes_rejected(upf_lib):
     with upf_lib.ParticleBatch.from_scenes(scs) as b:
         with pytest.raises(UpfError):
             b.set_launch_config(shape(256, 256, (512, 4), (256, 8)))  # a CTA across two scenes
+        with pytest.raises(UpfError):
+            b.set_launch_config(shape(128, 128, (2, 256, 4), (128, 4)))  # staged: single scenes only
         b.set_launch_config(shape(128, 128, (256, 2), (128, 4)))

@@ -107,6 +107,7 @@ def lib():
             "upf_adjoint_get_state": [vp, fp, fp],
             "upf_adjoint_times": [vp, fp, fp],
             "upf_test_fail_allocation": [C.c_int32],
+            "upf_test_stage_union_cap": [vp, C.c_uint32],
             "upf_selftest_bounded_wait": [C.c_int, C.c_uint32],
             "upf_selftest_support_bins": [C.c_int, P, fp, C.c_uint32, i32p],
             "upf_morton_keys": [vp, C.c_uint32, fp, fp, vp, vp],

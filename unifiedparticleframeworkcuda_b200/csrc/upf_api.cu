@@ -209,8 +209,10 @@ bool shape_valid(const LaunchShape& s, bool batched, const char** why) {
   if (!pair_ok(s.density_mode, s.density_threads, s.density_rows) ||
       !pair_ok(s.pforce_mode, s.pforce_threads, s.pforce_rows))
     return bad("(threads, rows) of a loop pass must be one of (128,4) (128,8) (128,16) (256,2) (256,4) (256,8) "
-               "(512,2) (512,4) (1024,2) with the TMA ring (mode 0), or (128,4) (128,8) (256,4) (256,8) (512,4) "
-               "(512,8) with direct loads (mode 1)");
+               "(512,2) (512,4) (1024,2) with the TMA ring (mode 0), (128,4) (128,8) (256,4) (256,8) (512,4) "
+               "(512,8) with direct loads (mode 1), or (256,4) (256,8) with staged neighbourhoods (mode 2)");
+  if (batched && (loop_mode_staged(s.density_mode) || loop_mode_staged(s.pforce_mode)))
+    return bad("batched scenes: staged neighbourhoods (mode 2) are for single scenes");
   if (!pforce_ring_fits(s.pforce_mode, s.pforce_threads, s.pforce_rows))
     return bad("the pressure-force pass's TMA ring takes (128,4) (128,8) (256,2) (256,4) (512,2); its list values "
                "leave the larger rings no room in shared memory");
@@ -315,29 +317,69 @@ upf_status autotune_shapes(const TuneOps& ops, int repeats, upf_launch_config* o
       sh.external_threads = best;
       chosen_ms[1] = best_ms;
     }
+    // the loop passes: the fastest shape of each pass, and the fastest that
+    // reads the plain lists; staged shapes (mode 2) also cost the staging
+    // kernel once per step, which the choice weighs against the passes'
+    // saving times the iterations a step takes
     const auto& pairs = kLoopShapes;
+    struct Pick {
+      int mode, threads, rows;
+      float ms;
+    };
+    Pick best_any[2], best_plain[2];
+    bool tuned[2] = {false, false};
     for (int pass = 0; pass < 2 && rc == UPF_OK; ++pass) {
       cudaError_t (*launch)(void*, cudaStream_t) = pass == 0 ? ops.density : ops.pforce;
       if (!launch) continue;
       int& mode = pass == 0 ? sh.density_mode : sh.pforce_mode;
       int& threads = pass == 0 ? sh.density_threads : sh.pforce_threads;
       int& rows = pass == 0 ? sh.density_rows : sh.pforce_rows;
-      int bm = mode, bt = threads, br = rows;
-      float best_ms = 1e30f;
+      best_any[pass] = best_plain[pass] = Pick{mode, threads, rows, 1e30f};
       for (const auto& pr : pairs) {
-        if (ops.batched && pr[1] > 256) continue;
+        if (ops.batched && (pr[1] > 256 || loop_mode_staged(pr[0]))) continue;
+        if (!ops.stage && loop_mode_staged(pr[0])) continue;
         if (pass == 1 && !pforce_ring_fits(pr[0], pr[1], pr[2])) continue;
         mode = pr[0];
         threads = pr[1];
         rows = pr[2];
         float ms;
         if ((rc = time_pass(launch, &ms)) != UPF_OK) break;
-        if (ms < best_ms) best_ms = ms, bm = pr[0], bt = pr[1], br = pr[2];
+        const Pick pk{pr[0], pr[1], pr[2], ms};
+        if (ms < best_any[pass].ms) best_any[pass] = pk;
+        if (!loop_mode_staged(pr[0]) && ms < best_plain[pass].ms) best_plain[pass] = pk;
       }
-      mode = bm;
-      threads = bt;
-      rows = br;
-      chosen_ms[2 + pass] = best_ms;
+      tuned[pass] = rc == UPF_OK;
+    }
+    if (rc == UPF_OK && tuned[0] && tuned[1]) {
+      Pick pick[2] = {best_any[0], best_any[1]};
+      if (loop_mode_staged(pick[0].mode) || loop_mode_staged(pick[1].mode)) {
+        float stage_ms = 0.0f;
+        if ((rc = time_pass(ops.stage, &stage_ms)) != UPF_OK) break;
+        const float it = ops.loop_iterations > 0.0f ? ops.loop_iterations : 1.0f;
+        float best_cost = 1e30f;
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) {
+            const Pick& d = a ? best_any[0] : best_plain[0];
+            const Pick& f = b ? best_any[1] : best_plain[1];
+            const bool staged = loop_mode_staged(d.mode) || loop_mode_staged(f.mode);
+            const float cost = it * (d.ms + f.ms) + (staged ? stage_ms : 0.0f);
+            if (cost < best_cost) best_cost = cost, pick[0] = d, pick[1] = f;
+          }
+      }
+      for (int pass = 0; pass < 2; ++pass) {
+        (pass == 0 ? sh.density_mode : sh.pforce_mode) = pick[pass].mode;
+        (pass == 0 ? sh.density_threads : sh.pforce_threads) = pick[pass].threads;
+        (pass == 0 ? sh.density_rows : sh.pforce_rows) = pick[pass].rows;
+        chosen_ms[2 + pass] = pick[pass].ms;
+      }
+    } else {
+      for (int pass = 0; pass < 2; ++pass) {
+        if (!tuned[pass]) continue;
+        (pass == 0 ? sh.density_mode : sh.pforce_mode) = best_any[pass].mode;
+        (pass == 0 ? sh.density_threads : sh.pforce_threads) = best_any[pass].threads;
+        (pass == 0 ? sh.density_rows : sh.pforce_rows) = best_any[pass].rows;
+        chosen_ms[2 + pass] = best_any[pass].ms;
+      }
     }
   } while (0);
   const upf_status rr = ops.restore(ops.ctx);
@@ -622,6 +664,16 @@ const char* upf_status_string(upf_status st) {
 
 int32_t upf_abi_version(void) { return UPF_ABI_VERSION; }
 
+upf_status upf_test_stage_union_cap(upf_system* s, uint32_t cap) {
+  if (!s || cap > kUnionMax) {
+    set_error("upf_test_stage_union_cap: null system or cap above %u", kUnionMax);
+    return UPF_ERR_INVALID_ARG;
+  }
+  UPF_CUDA(cudaStreamSynchronize(s->stream));
+  s->stage_cap = cap;
+  return s->have_particles ? build_step_graph(*s) : UPF_OK;
+}
+
 upf_status upf_test_fail_allocation(int32_t nth) {
   g_fail_alloc_at.store(nth < 0 ? -1 : (int64_t)nth);
   return UPF_OK;
@@ -810,6 +862,13 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   ALLOC(s->spos, c); ALLOC(s->skeys, c); ALLOC(s->sid, c);
   ALLOC(s->luts, 5 * UPF_LUT_ENTRIES + kThresholds);
   ALLOC(s->st, 1);
+  if (p->method == UPF_METHOD_PCISPH) {
+    // staged neighbourhoods of the loop passes (loop-pass mode 2)
+    const size_t chunks = ((size_t)c + kStageChunk - 1) / kStageChunk;
+    ALLOC(s->ucodes, chunks * kUnionMax);
+    ALLOC(s->ucount, chunks);
+    ALLOC(s->lloc, (size_t)((p->max_neighbors + 3) / 4) * s->nstride);
+  }
 #undef ALLOC
   if ((st = encode_list_maps(s->nbr_maps, s->lval_maps, s->nbr, s->lval, s->nstride, p->max_neighbors)) != UPF_OK)
     return bail(st);
@@ -828,6 +887,9 @@ upf_status upf_create(const upf_params* p, int device, uint32_t capacity, upf_sy
   if (e == cudaSuccess) e = cudaMemset(s->pq, 0, sizeof(float4) * ct);
   if (e == cudaSuccess) e = cudaMemset(s->press, 0, sizeof(float) * ct);
   if (e == cudaSuccess) e = cudaMemset(s->rho, 0, sizeof(float) * ct);
+  // no chunk is staged before the first staged list build: the passes read the plain lists
+  if (e == cudaSuccess && s->ucount)
+    e = cudaMemset(s->ucount, 0xff, sizeof(uint32_t) * (((size_t)c + kStageChunk - 1) / kStageChunk));
   if (e == cudaSuccess) e = cudaMemset(s->st, 0, sizeof(DevState));
   if (e != cudaSuccess) {
     set_error("upload: %s", cudaGetErrorString(e));
@@ -1554,11 +1616,21 @@ upf_status upf_autotune(upf_system* s, int32_t repeats, upf_launch_config* chose
   };
   ops.nlist = [](void* c, cudaStream_t st) { return launch_neighbor_phase(*static_cast<SysTune*>(c)->s, st); };
   if (pcisph) {
+    ops.stage = [](void* c, cudaStream_t st) { return launch_list_staging(*static_cast<SysTune*>(c)->s, st); };
+    // the iterations of the last step weigh the staging kernel against the
+    // passes' per-iteration saving
+    UPF_CUDA(cudaMemcpy(s->st_host, s->st, sizeof(DevState), cudaMemcpyDeviceToHost));
+    ops.loop_iterations = (float)std::max(s->st_host->final_iterations, std::max(s->prm.min_loops, 1));
     ops.external = [](void* c, cudaStream_t st) { return launch_force_phase(*static_cast<SysTune*>(c)->s, st); };
     ops.density = [](void* c, cudaStream_t st) { return launch_loop_density(*static_cast<SysTune*>(c)->s, st); };
     ops.pforce = [](void* c, cudaStream_t st) { return launch_loop_pforce(*static_cast<SysTune*>(c)->s, st); };
   }
-  UPF_TRY(autotune_shapes(ops, repeats, chosen));
+  // every mode is timed on the lists of the same step: stage them whatever
+  // the shape while tuning
+  s->stage_always = pcisph;
+  const upf_status rc = autotune_shapes(ops, repeats, chosen);
+  s->stage_always = false;
+  UPF_TRY(rc);
   UPF_TRY(check_device_errors(*s));
   return build_step_graph(*s);
 }

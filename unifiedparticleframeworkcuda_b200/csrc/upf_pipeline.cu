@@ -1145,6 +1145,374 @@ __global__ void __launch_bounds__(kSegAlign) k_pcisph_pressure_force_active(
   }
 }
 
+// ---------------------------------------------------------------- staged neighbourhoods
+// Loop-pass mode 2. The 256 particles of a chunk (one CTA) sit close together
+// in Morton order, so their lists draw on one small neighbourhood: about 830
+// distinct neighbours on the 1M dam against 256 x 29 list entries. Once per
+// step k_stage_lists writes that union and rewrites the chunk's list entries
+// as positions in it; each loop pass then copies the union's data into
+// shared memory (one gather per distinct neighbour instead of one per list
+// entry) and reads every neighbour from there. The entries keep their list
+// order, so every sum keeps the reference's order and the results are
+// bit-identical to the other modes.
+// The union is kept as a set of 8-index blocks (a block id and a mask of the
+// indices present), so that neighbour indices that follow one another get
+// consecutive positions: the k-th neighbours of a warp's consecutive
+// particles are mostly consecutive indices, and consecutive 16-byte entries
+// in shared memory fall in different banks.
+constexpr uint32_t kStageBlocks = 1024;  // block slots, open addressing
+constexpr uint32_t kMaxStageBlocks = kStageBlocks / 2;
+constexpr uint32_t kHashEmpty = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t stage_hash(uint32_t blk) {
+  return (blk * 2654435761u) >> (32 - 10);  // Fibonacci hashing onto kStageBlocks = 1024 slots
+}
+static_assert(kStageBlocks == 1024, "stage_hash maps onto 1024 slots");
+static_assert((kUnionMax & (kUnionMax - 1)) == 0, "union positions are masked with kUnionMax - 1");
+
+// One CTA per chunk: (1) insert the chunk's neighbour indices into the block
+// set in shared memory, stopping at more than kMaxStageBlocks blocks;
+// (2) number the indices (blocks in slot order, indices in a block in
+// order), stopping at more than `cap`, and write the union; (3) rewrite each
+// list entry as its index's number. Liquid particles only (the loop passes
+// read no other lists).
+__global__ void __launch_bounds__(kStageChunk) k_stage_lists(uint32_t n, const int32_t* __restrict__ type,
+                                                              const uint32_t* __restrict__ nbr,
+                                                              const uint32_t* __restrict__ ncnt, uint32_t stride,
+                                                              uint32_t cap, uint32_t* __restrict__ ucodes,
+                                                              uint32_t* __restrict__ ucount,
+                                                              unsigned long long* __restrict__ lloc) {
+  __shared__ uint32_t bkey[kStageBlocks];
+  __shared__ uint32_t bmask[kStageBlocks];
+  __shared__ uint16_t bbase[kStageBlocks];
+  __shared__ uint32_t warp_tot[kStageChunk / 32];
+  __shared__ uint32_t nblocks;
+  __shared__ int over;
+  const uint32_t chunk = blockIdx.x, tid = threadIdx.x;
+  for (uint32_t k = tid; k < kStageBlocks; k += kStageChunk) {
+    bkey[k] = kHashEmpty;
+    bmask[k] = 0u;
+  }
+  if (tid == 0) {
+    nblocks = 0;
+    over = 0;
+  }
+  __syncthreads();
+  const uint32_t i = chunk * kStageChunk + tid;
+  const bool active = i < n && type[i] == UPF_LIQUID;
+  const uint32_t cnt = active ? ncnt[i] : 0u;
+  const uint32_t* __restrict__ col = nbr + i;
+  unsigned long long* __restrict__ out = lloc + i;
+  volatile int* vover = &over;
+  volatile uint32_t* vkey = bkey;
+  // each entry's (block slot, index in the block) goes to lloc for now, four
+  // to a word; step (3) turns them into union positions in place
+  // the codes come four at a time, the next four loaded before these are
+  // inserted (the insertions' shared-memory atomics keep the compiler from
+  // moving later loads ahead of them)
+  uint32_t nxt[4];
+#pragma unroll
+  for (uint32_t r = 0; r < 4; ++r) nxt[r] = r < cnt ? __ldg(col + (size_t)r * stride) : 0u;
+  for (uint32_t k0 = 0; k0 < cnt && !*vover; k0 += 4) {
+    uint32_t codes[4];
+#pragma unroll
+    for (uint32_t r = 0; r < 4; ++r) {
+      codes[r] = nxt[r];
+      if (k0 + 4 + r < cnt) nxt[r] = __ldg(col + (size_t)(k0 + 4 + r) * stride);
+    }
+    unsigned long long w = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < 4; ++r) {
+      if (k0 + r >= cnt) break;
+      const uint32_t code = codes[r];
+      const uint32_t blk = code >> 3, bit = 1u << (code & 7u);
+      uint32_t slot = stage_hash(blk);
+      // a plain read first: most entries find their block present (each
+      // neighbour is in about nine lists of the chunk), and the atomics of a
+      // warp's lanes on one shared-memory word serialise. At most
+      // kMaxStageBlocks + kStageChunk < kStageBlocks blocks are ever
+      // inserted, so an empty slot is always found; the probes are bounded
+      // all the same.
+      for (uint32_t probe = 0; probe < kStageBlocks; ++probe) {
+        const uint32_t cur = vkey[slot];
+        if (cur == blk) break;
+        if (cur == kHashEmpty) {
+          const uint32_t prev = atomicCAS(&bkey[slot], kHashEmpty, blk);
+          if (prev == kHashEmpty) {
+            if (atomicAdd(&nblocks, 1u) >= kMaxStageBlocks) *vover = 1;
+            break;
+          }
+          if (prev == blk) break;
+        }
+        slot = (slot + 1) & (kStageBlocks - 1);
+      }
+      if (!(bmask[slot] & bit)) atomicOr(&bmask[slot], bit);
+      w |= (unsigned long long)((slot << 3) | (code & 7u)) << (16 * r);
+    }
+    out[(size_t)(k0 / 4) * stride] = w;
+  }
+  __syncthreads();
+  if (over) {
+    if (tid == 0) ucount[chunk] = kUnionOverflow;
+    return;  // uniform: the chunk's passes read the plain lists
+  }
+  // (2) thread t numbers the blocks in slots [t * 4, t * 4 + 4); an exclusive
+  // scan over the threads' index counts gives each block its first position
+  constexpr uint32_t kPer = kStageBlocks / kStageChunk;
+  uint32_t mine = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < kPer; ++j) mine += __popc(bmask[tid * kPer + j]);
+  const uint32_t lane = tid & 31, warp = tid >> 5;
+  uint32_t incl = mine;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= (uint32_t)d) incl += v;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kStageChunk / 32 ? warp_tot[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= (uint32_t)d) w += v;
+    }
+    if (lane < kStageChunk / 32) warp_tot[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  const uint32_t total = warp_tot[kStageChunk / 32 - 1];
+  if (total > cap) {
+    if (tid == 0) ucount[chunk] = kUnionOverflow;
+    return;  // uniform
+  }
+  uint32_t at = (warp ? warp_tot[warp - 1] : 0u) + incl - mine;
+  uint32_t* __restrict__ uc = ucodes + (size_t)chunk * kUnionMax;
+#pragma unroll
+  for (uint32_t j = 0; j < kPer; ++j) {
+    const uint32_t slot = tid * kPer + j;
+    uint32_t m = bmask[slot];
+    bbase[slot] = (uint16_t)at;
+    const uint32_t base = bkey[slot] << 3;
+    while (m) {
+      const uint32_t b = __ffs(m) - 1;
+      m &= m - 1;
+      uc[at++] = base + b;
+    }
+  }
+  if (tid == 0) ucount[chunk] = total;
+  __syncthreads();
+  // (3) the chunk's entries as union positions, four to a word, in place
+  // (the next word loaded before this one is rewritten)
+  unsigned long long vn = cnt ? out[0] : 0ull;
+  for (uint32_t k0 = 0; k0 < cnt; k0 += 4) {
+    const unsigned long long v = vn;
+    if (k0 + 4 < cnt) vn = out[(size_t)(k0 / 4 + 1) * stride];
+    unsigned long long w2 = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < 4; ++r) {
+      if (k0 + r < cnt) {
+        const uint32_t e = (uint32_t)(v >> (16 * r)) & 0xffffu;
+        const uint32_t slot = e >> 3, b = e & 7u;
+        const uint32_t posn = bbase[slot] + __popc(bmask[slot] & ((1u << b) - 1u));
+        w2 |= (unsigned long long)posn << (16 * r);
+      }
+    }
+    out[(size_t)(k0 / 4) * stride] = w2;
+  }
+}
+
+// The staged list walk of one lane: batches of kRows entries (kRows / 4
+// words of lloc, the next batch's words loaded before this batch's
+// arithmetic); `body(pos, k0)` gets the union positions of the batch.
+template <int kRows, class Body>
+__device__ __forceinline__ void walk_staged(const unsigned long long* __restrict__ col, uint32_t stride, uint32_t cnt,
+                                            Body&& body) {
+  constexpr int kWords = kRows / 4;
+  unsigned long long w[kWords];
+#pragma unroll
+  for (int q = 0; q < kWords; ++q) w[q] = (4 * q < (int)cnt) ? __ldg(col + (size_t)q * stride) : 0ull;
+  for (uint32_t k0 = 0; k0 < cnt; k0 += kRows) {
+    unsigned long long cur[kWords];
+#pragma unroll
+    for (int q = 0; q < kWords; ++q) {
+      cur[q] = w[q];
+      const uint32_t kn = k0 + kRows + 4 * q;
+      if (kn < cnt) w[q] = __ldg(col + (size_t)(kn / 4) * stride);
+    }
+    // (positions are below kUnionMax by construction; the mask keeps every
+    // shared-memory read in bounds even on lists staged for another step)
+    body([&](int r) { return (uint32_t)(cur[r >> 2] >> (16 * (r & 3))) & (kUnionMax - 1); }, (int)k0);
+  }
+}
+
+// The predicted-density pass over staged neighbourhoods (density_block's
+// arithmetic, ComputePredictedDensityAndPressure, UnifiedPhysics.cpp:5456-5491).
+// Register caps (CTAs an SM the launch bounds ask for; six fit the shared
+// memory, 33-34 KB each): 4-entry batches are held to 48 registers, 8-entry
+// batches to 64 (density) and 80 (pressure force), the caps below which
+// they spill.
+constexpr int density_staged_min_blocks(int rows) { return rows == 4 ? 5 : 4; }
+constexpr int pforce_staged_min_blocks(int rows) { return rows == 4 ? 5 : 3; }
+
+template <int kRows>
+__global__ void __launch_bounds__(kStageChunk, density_staged_min_blocks(kRows)) k_pcisph_density_staged(
+    const __grid_constant__ DevParams P, uint32_t n, const int32_t* __restrict__ type,
+    const float4* __restrict__ xs, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
+    const uint32_t* __restrict__ ucodes, const uint32_t* __restrict__ ucount,
+    const unsigned long long* __restrict__ lloc, const float* __restrict__ luts, float* __restrict__ rho,
+    float* __restrict__ press, float4* __restrict__ pq, DevState* __restrict__ st) {
+  __shared__ float4 xsm[kUnionMax];
+  __shared__ float m4[UPF_LUT_ENTRIES];
+  __shared__ uint32_t wmax[kStageChunk / 32];
+  const uint32_t chunk = blockIdx.x;
+  const uint32_t U = ucount[chunk];
+  const bool staged = U != kUnionOverflow;
+  // the table times the mass, as in density_block
+  for (int k = threadIdx.x; k < UPF_LUT_ENTRIES; k += kStageChunk)
+    m4[k] = fmul(__ldg(luts + LUT_M4 * UPF_LUT_ENTRIES + k), P.mass);
+  if (staged) {
+    const uint32_t* __restrict__ uc = ucodes + (size_t)chunk * kUnionMax;
+    const uint32_t nu = U < kUnionMax ? U : kUnionMax;
+    for (uint32_t l = threadIdx.x; l < nu; l += kStageChunk) xsm[l] = __ldg(xs + __ldg(uc + l));
+  }
+  const float r2_edge = __ldg(luts + 5 * UPF_LUT_ENTRIES + kLut);
+  __syncthreads();
+  const uint32_t i = chunk * kStageChunk + threadIdx.x;
+  const bool active = i < n && type[i] == UPF_LIQUID;
+  const uint32_t cnt = active ? ncnt[i] : 0u;
+  const float4 xi = active ? xs[i] : make_float4(0, 0, 0, 0);
+  const unsigned long long xiy = pk2(xi.x, xi.y);
+  float den = P.kernel_self * P.mass;
+  auto add = [&](float4 xj) {
+    const float r2 = dist2_xy(xiy, xi.z, xj);
+    den += m4[bin_of_r2_edge(r2, P.lut_factor, r2_edge)];
+  };
+  if (staged) {
+    walk_staged<kRows>(lloc + i, P.nstride, cnt, [&](auto pos, int k0) {
+      float4 xj[kRows];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r)
+        if (k0 + r < (int)cnt) xj[r] = xsm[pos(r)];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r)
+        if (k0 + r < (int)cnt) add(xj[r]);
+    });
+  } else {
+    const uint32_t* __restrict__ col = nbr + i;
+    for (uint32_t k0 = 0; k0 < cnt; k0 += 4) {
+      float4 xj[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (k0 + r < cnt) xj[r] = __ldg(xs + __ldg(col + (size_t)(k0 + r) * P.nstride));
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (k0 + r < cnt) add(xj[r]);
+    }
+  }
+  uint32_t best = 0;
+  if (active) {
+    const float err = mx0(den - P.rho0, 0.0f);
+    const float pnew = press[i] + mx0(err * P.delta, 0.0f);
+    press[i] = pnew;
+    reinterpret_cast<float*>(pq + i)[3] = pnew / (P.rho0 * P.rho0);
+    rho[i] = den;
+    best = __float_as_uint(den);
+  }
+  best = warp_max(best);
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t v = threadIdx.x < kStageChunk / 32 ? wmax[threadIdx.x] : 0u;
+    v = warp_max(v);
+    if (threadIdx.x == 0 && v) atomicMax(&st->max_rho_bits, v);
+  }
+}
+
+// The pressure-force pass over staged neighbourhoods (pforce_block's
+// arithmetic, ComputeCorrectivePressureForce, UnifiedPhysics.cpp:5493-5522,
+// then the next prediction): the union's (position, p / rho0^2) in shared
+// memory, the entries' pressure-gradient values from the list values.
+template <int kRows>
+__global__ void __launch_bounds__(kStageChunk, pforce_staged_min_blocks(kRows)) k_pcisph_pressure_force_staged(
+    const __grid_constant__ DevParams P, uint32_t n, DynArrays B, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt, const uint32_t* __restrict__ ucodes,
+    const uint32_t* __restrict__ ucount, const unsigned long long* __restrict__ lloc,
+    const float4* __restrict__ pq, const float4* __restrict__ force, float4* __restrict__ pforce,
+    float4* __restrict__ xs, DevState* __restrict__ st) {
+  __shared__ float4 qsm[kUnionMax];
+  const uint32_t chunk = blockIdx.x;
+  const uint32_t U = ucount[chunk];
+  const bool staged = U != kUnionOverflow;
+  if (staged) {
+    const uint32_t* __restrict__ uc = ucodes + (size_t)chunk * kUnionMax;
+    const uint32_t nu = U < kUnionMax ? U : kUnionMax;
+    for (uint32_t l = threadIdx.x; l < nu; l += kStageChunk) qsm[l] = __ldg(pq + __ldg(uc + l));
+  }
+  __syncthreads();
+  const uint32_t i = chunk * kStageChunk + threadIdx.x;
+  const bool active = i < n && B.type[i] == UPF_LIQUID;
+  if (!active) return;  // no barrier follows
+  const uint32_t cnt = ncnt[i];
+  const float4 xi = B.pos[i];
+  const float m = P.mass;
+  const float qi = pq[i].w;
+  // scalar arithmetic, as in pforce_block
+  float fx = 0, fy = 0, fz = 0;
+  const uint32_t* __restrict__ vcol = lval + i;
+  auto add = [&](float4 xj, float g) {
+    const float kx = (xi.x - xj.x) * g, ky = (xi.y - xj.y) * g, kz = (xi.z - xj.z) * g;
+    const float grad = qi + xj.w;
+    fx = fx - kx * grad * m * m;
+    fy = fy - ky * grad * m * m;
+    fz = fz - kz * grad * m * m;
+  };
+  if (staged) {
+    // the list values of the next batch are loaded with its positions,
+    // before this batch's arithmetic (walk_staged's prefetch, extended)
+    float gn[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) gn[r] = r < (int)cnt ? __uint_as_float(__ldg(vcol + (size_t)r * P.nstride)) : 0.0f;
+    walk_staged<kRows>(lloc + i, P.nstride, cnt, [&](auto pos, int k0) {
+      float4 xj[kRows];
+      float g[kRows];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) {
+        g[r] = gn[r];
+        const uint32_t kn = (uint32_t)k0 + kRows + r;
+        if (kn < cnt) gn[r] = __uint_as_float(__ldg(vcol + (size_t)kn * P.nstride));
+      }
+#pragma unroll
+      for (int r = 0; r < kRows; ++r)
+        if (k0 + r < (int)cnt) xj[r] = qsm[pos(r)];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r)
+        if (k0 + r < (int)cnt) add(xj[r], g[r]);
+    });
+  } else {
+    const uint32_t* __restrict__ col = nbr + i;
+    for (uint32_t k0 = 0; k0 < cnt; k0 += 4) {
+      float4 xj[4];
+      float g[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (k0 + r < cnt) {
+          g[r] = __uint_as_float(__ldg(vcol + (size_t)(k0 + r) * P.nstride));
+          xj[r] = __ldg(pq + __ldg(col + (size_t)(k0 + r) * P.nstride));
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (k0 + r < cnt) add(xj[r], g[r]);
+    }
+  }
+  pforce[i] = f4(fx, fy, fz);
+  const float4 F = force[i];
+  bool bad;
+  xs[i] = predict(P, xi, B.vel[i], make_float3(F.x, F.y, F.z), make_float3(fx, fy, fz), bad);
+  if (bad) atomicOr(&st->error_flags, (uint32_t)ERR_NAN);
+}
+
 __global__ void k_loop_init(DevState* st) {
   st->iteration = 0;
   st->too_large = 1;
@@ -1557,12 +1925,35 @@ cudaError_t launch_sort_phase(System& s, cudaStream_t st) {
   return cell_ranges(s.keysA, n, 3 * (int)s.dp.cell_shift, s.ncells, s.cstart, s.cend, st);
 }
 
+// The union and union positions of each chunk's lists (k_stage_lists).
+static cudaError_t launch_stage_lists(System& s, cudaStream_t st) {
+  const uint32_t n = s.n_dyn;
+  k_stage_lists<<<(n + kStageChunk - 1) / kStageChunk, kStageChunk, 0, st>>>(
+      n, s.B.type, s.nbr, s.ncnt, s.nstride, s.stage_cap, s.ucodes, s.ucount, s.lloc);
+  s.lists_staged = true;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_list_staging(System& s, cudaStream_t st) {
+  return s.n_dyn && s.ucodes ? launch_stage_lists(s, st) : cudaSuccess;
+}
+
+// the lists are staged when a loop pass reads staged neighbourhoods (or
+// while the autotuner times every mode)
+static bool stages_lists(const System& s) {
+  return s.ucodes && (s.stage_always || loop_mode_staged(s.shape.density_mode) ||
+                      loop_mode_staged(s.shape.pforce_mode));
+}
+
 cudaError_t launch_neighbor_phase(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
   k_step_init<<<1, 1, 0, st>>>(s.st, s.prm.method == UPF_METHOD_WCSPH ? 1 : 0);
   if (n == 0) return cudaGetLastError();
-  return run_nlist<false>(s.shape, st, s.dp, BatchView{}, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static, s.spos,
-                          s.skeys, s.sstart, s.send, s.nbr, s.lval, s.ncnt, s.luts, s.st);
+  s.lists_staged = false;
+  cudaError_t e = run_nlist<false>(s.shape, st, s.dp, BatchView{}, n, s.B.pos, s.keysA, s.cstart, s.cend, s.n_static,
+                                   s.spos, s.skeys, s.sstart, s.send, s.nbr, s.lval, s.ncnt, s.luts, s.st);
+  if (e != cudaSuccess || !stages_lists(s)) return e;
+  return launch_stage_lists(s, st);
 }
 
 cudaError_t launch_force_phase(System& s, cudaStream_t st) {
@@ -1585,6 +1976,23 @@ cudaError_t launch_loop_init(System& s, cudaStream_t st) {
 
 cudaError_t launch_loop_density(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
+  if (n && loop_mode_staged(s.shape.density_mode)) {
+    // lists built under another shape (phase by phase) are staged first
+    if (!s.lists_staged) {
+      cudaError_t e = launch_stage_lists(s, st);
+      if (e != cudaSuccess) return e;
+    }
+    const uint32_t g = (n + kStageChunk - 1) / kStageChunk;
+    if (s.shape.density_rows == 4)
+      k_pcisph_density_staged<4><<<g, kStageChunk, 0, st>>>(s.dp, n, s.B.type, s.xs, s.nbr, s.ncnt, s.ucodes,
+                                                           s.ucount, s.lloc, s.luts, s.rho, s.press, s.pq, s.st);
+    else if (s.shape.density_rows == 8)
+      k_pcisph_density_staged<8><<<g, kStageChunk, 0, st>>>(s.dp, n, s.B.type, s.xs, s.nbr, s.ncnt, s.ucodes,
+                                                           s.ucount, s.lloc, s.luts, s.rho, s.press, s.pq, s.st);
+    else
+      return cudaErrorInvalidConfiguration;
+    return cudaGetLastError();
+  }
   if (n)
     return run_density<false>(s.shape, st, s.dp, BatchView{}, n, s.B.type, s.xs, s.nbr_maps, s.nbr, s.ncnt, s.luts, s.rho,
                               s.press, s.pq, s.st);
@@ -1593,6 +2001,24 @@ cudaError_t launch_loop_density(System& s, cudaStream_t st) {
 
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st) {
   const uint32_t n = s.n_dyn;
+  if (n && loop_mode_staged(s.shape.pforce_mode)) {
+    if (!s.lists_staged) {
+      cudaError_t e = launch_stage_lists(s, st);
+      if (e != cudaSuccess) return e;
+    }
+    const uint32_t g = (n + kStageChunk - 1) / kStageChunk;
+    if (s.shape.pforce_rows == 4)
+      k_pcisph_pressure_force_staged<4><<<g, kStageChunk, 0, st>>>(s.dp, n, s.B, s.nbr, s.lval, s.ncnt, s.ucodes,
+                                                                  s.ucount, s.lloc, s.pq, s.force, s.pforce, s.xs,
+                                                                  s.st);
+    else if (s.shape.pforce_rows == 8)
+      k_pcisph_pressure_force_staged<8><<<g, kStageChunk, 0, st>>>(s.dp, n, s.B, s.nbr, s.lval, s.ncnt, s.ucodes,
+                                                                  s.ucount, s.lloc, s.pq, s.force, s.pforce, s.xs,
+                                                                  s.st);
+    else
+      return cudaErrorInvalidConfiguration;
+    return cudaGetLastError();
+  }
   if (n)
     return run_pforce<false>(s.shape, st, s.dp, BatchView{}, n, s.B, s.nbr_maps, s.lval_maps, s.nbr, s.lval, s.ncnt, s.luts, s.pq,
                              s.force, s.pforce, s.xs, s.st);
@@ -1826,7 +2252,7 @@ cudaError_t batch_launch_integrate(BatchSystem& b, cudaStream_t st) {
 
 int pipeline_launches_per_step(const System& s, int iterations) {
   int sort = radix_launches(s.key_bits) + 1 /*reorder*/ + 1 /*cells*/ + (s.rb.n_rigid ? 1 : 0) /*rigid slots*/;
-  int nl = 2;  // step init + neighbour lists
+  int nl = 2 + (stages_lists(s) ? 1 : 0);  // step init + neighbour lists (+ staging)
   if (s.prm.method == UPF_METHOD_WCSPH) return sort + nl + 2;
   return sort + nl + 1 /*external*/ + 1 /*loop init*/ + 3 * iterations + 1 /*integrate*/ + rigid_launches_per_step(s);
 }

@@ -62,16 +62,18 @@ struct LaunchShape {
   int density_rows = 8;
   int pforce_threads = 256;    // with pforce_rows: the same pairs, where the ring fits
   int pforce_rows = 4;
-  int density_mode = 0;        // list entries by 0: the TMA ring, 1: direct loads (rows = entries per batch)
+  int density_mode = 0;        // list entries by 0: the TMA ring, 1: direct loads (rows = entries per batch),
+                               // 2: staged neighbourhoods (256 threads; rows = entries per batch)
   int pforce_mode = 0;
   int nlist_mode = 0;          // 0: each lane its own query box; 1: the warp's union of boxes
 };
 bool shape_valid(const LaunchShape& s, bool batched, const char** why);
-// (mode, threads, rows) triples of the loop passes: TMA ring (mode 0) and
-// direct loads (mode 1)
+// (mode, threads, rows) triples of the loop passes: TMA ring (mode 0),
+// direct loads (mode 1) and staged neighbourhoods (mode 2, single scenes)
 constexpr int kLoopShapes[][3] = {{0, 128, 4}, {0, 128, 8}, {0, 128, 16}, {0, 256, 2}, {0, 256, 4},
                                   {0, 256, 8}, {0, 512, 2}, {0, 512, 4},  {0, 1024, 2}, {1, 128, 4},
-                                  {1, 128, 8}, {1, 256, 4}, {1, 256, 8},  {1, 512, 4},  {1, 512, 8}};
+                                  {1, 128, 8}, {1, 256, 4}, {1, 256, 8},  {1, 512, 4},  {1, 512, 8},
+                                  {2, 256, 4}, {2, 256, 8}};
 constexpr int kNumLoopShapes = sizeof(kLoopShapes) / sizeof(kLoopShapes[0]);
 // The pressure-force pass's TMA ring carries a 32-bit value per list entry
 // beside its code: shapes whose rings (three stages a warp) leave no room
@@ -81,6 +83,19 @@ constexpr bool pforce_ring_fits(int mode, int threads, int rows) {
 }
 static_assert(pforce_ring_fits(LaunchShape{}.pforce_mode, LaunchShape{}.pforce_threads, LaunchShape{}.pforce_rows),
               "the default pressure-force shape must be one that is built");
+// Staged neighbourhoods (loop-pass mode 2). The lists of each chunk of
+// kStageChunk consecutive sorted particles (one CTA of a staged pass) are
+// rewritten once per step against the chunk's union of neighbours: ucodes
+// holds the union's neighbour indices (at most kUnionMax a chunk), ucount its
+// size (kUnionOverflow: the union did not fit, the chunk's passes read the
+// plain lists), and lloc the list entries as 16-bit positions in the union,
+// four to a 64-bit word, lloc[(k / 4) * stride + i]. A staged pass copies the
+// union's data into shared memory once and reads each neighbour from there.
+constexpr int kStageChunk = 256;
+constexpr uint32_t kUnionMax = 2048;
+constexpr uint32_t kUnionOverflow = 0xffffffffu;
+constexpr bool loop_mode_staged(int mode) { return mode == 2; }
+
 constexpr int kListRowVariants = 4;  // tensor maps for 2, 4, 8 and 16 rows per box
 inline int rows_index(int rows) { return rows == 2 ? 0 : (rows == 4 ? 1 : (rows == 8 ? 2 : 3)); }
 
@@ -165,6 +180,13 @@ struct System {
   CUtensorMap lval_maps[kListRowVariants];  // same views of lval (uint32)
   uint32_t nstride = 0;
   LaunchShape shape;
+  // staged neighbourhoods (PCISPH systems; see kStageChunk)
+  uint32_t* ucodes = nullptr;            // [chunks][kUnionMax]
+  uint32_t* ucount = nullptr;            // [chunks]
+  unsigned long long* lloc = nullptr;    // [ceil(max_neighbors / 4)][nstride]
+  uint32_t stage_cap = kUnionMax;        // union capacity used (tests lower it to reach the fallback)
+  bool stage_always = false;             // stage the lists whatever the shape (set while autotuning)
+  bool lists_staged = false;             // the last list build was staged (host-side, in launch order)
 
   // cells
   uint32_t ncells = 0;
@@ -312,6 +334,10 @@ struct TuneOps {
   cudaError_t (*external)(void* ctx, cudaStream_t st) = nullptr;
   cudaError_t (*density)(void* ctx, cudaStream_t st) = nullptr;
   cudaError_t (*pforce)(void* ctx, cudaStream_t st) = nullptr;
+  // staging of the lists for the staged loop-pass modes (null: those modes
+  // are not tried), and the loop iterations a step is expected to take
+  cudaError_t (*stage)(void* ctx, cudaStream_t st) = nullptr;
+  float loop_iterations = 0.0f;
   upf_status (*save)(void* ctx) = nullptr;
   upf_status (*restore)(void* ctx) = nullptr;
 };
@@ -338,6 +364,7 @@ cudaError_t launch_loop_body(System& s, cudaStream_t st, cudaGraphConditionalHan
 cudaError_t launch_loop_density(System& s, cudaStream_t st);
 cudaError_t launch_loop_pforce(System& s, cudaStream_t st);
 cudaError_t launch_loop_ctl(System& s, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle);
+cudaError_t launch_list_staging(System& s, cudaStream_t st);  // k_stage_lists over the current lists
 cudaError_t launch_upload_keys(System& s, cudaStream_t st);
 cudaError_t launch_integrate_phase(System& s, cudaStream_t st);
 cudaError_t launch_static_setup(System& s, cudaStream_t st);
