@@ -851,15 +851,16 @@ def io_reference_baseline(st, d, records=200_000):
 
 
 def parse_shape(text):
-    """'nlist,external,density_threads,density_rows,pforce_threads,pforce_rows[,density_mode,pforce_mode]'"""
+    """'nlist,external,density_threads,density_rows,pforce_threads,pforce_rows[,density_mode,pforce_mode
+    [,nlist_mode]]'"""
     from unifiedparticleframeworkcuda_b200 import UpfLaunchConfig
     v = [int(t) for t in text.split(",")]
-    if len(v) not in (6, 8):
-        raise SystemExit("--shape needs six or eight integers")
-    v += [0, 0] if len(v) == 6 else []
+    if len(v) not in (6, 8, 9):
+        raise SystemExit("--shape needs six, eight or nine integers")
+    v += [0, 0, 0][: 9 - len(v)]
     c = UpfLaunchConfig()
     (c.nlist_threads, c.external_threads, c.density_threads, c.density_rows, c.pforce_threads,
-     c.pforce_rows, c.density_mode, c.pforce_mode) = v
+     c.pforce_rows, c.density_mode, c.pforce_mode, c.nlist_mode) = v
     return c
 
 
@@ -959,12 +960,16 @@ def run_ours(args, rank, world, local_rank):
         kname, kms, kbytes = "k_wcsph_force_integrate", pr.integrate_ms, (16 + 16 + 4 + 4 + 16 + 16 + 4) * nf
     achieved = kbytes / (kms / 1e3) / 1e9
     step_bytes = algorithmic_bytes(nf, nb, args.steps, total_iters, method)
-    # DRAM bytes per fluid particle per launch, measured by one ncu capture
-    # of the same kernels at the tuned shapes on the 262k-fluid dam and
+    # DRAM bytes per fluid particle per launch, measured by ncu captures of
+    # the same kernels on the 262k-fluid dam (read + write, one launch) and
     # scaled here by the fluid count (the list length per particle does not
-    # depend on the scene size); not measured in this run
-    traffic_per_particle = {"k_pcisph_density": 156.0, "k_pcisph_pressure_force": 276.0}
-    traffic = traffic_per_particle[kname] * nf if kname in traffic_per_particle else None
+    # depend on the scene size); not measured in this run. Keyed by the list
+    # mode the tuned shape reads: staged neighbourhoods (mode 2) stream
+    # 16-bit union positions in place of 32-bit list entries
+    staged = (tuned.get("density_mode" if kname == "k_pcisph_density" else "pforce_mode") == 2)
+    traffic_per_particle = {("k_pcisph_density", False): 157.9, ("k_pcisph_density", True): 110.8,
+                            ("k_pcisph_pressure_force", False): 359.6, ("k_pcisph_pressure_force", True): 280.8}
+    traffic = traffic_per_particle[(kname, staged)] * nf if (kname, staged) in traffic_per_particle else None
     traffic_source = ("ncu dram__bytes_read+write per fluid particle on the 262k-fluid dam, scaled to %d fluid "
                       "particles" % nf) if traffic is not None else None
 
@@ -1093,7 +1098,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--shape", default="", help="fixed launch shapes instead of the autotuner: "
                                                 "nlist,external,density_threads,density_rows,pforce_threads,pforce_rows"
-                                                "[,density_mode,pforce_mode]")
+                                                "[,density_mode,pforce_mode[,nlist_mode]]")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()

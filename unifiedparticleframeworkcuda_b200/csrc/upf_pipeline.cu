@@ -54,34 +54,42 @@ __device__ __forceinline__ float4 f4(float x, float y, float z) { return make_fl
 // sequential order). `load(code)` gathers a neighbour's data, `use(code, v)`
 // accumulates it.
 constexpr int kUnroll = 8;
+// The external-force pass gathers 36 bytes per neighbour (position,
+// velocity, type): batches of 2 hold it to 64 registers a thread (batches of
+// 8 took 128, a quarter of the SM's warps resident), which measured 0.24
+// against 0.38-0.45 ms per launch on the 1M dam.
+constexpr int kExternalUnroll = 2;
+// The list build gathers candidate positions 4 at a time: 40 registers a
+// thread against 56 with 8 (1.22 against 1.35 ms per build on the 1M dam).
+constexpr int kNlistUnroll = 4;
 
-template <class Load, class Use>
+template <int kU = kUnroll, class Load, class Use>
 __device__ __forceinline__ void for_neighbors(const uint32_t* __restrict__ col, uint32_t stride, uint32_t cnt,
                                               Load&& load, Use&& use) {
   using T = decltype(load(0u));
   uint32_t k = 0;
-  for (; k + kUnroll <= cnt; k += kUnroll) {
-    uint32_t code[kUnroll];
-    T v[kUnroll];
+  for (; k + kU <= cnt; k += kU) {
+    uint32_t code[kU];
+    T v[kU];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) code[u] = __ldg(col + (size_t)(k + u) * stride);
+    for (int u = 0; u < kU; ++u) code[u] = __ldg(col + (size_t)(k + u) * stride);
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) v[u] = load(code[u]);
+    for (int u = 0; u < kU; ++u) v[u] = load(code[u]);
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) use(code[u], v[u]);
+    for (int u = 0; u < kU; ++u) use(code[u], v[u]);
   }
   if (k < cnt) {
-    uint32_t code[kUnroll];
-    T v[kUnroll];
+    uint32_t code[kU];
+    T v[kU];
     const uint32_t rem = cnt - k;
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u)
+    for (int u = 0; u < kU; ++u)
       if (u < rem) code[u] = __ldg(col + (size_t)(k + u) * stride);
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u)
+    for (int u = 0; u < kU; ++u)
       if (u < rem) v[u] = load(code[u]);
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u)
+    for (int u = 0; u < kU; ++u)
       if (u < rem) use(code[u], v[u]);
   }
 }
@@ -245,7 +253,7 @@ __device__ __forceinline__ float dist2_xy(unsigned long long axy, float az, floa
 // key range; within a cell the dynamic and boundary ranges are merged by
 // key. The list therefore comes out in the reference's ascending
 // sorted-index order, and membership is the reference's exact test: j != i
-// and |x_i - x_j| < h in float. Candidate positions are gathered kUnroll at
+// and |x_i - x_j| < h in float. Candidate positions are gathered kNlistUnroll at
 // a time. Each entry also records a list value at the current positions:
 // its kernel-table bin (WCSPH: the density and force passes read their
 // tables by it), or the pressure-gradient table's value at that bin
@@ -358,12 +366,12 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
   // one contiguous range of one set; `base` turns a set index into a
   // neighbour index (0 for dynamic, static_base for boundary particles)
   auto scan_range = [&](const float4* __restrict__ set, uint32_t b, uint32_t e, uint32_t base, bool skip_self) {
-    for (; b + kUnroll <= e; b += kUnroll) {
-      float4 xj[kUnroll];
+    for (; b + kNlistUnroll <= e; b += kNlistUnroll) {
+      float4 xj[kNlistUnroll];
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) xj[u] = __ldg(set + b + u);
+      for (int u = 0; u < kNlistUnroll; ++u) xj[u] = __ldg(set + b + u);
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
+      for (int u = 0; u < kNlistUnroll; ++u) {
         const uint32_t j = b + u;
         const float r2 = dist2(xi, xj[u]);
         if (!(skip_self && j == i) && r2 < thr[kThresholds - 1]) append(j + base, r2);
@@ -895,7 +903,7 @@ __global__ void __launch_bounds__(kThreads) k_pcisph_external(
   const float4* __restrict__ bvel = B.vel;
   const int32_t* __restrict__ btype = B.type;
   // boundary particles sit in the tails of the B arrays (type FROZEN, velocity 0)
-  for_neighbors(
+  for_neighbors<kExternalUnroll>(
       nbr + i, P.nstride, ncnt[i],
       [&](uint32_t code) {
         NbState s;
