@@ -354,12 +354,14 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
   uint32_t* __restrict__ out = nbr + i;
   uint32_t* __restrict__ ov = lval + i;
   const bool grad = P.list_grad != 0;
+  // An append stores the entry and its squared distance; the list value
+  // (bin_of_r2 and the table) follows in one pass over the finished list,
+  // where the lanes of a warp run together instead of one append at a time.
   auto append = [&](uint32_t code, float r2) {
     if (!active) return;
     if (cnt < maxn) {
       out[(size_t)cnt * stride] = code;
-      const int bin = bin_of_r2(r2, P.lut_factor, thr);
-      ov[(size_t)cnt * stride] = grad ? __float_as_uint(pg[bin]) : (uint32_t)bin;
+      ov[(size_t)cnt * stride] = __float_as_uint(r2);
     }
     cnt++;
   };
@@ -435,7 +437,25 @@ __global__ void __launch_bounds__(kThreads) k_build_nlist(
           if (may_hold(bx, by, bz)) visit(morton3(bx, by, bz));
   }
   if (!active) return;
-  ncnt[i] = cnt < maxn ? cnt : maxn;
+  const uint32_t m = cnt < maxn ? cnt : maxn;
+  // the list values at the entries' squared distances, four entries' loads
+  // in flight at a time
+  uint32_t k = 0;
+  for (; k + 4 <= m; k += 4) {
+    float r2[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) r2[u] = __uint_as_float(ov[(size_t)(k + u) * stride]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int bin = bin_of_r2(r2[u], P.lut_factor, thr);
+      ov[(size_t)(k + u) * stride] = grad ? __float_as_uint(pg[bin]) : (uint32_t)bin;
+    }
+  }
+  for (; k < m; ++k) {
+    const int bin = bin_of_r2(__uint_as_float(ov[(size_t)k * stride]), P.lut_factor, thr);
+    ov[(size_t)k * stride] = grad ? __float_as_uint(pg[bin]) : (uint32_t)bin;
+  }
+  ncnt[i] = m;
   if (cnt > maxn) atomicOr(&st->error_flags, (uint32_t)ERR_OVERFLOW);
   atomicMax(&st->max_neighbors, cnt);
 }
