@@ -94,6 +94,29 @@ def test_staged_passes_with_and_without_room_for_the_union(upf_lib, cap):
                 assert np.array_equal(got[f], ref[f]), (name, cap, f)
 
 
+def test_staged_mode_chosen_between_phases(upf_lib):
+    """Lists built under a plain shape, then the staged mode set before the
+    loop (phase by phase): the loop passes stage the lists themselves, and
+    the step equals one taken wholly under the default shape."""
+    sc = scenes.small_pcisph()
+    p = upf_lib.derive_params(sc.params)
+    with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
+        s.set_particles(sc.pos, sc.vel, sc.type)
+        s.step(1)
+        ref = s.particles()
+    with upf_lib.ParticleSystem(p, capacity=sc.n, derive=False) as s:
+        s.set_particles(sc.pos, sc.vel, sc.type)
+        s.phase("sort")
+        s.phase("neighbors")
+        s.set_launch_config(shape(128, 256, STAGED[0], STAGED[1]))
+        for ph in ("forces", "predict_correct", "integrate"):
+            s.phase(ph)
+        s.synchronize()
+        got = s.particles()
+    for f in ("pos", "vel", "density", "pressure"):
+        assert np.array_equal(got[f][np.argsort(got["id"])], ref[f][np.argsort(ref["id"])]), f
+
+
 @pytest.mark.parametrize("scene", ["small_pcisph", "small_coupling"])
 def test_every_list_mode_builds_the_same_lists(upf_lib, scene):
     """Neighbour lists (ids, order, counts) of both list-building modes and

@@ -496,7 +496,14 @@ upf_status build_step_graph(System& s) {
       return launch_loop_body(*static_cast<System*>(c), st, h, true);
     };
   parts.post = [](void* c, cudaStream_t st) { return launch_integrate_phase(*static_cast<System*>(c), st); };
-  return capture_step_graph(parts, &s.step_graph, &s.step_exec);
+  // capturing runs the launchers' host code without running the kernels:
+  // the host-side record of whether the current lists are staged is kept,
+  // and whether a step of this graph stages them is noted for upf_step
+  const bool staged_now = s.lists_staged;
+  const upf_status rc = capture_step_graph(parts, &s.step_graph, &s.step_exec);
+  s.graph_stages = s.lists_staged;
+  s.lists_staged = staged_now;
+  return rc;
 }
 
 upf_status check_device_errors(System& s) {
@@ -1176,6 +1183,7 @@ upf_status upf_step(upf_system* s, int32_t nsteps) {
   }
   s->stepped = true;
   for (int32_t k = 0; k < nsteps; ++k) UPF_CUDA(cudaGraphLaunch(s->step_exec, s->stream));
+  if (nsteps > 0) s->lists_staged = s->graph_stages;
   return UPF_OK;
 }
 

@@ -187,6 +187,7 @@ struct System {
   uint32_t stage_cap = kUnionMax;        // union capacity used (tests lower it to reach the fallback)
   bool stage_always = false;             // stage the lists whatever the shape (set while autotuning)
   bool lists_staged = false;             // the last list build was staged (host-side, in launch order)
+  bool graph_stages = false;             // a step of the captured step graph stages its lists
 
   // cells
   uint32_t ncells = 0;
