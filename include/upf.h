@@ -346,6 +346,17 @@ upf_status upf_upload_state_async(upf_system* s, const float* pos4, const float*
 upf_status upf_get_particles_async(upf_system* s, float* pos4, float* vel4, float* density, float* pressure,
                                    int32_t* type, uint32_t* id, uint32_t* n_out);
 upf_status upf_wait_frames(upf_system* s);
+/* A host round trip of the current frame: reads it back into the host arrays
+ * (as upf_get_particles_async; density, pressure, type and id may be NULL)
+ * and uploads pos4 and vel4 from those same host arrays as the next step's
+ * input (as upf_upload_state_async), in `chunks` pieces (1..16): each piece's
+ * upload starts as soon as its readback has reached host memory, so the two
+ * copy directions overlap. Returns at once; upf_wait_frames waits for the
+ * copies, and until then the host arrays may not be touched (the data a
+ * caller would change before uploading needs upf_get_particles_async, a wait
+ * and upf_upload_state_async instead). Pinned host memory. */
+upf_status upf_exchange_frame_async(upf_system* s, float* pos4, float* vel4, float* density, float* pressure,
+                                    int32_t* type, uint32_t* id, uint32_t chunks, uint32_t* n_out);
 
 /* ---- checkpoint / resume ------------------------------------------------- */
 /* The reference only has text dumps and readers (src/cpu/UnifiedIO.cpp:14-220).

@@ -118,6 +118,7 @@ def lib():
             "upf_upload_state_async": [vp, fp, fp, C.c_uint32],
             "upf_get_particles_async": [vp, fp, fp, fp, fp, i32p, u32p, u32p],
             "upf_wait_frames": [vp],
+            "upf_exchange_frame_async": [vp, fp, fp, fp, fp, i32p, u32p, C.c_uint32, u32p],
             "upf_batch_upload_state_async": [vp, fp, fp],
             "upf_batch_download_state_async": [vp, fp, fp],
             "upf_batch_wait_frames": [vp],

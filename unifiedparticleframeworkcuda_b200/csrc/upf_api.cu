@@ -1800,6 +1800,8 @@ cudaError_t upf::frame_streams_create(FrameIO& io, cudaStream_t compute) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&io.down, cudaStreamNonBlocking);
   for (cudaEvent_t* ev : {&io.staged, &io.consumed, &io.snapped, &io.read_done})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  for (cudaEvent_t& ev : io.chunk_down)
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   for (cudaEvent_t ev : {io.staged, io.consumed, io.snapped, io.read_done})  // all four start completed
     if (e == cudaSuccess) e = cudaEventRecord(ev, compute);
   return e;
@@ -1809,6 +1811,8 @@ void upf::frame_streams_destroy(FrameIO& io) {
   for (cudaStream_t c : {io.up, io.down})
     if (c) cudaStreamSynchronize(c);
   for (cudaEvent_t e : {io.staged, io.consumed, io.snapped, io.read_done})
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : io.chunk_down)
     if (e) cudaEventDestroy(e);
   for (cudaStream_t c : {io.up, io.down})
     if (c) cudaStreamDestroy(c);
@@ -1883,6 +1887,67 @@ upf_status upf_get_particles_async(upf_system* s, float* pos4, float* vel4, floa
   for (const Item& it : items)
     if (it.host) UPF_CUDA(cudaMemcpyAsync(it.host, it.snap, it.bytes, cudaMemcpyDeviceToHost, io.down));
   UPF_CUDA(cudaEventRecord(io.read_done, io.down));
+  return UPF_OK;
+}
+
+upf_status upf_exchange_frame_async(upf_system* s, float* pos4, float* vel4, float* density, float* pressure,
+                                    int32_t* type, uint32_t* id, uint32_t chunks, uint32_t* n_out) {
+  UPF_TRY(phase_guard(s));
+  const uint32_t n = s->n_dyn;
+  if (n_out) *n_out = n;
+  if (!pos4 || !vel4 || chunks < 1 || chunks > (uint32_t)FrameIO::kMaxChunks) {
+    set_error("upf_exchange_frame_async: positions and velocities are required, chunks in 1..%d",
+              FrameIO::kMaxChunks);
+    return UPF_ERR_INVALID_ARG;
+  }
+  if (!n) return UPF_OK;
+  UPF_TRY(frames_ready(*s));
+  FrameIO& io = s->io;
+  cudaStream_t st = s->stream;
+  // the frame, as upf_get_particles_async takes it
+  UPF_CUDA(cudaStreamWaitEvent(st, io.read_done, 0));  // the last readback has left the snapshot
+  struct Item {
+    char* host;
+    char* snap;
+    const void* src;
+    size_t elem;
+  } items[] = {{(char*)pos4, (char*)io.out_pos, s->A.pos, sizeof(float4)},
+               {(char*)vel4, (char*)io.out_vel, s->A.vel, sizeof(float4)},
+               {(char*)density, (char*)io.out_rho, s->rho, sizeof(float)},
+               {(char*)pressure, (char*)io.out_press, s->press, sizeof(float)},
+               {(char*)type, (char*)io.out_type, s->A.type, sizeof(int32_t)},
+               {(char*)id, (char*)io.out_id, s->A.id, sizeof(uint32_t)}};
+  for (const Item& it : items)
+    if (it.host) UPF_CUDA(cudaMemcpyAsync(it.snap, it.src, it.elem * n, cudaMemcpyDeviceToDevice, st));
+  UPF_CUDA(cudaEventRecord(io.snapped, st));
+  // chunk by chunk: the down stream copies the chunk to the host; once it has
+  // landed, the up stream copies its positions and velocities back from
+  // those host arrays into the staging buffers
+  UPF_CUDA(cudaStreamWaitEvent(io.down, io.snapped, 0));
+  UPF_CUDA(cudaStreamWaitEvent(io.up, io.consumed, 0));  // the last upload has left the staging buffers
+  const uint32_t per = (n + chunks - 1) / chunks;
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t b = c * per, e = std::min(n, b + per);
+    if (b >= e) break;
+    for (const Item& it : items)
+      if (it.host)
+        UPF_CUDA(cudaMemcpyAsync(it.host + it.elem * b, it.snap + it.elem * b, it.elem * (e - b),
+                                 cudaMemcpyDeviceToHost, io.down));
+    UPF_CUDA(cudaEventRecord(io.chunk_down[c], io.down));
+    UPF_CUDA(cudaStreamWaitEvent(io.up, io.chunk_down[c], 0));
+    UPF_CUDA(cudaMemcpyAsync(io.in_pos + b, pos4 + 4 * (size_t)b, sizeof(float4) * (e - b), cudaMemcpyHostToDevice,
+                             io.up));
+    UPF_CUDA(cudaMemcpyAsync(io.in_vel + b, vel4 + 4 * (size_t)b, sizeof(float4) * (e - b), cudaMemcpyHostToDevice,
+                             io.up));
+  }
+  UPF_CUDA(cudaEventRecord(io.read_done, io.down));
+  UPF_CUDA(cudaEventRecord(io.staged, io.up));
+  // the upload enters the state before the next step, as in upf_upload_state_async
+  UPF_CUDA(cudaStreamWaitEvent(st, io.staged, 0));
+  UPF_CUDA(cudaMemcpyAsync(s->A.pos, io.in_pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  UPF_CUDA(cudaMemcpyAsync(s->A.vel, io.in_vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st));
+  UPF_CUDA(launch_upload_keys(*s, st));
+  UPF_CUDA(cudaEventRecord(io.consumed, st));
   return UPF_OK;
 }
 

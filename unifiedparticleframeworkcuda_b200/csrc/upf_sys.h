@@ -127,6 +127,8 @@ struct FrameIO {
   cudaEvent_t consumed = nullptr;   // in_* entered into the state
   cudaEvent_t snapped = nullptr;    // result copied into out_*
   cudaEvent_t read_done = nullptr;  // out_* copied to the host
+  static constexpr int kMaxChunks = 16;
+  cudaEvent_t chunk_down[kMaxChunks] = {};  // upf_exchange_frame_async: chunk c has reached the host
   float4* in_pos = nullptr;
   float4* in_vel = nullptr;
   float4* out_pos = nullptr;
