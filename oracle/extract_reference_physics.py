@@ -1,0 +1,74 @@
+"""TEST INFRASTRUCTURE (oracle build step): extracts, unchanged, the member
+functions of the reference's CPU step (src/cpu/UnifiedPhysics.cpp) that the
+PCISPH step with static boundaries runs, so that oracle/Makefile can compile
+them beside a minimal class declaration of its own (ref_physics_harness.h)
+instead of the whole translation unit, whose includes need a graphics
+stack. The output goes to oracle/_ref/ only (never committed).
+
+    python extract_reference_physics.py <reference UnifiedPhysics.cpp> <output .cpp>
+"""
+import re
+import sys
+
+# CpuParticlePhysicsVersatileCouplingPCISPH (UnifiedPhysics.cpp:4991-5024)
+# and every member function it reaches on a scene of liquid and frozen
+# boundary particles, plus the weighted boundary volume of set-up
+FUNCTIONS = [
+    "CpuParticlePhysicsVersatileCouplingPCISPH",
+    "NeighborSearchOMP", "GetNeighbors",
+    "CalculateWeightedVolumeOMP", "CalculateWeightedVolume",
+    "CalculateExternalForcesVersatilCouplingPCISPHOMP", "CalculateExternalForcesVersatilCouplingPCISPH",
+    "CalculateBoundaryFluidPressureForceHost", "CalculateSurfaceTensionForcePCISPHHost",
+    "CalculateSurfaceCohesionForcePCISPHHost", "CalculateSpringForceHost", "CalculateDampingForceHost",
+    "CalculateBoundaryForcePerLiquidParticleHost", "CalculateBoundaryForcePerRigidParticleHost",
+    "PredictionCorrectionStep", "PredictPositionAndVelocity", "CollisionHandling",
+    "ComputePredictedDensityAndPressure", "ComputeCorrectivePressureForce",
+    "UpdateLiquidParticlePosVelSphCPUOMP", "UpdateLiquidParticlePosVelSphCPU",
+    "BoundaryHandlingPureFluidOMP", "BoundaryHandlingBoxPerNonRigidParticle",
+    "SortParticles",
+    "RigidBodyIntegrationOMP", "UpdateRigidBodyParticleInformationOMP", "SynRigidParticlesOMP",
+]
+# Not extracted: the per-body functions these three call for each rigid body
+# (CalculateRigidBodyForceTorqueMomenta binds a temporary to a non-const
+# reference, which only MSVC accepts); the scenes the pin runs have no rigid
+# bodies, so those loops run zero times and the harness only declares them.
+
+
+def definition(src, name):
+    """The text of `... UnifiedPhysics::name(...) { ... }` (first definition)."""
+    m = re.search(r"^[^\n;{}]*\bUnifiedPhysics::" + name + r"\s*\(", src, re.M)
+    if not m:
+        raise SystemExit("definition of UnifiedPhysics::%s not found" % name)
+    start = m.start()
+    brace = src.index("{", m.end())
+    depth, k = 0, brace
+    while True:
+        c = src[k]
+        if c == "{":
+            depth += 1
+        elif c == "}":
+            depth -= 1
+            if depth == 0:
+                break
+        k += 1
+    line = src.count("\n", 0, start) + 1
+    return "#line %d \"UnifiedPhysics.cpp\"\n" % line + src[start:k + 1] + "\n"
+
+
+def quicksort_pointer(src):
+    """The file-scope QuickSort function pointer the range sort calls."""
+    m = re.search(r"^void \(\*QuickSort\)\(.*?>;\s*$", src, re.M | re.S)
+    if not m:
+        raise SystemExit("QuickSort definition not found")
+    return src[m.start():m.end()] + "\n"
+
+
+def main():
+    src = open(sys.argv[1], encoding="utf-8-sig", errors="replace").read().replace("\r\n", "\n")
+    out = ['#include "ref_physics_harness.h"\n', quicksort_pointer(src)]
+    out += [definition(src, f) for f in FUNCTIONS]
+    open(sys.argv[2], "w").write("\n".join(out))
+
+
+if __name__ == "__main__":
+    main()

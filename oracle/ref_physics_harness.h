@@ -1,0 +1,86 @@
+// ref_physics_harness.h — TEST INFRASTRUCTURE ONLY.
+//
+// The reference's CPU step lives in src/cpu/UnifiedPhysics.cpp, whose
+// includes (windows.h, GL, render_particles.h, the CUDA interop header) need
+// a graphics stack this build does not have. oracle/extract_reference_physics.py
+// copies, unchanged and into oracle/_ref/ only, the member functions of the
+// PCISPH step with static boundaries and rigid bodies; this header gives them
+// the class they are members of: the data members and member functions they
+// use, declared with the reference's own names and types
+// (src/cpu/UnifiedPhysics.h:40-500), and nothing of its rendering, CUDA or
+// file state. ref_pins_physics.cpp drives the result.
+#pragma once
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <iostream>
+#include <limits>
+#include <vector>
+
+#include "Matrix3x3.h"
+#include "RigidBody.h"
+#include "UnifiedConstants.h"
+#include "UnifiedParticle.h"
+#include "WeightingKernel.h"
+#include "global.h"
+#include "sort.h"
+#include "vmmlib/vector3.h"
+#include "zIndex.h"
+
+class UnifiedPhysics {
+ public:
+  // data members the step reads and writes (UnifiedPhysics.h:413-500)
+  std::vector<UnifiedParticle> particles_;
+  std::vector<std::vector<int> > neighbor_indices_;
+  std::vector<RigidBody*> rigid_bodies_;
+  UnifiedConstants* fc_;
+  WeightingKernel* my_kernel_;
+  float kernel_self_;
+  bool density_error_too_large_;
+  int max_loops_sim_;
+  float avg_loops_sim_;
+  float max_predicted_density_;
+  size_t num_nonfrozen_particles_;
+  int iteration_counter_;
+
+  // the step (UnifiedPhysics.cpp:4991-5024) and what it calls
+  void CpuParticlePhysicsVersatileCouplingPCISPH();
+  void NeighborSearchOMP();
+  void GetNeighbors(const int i);
+  void CalculateWeightedVolumeOMP();
+  void CalculateWeightedVolume(const int i);
+  void CalculateExternalForcesVersatilCouplingPCISPHOMP();
+  void CalculateExternalForcesVersatilCouplingPCISPH(const int i);
+  vmml::Vector3f CalculateBoundaryFluidPressureForceHost(uint dist_lut, vmml::Vector3f p_pos, vmml::Vector3f neigh_pos,
+                                                         float p_density, float p_corr_pressure, float weighted_vol);
+  vmml::Vector3f CalculateSurfaceTensionForcePCISPHHost(const uint dist_lut, const float dist,
+                                                        const vmml::Vector3f p_pos, const vmml::Vector3f neigh_pos);
+  vmml::Vector3f CalculateSurfaceCohesionForcePCISPHHost(const uint dist_lut, const float dist,
+                                                         const vmml::Vector3f p_pos, const vmml::Vector3f neigh_pos,
+                                                         float neigh_weighted_vol);
+  vmml::Vector3f CalculateSpringForceHost(const float& dist, const float& overlap, const vmml::Vector3f& r_ij);
+  vmml::Vector3f CalculateDampingForceHost(const vmml::Vector3f& v_ij);
+  vmml::Vector3f CalculateBoundaryForcePerLiquidParticleHost(const vmml::Vector3f& position);
+  vmml::Vector3f CalculateBoundaryForcePerRigidParticleHost(const vmml::Vector3f& position, const vmml::Vector3f& vel);
+  void PredictionCorrectionStep();
+  void PredictPositionAndVelocity(const int i);
+  void CollisionHandling(vmml::Vector3f& pos, vmml::Vector3f& vel);
+  void ComputePredictedDensityAndPressure(const int i);
+  void ComputeCorrectivePressureForce(const int i);
+  void UpdateLiquidParticlePosVelSphCPUOMP();
+  void UpdateLiquidParticlePosVelSphCPU(const int i);
+  void BoundaryHandlingPureFluidOMP();
+  void BoundaryHandlingBoxPerNonRigidParticle(const vmml::Vector3f& minBox, const vmml::Vector3f& maxBox,
+                                              const float damping, vmml::Vector3f& pos, vmml::Vector3f& vel);
+  void SortParticles();
+  void RigidBodyIntegrationOMP();
+  void UpdateRigidBodyParticleInformationOMP();
+  void SynRigidParticlesOMP();
+  void CalculateRigidBodyForceTorqueMomenta(const int i);
+  void SynRigidParticlesPerRigidBody(RigidBody* body);
+  void ApplyRotationToParticlesHost(RigidBody& body);
+};

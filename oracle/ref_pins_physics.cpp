@@ -1,0 +1,156 @@
+// ref_pins_physics.cpp — TEST INFRASTRUCTURE ONLY.
+//
+// Runs the reference's own CPU step — CpuParticlePhysicsVersatileCouplingPCISPH
+// (src/cpu/UnifiedPhysics.cpp:4991-5024) and the member functions it calls,
+// copied unchanged by extract_reference_physics.py and compiled beside
+// ref_physics_harness.h into oracle/_ref/libupfref_physics.so — on a scene
+// of liquid and frozen boundary particles, so that the oracle's restatement
+// of the step (density, pressure, forces, the predict-correct loop,
+// integration) can be pinned to the reference itself.
+//
+// What the harness sets up, since the reference's own set-up (Scene.cpp and
+// the UnifiedPhysics constructor) does not compile here:
+//  * UnifiedConstants from the scene's derived parameters (the same values
+//    the oracle and the library use), WeightingKernel from them, kernel_self_
+//    as the constructor computes it (UnifiedPhysics.cpp:113), the Morton
+//    block size as CreatePartilcesCPU does (UnifiedPhysics.cpp:2152-2159);
+//  * particles with the 7-argument UnifiedParticle constructor (correction
+//    pressure 0, predicted density = rest density), the fields that
+//    constructor leaves unset and the step reads set to what the oracle
+//    assumes (previous correction pressure 0, no parent rigid body), and the
+//    particle's input index kept in color_ (which the step never touches);
+//  * optionally the boundary volumes by the reference's CalculateWeightedVolume
+//    at set-up (the CPU coupling step has that call commented out,
+//    UnifiedPhysics.cpp:4997; the oracle and the GPU path compute them when
+//    adhesion is on);
+//  * one OpenMP thread: the loop's maximum predicted density is a shared
+//    member updated without a reduction (UnifiedPhysics.cpp:5488), which races
+//    with several threads.
+// Function-local statics in the reference (collision box, time step, particle
+// count, lookup factor) take the first scene's values: one scene per process.
+#include <cstdio>
+#include <sstream>
+
+#include "../include/upf.h"
+#include "ref_physics_harness.h"
+
+ZIndex zIndex;  // the reference's file-scope index (UnifiedPhysics.cpp:36)
+
+namespace {
+int g_rigid_reached = 0;
+struct Quiet {
+  std::streambuf* old;
+  std::ostringstream sink;
+  Quiet() : old(std::cout.rdbuf(sink.rdbuf())) {}
+  ~Quiet() { std::cout.rdbuf(old); }
+};
+}  // namespace
+
+// Per-body functions of the rigid phase: declared by the harness, not
+// extracted; the scenes here have no rigid bodies, so they are never reached.
+void UnifiedPhysics::CalculateRigidBodyForceTorqueMomenta(const int) { g_rigid_reached = 1; }
+void UnifiedPhysics::SynRigidParticlesPerRigidBody(RigidBody*) { g_rigid_reached = 1; }
+void UnifiedPhysics::ApplyRotationToParticlesHost(RigidBody&) { g_rigid_reached = 1; }
+
+extern "C" {
+
+// Returns 0 on success; 1 if two particles share a Morton key (the
+// reference's std::sort leaves their order unspecified, so no comparison is
+// possible), 2 if the rigid phase was reached, 3 on bad arguments.
+// Outputs are in the reference's final particle order (ascending key).
+int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
+                             uint32_t n, int32_t steps, int32_t weighted_volumes, float* out_pos4, float* out_vel4,
+                             float* out_density, float* out_pressure, int32_t* out_type, uint32_t* out_id) {
+  if (!prm || !pos4 || !vel4 || !type || steps < 0) return 3;
+  Quiet quiet;
+  omp_set_num_threads(1);
+  static UnifiedConstants fc;
+  fc.globalSupportRadius = prm->support_radius;
+  fc.initialMass = prm->mass;
+  fc.fluidRestDensity = prm->rest_density;
+  fc.fluidViscConst = prm->viscosity;
+  fc.gravityConst = prm->gravity;
+  fc.deltaT = prm->dt;
+  fc.densityErrorFactor = prm->density_error_factor;
+  fc.maxDensityErrorAllowed = prm->max_density_error;
+  fc.minLoops = prm->min_loops;
+  fc.maxLoops = prm->max_loops;
+  fc.scales = vmml::Vector3f(prm->scales[0], prm->scales[1], prm->scales[2]);
+  fc.collisionBox.set(vmml::Vector3f(prm->collision_min[0], prm->collision_min[1], prm->collision_min[2]),
+                      vmml::Vector3f(prm->collision_max[0], prm->collision_max[1], prm->collision_max[2]));
+  fc.physicsType = 'i';
+  fc.surface_tension_gamma = prm->surface_tension_gamma;
+  fc.surface_adhesion_beta = prm->surface_adhesion_beta;
+  fc.particleRadius = prm->particle_radius;
+  fc.forceDistance = prm->force_distance;
+  fc.maxBoundaryForce = prm->max_boundary_force;
+  fc.springCoefficient = prm->spring_coefficient;
+  fc.springCoefficientBoundary = prm->spring_coefficient_boundary;
+  fc.dampingCoefficient = prm->damping_coefficient;
+  fc.terminalSpeed = prm->terminal_speed;
+  fc.printDebuggingInfo = 0;
+  static WeightingKernel kernel(&fc);
+
+  UnifiedPhysics up;
+  up.fc_ = &fc;
+  up.my_kernel_ = &kernel;
+  up.kernel_self_ = kernel.KernelM4(0.0f, fc.globalSupportRadius);
+  up.density_error_too_large_ = true;
+  up.max_loops_sim_ = 0;
+  up.avg_loops_sim_ = 0.0f;
+  up.max_predicted_density_ = 0.0f;
+  up.num_nonfrozen_particles_ = 0;
+  up.iteration_counter_ = 0;
+  float block = fc.scales.x * fc.globalSupportRadius;
+  block = MAX(block, fc.scales.y * fc.globalSupportRadius);
+  block = MAX(block, fc.scales.z * fc.globalSupportRadius);
+  zIndex.SetBlockSize(block);
+
+  up.particles_.reserve(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    UnifiedParticle q(vmml::Vector3f(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2]), type[i],
+                      vmml::Vector3f(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2]), 0.0f, prm->rest_density,
+                      prm->rest_density, prm->mass);
+    q.previous_correction_pressure_ = 0.0f;
+    q.correction_pressure_force_ = vmml::Vector3f(0.0f, 0.0f, 0.0f);
+    q.density_error_ = 0.0f;
+    q.parent_rigidbody_ = nullptr;
+    q.color_ = vmml::Vector3f((float)i, 0.0f, 0.0f);
+    q.index_ = zIndex.CalcIndex(fc.scales * q.position_);
+    if (type[i] != FROZEN_PARTICLE) up.num_nonfrozen_particles_++;
+    up.particles_.push_back(q);
+  }
+  auto keys_unique = [&]() {
+    for (size_t k = 1; k < up.particles_.size(); ++k)
+      if (up.particles_[k].index_ == up.particles_[k - 1].index_) return false;
+    return true;
+  };
+  up.SortParticles();
+  if (!keys_unique()) return 1;
+  up.neighbor_indices_.resize(n);
+  if (weighted_volumes) {
+    up.NeighborSearchOMP();
+    up.CalculateWeightedVolumeOMP();
+  }
+  for (int32_t s = 0; s < steps; ++s) {
+    up.CpuParticlePhysicsVersatileCouplingPCISPH();
+    if (!keys_unique()) return 1;
+  }
+  if (g_rigid_reached) return 2;
+  for (uint32_t k = 0; k < n; ++k) {
+    const UnifiedParticle& q = up.particles_[k];
+    for (int a = 0; a < 3; ++a) {
+      out_pos4[4 * k + a] = q.position_[a];
+      out_vel4[4 * k + a] = q.velocity_[a];
+    }
+    out_pos4[4 * k + 3] = 0.0f;
+    out_vel4[4 * k + 3] = 0.0f;
+    out_density[k] = q.predicted_density_;
+    out_pressure[k] = q.correction_pressure_;
+    out_type[k] = q.type_;
+    out_id[k] = (uint32_t)q.color_.x;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -97,6 +97,9 @@ def main():
     mesh = mesh_vectors()
     np.savez_compressed(os.path.join(HERE, "reference_mesh.npz"), **mesh)
     print("wrote", os.path.join(HERE, "reference_mesh.npz"))
+    step = step_vectors()
+    np.savez_compressed(os.path.join(HERE, "reference_step.npz"), **step)
+    print("wrote", os.path.join(HERE, "reference_step.npz"))
 
 
 def random_body_state(rng):
@@ -266,6 +269,45 @@ def mesh_vectors():
             out[name + "_scale"] = np.array(scale, np.float32)
             out[name + "_spacing"] = np.float32(spacing)
             out[name + "_pos"] = n
+    return out
+
+
+def step_cases():
+    """(name, scene, flags, steps, weighted boundary volumes): the PCISPH dam
+    in a box of frozen boundary particles, with the terms the reference's CPU
+    coupling step applies to liquid particles (surface tension, penalty
+    walls, and adhesion with Akinci boundary volumes). Its boundary pressure
+    term evaluates to zero (the pressure-gradient lookup is given the bin
+    index as a distance, UnifiedPhysics.cpp:4245), so the flag is off."""
+    import unifiedparticleframeworkcuda_b200 as upf
+    from unifiedparticleframeworkcuda_b200 import scenes
+    st_pw = upf.FLAG_SURFACE_TENSION | upf.FLAG_PENALTY_WALLS
+    return [("dam_st_pw", scenes.small_pcisph(), st_pw, 5, False),
+            ("dam_st_pw_adh", scenes.small_pcisph(seed=29), st_pw | upf.FLAG_ADHESION, 3, True)]
+
+
+def step_vectors():
+    """The reference's own CPU step (CpuParticlePhysicsVersatileCouplingPCISPH
+    and the member functions it calls, oracle/_ref/libupfref_physics.so) on
+    each case: the liquid particles' final position, velocity, predicted
+    density and correction pressure, by input index, and the inputs."""
+    import unifiedparticleframeworkcuda_b200 as upf
+    from oracle import refstep
+    out = {}
+    for name, sc, flags, steps, wv in step_cases():
+        sc.params.flags = flags
+        p = upf.derive_params(sc.params)
+        r = refstep.reference_steps(p, sc.pos, sc.vel, sc.type, steps, wv)
+        liq = r["type"] == 2
+        order = np.argsort(r["id"][liq])
+        out[name + "_params"] = np.frombuffer(bytes(p), np.uint8)
+        out[name + "_pos_in"] = np.ascontiguousarray(sc.pos, np.float32)
+        out[name + "_vel_in"] = np.ascontiguousarray(sc.vel, np.float32)
+        out[name + "_type_in"] = np.ascontiguousarray(sc.type, np.int32)
+        out[name + "_steps"] = np.int32(steps)
+        out[name + "_weighted_volumes"] = np.int32(1 if wv else 0)
+        for k in ("pos", "vel", "density", "pressure", "id"):
+            out[name + "_" + k] = r[k][liq][order]
     return out
 
 

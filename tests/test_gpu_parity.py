@@ -317,3 +317,29 @@ def test_density_pass_bins_follow_the_reference_rule(upf_lib, h):
     want = reference_bins(r2, h)
     bad = np.flatnonzero(out != want)
     assert bad.size == 0, list(zip(r2[bad[:5]], out[bad[:5]], want[bad[:5]]))
+
+
+@pytest.mark.parametrize("name", ["dam_st_pw", "dam_st_pw_adh"])
+def test_device_steps_bit_equal_to_reference_steps(upf_lib, name):
+    """The device path against the reference's own compiled CPU step
+    (tests/golden/reference_step.npz, made from
+    CpuParticlePhysicsVersatileCouplingPCISPH and the member functions it
+    calls, UnifiedPhysics.cpp:4991-5024): from the same particles and
+    parameters, every liquid particle's position, velocity, predicted density
+    and correction pressure after several steps at the 50-iteration cap are
+    bit-identical."""
+    import os
+    from unifiedparticleframeworkcuda_b200._abi import UpfParams
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_step.npz"))
+    p = UpfParams.from_buffer_copy(g[name + "_params"].tobytes())
+    typ = g[name + "_type_in"]
+    with upf_lib.ParticleSystem(p, capacity=len(typ), derive=False) as s:
+        s.set_particles(g[name + "_pos_in"], g[name + "_vel_in"], typ)
+        s.step(int(g[name + "_steps"]))
+        got = s.particles()
+    liq = got["type"] == LIQUID
+    order = np.argsort(got["id"][liq])
+    assert np.array_equal(got["id"][liq][order].astype(np.uint32), g[name + "_id"])
+    for k in ("pos", "vel", "density", "pressure"):
+        a = np.ascontiguousarray(got[k][liq][order], np.float32)
+        assert np.array_equal(a.view(np.uint32), g[name + "_" + k].view(np.uint32)), k

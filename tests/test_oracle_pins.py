@@ -144,3 +144,59 @@ def test_oracle_multi_step_runs(oracle_lib):
     assert np.all(st["pos"][liquid, :3] <= np.float32(p.collision_max) + 1e-7)
     # sorted by key after the step (SortParticles)
     assert np.all(np.diff(st["key"].astype(np.int64)) >= 0)
+
+
+# ---- the step itself, pinned to the reference's own compiled CPU step ------
+# tests/golden/reference_step.npz holds what the reference's
+# CpuParticlePhysicsVersatileCouplingPCISPH (UnifiedPhysics.cpp:4991-5024, with
+# the member functions it calls, compiled unchanged by oracle/Makefile into
+# oracle/_ref/libupfref_physics.so) makes of two seeded dams in a box of
+# frozen boundary particles over 5 and 3 steps (tests/golden/make_golden.py,
+# step_cases): neighbour search, external forces, the predict-correct loop,
+# integration, boundary handling and the re-sort, every step.
+GOLDEN_STEP = os.path.join(os.path.dirname(__file__), "golden", "reference_step.npz")
+STEP_CASES = ("dam_st_pw", "dam_st_pw_adh")
+
+
+def step_case(g, name):
+    from unifiedparticleframeworkcuda_b200._abi import UpfParams
+    p = UpfParams.from_buffer_copy(g[name + "_params"].tobytes())
+    return p, g[name + "_pos_in"], g[name + "_vel_in"], g[name + "_type_in"], int(g[name + "_steps"])
+
+
+@pytest.mark.parametrize("name", STEP_CASES)
+def test_oracle_steps_bit_equal_to_reference_steps(oracle_lib, name):
+    """The oracle's restatement of the step, run from the same particles and
+    parameters, gives every liquid particle's position, velocity, predicted
+    density and correction pressure bit for bit as the reference's own step
+    does, after every one of several steps at the 50-iteration cap."""
+    g = np.load(GOLDEN_STEP)
+    p, pos, vel, typ, steps = step_case(g, name)
+    o = oracle_lib.OracleSim(p, pos, vel, typ)
+    for _ in range(steps):
+        o.step()
+    st = o.state()
+    o.close()
+    liq = st["type"] == 2
+    order = np.argsort(st["id"][liq])
+    assert np.array_equal(st["id"][liq][order], g[name + "_id"])
+    for k in ("pos", "vel", "density", "pressure"):
+        got = st[k][liq][order]
+        assert np.array_equal(got.view(np.uint32), g[name + "_" + k].view(np.uint32)), k
+
+
+@pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
+def test_step_fixture_regenerates_identically(oracle_lib):
+    """The committed step fixture is what the compiled reference step
+    produces now (each case in a fresh process, oracle/refstep.py)."""
+    from oracle import refstep
+    if not refstep.available():
+        pytest.skip("oracle/_ref/libupfref_physics.so not built")
+    g = np.load(GOLDEN_STEP)
+    for name in STEP_CASES:
+        p, pos, vel, typ, steps = step_case(g, name)
+        r = refstep.reference_steps(p, pos, vel, typ, steps, bool(g[name + "_weighted_volumes"]))
+        liq = r["type"] == 2
+        order = np.argsort(r["id"][liq])
+        for k in ("pos", "vel", "density", "pressure", "id"):
+            assert np.array_equal(r[k][liq][order], g[name + "_" + k]), (name, k)
