@@ -20,13 +20,20 @@ FUNCTIONS = [
     "CalculateExternalForcesVersatilCouplingPCISPHOMP", "CalculateExternalForcesVersatilCouplingPCISPH",
     "CalculateBoundaryFluidPressureForceHost", "CalculateSurfaceTensionForcePCISPHHost",
     "CalculateSurfaceCohesionForcePCISPHHost", "CalculateSpringForceHost", "CalculateDampingForceHost",
-    "CalculateBoundaryForcePerLiquidParticleHost", "CalculateBoundaryForcePerRigidParticleHost",
+    "CalculateBoundaryForcePerLiquidParticleHost", "CalculateBoundaryForcePerRigidParticleHost", "BoxBoundaryForce",
     "PredictionCorrectionStep", "PredictPositionAndVelocity", "CollisionHandling",
     "ComputePredictedDensityAndPressure", "ComputeCorrectivePressureForce",
     "UpdateLiquidParticlePosVelSphCPUOMP", "UpdateLiquidParticlePosVelSphCPU",
     "BoundaryHandlingPureFluidOMP", "BoundaryHandlingBoxPerNonRigidParticle",
     "SortParticles",
     "RigidBodyIntegrationOMP", "UpdateRigidBodyParticleInformationOMP", "SynRigidParticlesOMP",
+]
+# CpuParticlePhysicsPureFluidsSPH (the WCSPH step, UnifiedPhysics.cpp:4200-4260)
+# and what it calls beyond the functions above
+FUNCTIONS += [
+    "CpuParticlePhysicsPureFluidsSPH", "CalculateDensityPressurePureFluidSPH", "CalculatePressureSPH",
+    "CalculatePressureWCSPH", "CalculateLiquidParticleForces", "CalculateSurfaceTensionForcePCISPH",
+    "DistanceToWall", "WallWeight",
 ]
 # Not extracted: the per-body functions these three call for each rigid body
 # (CalculateRigidBodyForceTorqueMomenta binds a temporary to a non-const

@@ -47,6 +47,7 @@ def build(with_ref: bool = True) -> None:
 LITERAL_GRANULAR_TANGENTIAL_ONLY = 1
 LITERAL_OWN_BODY_SPRING = 2
 LITERAL_ZERO_INVERSE_INERTIA = 4
+LITERAL_WCSPH_CLAMP_ALL = 8
 
 
 class StepInfo(C.Structure):

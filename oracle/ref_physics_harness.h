@@ -11,6 +11,7 @@
 // file state. ref_pins_physics.cpp drives the result.
 #pragma once
 
+#include <math.h>  // float overloads of sqrt and pow, as MSVC's math header gives them
 #include <omp.h>
 
 #include <algorithm>
@@ -46,6 +47,9 @@ class UnifiedPhysics {
   float max_predicted_density_;
   size_t num_nonfrozen_particles_;
   int iteration_counter_;
+  float min_dens_;
+  float max_dens_;
+  float dens_avg_timestep_;
 
   // the step (UnifiedPhysics.cpp:4991-5024) and what it calls
   void CpuParticlePhysicsVersatileCouplingPCISPH();
@@ -80,6 +84,26 @@ class UnifiedPhysics {
   void RigidBodyIntegrationOMP();
   void UpdateRigidBodyParticleInformationOMP();
   void SynRigidParticlesOMP();
+  vmml::Vector3f BoxBoundaryForce(const int i);
+  // the WCSPH step (UnifiedPhysics.cpp:4200-4260) and what it calls
+  void CpuParticlePhysicsPureFluidsSPH();
+  void CalculateDensityPressurePureFluidSPH(const int i);
+  float CalculatePressureSPH(const float density);
+  float CalculatePressureWCSPH(const float density);
+  vmml::Vector3f CalculateLiquidParticleForces(UnifiedParticle& p, const int i);
+  vmml::Vector3f CalculateSurfaceTensionForcePCISPH(const float dist, const vmml::Vector3f p_pos,
+                                                    const vmml::Vector3f neigh_pos, const float splineCoefficient);
+  // the reference's default argument binds a temporary to the non-const
+  // reference (an MSVC extension); a scratch vector stands in for it
+  static vmml::Vector3f& scratch_normal() {
+    static vmml::Vector3f n;
+    n.set(0.0f, 0.0f, 0.0f);
+    return n;
+  }
+  float DistanceToWall(const float& x, const float& y, const float& z, vmml::Vector3f& norm = scratch_normal());
+  float WallWeight(float distToWall, float effectiveDist);
+  // inline in the reference's class (UnifiedPhysics.h:161)
+  float PythagoreanDist(float x, float y) { return sqrt(x * x + y * y); }
   void CalculateRigidBodyForceTorqueMomenta(const int i);
   void SynRigidParticlesPerRigidBody(RigidBody* body);
   void ApplyRotationToParticlesHost(RigidBody& body);

@@ -52,19 +52,9 @@ void UnifiedPhysics::CalculateRigidBodyForceTorqueMomenta(const int) { g_rigid_r
 void UnifiedPhysics::SynRigidParticlesPerRigidBody(RigidBody*) { g_rigid_reached = 1; }
 void UnifiedPhysics::ApplyRotationToParticlesHost(RigidBody&) { g_rigid_reached = 1; }
 
-extern "C" {
-
-// Returns 0 on success; 1 if two particles share a Morton key (the
-// reference's std::sort leaves their order unspecified, so no comparison is
-// possible), 2 if the rigid phase was reached, 3 on bad arguments.
-// Outputs are in the reference's final particle order (ascending key).
-int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
-                             uint32_t n, int32_t steps, int32_t weighted_volumes, float* out_pos4, float* out_vel4,
-                             float* out_density, float* out_pressure, int32_t* out_type, uint32_t* out_id) {
-  if (!prm || !pos4 || !vel4 || !type || steps < 0) return 3;
-  Quiet quiet;
-  omp_set_num_threads(1);
-  static UnifiedConstants fc;
+// UnifiedConstants from the derived parameters: the fields the extracted
+// functions read.
+static void set_constants(UnifiedConstants& fc, const upf_params* prm, char physics) {
   fc.globalSupportRadius = prm->support_radius;
   fc.initialMass = prm->mass;
   fc.fluidRestDensity = prm->rest_density;
@@ -78,7 +68,14 @@ int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const flo
   fc.scales = vmml::Vector3f(prm->scales[0], prm->scales[1], prm->scales[2]);
   fc.collisionBox.set(vmml::Vector3f(prm->collision_min[0], prm->collision_min[1], prm->collision_min[2]),
                       vmml::Vector3f(prm->collision_max[0], prm->collision_max[1], prm->collision_max[2]));
-  fc.physicsType = 'i';
+  fc.realBoxContainer.set(vmml::Vector3f(prm->container_min[0], prm->container_min[1], prm->container_min[2]),
+                          vmml::Vector3f(prm->container_max[0], prm->container_max[1], prm->container_max[2]));
+  fc.boxLength = prm->container_max[0] - prm->container_min[0];
+  fc.boxHeight = prm->container_max[1] - prm->container_min[1];
+  fc.boxWidth = prm->container_max[2] - prm->container_min[2];
+  fc.physicsType = physics;
+  fc.particleSpacing = prm->particle_spacing;
+  fc.fluidGasConstantWCSPH = prm->gas_constant;
   fc.surface_tension_gamma = prm->surface_tension_gamma;
   fc.surface_adhesion_beta = prm->surface_adhesion_beta;
   fc.particleRadius = prm->particle_radius;
@@ -88,7 +85,21 @@ int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const flo
   fc.springCoefficientBoundary = prm->spring_coefficient_boundary;
   fc.dampingCoefficient = prm->damping_coefficient;
   fc.terminalSpeed = prm->terminal_speed;
+  fc.useSurfaceTension = (prm->flags & UPF_FLAG_SURFACE_TENSION) != 0;
+  fc.addWallWeightFunction = (prm->flags & UPF_FLAG_WALL_WEIGHT) != 0;
+  fc.addBoundaryForce = false;
   fc.printDebuggingInfo = 0;
+}
+
+static int run_steps(char physics, const upf_params* prm, const float* pos4, const float* vel4,
+                     const int32_t* type, uint32_t n, int32_t steps, int32_t weighted_volumes, float* out_pos4,
+                     float* out_vel4, float* out_density, float* out_pressure, int32_t* out_type,
+                     uint32_t* out_id) {
+  if (!prm || !pos4 || !vel4 || !type || steps < 0) return 3;
+  Quiet quiet;
+  omp_set_num_threads(1);
+  static UnifiedConstants fc;
+  set_constants(fc, prm, physics);
   static WeightingKernel kernel(&fc);
 
   UnifiedPhysics up;
@@ -101,6 +112,9 @@ int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const flo
   up.max_predicted_density_ = 0.0f;
   up.num_nonfrozen_particles_ = 0;
   up.iteration_counter_ = 0;
+  up.min_dens_ = std::numeric_limits<float>::max();
+  up.max_dens_ = 0.0f;
+  up.dens_avg_timestep_ = 0.0f;
   float block = fc.scales.x * fc.globalSupportRadius;
   block = MAX(block, fc.scales.y * fc.globalSupportRadius);
   block = MAX(block, fc.scales.z * fc.globalSupportRadius);
@@ -133,7 +147,10 @@ int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const flo
     up.CalculateWeightedVolumeOMP();
   }
   for (int32_t s = 0; s < steps; ++s) {
-    up.CpuParticlePhysicsVersatileCouplingPCISPH();
+    if (physics == 'i')
+      up.CpuParticlePhysicsVersatileCouplingPCISPH();
+    else
+      up.CpuParticlePhysicsPureFluidsSPH();
     if (!keys_unique()) return 1;
   }
   if (g_rigid_reached) return 2;
@@ -145,12 +162,36 @@ int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const flo
     }
     out_pos4[4 * k + 3] = 0.0f;
     out_vel4[4 * k + 3] = 0.0f;
-    out_density[k] = q.predicted_density_;
-    out_pressure[k] = q.correction_pressure_;
+    out_density[k] = physics == 'i' ? q.predicted_density_ : q.density_;
+    out_pressure[k] = physics == 'i' ? q.correction_pressure_ : q.pressure_;
     out_type[k] = q.type_;
     out_id[k] = (uint32_t)q.color_.x;
   }
   return 0;
+}
+
+extern "C" {
+
+// The PCISPH step with static boundaries (CpuParticlePhysicsVersatileCouplingPCISPH).
+// Returns 0 on success; 1 if two particles share a Morton key (the
+// reference's std::sort leaves their order unspecified, so no comparison is
+// possible), 2 if the rigid phase was reached, 3 on bad arguments. Outputs
+// are in the reference's final particle order (ascending key); density and
+// pressure are the predicted density and correction pressure.
+int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
+                             uint32_t n, int32_t steps, int32_t weighted_volumes, float* out_pos4, float* out_vel4,
+                             float* out_density, float* out_pressure, int32_t* out_type, uint32_t* out_id) {
+  return run_steps('i', prm, pos4, vel4, type, n, steps, weighted_volumes, out_pos4, out_vel4, out_density,
+                   out_pressure, out_type, out_id);
+}
+
+// The WCSPH step (CpuParticlePhysicsPureFluidsSPH), the same way; density
+// and pressure are the step's density_ and pressure_.
+int ref_physics_wcsph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
+                            uint32_t n, int32_t steps, float* out_pos4, float* out_vel4, float* out_density,
+                            float* out_pressure, int32_t* out_type, uint32_t* out_id) {
+  return run_steps('w', prm, pos4, vel4, type, n, steps, 0, out_pos4, out_vel4, out_density, out_pressure, out_type,
+                   out_id);
 }
 
 }  // extern "C"

@@ -6,7 +6,7 @@ The reference keeps function-local statics (collision box, time step,
 particle count, the lookup tables' distance factor) from the first scene a
 process runs, so every call runs in a fresh Python process.
 
-    reference_steps(params, pos4, vel4, type, steps, weighted_volumes)
+    reference_steps(params, pos4, vel4, type, steps, weighted_volumes, method)
         -> dict(pos, vel, density, pressure, type, id), particles in the
            reference's final order (ascending Morton key); id = input index
 """
@@ -25,12 +25,13 @@ def available() -> bool:
     return os.path.exists(LIB)
 
 
-def reference_steps(params, pos4, vel4, type_, steps, weighted_volumes=False):
+def reference_steps(params, pos4, vel4, type_, steps, weighted_volumes=False, method="pcisph"):
     with tempfile.TemporaryDirectory() as d:
         src, dst = os.path.join(d, "in.npz"), os.path.join(d, "out.npz")
         np.savez(src, params=np.frombuffer(bytes(params), np.uint8), pos=np.ascontiguousarray(pos4, np.float32),
                  vel=np.ascontiguousarray(vel4, np.float32), type=np.ascontiguousarray(type_, np.int32),
-                 steps=np.int32(steps), wv=np.int32(1 if weighted_volumes else 0))
+                 steps=np.int32(steps), wv=np.int32(1 if weighted_volumes else 0),
+                 wcsph=np.int32(1 if method == "wcsph" else 0))
         r = subprocess.run([sys.executable, os.path.abspath(__file__), src, dst], capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("reference step failed: " + r.stderr[-2000:])
@@ -50,11 +51,13 @@ def _main(src, dst):
            "density": np.zeros(n, np.float32), "pressure": np.zeros(n, np.float32),
            "type": np.zeros(n, np.int32), "id": np.zeros(n, np.uint32)}
     vp = C.c_void_p
-    rc = L.ref_physics_pcisph_steps(C.byref(p), a["pos"].ctypes.data_as(vp), a["vel"].ctypes.data_as(vp),
-                                    a["type"].ctypes.data_as(vp), C.c_uint32(n), C.c_int32(int(a["steps"])),
-                                    C.c_int32(int(a["wv"])),
-                                    *[out[k].ctypes.data_as(vp) for k in ("pos", "vel", "density", "pressure",
-                                                                          "type", "id")])
+    args = [C.byref(p), a["pos"].ctypes.data_as(vp), a["vel"].ctypes.data_as(vp), a["type"].ctypes.data_as(vp),
+            C.c_uint32(n), C.c_int32(int(a["steps"]))]
+    outs = [out[k].ctypes.data_as(vp) for k in ("pos", "vel", "density", "pressure", "type", "id")]
+    if int(a["wcsph"]):
+        rc = L.ref_physics_wcsph_steps(*args, *outs)
+    else:
+        rc = L.ref_physics_pcisph_steps(*args, C.c_int32(int(a["wv"])), *outs)
     if rc != 0:
         raise SystemExit("ref_physics_pcisph_steps returned %d (1: equal Morton keys, 2: rigid bodies, "
                          "3: arguments)" % rc)

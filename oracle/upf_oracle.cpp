@@ -621,12 +621,14 @@ struct Sim : SimBase {
     // Boundary handling (UnifiedPhysics.cpp:4296-4326). The reference clamps
     // every particle here; static boundary particles may sit outside the
     // collision box, so only liquid particles are clamped (as in
-    // BoundaryHandlingPureFluidOMP, UnifiedPhysics.cpp:3972-3998).
+    // BoundaryHandlingPureFluidOMP, UnifiedPhysics.cpp:3972-3998), unless
+    // the reference's literal rule is asked for.
     const R damping = R(-0.5);
+    const bool all = (literal & ORC_LITERAL_WCSPH_CLAMP_ALL) != 0;
 #pragma omp parallel for num_threads(threads) schedule(dynamic, 100)
     for (int i = 0; i < n; i++) {
       Particle<R>& p = ps[i];
-      if (p.type == UPF_LIQUID) clamp_box(p.x, p.v, damping);
+      if (p.type == UPF_LIQUID || all) clamp_box(p.x, p.v, damping);
       p.key = key_of(p.x);
     }
     finish_step_stats(info);

@@ -67,6 +67,7 @@ void orc_keep_fields(orc_sim* s, int on);
 #define ORC_LITERAL_GRANULAR_TANGENTIAL_ONLY 1u
 #define ORC_LITERAL_OWN_BODY_SPRING 2u
 #define ORC_LITERAL_ZERO_INVERSE_INERTIA 4u
+#define ORC_LITERAL_WCSPH_CLAMP_ALL 8u
 void orc_set_reference_literal(orc_sim* s, uint32_t mask);
 /* continue from another run's state, per particle in creation order: the
  * final correction pressure of the step before last and of the last step,

@@ -273,41 +273,59 @@ def mesh_vectors():
 
 
 def step_cases():
-    """(name, scene, flags, steps, weighted boundary volumes): the PCISPH dam
-    in a box of frozen boundary particles, with the terms the reference's CPU
-    coupling step applies to liquid particles (surface tension, penalty
-    walls, and adhesion with Akinci boundary volumes). Its boundary pressure
-    term evaluates to zero (the pressure-gradient lookup is given the bin
-    index as a distance, UnifiedPhysics.cpp:4245), so the flag is off."""
+    """(name, scene, params, method, steps, weighted boundary volumes).
+    PCISPH: the dam in a box of frozen boundary particles, with the terms the
+    reference's CPU coupling step applies to liquid particles (surface
+    tension, penalty walls, and adhesion with Akinci boundary volumes); its
+    boundary pressure term evaluates to zero (the pressure-gradient lookup is
+    given the bin index as a distance, UnifiedPhysics.cpp:4245), so that
+    flag is off. WCSPH: the pure-fluid step with wall weights and surface
+    tension; it clamps every particle to the collision box, frozen ones
+    included, so over several steps the box encloses the boundary (else
+    clamped boundary particles come to share Morton keys, and the
+    reference's unstable sort leaves their order unspecified), and one step
+    runs with the scene's own box."""
     import unifiedparticleframeworkcuda_b200 as upf
     from unifiedparticleframeworkcuda_b200 import scenes
     st_pw = upf.FLAG_SURFACE_TENSION | upf.FLAG_PENALTY_WALLS
-    return [("dam_st_pw", scenes.small_pcisph(), st_pw, 5, False),
-            ("dam_st_pw_adh", scenes.small_pcisph(seed=29), st_pw | upf.FLAG_ADHESION, 3, True)]
+    ww_st = upf.FLAG_WALL_WEIGHT | upf.FLAG_SURFACE_TENSION
+    cases = []
+
+    def case(name, sc, flags, method, steps, wv, box=None):
+        sc.params.flags = flags
+        p = upf.derive_params(sc.params)
+        if box is not None:
+            for a in range(3):
+                p.collision_min[a], p.collision_max[a] = box
+        cases.append((name, sc, p, method, steps, wv))
+
+    case("dam_st_pw", scenes.small_pcisph(), st_pw, "pcisph", 5, False)
+    case("dam_st_pw_adh", scenes.small_pcisph(seed=29), st_pw | upf.FLAG_ADHESION, "pcisph", 3, True)
+    case("wcsph_ww_st", scenes.small_wcsph(), ww_st, "wcsph", 1, False)
+    case("wcsph_ww_st_box", scenes.small_wcsph(), ww_st, "wcsph", 5, False, box=(0.03, 0.45))
+    return cases
 
 
 def step_vectors():
     """The reference's own CPU step (CpuParticlePhysicsVersatileCouplingPCISPH
-    and the member functions it calls, oracle/_ref/libupfref_physics.so) on
-    each case: the liquid particles' final position, velocity, predicted
-    density and correction pressure, by input index, and the inputs."""
-    import unifiedparticleframeworkcuda_b200 as upf
+    or CpuParticlePhysicsPureFluidsSPH and the member functions they call,
+    oracle/_ref/libupfref_physics.so) on each case: every particle's final
+    position, velocity, density and pressure (PCISPH: predicted density and
+    correction pressure) and type, by input index, and the inputs."""
     from oracle import refstep
     out = {}
-    for name, sc, flags, steps, wv in step_cases():
-        sc.params.flags = flags
-        p = upf.derive_params(sc.params)
-        r = refstep.reference_steps(p, sc.pos, sc.vel, sc.type, steps, wv)
-        liq = r["type"] == 2
-        order = np.argsort(r["id"][liq])
+    for name, sc, p, method, steps, wv in step_cases():
+        r = refstep.reference_steps(p, sc.pos, sc.vel, sc.type, steps, wv, method)
+        order = np.argsort(r["id"])
         out[name + "_params"] = np.frombuffer(bytes(p), np.uint8)
         out[name + "_pos_in"] = np.ascontiguousarray(sc.pos, np.float32)
         out[name + "_vel_in"] = np.ascontiguousarray(sc.vel, np.float32)
         out[name + "_type_in"] = np.ascontiguousarray(sc.type, np.int32)
         out[name + "_steps"] = np.int32(steps)
         out[name + "_weighted_volumes"] = np.int32(1 if wv else 0)
-        for k in ("pos", "vel", "density", "pressure", "id"):
-            out[name + "_" + k] = r[k][liq][order]
+        out[name + "_method"] = np.array(method)
+        for k in ("pos", "vel", "density", "pressure", "type", "id"):
+            out[name + "_" + k] = r[k][order]
     return out
 
 

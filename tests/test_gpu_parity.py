@@ -319,15 +319,19 @@ def test_density_pass_bins_follow_the_reference_rule(upf_lib, h):
     assert bad.size == 0, list(zip(r2[bad[:5]], out[bad[:5]], want[bad[:5]]))
 
 
-@pytest.mark.parametrize("name", ["dam_st_pw", "dam_st_pw_adh"])
+@pytest.mark.parametrize("name", ["dam_st_pw", "dam_st_pw_adh", "wcsph_ww_st", "wcsph_ww_st_box"])
 def test_device_steps_bit_equal_to_reference_steps(upf_lib, name):
-    """The device path against the reference's own compiled CPU step
-    (tests/golden/reference_step.npz, made from
-    CpuParticlePhysicsVersatileCouplingPCISPH and the member functions it
-    calls, UnifiedPhysics.cpp:4991-5024): from the same particles and
-    parameters, every liquid particle's position, velocity, predicted density
-    and correction pressure after several steps at the 50-iteration cap are
-    bit-identical."""
+    """The device path against the reference's own compiled CPU steps
+    (tests/golden/reference_step.npz: CpuParticlePhysicsVersatileCouplingPCISPH,
+    UnifiedPhysics.cpp:4991-5024, and CpuParticlePhysicsPureFluidsSPH, with
+    the member functions they call), from the same particles and parameters:
+    every liquid particle's position, velocity, density and pressure after
+    each case's steps. PCISPH (several steps at the 50-iteration cap):
+    bit-identical. WCSPH: within 1e-5 of each field's scale. Its Tait
+    pressure takes pow(density ratio, 7); the host's powf (glibc, within 0.82
+    ulp) and the device's double-precision pow rounded once to float
+    disagree in the last bit for a few particles a step, which the next
+    steps carry into velocities at the 1e-7 level."""
     import os
     from unifiedparticleframeworkcuda_b200._abi import UpfParams
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_step.npz"))
@@ -339,7 +343,15 @@ def test_device_steps_bit_equal_to_reference_steps(upf_lib, name):
         got = s.particles()
     liq = got["type"] == LIQUID
     order = np.argsort(got["id"][liq])
-    assert np.array_equal(got["id"][liq][order].astype(np.uint32), g[name + "_id"])
+    ids = got["id"][liq][order].astype(np.int64)
+    ref_liq = g[name + "_type"] == LIQUID
+    assert np.array_equal(ids, g[name + "_id"][ref_liq].astype(np.int64))
+    wcsph = str(g[name + "_method"]) == "wcsph"
     for k in ("pos", "vel", "density", "pressure"):
         a = np.ascontiguousarray(got[k][liq][order], np.float32)
-        assert np.array_equal(a.view(np.uint32), g[name + "_" + k].view(np.uint32)), k
+        b = np.ascontiguousarray(g[name + "_" + k][ref_liq], np.float32)
+        if wcsph:
+            ok, err = close(a, b)
+            assert ok, (k, err)
+        else:
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), k

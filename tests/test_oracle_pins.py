@@ -147,15 +147,17 @@ def test_oracle_multi_step_runs(oracle_lib):
 
 
 # ---- the step itself, pinned to the reference's own compiled CPU step ------
-# tests/golden/reference_step.npz holds what the reference's
-# CpuParticlePhysicsVersatileCouplingPCISPH (UnifiedPhysics.cpp:4991-5024, with
-# the member functions it calls, compiled unchanged by oracle/Makefile into
-# oracle/_ref/libupfref_physics.so) makes of two seeded dams in a box of
-# frozen boundary particles over 5 and 3 steps (tests/golden/make_golden.py,
-# step_cases): neighbour search, external forces, the predict-correct loop,
-# integration, boundary handling and the re-sort, every step.
+# tests/golden/reference_step.npz holds what the reference's own CPU steps
+# make of seeded scenes (tests/golden/make_golden.py, step_cases): the PCISPH
+# coupling step CpuParticlePhysicsVersatileCouplingPCISPH
+# (UnifiedPhysics.cpp:4991-5024) on two dams in a box of frozen boundary
+# particles over 5 and 3 steps at the 50-iteration cap, and the WCSPH step
+# CpuParticlePhysicsPureFluidsSPH over 1 and 5 steps; each with the member
+# functions it calls (neighbour search, forces, the predict-correct loop,
+# integration, boundary handling, the re-sort), compiled unchanged by
+# oracle/Makefile into oracle/_ref/libupfref_physics.so.
 GOLDEN_STEP = os.path.join(os.path.dirname(__file__), "golden", "reference_step.npz")
-STEP_CASES = ("dam_st_pw", "dam_st_pw_adh")
+STEP_CASES = ("dam_st_pw", "dam_st_pw_adh", "wcsph_ww_st", "wcsph_ww_st_box")
 
 
 def step_case(g, name):
@@ -164,39 +166,70 @@ def step_case(g, name):
     return p, g[name + "_pos_in"], g[name + "_vel_in"], g[name + "_type_in"], int(g[name + "_steps"])
 
 
-@pytest.mark.parametrize("name", STEP_CASES)
-def test_oracle_steps_bit_equal_to_reference_steps(oracle_lib, name):
-    """The oracle's restatement of the step, run from the same particles and
-    parameters, gives every liquid particle's position, velocity, predicted
-    density and correction pressure bit for bit as the reference's own step
-    does, after every one of several steps at the 50-iteration cap."""
-    g = np.load(GOLDEN_STEP)
+def oracle_run(oracle_lib, g, name, literal=0):
     p, pos, vel, typ, steps = step_case(g, name)
     o = oracle_lib.OracleSim(p, pos, vel, typ)
+    o.set_reference_literal(literal)
     for _ in range(steps):
         o.step()
     st = o.state()
     o.close()
-    liq = st["type"] == 2
-    order = np.argsort(st["id"][liq])
-    assert np.array_equal(st["id"][liq][order], g[name + "_id"])
+    order = np.argsort(st["id"])
+    return {k: st[k][order] for k in ("pos", "vel", "density", "pressure", "type", "id")}
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.uint32), np.ascontiguousarray(b).view(np.uint32))
+
+
+@pytest.mark.parametrize("name", STEP_CASES)
+def test_oracle_steps_bit_equal_to_reference_steps(oracle_lib, name):
+    """The oracle's restatement, run from the same particles and parameters,
+    against the reference's own steps: every particle's position and velocity
+    and every liquid particle's density and pressure are bit-identical after
+    each case's steps. The one-step WCSPH case runs with the reference's
+    literal boundary handling (every particle clamped to the collision box,
+    frozen ones included)."""
+    from oracle import pyoracle
+    g = np.load(GOLDEN_STEP)
+    literal = pyoracle.LITERAL_WCSPH_CLAMP_ALL if name == "wcsph_ww_st" else 0
+    got = oracle_run(oracle_lib, g, name, literal)
+    assert np.array_equal(got["id"], g[name + "_id"]) and np.array_equal(got["type"], g[name + "_type"])
+    liq = got["type"] == 2
+    for k in ("pos", "vel"):
+        assert bits_equal(got[k], g[name + "_" + k]), k
+    for k in ("density", "pressure"):
+        assert bits_equal(got[k][liq], g[name + "_" + k][liq]), k
+
+
+def test_wcsph_boundary_clamp_deviation_moves_only_boundary_particles(oracle_lib):
+    """The deliberate deviation in WCSPH boundary handling (only liquid
+    particles clamped, so the static boundary stays where it was built),
+    measured against the reference's own step: after one step every liquid
+    particle is bit-identical; only frozen particles that lie outside the
+    collision box differ, by their clamped coordinates."""
+    g = np.load(GOLDEN_STEP)
+    name = "wcsph_ww_st"
+    got = oracle_run(oracle_lib, g, name)
+    liq = got["type"] == 2
     for k in ("pos", "vel", "density", "pressure"):
-        got = st[k][liq][order]
-        assert np.array_equal(got.view(np.uint32), g[name + "_" + k].view(np.uint32)), k
+        assert bits_equal(got[k][liq], g[name + "_" + k][liq]), k
+    moved = np.any(got["pos"][:, :3] != g[name + "_pos"][:, :3], axis=1)
+    assert moved.any() and not moved[liq].any()
 
 
 @pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
 def test_step_fixture_regenerates_identically(oracle_lib):
-    """The committed step fixture is what the compiled reference step
-    produces now (each case in a fresh process, oracle/refstep.py)."""
+    """The committed step fixture is what the compiled reference steps
+    produce now (each case in a fresh process, oracle/refstep.py)."""
     from oracle import refstep
     if not refstep.available():
         pytest.skip("oracle/_ref/libupfref_physics.so not built")
     g = np.load(GOLDEN_STEP)
     for name in STEP_CASES:
         p, pos, vel, typ, steps = step_case(g, name)
-        r = refstep.reference_steps(p, pos, vel, typ, steps, bool(g[name + "_weighted_volumes"]))
-        liq = r["type"] == 2
-        order = np.argsort(r["id"][liq])
-        for k in ("pos", "vel", "density", "pressure", "id"):
-            assert np.array_equal(r[k][liq][order], g[name + "_" + k]), (name, k)
+        r = refstep.reference_steps(p, pos, vel, typ, steps, bool(g[name + "_weighted_volumes"]),
+                                    str(g[name + "_method"]))
+        order = np.argsort(r["id"])
+        for k in ("pos", "vel", "density", "pressure", "type", "id"):
+            assert np.array_equal(r[k][order], g[name + "_" + k]), (name, k)
