@@ -218,6 +218,37 @@ def test_wcsph_boundary_clamp_deviation_moves_only_boundary_particles(oracle_lib
     assert moved.any() and not moved[liq].any()
 
 
+def test_boundary_pressure_deviation_measured_against_reference_step(oracle_lib):
+    """The deliberate deviation in the Akinci boundary pressure (table indexed
+    by distance, flag FLAG_BOUNDARY_PRESSURE) measured against the
+    reference's own step, whose lookup by bin index
+    (UnifiedPhysics.cpp:4240-4250) makes the term 0 for every pair: the
+    fixture runs with the flag clear and the oracle equals it; with the flag
+    set the liquid moves differently within three steps (the term reads the
+    lagged pressure, which starts at 0) while the frozen boundary stays
+    bit-identical."""
+    from unifiedparticleframeworkcuda_b200._abi import FLAG_BOUNDARY_PRESSURE
+    g = np.load(GOLDEN_STEP)
+    name = "dam_st_pw"
+    p, pos, vel, typ, _ = step_case(g, name)
+    assert not (p.flags & FLAG_BOUNDARY_PRESSURE)
+    runs = []
+    for flags in (p.flags, p.flags | FLAG_BOUNDARY_PRESSURE):
+        p.flags = flags
+        o = oracle_lib.OracleSim(p, pos, vel, typ)
+        for _ in range(3):
+            o.step()
+        st = o.state()
+        o.close()
+        order = np.argsort(st["id"])
+        runs.append({k: st[k][order] for k in ("pos", "vel", "type")})
+    liq = runs[0]["type"] == 2
+    moved = np.any(runs[0]["vel"][:, :3] != runs[1]["vel"][:, :3], axis=1)
+    assert moved[liq].sum() > 0.05 * liq.sum()
+    for k in ("pos", "vel"):
+        assert bits_equal(runs[0][k][~liq], runs[1][k][~liq]), k
+
+
 @pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
 def test_step_fixture_regenerates_identically(oracle_lib):
     """The committed step fixture is what the compiled reference steps
