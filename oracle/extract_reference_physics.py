@@ -1,6 +1,7 @@
 """TEST INFRASTRUCTURE (oracle build step): extracts, unchanged, the member
-functions of the reference's CPU step (src/cpu/UnifiedPhysics.cpp) that the
-PCISPH step with static boundaries runs, so that oracle/Makefile can compile
+functions of the reference's CPU steps (src/cpu/UnifiedPhysics.cpp) that the
+PCISPH coupling step with static boundaries and rigid bodies and the WCSPH
+step run, so that oracle/Makefile can compile
 them beside a minimal class declaration of its own (ref_physics_harness.h)
 instead of the whole translation unit, whose includes need a graphics
 stack. The output goes to oracle/_ref/ only (never committed).
@@ -35,10 +36,14 @@ FUNCTIONS += [
     "CalculatePressureWCSPH", "CalculateLiquidParticleForces", "CalculateSurfaceTensionForcePCISPH",
     "DistanceToWall", "WallWeight",
 ]
-# Not extracted: the per-body functions these three call for each rigid body
-# (CalculateRigidBodyForceTorqueMomenta binds a temporary to a non-const
-# reference, which only MSVC accepts); the scenes the pin runs have no rigid
-# bodies, so those loops run zero times and the harness only declares them.
+# The per-body functions of the rigid phase (force and torque sums and the
+# body update, the particle sync) and AddToRigidBody, with which the pin's
+# set-up assembles bodies as the reference's scene construction does, one
+# particle at a time. CalculateRigidBodyForceTorqueMomenta's old-method branch
+# binds a temporary to a non-const reference (an MSVC extension);
+# ref_physics_harness.h gives GCC an overload that makes the same call on a
+# copy.
+FUNCTIONS += ["CalculateRigidBodyForceTorqueMomenta", "SynRigidParticlesPerRigidBody", "AddToRigidBody"]
 
 
 def definition(src, name):

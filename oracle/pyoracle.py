@@ -48,6 +48,10 @@ LITERAL_GRANULAR_TANGENTIAL_ONLY = 1
 LITERAL_OWN_BODY_SPRING = 2
 LITERAL_ZERO_INVERSE_INERTIA = 4
 LITERAL_WCSPH_CLAMP_ALL = 8
+LITERAL_FLOAT_RIGID_ASSEMBLY = 16
+LITERAL_FLOAT_BODY_SUMS = 32
+LITERAL_STALE_RIGID_KEYS = 64
+LITERAL_STALE_RIGID_PREDICTED = 128
 
 
 class StepInfo(C.Structure):
@@ -252,7 +256,7 @@ class OracleSim:
 
     def set_reference_literal(self, mask: int):
         """Switch deviations back to the reference's literal rule (the
-        LITERAL_* bits; before set_rigid_bodies for the inertia bit)."""
+        LITERAL_* bits; before set_rigid_bodies for the inertia and assembly bits)."""
         lib().orc_set_reference_literal(self._h, int(mask))
 
     def set_lagged(self, pressure_prev, pressure, density):

@@ -104,7 +104,19 @@ class UnifiedPhysics {
   float WallWeight(float distToWall, float effectiveDist);
   // inline in the reference's class (UnifiedPhysics.h:161)
   float PythagoreanDist(float x, float y) { return sqrt(x * x + y * y); }
+  // the rigid phase's per-body functions and the assembly of a body
   void CalculateRigidBodyForceTorqueMomenta(const int i);
   void SynRigidParticlesPerRigidBody(RigidBody* body);
-  void ApplyRotationToParticlesHost(RigidBody& body);
+  void AddToRigidBody(RigidBody* rigid, const int pIndex);
 };
+
+// Matrix3x3::operator*(vmml::Vector3f&) takes a non-const reference
+// (Matrix3x3.h:23), and CalculateRigidBodyForceTorqueMomenta passes it the
+// temporary that angular_momentum() returns (UnifiedPhysics.cpp:3676), which
+// only MSVC accepts. This overload is chosen only where the member cannot
+// bind (an rvalue vector); it makes the member call on copies, as MSVC does.
+inline vmml::Vector3f operator*(const Matrix3x3& m, const vmml::Vector3f& v) {
+  Matrix3x3 mm(m);
+  vmml::Vector3f vv(v);
+  return mm * vv;
+}

@@ -4,9 +4,10 @@
 // (src/cpu/UnifiedPhysics.cpp:4991-5024) and the member functions it calls,
 // copied unchanged by extract_reference_physics.py and compiled beside
 // ref_physics_harness.h into oracle/_ref/libupfref_physics.so — on a scene
-// of liquid and frozen boundary particles, so that the oracle's restatement
-// of the step (density, pressure, forces, the predict-correct loop,
-// integration) can be pinned to the reference itself.
+// of liquid, frozen boundary and rigid particles, so that the oracle's
+// restatement of the step (density, pressure, forces, the predict-correct
+// loop, integration, the rigid bodies) can be pinned to the reference
+// itself; and the WCSPH step CpuParticlePhysicsPureFluidsSPH the same way.
 //
 // What the harness sets up, since the reference's own set-up (Scene.cpp and
 // the UnifiedPhysics constructor) does not compile here:
@@ -37,7 +38,6 @@
 ZIndex zIndex;  // the reference's file-scope index (UnifiedPhysics.cpp:36)
 
 namespace {
-int g_rigid_reached = 0;
 struct Quiet {
   std::streambuf* old;
   std::ostringstream sink;
@@ -45,12 +45,6 @@ struct Quiet {
   ~Quiet() { std::cout.rdbuf(old); }
 };
 }  // namespace
-
-// Per-body functions of the rigid phase: declared by the harness, not
-// extracted; the scenes here have no rigid bodies, so they are never reached.
-void UnifiedPhysics::CalculateRigidBodyForceTorqueMomenta(const int) { g_rigid_reached = 1; }
-void UnifiedPhysics::SynRigidParticlesPerRigidBody(RigidBody*) { g_rigid_reached = 1; }
-void UnifiedPhysics::ApplyRotationToParticlesHost(RigidBody&) { g_rigid_reached = 1; }
 
 // UnifiedConstants from the derived parameters: the fields the extracted
 // functions read.
@@ -92,10 +86,12 @@ static void set_constants(UnifiedConstants& fc, const upf_params* prm, char phys
 }
 
 static int run_steps(char physics, const upf_params* prm, const float* pos4, const float* vel4,
-                     const int32_t* type, uint32_t n, int32_t steps, int32_t weighted_volumes, float* out_pos4,
-                     float* out_vel4, float* out_density, float* out_pressure, int32_t* out_type,
-                     uint32_t* out_id) {
-  if (!prm || !pos4 || !vel4 || !type || steps < 0) return 3;
+                     const int32_t* type, const int32_t* body_of, uint32_t n_bodies, uint32_t n, int32_t steps,
+                     int32_t weighted_volumes, float* out_pos4, float* out_vel4, float* out_density,
+                     float* out_pressure, int32_t* out_type, uint32_t* out_id, float* out_body) {
+  if (!prm || !pos4 || !vel4 || !type || steps < 0 || (n_bodies && !body_of)) return 3;
+  for (uint32_t i = 0; body_of && i < n; ++i)
+    if (body_of[i] >= (int32_t)n_bodies || (body_of[i] >= 0) != (type[i] == RIGID_PARTICLE)) return 3;
   Quiet quiet;
   omp_set_num_threads(1);
   static UnifiedConstants fc;
@@ -142,6 +138,33 @@ static int run_steps(char physics, const upf_params* prm, const float* pos4, con
   up.SortParticles();
   if (!keys_unique()) return 1;
   up.neighbor_indices_.resize(n);
+  // Rigid bodies: each particle added to its body by the reference's
+  // AddToRigidBody, in array order. The reference's scene construction
+  // (SolidifyParticle, UnifiedPhysics.cpp:810-850) adds particles with the
+  // same function, in an order its solid-neighbour lists decide, which this
+  // set-up does not build. Then the constructor's loop over the bodies
+  // (UnifiedPhysics.cpp:144-160): parent index, order in the body, initial
+  // relative position. That loop's
+  // Matrix3x3::CalculateInverse(rb->inertia(), rb->inverted_inertia_local())
+  // writes into the temporary the getter returns, so the body's local
+  // inverse inertia keeps its zero initial value; it is left out here with
+  // the same effect.
+  std::vector<RigidBody> bodies(n_bodies);
+  for (uint32_t b = 0; b < n_bodies; ++b) up.rigid_bodies_.push_back(&bodies[b]);
+  for (uint32_t k = 0; k < n && n_bodies; ++k) {
+    const int b = body_of[(uint32_t)up.particles_[k].color_.x];
+    if (b >= 0) up.AddToRigidBody(up.rigid_bodies_[b], (int)k);
+  }
+  for (uint32_t b = 0; b < n_bodies; ++b) {
+    RigidBody* rb = up.rigid_bodies_[b];
+    const size_t count = rb->rigid_particle_indices().size();
+    for (size_t j = 0; j < count; ++j) {
+      UnifiedParticle& p = up.particles_[rb->rigid_particle_indices()[j]];
+      p.parent_rigid_body_index_ = (int)b;
+      p.order_in_child_particles_array_ = (int)j;
+      p.init_relative_pos_ = p.position_ - rb->rigidbody_pos();
+    }
+  }
   if (weighted_volumes) {
     up.NeighborSearchOMP();
     up.CalculateWeightedVolumeOMP();
@@ -153,7 +176,18 @@ static int run_steps(char physics, const upf_params* prm, const float* pos4, con
       up.CpuParticlePhysicsPureFluidsSPH();
     if (!keys_unique()) return 1;
   }
-  if (g_rigid_reached) return 2;
+  for (uint32_t b = 0; b < n_bodies && out_body; ++b) {
+    const RigidBody* rb = up.rigid_bodies_[b];
+    float* o = out_body + 16 * b;
+    for (int a = 0; a < 3; ++a) {
+      o[a] = rb->rigidbody_pos()[a];
+      o[3 + a] = rb->velocity()[a];
+      o[6 + a] = rb->angular_velocity()[a];
+    }
+    o[9] = rb->mass();
+    for (int a = 0; a < 4; ++a) o[10 + a] = rb->quaternion()[a];
+    o[14] = o[15] = 0.0f;
+  }
   for (uint32_t k = 0; k < n; ++k) {
     const UnifiedParticle& q = up.particles_[k];
     for (int a = 0; a < 3; ++a) {
@@ -172,26 +206,30 @@ static int run_steps(char physics, const upf_params* prm, const float* pos4, con
 
 extern "C" {
 
-// The PCISPH step with static boundaries (CpuParticlePhysicsVersatileCouplingPCISPH).
-// Returns 0 on success; 1 if two particles share a Morton key (the
-// reference's std::sort leaves their order unspecified, so no comparison is
-// possible), 2 if the rigid phase was reached, 3 on bad arguments. Outputs
-// are in the reference's final particle order (ascending key); density and
-// pressure are the predicted density and correction pressure.
+// The PCISPH coupling step (CpuParticlePhysicsVersatileCouplingPCISPH).
+// body_of[i] is input particle i's body (-1 for none; rigid particles and
+// only they have one), n_bodies the number of bodies (body_of may be null
+// when it is 0). Returns 0 on success; 1 if two particles share a Morton key
+// (the reference's std::sort leaves their order unspecified, so no
+// comparison is possible); 3 on bad arguments. Outputs are in the
+// reference's final particle order (ascending key); density and pressure are
+// the predicted density and correction pressure; out_body (16 floats a body,
+// may be null) holds position, velocity, angular velocity, mass, quaternion.
 int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
-                             uint32_t n, int32_t steps, int32_t weighted_volumes, float* out_pos4, float* out_vel4,
-                             float* out_density, float* out_pressure, int32_t* out_type, uint32_t* out_id) {
-  return run_steps('i', prm, pos4, vel4, type, n, steps, weighted_volumes, out_pos4, out_vel4, out_density,
-                   out_pressure, out_type, out_id);
+                             const int32_t* body_of, uint32_t n_bodies, uint32_t n, int32_t steps,
+                             int32_t weighted_volumes, float* out_pos4, float* out_vel4, float* out_density,
+                             float* out_pressure, int32_t* out_type, uint32_t* out_id, float* out_body) {
+  return run_steps('i', prm, pos4, vel4, type, body_of, n_bodies, n, steps, weighted_volumes, out_pos4, out_vel4,
+                   out_density, out_pressure, out_type, out_id, out_body);
 }
 
-// The WCSPH step (CpuParticlePhysicsPureFluidsSPH), the same way; density
-// and pressure are the step's density_ and pressure_.
+// The WCSPH step (CpuParticlePhysicsPureFluidsSPH), the same way, without
+// rigid bodies; density and pressure are the step's density_ and pressure_.
 int ref_physics_wcsph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
                             uint32_t n, int32_t steps, float* out_pos4, float* out_vel4, float* out_density,
                             float* out_pressure, int32_t* out_type, uint32_t* out_id) {
-  return run_steps('w', prm, pos4, vel4, type, n, steps, 0, out_pos4, out_vel4, out_density, out_pressure, out_type,
-                   out_id);
+  return run_steps('w', prm, pos4, vel4, type, nullptr, 0, n, steps, 0, out_pos4, out_vel4, out_density,
+                   out_pressure, out_type, out_id, nullptr);
 }
 
 }  // extern "C"

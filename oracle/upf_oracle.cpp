@@ -703,10 +703,12 @@ struct Sim : SimBase {
       p.F.y -= m * R(prm.gravity);
       if (prm.flags & UPF_FLAG_PENALTY_WALLS) p.F = p.F + penalty_walls(p.x);
     } else {
-      // predicted position of a non-liquid particle: its current position
-      // (the reference's integration leaves there the position a moving
-      // particle was advanced to, UnifiedPhysics.cpp:5781-5792)
-      p.xs = p.x;
+      // predicted position of a non-liquid particle: its current position.
+      // Literal: nothing in the reference's coupling step writes a rigid
+      // particle's predicted_position_, so it keeps the position it was
+      // created with (UnifiedParticle.cpp:17), and the liquid's predicted
+      // density sees the body where it started.
+      if (!(p.type == UPF_RIGID && (literal & ORC_LITERAL_STALE_RIGID_PREDICTED))) p.xs = p.x;
       if (p.type == UPF_RIGID) rigid_external(i);
       else if (p.type == UPF_GRANULAR) granular_external(i);
     }
@@ -840,6 +842,20 @@ struct Sim : SimBase {
   void rigid_step() {
     const int nb = (int)bodies.size();
     if (!nb) return;
+    if (literal & ORC_LITERAL_FLOAT_BODY_SUMS) {
+      // literal: RigidBody::ApplyForce / ApplyTorque (RigidBody.cpp:16-19)
+      // add each particle's force, its torque about the body's position, then
+      // the particle's weight, in the precision of the state
+      std::vector<V3<R>> F(nb, V3<R>{0, 0, 0}), T(nb, V3<R>{0, 0, 0});
+      for (const Particle<R>& p : ps) {
+        if (p.type != UPF_RIGID || p.body < 0) continue;
+        F[p.body] = F[p.body] + p.F;
+        T[p.body] = T[p.body] + cross(p.x - bodies[p.body].pos, p.F);
+        F[p.body] = F[p.body] + V3<R>{R(0), -R(prm.mass) * R(prm.gravity), R(0)};
+      }
+      for (int k = 0; k < nb; ++k) body_update(bodies[k], F[k], T[k], R(prm.dt), R(prm.terminal_speed));
+      return;
+    }
     std::vector<double> F(3 * nb, 0.0), T(3 * nb, 0.0);
     for (const Particle<R>& p : ps) {
       if (p.type != UPF_RIGID || p.body < 0) continue;
@@ -977,12 +993,21 @@ struct Sim : SimBase {
       if (p.type == UPF_LIQUID || p.type == UPF_GRANULAR) clamp_box(p.x, p.v, damping);
     }
     // RigidBodyIntegrationOMP + SynRigidParticlesOMP (UnifiedPhysics.cpp:5011-5023).
-    // Keys are taken after the rigid particles move (the reference keys them
-    // before, so its next neighbour search uses stale rigid keys).
+    // Keys are taken after the rigid particles move. Literal: the reference
+    // keys every particle in BoundaryHandlingPureFluidOMP
+    // (UnifiedPhysics.cpp:3995), before the rigid phase, so its sort and next
+    // neighbour search use the rigid particles' keys from before the sync.
+    const bool stale_keys = (literal & ORC_LITERAL_STALE_RIGID_KEYS) != 0;
+    if (stale_keys) {
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 100)
+      for (int i = 0; i < n; i++) ps[i].key = key_of(ps[i].x);
+    }
     rigid_step();
     rigid_sync();
+    if (!stale_keys) {
 #pragma omp parallel for num_threads(threads) schedule(dynamic, 100)
-    for (int i = 0; i < n; i++) ps[i].key = key_of(ps[i].x);
+      for (int i = 0; i < n; i++) ps[i].key = key_of(ps[i].x);
+    }
     finish_step_stats(info);
     sort_particles();
     if (info) {
@@ -1123,6 +1148,54 @@ struct Sim : SimBase {
         // body's local inverse inertia keeps its zero initial value
         for (int j = 0; j < 3; ++j)
           B.inv_inertia_local[i][j] = (literal & ORC_LITERAL_ZERO_INVERSE_INERTIA) ? R(0) : R(inv[3 * i + j]);
+      }
+    }
+    if (literal & ORC_LITERAL_FLOAT_RIGID_ASSEMBLY) {
+      // literal: AddToRigidBody (UnifiedPhysics.cpp:825-885) for each rigid
+      // particle in array order, in the precision of the state, on a body the
+      // RigidBody constructor zeroed (RigidBody.cpp:4-13). The linear momentum
+      // is never set there, so it stays zero; the angular momentum update on
+      // the temporary angular_momentum() returns (:871) has no effect.
+      std::vector<R> In(9 * nb, R(0));
+      for (uint32_t b = 0; b < nb; ++b) {
+        Body<R>& B = bodies[b];
+        B.mass = 0;
+        B.pos = B.vel = B.P = B.L = V3<R>{0, 0, 0};
+      }
+      for (size_t k = 0; k < ps.size(); ++k) {
+        const Particle<R>& p = ps[k];
+        const int b = bop[p.id];
+        if (b < 0) continue;
+        Body<R>& B = bodies[b];
+        R* I = &In[9 * b];
+        const R pm = R(prm.mass);
+        const R nm = B.mass + pm;
+        const V3<R> c = divs(B.pos * B.mass + p.x * pm, nm);
+        const V3<R> dc = B.pos - c, dp = p.x - c;
+        const R c0 = dc.x * dc.x, c1 = dc.y * dc.y, c2 = dc.z * dc.z;
+        const R q0 = dp.x * dp.x, q1 = dp.y * dp.y, q2 = dp.z * dp.z;
+        I[0] += B.mass * (c1 + c2) + pm * (q1 + q2);
+        I[4] += B.mass * (c0 + c2) + pm * (q0 + q2);
+        I[8] += B.mass * (c1 + c0) + pm * (q1 + q0);
+        I[1] -= B.mass * dc.x * dc.y + pm * dp.x * dp.y;
+        I[2] -= B.mass * dc.x * dc.z + pm * dp.x * dp.z;
+        I[5] -= B.mass * dc.y * dc.z + pm * dp.y * dp.z;
+        I[3] = I[1];
+        I[6] = I[2];
+        I[7] = I[5];
+        B.L = B.L + cross(dc, B.vel * B.mass);
+        B.vel = divs(B.vel * B.mass + p.v * pm, nm);
+        B.pos = c;
+        B.mass = nm;
+      }
+      for (uint32_t b = 0; b < nb; ++b) {
+        Body<R>& B = bodies[b];
+        double I64[9], inv[9] = {0};
+        for (int a = 0; a < 9; ++a) I64[a] = (double)In[9 * b + a];
+        inverse3_fp64(I64, inv);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            B.inv_inertia_local[i][j] = (literal & ORC_LITERAL_ZERO_INVERSE_INERTIA) ? R(0) : R(inv[3 * i + j]);
       }
     }
     for (uint32_t id = 0; id < n; ++id) {

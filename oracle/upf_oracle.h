@@ -63,11 +63,32 @@ void orc_keep_fields(orc_sim* s, int on);
  *                             of the same body too (UnifiedPhysics.cpp:5300-5311)
  *   ZERO_INVERSE_INERTIA      the local inverse inertia stays zero, as the
  *                             reference's inverse lands in a temporary
- *                             (UnifiedPhysics.cpp:150) */
+ *                             (UnifiedPhysics.cpp:150)
+ *   WCSPH_CLAMP_ALL           the WCSPH step clamps every particle to the
+ *                             collision box, frozen ones included
+ *                             (UnifiedPhysics.cpp:4296-4326)
+ *   FLOAT_RIGID_ASSEMBLY      bodies assembled one particle at a time in
+ *                             float, in array order (AddToRigidBody,
+ *                             UnifiedPhysics.cpp:825-885), with the linear
+ *                             momentum left at the constructor's zero
+ *   FLOAT_BODY_SUMS           per-body force and torque summed in float in
+ *                             array order, gravity after each particle's
+ *                             force (UnifiedPhysics.cpp:3631-3643)
+ *   STALE_RIGID_KEYS          rigid particles keep the key of their position
+ *                             before the rigid sync (UnifiedPhysics.cpp:3995,
+ *                             5011-5023)
+ *   STALE_RIGID_PREDICTED     rigid particles keep the predicted position
+ *                             they were created with (nothing in the coupling
+ *                             step writes it; UnifiedParticle.cpp:17)
+ * Set before orc_set_rigid_bodies for the inertia and assembly bits. */
 #define ORC_LITERAL_GRANULAR_TANGENTIAL_ONLY 1u
 #define ORC_LITERAL_OWN_BODY_SPRING 2u
 #define ORC_LITERAL_ZERO_INVERSE_INERTIA 4u
 #define ORC_LITERAL_WCSPH_CLAMP_ALL 8u
+#define ORC_LITERAL_FLOAT_RIGID_ASSEMBLY 16u
+#define ORC_LITERAL_FLOAT_BODY_SUMS 32u
+#define ORC_LITERAL_STALE_RIGID_KEYS 64u
+#define ORC_LITERAL_STALE_RIGID_PREDICTED 128u
 void orc_set_reference_literal(orc_sim* s, uint32_t mask);
 /* continue from another run's state, per particle in creation order: the
  * final correction pressure of the step before last and of the last step,

@@ -6,11 +6,14 @@ oracle/_ref/libupfref.so. Run in a checkout where the reference source tree
 is available:
 
     make -C oracle ref REF=/path/to/reference
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py step     # reference_step.npz only
 
-The reference has no tests, fixtures or known-answer vectors of its own;
-these files pin the oracle (and through it the device path) to the
-reference's tables and constants.
+reference_step.npz comes from the reference's CPU steps themselves
+(src/cpu/UnifiedPhysics.cpp's step functions, extracted unchanged into
+oracle/_ref/libupfref_physics.so). The reference has no tests, fixtures or
+known-answer vectors of its own; these files pin the oracle (and through it
+the device path) to the reference's tables, constants and steps.
 """
 import ctypes as C
 import os
@@ -37,6 +40,11 @@ def fp(a):
 def main():
     if not pyoracle.ref_available():
         raise SystemExit("oracle/_ref/libupfref.so missing: make -C oracle ref")
+    if sys.argv[1:] == ["step"]:  # only reference_step.npz
+        step = step_vectors()
+        np.savez_compressed(os.path.join(HERE, "reference_step.npz"), **step)
+        print("wrote", os.path.join(HERE, "reference_step.npz"))
+        return
     R = pyoracle.ref()
     out = {}
     tab = np.zeros((1024, 3), np.uint32)
@@ -272,6 +280,44 @@ def mesh_vectors():
     return out
 
 
+def rigid_contact_scene(seed=5):
+    """The small coupling scene without its granular pile (the reference's
+    coupling step has no grains), its three bodies moved into contact: a
+    sphere half sunk into the top of the fluid, a cube beside it with half a
+    spacing between their surfaces (spring-damper contacts), a torus resting
+    on the collision box's floor (the rigid box force); liquid inside the
+    sphere or within 0.75 spacing of a rigid particle removed. Key units of
+    0.5 mm (the container is 0.42 m) keep every Morton key distinct over the
+    steps the case runs."""
+    from unifiedparticleframeworkcuda_b200 import GRANULAR, LIQUID, RIGID, scenes
+    sc = scenes.small_coupling(seed=seed)
+    p = sc.params
+    s = float(p.particle_spacing)
+    keep = sc.type != GRANULAR
+    pos, typ, body = sc.pos[keep].copy(), sc.type[keep].copy(), sc.body[keep].copy()
+    liq = typ == LIQUID
+    top = pos[liq, 1].max()
+    fluid_centre = pos[liq, :3].mean(0)
+    floor = float(p.collision_min[1])
+    pts = {b: pos[body == b, :3].astype(np.float64) for b in range(sc.num_bodies)}
+    half = {b: (pts[b].max(0) - pts[b].min(0)) / 2 for b in pts}
+    mid = {b: (pts[b].max(0) + pts[b].min(0)) / 2 for b in pts}
+    t0 = np.array([fluid_centre[0], top, fluid_centre[2]])
+    t1 = t0 + np.array([half[0][0] + half[1][0] + 0.5 * s, 0.0, 0.0])
+    t2 = np.array([0.33, floor + half[2][1] + 0.2 * s, 0.15])
+    for b, t in ((0, t0), (1, t1), (2, t2)):
+        pos[body == b, :3] = (pts[b] - mid[b] + t).astype(np.float32)
+    x = pos[:, :3].astype(np.float64)
+    near = np.full(len(x), np.inf)
+    for c in np.array_split(pos[typ == RIGID, :3].astype(np.float64), 8):
+        near = np.minimum(near, np.sqrt(((x[:, None, :] - c[None]) ** 2).sum(-1)).min(1))
+    inside = np.linalg.norm(x - t0, axis=1) < half[0].max()
+    k = ~(liq & ((near < 0.75 * s) | inside))
+    unit = 1024.0 * (s / 20.0)
+    p.zindex_extent[:] = (unit, unit, unit)
+    return scenes.Scene("rigid_contact", p, pos[k], np.zeros_like(pos[k]), typ[k], body[k], sc.num_bodies)
+
+
 def step_cases():
     """(name, scene, params, method, steps, weighted boundary volumes).
     PCISPH: the dam in a box of frozen boundary particles, with the terms the
@@ -284,7 +330,9 @@ def step_cases():
     included, so over several steps the box encloses the boundary (else
     clamped boundary particles come to share Morton keys, and the
     reference's unstable sort leaves their order unspecified), and one step
-    runs with the scene's own box."""
+    runs with the scene's own box. Rigid: the coupling step on
+    rigid_contact_scene with surface tension, penalty walls and adhesion, 20
+    steps."""
     import unifiedparticleframeworkcuda_b200 as upf
     from unifiedparticleframeworkcuda_b200 import scenes
     st_pw = upf.FLAG_SURFACE_TENSION | upf.FLAG_PENALTY_WALLS
@@ -303,6 +351,7 @@ def step_cases():
     case("dam_st_pw_adh", scenes.small_pcisph(seed=29), st_pw | upf.FLAG_ADHESION, "pcisph", 3, True)
     case("wcsph_ww_st", scenes.small_wcsph(), ww_st, "wcsph", 1, False)
     case("wcsph_ww_st_box", scenes.small_wcsph(), ww_st, "wcsph", 5, False, box=(0.03, 0.45))
+    case("rigid_contact", rigid_contact_scene(), st_pw | upf.FLAG_ADHESION, "pcisph", 20, False)
     return cases
 
 
@@ -311,11 +360,16 @@ def step_vectors():
     or CpuParticlePhysicsPureFluidsSPH and the member functions they call,
     oracle/_ref/libupfref_physics.so) on each case: every particle's final
     position, velocity, density and pressure (PCISPH: predicted density and
-    correction pressure) and type, by input index, and the inputs."""
+    correction pressure) and type, by input index, the rigid bodies' final
+    state, and the inputs."""
     from oracle import refstep
     out = {}
     for name, sc, p, method, steps, wv in step_cases():
-        r = refstep.reference_steps(p, sc.pos, sc.vel, sc.type, steps, wv, method)
+        body = sc.body if sc.body is not None else np.full(sc.n, -1, np.int32)
+        r = refstep.reference_steps(p, sc.pos, sc.vel, sc.type, steps, wv, method, body, sc.num_bodies)
+        out[name + "_body_in"] = np.ascontiguousarray(body, np.int32)
+        out[name + "_num_bodies"] = np.int32(sc.num_bodies)
+        out[name + "_bodies"] = r["body"]
         order = np.argsort(r["id"])
         out[name + "_params"] = np.frombuffer(bytes(p), np.uint8)
         out[name + "_pos_in"] = np.ascontiguousarray(sc.pos, np.float32)

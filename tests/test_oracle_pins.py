@@ -151,13 +151,19 @@ def test_oracle_multi_step_runs(oracle_lib):
 # make of seeded scenes (tests/golden/make_golden.py, step_cases): the PCISPH
 # coupling step CpuParticlePhysicsVersatileCouplingPCISPH
 # (UnifiedPhysics.cpp:4991-5024) on two dams in a box of frozen boundary
-# particles over 5 and 3 steps at the 50-iteration cap, and the WCSPH step
-# CpuParticlePhysicsPureFluidsSPH over 1 and 5 steps; each with the member
-# functions it calls (neighbour search, forces, the predict-correct loop,
-# integration, boundary handling, the re-sort), compiled unchanged by
-# oracle/Makefile into oracle/_ref/libupfref_physics.so.
+# particles over 5 and 3 steps at the 50-iteration cap and on three rigid
+# bodies in contact with the fluid, each other and the floor over 20 steps,
+# and the WCSPH step CpuParticlePhysicsPureFluidsSPH over 1 and 5 steps;
+# each with the member functions it calls (neighbour search, forces, the
+# predict-correct loop, integration, boundary handling, the re-sort, the
+# per-body force and torque sums, body update and particle sync), compiled
+# unchanged by oracle/Makefile into oracle/_ref/libupfref_physics.so.
 GOLDEN_STEP = os.path.join(os.path.dirname(__file__), "golden", "reference_step.npz")
-STEP_CASES = ("dam_st_pw", "dam_st_pw_adh", "wcsph_ww_st", "wcsph_ww_st_box")
+STEP_CASES = ("dam_st_pw", "dam_st_pw_adh", "wcsph_ww_st", "wcsph_ww_st_box", "rigid_contact")
+# the reference's literal rules for rigid bodies (see oracle/upf_oracle.h)
+RIGID_LITERAL = (pyoracle.LITERAL_OWN_BODY_SPRING | pyoracle.LITERAL_ZERO_INVERSE_INERTIA
+                 | pyoracle.LITERAL_FLOAT_RIGID_ASSEMBLY | pyoracle.LITERAL_FLOAT_BODY_SUMS
+                 | pyoracle.LITERAL_STALE_RIGID_KEYS | pyoracle.LITERAL_STALE_RIGID_PREDICTED)
 
 
 def step_case(g, name):
@@ -166,16 +172,21 @@ def step_case(g, name):
     return p, g[name + "_pos_in"], g[name + "_vel_in"], g[name + "_type_in"], int(g[name + "_steps"])
 
 
-def oracle_run(oracle_lib, g, name, literal=0):
-    p, pos, vel, typ, steps = step_case(g, name)
+def oracle_run(oracle_lib, g, name, literal=0, steps=None):
+    p, pos, vel, typ, n_steps = step_case(g, name)
     o = oracle_lib.OracleSim(p, pos, vel, typ)
     o.set_reference_literal(literal)
-    for _ in range(steps):
+    if int(g[name + "_num_bodies"]):
+        o.set_rigid_bodies(g[name + "_body_in"], int(g[name + "_num_bodies"]))
+    for _ in range(n_steps if steps is None else steps):
         o.step()
     st = o.state()
+    bodies = o.rigid() if int(g[name + "_num_bodies"]) else None
     o.close()
     order = np.argsort(st["id"])
-    return {k: st[k][order] for k in ("pos", "vel", "density", "pressure", "type", "id")}
+    out = {k: st[k][order] for k in ("pos", "vel", "density", "pressure", "type", "id")}
+    out["bodies"] = bodies
+    return out
 
 
 def bits_equal(a, b):
@@ -189,10 +200,11 @@ def test_oracle_steps_bit_equal_to_reference_steps(oracle_lib, name):
     and every liquid particle's density and pressure are bit-identical after
     each case's steps. The one-step WCSPH case runs with the reference's
     literal boundary handling (every particle clamped to the collision box,
-    frozen ones included)."""
-    from oracle import pyoracle
+    frozen ones included), the rigid case with the reference's literal
+    rigid-body rules (RIGID_LITERAL), and there every body's position,
+    velocity, angular velocity and quaternion is bit-identical too."""
     g = np.load(GOLDEN_STEP)
-    literal = pyoracle.LITERAL_WCSPH_CLAMP_ALL if name == "wcsph_ww_st" else 0
+    literal = {"wcsph_ww_st": pyoracle.LITERAL_WCSPH_CLAMP_ALL, "rigid_contact": RIGID_LITERAL}.get(name, 0)
     got = oracle_run(oracle_lib, g, name, literal)
     assert np.array_equal(got["id"], g[name + "_id"]) and np.array_equal(got["type"], g[name + "_type"])
     liq = got["type"] == 2
@@ -200,6 +212,12 @@ def test_oracle_steps_bit_equal_to_reference_steps(oracle_lib, name):
         assert bits_equal(got[k], g[name + "_" + k]), k
     for k in ("density", "pressure"):
         assert bits_equal(got[k][liq], g[name + "_" + k][liq]), k
+    if got["bodies"] is not None:
+        pos, vel, omega, quat = got["bodies"]
+        ref = g[name + "_bodies"]
+        for k, (a, b) in {"pos": (pos, ref[:, 0:3]), "vel": (vel, ref[:, 3:6]), "omega": (omega, ref[:, 6:9]),
+                          "quat": (quat, ref[:, 10:14])}.items():
+            assert bits_equal(a, b), k
 
 
 def test_wcsph_boundary_clamp_deviation_moves_only_boundary_particles(oracle_lib):
@@ -249,6 +267,50 @@ def test_boundary_pressure_deviation_measured_against_reference_step(oracle_lib)
         assert bits_equal(runs[0][k][~liq], runs[1][k][~liq]), k
 
 
+@pytest.mark.parametrize("bit", [pyoracle.LITERAL_OWN_BODY_SPRING, pyoracle.LITERAL_FLOAT_RIGID_ASSEMBLY,
+                                 pyoracle.LITERAL_FLOAT_BODY_SUMS, pyoracle.LITERAL_STALE_RIGID_KEYS,
+                                 pyoracle.LITERAL_STALE_RIGID_PREDICTED, pyoracle.LITERAL_ZERO_INVERSE_INERTIA])
+def test_rigid_deviations_measured_against_reference_step(oracle_lib, bit):
+    """Each deliberate deviation of the rigid-body rules, measured against
+    the reference's own coupling step on the rigid case (20 steps): the
+    oracle with every literal rule but one against the fixture.
+    * own-body spring-damper, float assembly, float per-body sums: rounding
+      only. Liquid and rigid positions stay bit-identical; body velocities
+      move by under 1e-4 of the largest body speed.
+    * rigid keys taken after the sync: a different sort and summation order
+      for the particles near moving bodies, positions within 1e-7 m.
+    * rigid predicted positions kept current: the liquid's predicted density
+      sees the bodies where they are, so the liquid moves differently; the
+      bodies themselves stay bit-identical over these steps.
+    * inverse inertia stored: the bodies rotate (the reference's never do)."""
+    g = np.load(GOLDEN_STEP)
+    name = "rigid_contact"
+    got = oracle_run(oracle_lib, g, name, RIGID_LITERAL & ~bit)
+    ref = g[name + "_bodies"]
+    pos, vel, omega, _ = got["bodies"]
+    liq = got["type"] == 2
+    rig = got["type"] == 0
+    same = {k: bits_equal(got[k], g[name + "_" + k]) for k in ("pos", "vel")}
+    assert not (same["pos"] and same["vel"] and bits_equal(vel, ref[:, 3:6]) and bits_equal(pos, ref[:, 0:3]))
+    speed = np.abs(ref[:, 3:6]).max()
+    if bit in (pyoracle.LITERAL_OWN_BODY_SPRING, pyoracle.LITERAL_FLOAT_RIGID_ASSEMBLY,
+               pyoracle.LITERAL_FLOAT_BODY_SUMS):
+        assert same["pos"]
+        assert bits_equal(got["vel"][liq], g[name + "_vel"][liq])
+        assert np.abs(vel - ref[:, 3:6]).max() <= 1e-4 * speed
+        assert np.all(omega == 0)
+    elif bit == pyoracle.LITERAL_STALE_RIGID_KEYS:
+        assert np.abs(got["pos"] - g[name + "_pos"]).max() <= 1e-7
+        assert np.abs(got["vel"] - g[name + "_vel"]).max() <= 1e-4 * speed
+    elif bit == pyoracle.LITERAL_STALE_RIGID_PREDICTED:
+        assert bits_equal(pos, ref[:, 0:3]) and bits_equal(vel, ref[:, 3:6])
+        assert bits_equal(got["pos"][rig], g[name + "_pos"][rig])
+        assert not bits_equal(got["pos"][liq], g[name + "_pos"][liq])
+    else:
+        assert np.abs(omega).max() > 1.0
+        assert not np.any(np.all(got["pos"][rig] == g[name + "_pos"][rig], axis=1))
+
+
 @pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
 def test_step_fixture_regenerates_identically(oracle_lib):
     """The committed step fixture is what the compiled reference steps
@@ -260,7 +322,8 @@ def test_step_fixture_regenerates_identically(oracle_lib):
     for name in STEP_CASES:
         p, pos, vel, typ, steps = step_case(g, name)
         r = refstep.reference_steps(p, pos, vel, typ, steps, bool(g[name + "_weighted_volumes"]),
-                                    str(g[name + "_method"]))
+                                    str(g[name + "_method"]), g[name + "_body_in"], int(g[name + "_num_bodies"]))
         order = np.argsort(r["id"])
         for k in ("pos", "vel", "density", "pressure", "type", "id"):
             assert np.array_equal(r[k][order], g[name + "_" + k]), (name, k)
+        assert np.array_equal(r["body"], g[name + "_bodies"]), name
