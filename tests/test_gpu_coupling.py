@@ -131,6 +131,47 @@ def test_coupling_multi_step(upf_lib, oracle_lib):
     o.close()
 
 
+def test_bodies_in_contact_against_the_oracle(upf_lib, oracle_lib):
+    """The rigid case of tests/golden/reference_step.npz (a sphere half sunk
+    into the fluid, a cube beside it within spring range, a torus on the
+    floor; surface tension, penalty walls, adhesion), whose reference steps
+    the oracle reproduces bit for bit under the literal rigid rules: here
+    the device against the oracle under this build's rules. One step: forces
+    of every particle and the body states within 1e-5; 20 steps: iteration
+    counts equal every step, bodies and particles within 1e-4."""
+    import os
+    from unifiedparticleframeworkcuda_b200._abi import UpfParams
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_step.npz"))
+    name = "rigid_contact"
+    p = UpfParams.from_buffer_copy(g[name + "_params"].tobytes())
+    pos, vel, typ = g[name + "_pos_in"], g[name + "_vel_in"], g[name + "_type_in"]
+    body, nb = g[name + "_body_in"], int(g[name + "_num_bodies"])
+    sysm = upf_lib.ParticleSystem(p, capacity=len(typ), derive=False)
+    sysm.set_particles(pos, vel, typ)
+    sysm.set_rigid_bodies(body, nb)
+    o = oracle_lib.OracleSim(p, pos, vel, typ)
+    o.set_rigid_bodies(body, nb)
+    sysm.step(1)
+    info = o.step()
+    assert sysm.stats().iterations == info.iterations
+    res = compare_forces(sysm, o)
+    res.update(compare_bodies(sysm, o))
+    res.update(compare_particles(sysm, o))
+    bad = {k: v for k, v in res.items() if not v[0]}
+    assert not bad, "beyond %g relative after one step: %s" % (RTOL, bad)
+    for k in range(1, int(g[name + "_steps"])):
+        sysm.step(1)
+        it = sysm.stats().iterations
+        info = o.step()
+        assert it == info.iterations, "step %d: iterations %d vs %d" % (k, it, info.iterations)
+    res = compare_bodies(sysm, o, rtol=1e-4)
+    res.update(compare_particles(sysm, o, rtol=1e-4))
+    bad = {k: v for k, v in res.items() if not v[0]}
+    assert not bad, "beyond 1e-4 relative after the case's steps: %s" % bad
+    sysm.close()
+    o.close()
+
+
 def test_free_fall_body(upf_lib):
     """One cube far from everything: the momentum update P += (sum f + M g) dt
     with no contact force keeps omega = 0 and v_y = M g t / M in float."""
