@@ -851,7 +851,7 @@ def io_reference_baseline(st, d, records=200_000):
 
 
 # pieces of the per-step host round trip in the e2e line (upf_exchange_frame_async)
-E2E_CHUNKS = 8
+E2E_CHUNKS = 2
 
 
 def parse_shape(text):
@@ -1020,9 +1020,10 @@ def run_ours(args, rank, world, local_rank):
         # each step: its input uploaded from the host arrays, the step, its
         # result read back into the host arrays and waited for. After a step
         # the readback and the next step's upload are one host round trip
-        # (upf_exchange_frame_async): the upload of each eighth of the
-        # arrays starts once that eighth has reached host memory, so the two
-        # copy directions overlap; the bytes uploaded are those read back.
+        # (upf_exchange_frame_async): the upload of each piece of the
+        # positions and velocities starts once that piece has reached host
+        # memory, so the two copy directions overlap; the bytes uploaded are
+        # those read back.
         upf.check(L.upf_upload_state_async(s.handle, C.cast(hpos.data_ptr(), fp), C.cast(hvel.data_ptr(), fp), n),
                   "upf_upload_state_async")
         for k in range(k_e2e):
@@ -1031,7 +1032,7 @@ def run_ours(args, rank, world, local_rank):
                 upf.check(L.upf_exchange_frame_async(
                     s.handle, C.cast(hpos.data_ptr(), fp), C.cast(hvel.data_ptr(), fp), C.cast(hden.data_ptr(), fp),
                     C.cast(hpre.data_ptr(), fp), C.cast(htyp.data_ptr(), C.POINTER(C.c_int32)),
-                    C.cast(hid.data_ptr(), C.POINTER(C.c_uint32)), E2E_CHUNKS, C.byref(cnt)),
+                    C.cast(hid.data_ptr(), C.POINTER(C.c_uint32)), args.e2e_chunks, C.byref(cnt)),
                     "upf_exchange_frame_async")
             else:
                 readback()
@@ -1044,7 +1045,7 @@ def run_ours(args, rank, world, local_rank):
                "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * (16 + 16 + 4 + 4 + 4 + 4),
                "steps": k_e2e, "ms_per_step": e2e_ms / k_e2e,
                "input_of_each_step": "the previous step's readback (host round trip every step; readback and "
-                                     "upload overlapped in %d pieces)" % E2E_CHUNKS,
+                                     "upload overlapped in %d pieces)" % args.e2e_chunks,
                "same_steps_as_value": bool(st_e2e.total_iterations == total_iters
                                            and st_e2e.total_steps == stats.total_steps)}
 
@@ -1114,6 +1115,8 @@ def main():
                          "the dam's loop meets the 1%% criterion; 0 = time from rest); both arms time the state "
                          "after them")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-chunks", type=int, default=E2E_CHUNKS,
+                    help="pieces of each e2e host round trip (1..16)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--shape", default="", help="fixed launch shapes instead of the autotuner: "
                                                 "nlist,external,density_threads,density_rows,pforce_threads,pforce_rows"

@@ -350,8 +350,9 @@ upf_status upf_wait_frames(upf_system* s);
  * (as upf_get_particles_async; density, pressure, type and id may be NULL)
  * and uploads pos4 and vel4 from those same host arrays as the next step's
  * input (as upf_upload_state_async), in `chunks` pieces (1..16): each piece's
- * upload starts as soon as its readback has reached host memory, so the two
- * copy directions overlap. Returns at once; upf_wait_frames waits for the
+ * upload starts as soon as its positions and velocities have reached host
+ * memory, so the two copy directions overlap; the other fields are read back
+ * after the last piece's positions and velocities. Returns at once; upf_wait_frames waits for the
  * copies, and until then the host arrays may not be touched (the data a
  * caller would change before uploading needs upf_get_particles_async, a wait
  * and upf_upload_state_async instead). Pinned host memory. */

@@ -1920,19 +1920,20 @@ upf_status upf_exchange_frame_async(upf_system* s, float* pos4, float* vel4, flo
   for (const Item& it : items)
     if (it.host) UPF_CUDA(cudaMemcpyAsync(it.snap, it.src, it.elem * n, cudaMemcpyDeviceToDevice, st));
   UPF_CUDA(cudaEventRecord(io.snapped, st));
-  // chunk by chunk: the down stream copies the chunk to the host; once it has
-  // landed, the up stream copies its positions and velocities back from
-  // those host arrays into the staging buffers
+  // chunk by chunk: the down stream copies the chunk's positions and
+  // velocities to the host; once they have landed, the up stream copies them
+  // back from those host arrays into the staging buffers. The other fields
+  // follow all the chunks, so the upload's last chunk waits for no more than
+  // its own positions and velocities.
   UPF_CUDA(cudaStreamWaitEvent(io.down, io.snapped, 0));
   UPF_CUDA(cudaStreamWaitEvent(io.up, io.consumed, 0));  // the last upload has left the staging buffers
   const uint32_t per = (n + chunks - 1) / chunks;
   for (uint32_t c = 0; c < chunks; ++c) {
     const uint32_t b = c * per, e = std::min(n, b + per);
     if (b >= e) break;
-    for (const Item& it : items)
-      if (it.host)
-        UPF_CUDA(cudaMemcpyAsync(it.host + it.elem * b, it.snap + it.elem * b, it.elem * (e - b),
-                                 cudaMemcpyDeviceToHost, io.down));
+    for (int k = 0; k < 2; ++k)
+      UPF_CUDA(cudaMemcpyAsync(items[k].host + items[k].elem * b, items[k].snap + items[k].elem * b,
+                               items[k].elem * (e - b), cudaMemcpyDeviceToHost, io.down));
     UPF_CUDA(cudaEventRecord(io.chunk_down[c], io.down));
     UPF_CUDA(cudaStreamWaitEvent(io.up, io.chunk_down[c], 0));
     UPF_CUDA(cudaMemcpyAsync(io.in_pos + b, pos4 + 4 * (size_t)b, sizeof(float4) * (e - b), cudaMemcpyHostToDevice,
@@ -1940,6 +1941,9 @@ upf_status upf_exchange_frame_async(upf_system* s, float* pos4, float* vel4, flo
     UPF_CUDA(cudaMemcpyAsync(io.in_vel + b, vel4 + 4 * (size_t)b, sizeof(float4) * (e - b), cudaMemcpyHostToDevice,
                              io.up));
   }
+  for (int k = 2; k < 6; ++k)
+    if (items[k].host)
+      UPF_CUDA(cudaMemcpyAsync(items[k].host, items[k].snap, items[k].elem * n, cudaMemcpyDeviceToHost, io.down));
   UPF_CUDA(cudaEventRecord(io.read_done, io.down));
   UPF_CUDA(cudaEventRecord(io.staged, io.up));
   // the upload enters the state before the next step, as in upf_upload_state_async
