@@ -971,8 +971,8 @@ def run_ours(args, rank, world, local_rank):
     # mode the tuned shape reads: staged neighbourhoods (mode 2) stream
     # 16-bit union positions in place of 32-bit list entries
     staged = (tuned.get("density_mode" if kname == "k_pcisph_density" else "pforce_mode") == 2)
-    traffic_per_particle = {("k_pcisph_density", False): 157.9, ("k_pcisph_density", True): 110.8,
-                            ("k_pcisph_pressure_force", False): 359.6, ("k_pcisph_pressure_force", True): 280.8}
+    traffic_per_particle = {("k_pcisph_density", False): 157.9, ("k_pcisph_density", True): 110.7,
+                            ("k_pcisph_pressure_force", False): 361.2, ("k_pcisph_pressure_force", True): 280.8}
     traffic = traffic_per_particle[(kname, staged)] * nf if (kname, staged) in traffic_per_particle else None
     traffic_source = ("ncu dram__bytes_read+write per fluid particle on the 262k-fluid dam, scaled to %d fluid "
                       "particles" % nf) if traffic is not None else None
