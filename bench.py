@@ -102,13 +102,13 @@ def cpu_model():
     return "unknown"
 
 
-def oracle_from_system(s, sc, threads, fp64=False):
-    """The oracle (FP32, or its FP64 twin) holding system `s`'s current state
-    (the workload `sc` advanced on the GPU): positions, velocities and the
-    last step's pressure and predicted density of the dynamic particles, the
-    boundary as built."""
+def state_of_system(s, sc):
+    """System `s`'s current state (the workload `sc` advanced on the GPU) per
+    input particle: positions, velocities, and the lagged PCISPH state (the
+    step before last's and the last step's correction pressures, the last
+    predicted density) of the dynamic particles, the boundary as built.
+    Returns (params, pos, vel, (prev, pressure, density))."""
     import unifiedparticleframeworkcuda_b200 as upf
-    from oracle import pyoracle
     g = s.particles()
     lag = s.lagged_state()  # (previous correction pressure, last one, last predicted density), same order
     ids = g["id"].astype(np.int64)
@@ -123,9 +123,47 @@ def oracle_from_system(s, sc, threads, fp64=False):
     prev[ids] = lag[:, 0]
     pres[ids] = lag[:, 1]
     dens[ids] = lag[:, 2]
+    return p, pos, vel, (prev, pres, dens)
+
+
+def oracle_from_system(s, sc, threads, fp64=False):
+    """The oracle (FP32, or its FP64 twin) holding system `s`'s current state
+    (state_of_system)."""
+    from oracle import pyoracle
+    p, pos, vel, lag = state_of_system(s, sc)
     o = pyoracle.OracleSim(p, pos, vel, sc.type, threads=threads, keep_fields=False, fp64=fp64)
-    o.set_lagged(prev, pres, dens)
+    o.set_lagged(*lag)
     return o
+
+
+# Workloads whose CPU legs time the reference's own step: its
+# CpuParticlePhysicsVersatileCouplingPCISPH / CpuParticlePhysicsPureFluidsSPH
+# (src/cpu/UnifiedPhysics.cpp) compiled from its sources into
+# oracle/_ref/libupfref_physics.so by oracle/Makefile (oracle/refstep.py).
+# The coupling workload keeps the oracle: its granular pile is not part of
+# the reference's coupling step.
+REFERENCE_STEP_SCENES = {"c2": "pcisph", "c2-small": "pcisph", "c1": "wcsph"}
+
+
+def reference_step_available(args):
+    if args.scene not in REFERENCE_STEP_SCENES:
+        return False
+    from oracle import refstep
+    return refstep.available()
+
+
+def time_reference_step(args, p, sc, pos, vel, lagged, threads, warmup, steps, min_steps, max_seconds):
+    """The reference's step on the host cores from the given state; returns
+    (particle-steps/s, timed steps, mean iterations, steps at the cap, largest
+    final density error in percent, seconds)."""
+    from oracle import refstep
+    r = refstep.reference_time(p, pos, vel, sc.type, lagged, REFERENCE_STEP_SCENES[args.scene], threads=threads,
+                               warmup=warmup, steps=steps, max_seconds=max_seconds, min_steps=min_steps)
+    secs = float(r["seconds"].sum())
+    done = int(r["seconds"].size)
+    its = r["iterations"]
+    return (dynamic_count(sc) * done / secs, done, float(its.mean()), int((its >= p.max_loops).sum()),
+            float(r["error_percent"].max()), secs)
 
 
 def fp64_error(s, sc, threads):
@@ -262,15 +300,38 @@ def full_config_oracle(args, threads):
 
 
 def cpu_baseline(args, seconds=15.0, system=None):
-    """The oracle (FP32 OpenMP restatement of the reference CPU path). Given
-    the GPU arm's system (the dam workloads), it runs the full configuration
-    from that system's state: 2 warm-up steps, then steps until at least 5
-    and `seconds` have passed. The other workloads run a bounded sample of
-    the same scene (the same spacing, h, dt and boundary with fewer
-    particles)."""
+    """The CPU baseline on the host cores: the reference's own step where it
+    covers the workload (REFERENCE_STEP_SCENES, kind "reference"), else the
+    oracle (the FP32 OpenMP restatement of the reference CPU path, kind
+    "port"). Given the GPU arm's system (the dam workloads), it runs the full
+    configuration from that system's state: 2 warm-up steps, then steps
+    until at least 5 and `seconds` have passed. The other workloads run the
+    workload itself (WCSPH) or a bounded sample of the same scene (the same
+    spacing, h, dt and boundary with fewer particles)."""
     from oracle import pyoracle
     pyoracle.build(with_ref=False)
     threads = os.cpu_count() or 1
+    if reference_step_available(args):
+        # the reference's own step: from the GPU arm's state at the start of
+        # its timed steps (the dams), or the workload itself from rest
+        sc = scene_for(args)
+        if system is not None:
+            p, pos, vel, lag = state_of_system(system, sc)
+            label = "%s after %d steps from rest, the state the GPU arm times" % (workload_name(args),
+                                                                                 settle_steps(args))
+            warm, min_steps = 2, 5
+        else:
+            import unifiedparticleframeworkcuda_b200 as upf
+            p, pos, vel, lag = upf.derive_params(sc.params), sc.pos, sc.vel, None
+            label = "%s from rest" % workload_name(args)
+            warm, min_steps = 1, 2
+        v, done, mean_its, _, _, secs = time_reference_step(args, p, sc, pos, vel, lag, threads, warm, 100000,
+                                                            min_steps, seconds)
+        return {"value": v, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "reference",
+                "sample": "the reference's own step (src/cpu/UnifiedPhysics.cpp, compiled from its sources, %d "
+                          "OpenMP threads) on %d dynamic + %d boundary particles (%s), %d steps after %d warm-up, "
+                          "mean %.1f iterations, %.1f s" % (threads, dynamic_count(sc), sc.n_boundary, label, done,
+                                                            warm, mean_its, secs)}
     if system is not None:
         # the full configuration from the GPU arm's own state at the start of
         # its timed steps
@@ -303,8 +364,10 @@ def cpu_baseline(args, seconds=15.0, system=None):
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU algorithm (the oracle port; the
-    reference's UnifiedPhysics.cpp does not compile here) on the host cores."""
+    """--impl reference: the reference's CPU step on the host cores. The dam
+    and WCSPH workloads run the reference's own step functions, compiled
+    from its sources (oracle/_ref/libupfref_physics.so); the others, and a
+    checkout without the compiled reference, run the oracle port."""
     if rank != 0:
         return
     if args.scene == "c4":
@@ -341,6 +404,9 @@ def run_reference(args, rank, world):
     pyoracle.build(with_ref=False)
     threads = os.cpu_count() or 1
     full = args.scene in ("c2", "c2-small")
+    if reference_step_available(args):
+        run_reference_step(args, threads, full)
+        return
     if full:
         # the full configuration, advanced by the same settle steps as the
         # GPU arm before its timed steps
@@ -381,6 +447,53 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
                          "sample": "%s: %d dynamic + %d boundary per step" % (label, dynamic_count(sc),
                                                                               sc.n_boundary)},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_reference_step(args, threads, full):
+    """The reference arm on the reference's own step. The dams: the full
+    configuration advanced from rest by the workload's settle steps (by the
+    oracle, as in the other arms' CPU legs: the reference's own settle steps,
+    most of them at the 50-iteration cap, would take the 1M scene several
+    minutes of host time), handed over with its lagged PCISPH state, then the
+    reference's warm-up and timed steps: `--steps` of them, or as many as
+    `--ref-seconds` allow (at least 3). WCSPH: the workload from rest."""
+    import unifiedparticleframeworkcuda_b200 as upf
+    if full:
+        o, sc, label, settle_info = full_config_oracle(args, threads)
+        st = o.state()
+        lag = o.lagged()
+        o.close()
+        order = np.argsort(st["id"])
+        p = upf.derive_params(sc.params)
+        pos, vel = st["pos"][order], st["vel"][order]
+        label += " (settled by the oracle)"
+    else:
+        sc = scene_for(args)
+        p = upf.derive_params(sc.params)
+        pos, vel, lag, settle_info = sc.pos, sc.vel, None, {}
+        label = "%s from rest" % workload_name(args)
+    warm = min(args.warmup, 2) if full else args.warmup
+    v, done, mean_its, at_max, max_err, secs = time_reference_step(
+        args, p, sc, pos, vel, lag, threads, warm, args.steps, min(args.steps, 3), args.ref_seconds)
+    cfg = {"workload": workload_name(args), "fluid_particles": sc.n_fluid, "boundary_particles": sc.n_boundary,
+           **settle_info, "state": label, "timed_steps": done, "same_config": True,
+           **({"dt": C1_DT, "dt_note": C1_NOTE} if args.scene == "c1" else {})}
+    if REFERENCE_STEP_SCENES[args.scene] == "pcisph":
+        cfg.update({"mean_iterations": mean_its, "steps_at_max_loops": at_max,
+                    "max_step_density_error_percent": max_err})
+    sample = ("the reference's own step (src/cpu/UnifiedPhysics.cpp, compiled from its sources, %d OpenMP "
+              "threads): %d dynamic + %d boundary particles, %s; %d timed steps of the %d requested after %d "
+              "warm-up (bounded to %.0f s), %.1f s" % (threads, dynamic_count(sc), sc.n_boundary, label, done,
+                                                        args.steps, warm, args.ref_seconds, secs))
+    print(json.dumps({
+        "impl": "reference", "metric": metric_for(args), "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -1130,6 +1243,8 @@ def main():
                                                 "[,density_mode,pforce_mode[,nlist_mode]]")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=90.0,
+                    help="bound on the reference arm's timed steps on the host cores (at least 3 run)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

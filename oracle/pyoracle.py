@@ -103,6 +103,8 @@ def lib():
         L.orc_set_reference_literal.restype = None
         L.orc_set_lagged.argtypes = [C.c_void_p, fp, fp, fp]
         L.orc_set_lagged.restype = None
+        L.orc_get_lagged.argtypes = [C.c_void_p, fp, fp, fp]
+        L.orc_get_lagged.restype = None
         L.orc_get.argtypes = [C.c_void_p, fp, fp, fp, fp, i32p, u32p, u32p]
         L.orc_get_step_fields.argtypes = [C.c_void_p, fp, fp, fp, fp, fp, fp, u32p]
         L.orc_neighbors.argtypes = [C.c_void_p, u32p, u32p, C.c_uint32]
@@ -266,6 +268,13 @@ class OracleSim:
         arrs = [np.ascontiguousarray(a, np.float32) for a in (pressure_prev, pressure, density)]
         assert all(a.shape == (self.n,) for a in arrs)
         lib().orc_set_lagged(self._h, *[_ptr(a, C.c_float) for a in arrs])
+
+    def lagged(self):
+        """(pressure_prev, pressure, density) of the current state, per
+        particle in creation order (what set_lagged takes)."""
+        arrs = [np.zeros(self.n, np.float32) for _ in range(3)]
+        lib().orc_get_lagged(self._h, *[_ptr(a, C.c_float) for a in arrs])
+        return tuple(arrs)
 
     def step(self) -> StepInfo:
         info = StepInfo()

@@ -30,7 +30,9 @@
 // Function-local statics in the reference (collision box, time step, particle
 // count, lookup factor) take the first scene's values: one scene per process.
 #include <cstdio>
+#include <cstdlib>
 #include <sstream>
+#include <string>
 
 #include "../include/upf.h"
 #include "ref_physics_harness.h"
@@ -85,23 +87,20 @@ static void set_constants(UnifiedConstants& fc, const upf_params* prm, char phys
   fc.printDebuggingInfo = 0;
 }
 
-static int run_steps(char physics, const upf_params* prm, const float* pos4, const float* vel4,
-                     const int32_t* type, const int32_t* body_of, uint32_t n_bodies, uint32_t n, int32_t steps,
-                     int32_t weighted_volumes, float* out_pos4, float* out_vel4, float* out_density,
-                     float* out_pressure, int32_t* out_type, uint32_t* out_id, float* out_body) {
-  if (!prm || !pos4 || !vel4 || !type || steps < 0 || (n_bodies && !body_of)) return 3;
-  for (uint32_t i = 0; body_of && i < n; ++i)
-    if (body_of[i] >= (int32_t)n_bodies || (body_of[i] >= 0) != (type[i] == RIGID_PARTICLE)) return 3;
-  Quiet quiet;
-  omp_set_num_threads(1);
-  static UnifiedConstants fc;
-  set_constants(fc, prm, physics);
-  static WeightingKernel kernel(&fc);
-
-  UnifiedPhysics up;
-  up.fc_ = &fc;
+// The physics object over the particles, as the reference's constructor and
+// CreatePartilcesCPU leave it; lag_* (nullable) set the lagged PCISPH state of
+// a run resumed mid-trajectory, per input particle: the final correction
+// pressure of the step before last (previous_correction_pressure_) and of the
+// last step (correction_pressure_), and the last predicted density.
+static UnifiedConstants g_fc;
+static void set_up(UnifiedPhysics& up, char physics, const upf_params* prm, const float* pos4, const float* vel4,
+                   const int32_t* type, uint32_t n, const float* lag_prev, const float* lag_p,
+                   const float* lag_rho) {
+  set_constants(g_fc, prm, physics);
+  static WeightingKernel kernel(&g_fc);
+  up.fc_ = &g_fc;
   up.my_kernel_ = &kernel;
-  up.kernel_self_ = kernel.KernelM4(0.0f, fc.globalSupportRadius);
+  up.kernel_self_ = kernel.KernelM4(0.0f, g_fc.globalSupportRadius);
   up.density_error_too_large_ = true;
   up.max_loops_sim_ = 0;
   up.avg_loops_sim_ = 0.0f;
@@ -111,9 +110,9 @@ static int run_steps(char physics, const upf_params* prm, const float* pos4, con
   up.min_dens_ = std::numeric_limits<float>::max();
   up.max_dens_ = 0.0f;
   up.dens_avg_timestep_ = 0.0f;
-  float block = fc.scales.x * fc.globalSupportRadius;
-  block = MAX(block, fc.scales.y * fc.globalSupportRadius);
-  block = MAX(block, fc.scales.z * fc.globalSupportRadius);
+  float block = g_fc.scales.x * g_fc.globalSupportRadius;
+  block = MAX(block, g_fc.scales.y * g_fc.globalSupportRadius);
+  block = MAX(block, g_fc.scales.z * g_fc.globalSupportRadius);
   zIndex.SetBlockSize(block);
 
   up.particles_.reserve(n);
@@ -121,23 +120,40 @@ static int run_steps(char physics, const upf_params* prm, const float* pos4, con
     UnifiedParticle q(vmml::Vector3f(pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2]), type[i],
                       vmml::Vector3f(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2]), 0.0f, prm->rest_density,
                       prm->rest_density, prm->mass);
-    q.previous_correction_pressure_ = 0.0f;
+    q.previous_correction_pressure_ = lag_prev ? lag_prev[i] : 0.0f;
+    if (lag_p) q.correction_pressure_ = lag_p[i];
+    if (lag_rho) q.predicted_density_ = lag_rho[i];
     q.correction_pressure_force_ = vmml::Vector3f(0.0f, 0.0f, 0.0f);
     q.density_error_ = 0.0f;
     q.parent_rigidbody_ = nullptr;
     q.color_ = vmml::Vector3f((float)i, 0.0f, 0.0f);
-    q.index_ = zIndex.CalcIndex(fc.scales * q.position_);
+    q.index_ = zIndex.CalcIndex(g_fc.scales * q.position_);
     if (type[i] != FROZEN_PARTICLE) up.num_nonfrozen_particles_++;
     up.particles_.push_back(q);
   }
+  up.SortParticles();
+  up.neighbor_indices_.resize(n);
+}
+
+static int run_steps(char physics, const upf_params* prm, const float* pos4, const float* vel4,
+                     const int32_t* type, const float* const* lag, const int32_t* body_of, uint32_t n_bodies,
+                     uint32_t n, int32_t steps, int32_t weighted_volumes, float* out_pos4, float* out_vel4,
+                     float* out_density, float* out_pressure, int32_t* out_type, uint32_t* out_id,
+                     float* out_body) {
+  if (!prm || !pos4 || !vel4 || !type || steps < 0 || (n_bodies && !body_of)) return 3;
+  for (uint32_t i = 0; body_of && i < n; ++i)
+    if (body_of[i] >= (int32_t)n_bodies || (body_of[i] >= 0) != (type[i] == RIGID_PARTICLE)) return 3;
+  Quiet quiet;
+  omp_set_num_threads(1);
+  UnifiedPhysics up;
+  set_up(up, physics, prm, pos4, vel4, type, n, lag ? lag[0] : nullptr, lag ? lag[1] : nullptr,
+         lag ? lag[2] : nullptr);
   auto keys_unique = [&]() {
     for (size_t k = 1; k < up.particles_.size(); ++k)
       if (up.particles_[k].index_ == up.particles_[k - 1].index_) return false;
     return true;
   };
-  up.SortParticles();
   if (!keys_unique()) return 1;
-  up.neighbor_indices_.resize(n);
   // Rigid bodies: each particle added to its body by the reference's
   // AddToRigidBody, in array order. The reference's scene construction
   // (SolidifyParticle, UnifiedPhysics.cpp:810-850) adds particles with the
@@ -215,12 +231,16 @@ extern "C" {
 // reference's final particle order (ascending key); density and pressure are
 // the predicted density and correction pressure; out_body (16 floats a body,
 // may be null) holds position, velocity, angular velocity, mass, quaternion.
+// lag_prev, lag_p, lag_rho (all null for a run from rest) resume a run as in
+// set_up.
 int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
+                             const float* lag_prev, const float* lag_p, const float* lag_rho,
                              const int32_t* body_of, uint32_t n_bodies, uint32_t n, int32_t steps,
                              int32_t weighted_volumes, float* out_pos4, float* out_vel4, float* out_density,
                              float* out_pressure, int32_t* out_type, uint32_t* out_id, float* out_body) {
-  return run_steps('i', prm, pos4, vel4, type, body_of, n_bodies, n, steps, weighted_volumes, out_pos4, out_vel4,
-                   out_density, out_pressure, out_type, out_id, out_body);
+  const float* lag[3] = {lag_prev, lag_p, lag_rho};
+  return run_steps('i', prm, pos4, vel4, type, lag_prev ? lag : nullptr, body_of, n_bodies, n, steps,
+                   weighted_volumes, out_pos4, out_vel4, out_density, out_pressure, out_type, out_id, out_body);
 }
 
 // The WCSPH step (CpuParticlePhysicsPureFluidsSPH), the same way, without
@@ -228,8 +248,62 @@ int ref_physics_pcisph_steps(const upf_params* prm, const float* pos4, const flo
 int ref_physics_wcsph_steps(const upf_params* prm, const float* pos4, const float* vel4, const int32_t* type,
                             uint32_t n, int32_t steps, float* out_pos4, float* out_vel4, float* out_density,
                             float* out_pressure, int32_t* out_type, uint32_t* out_id) {
-  return run_steps('w', prm, pos4, vel4, type, nullptr, 0, n, steps, 0, out_pos4, out_vel4, out_density,
+  return run_steps('w', prm, pos4, vel4, type, nullptr, nullptr, 0, n, steps, 0, out_pos4, out_vel4, out_density,
                    out_pressure, out_type, out_id, nullptr);
+}
+
+// Times the reference's step on the host cores: the PCISPH coupling step
+// ('i') or the WCSPH step ('w') on a scene of liquid and frozen boundary
+// particles (lag_* as in set_up, nullable), `threads` OpenMP threads (the
+// reference's own parallel loops; with more than one the loop's maximum
+// predicted density is the reference's unsynchronised one), `warmup`
+// untimed steps, then timed steps until `steps` have run, or until at least
+// `min_steps` have run and `max_seconds` have passed. Per timed step: wall seconds, and for PCISPH
+// the predict-correct iterations and the last iteration's density error in
+// percent, read from the loop's own report (printDebuggingInfo = 1 prints
+// "ERROR: <percent>%" once per iteration, UnifiedPhysics.cpp:5390-5391).
+// Returns the number of timed steps, or -3 on bad arguments.
+int ref_physics_time(int32_t wcsph, const upf_params* prm, const float* pos4, const float* vel4,
+                     const int32_t* type, uint32_t n, const float* lag_prev, const float* lag_p, const float* lag_rho,
+                     int32_t threads, int32_t warmup, int32_t steps, int32_t min_steps, double max_seconds,
+                     double* seconds, int32_t* iterations, float* error_percent) {
+  if (!prm || !pos4 || !vel4 || !type || threads < 1 || warmup < 0 || steps < 1 || min_steps < 1 || !seconds)
+    return -3;
+  Quiet quiet;
+  omp_set_num_threads(threads);
+  const char physics = wcsph ? 'w' : 'i';
+  UnifiedPhysics up;
+  set_up(up, physics, prm, pos4, vel4, type, n, lag_prev, lag_p, lag_rho);
+  g_fc.printDebuggingInfo = 1;
+  auto one = [&]() {
+    if (physics == 'i')
+      up.CpuParticlePhysicsVersatileCouplingPCISPH();
+    else
+      up.CpuParticlePhysicsPureFluidsSPH();
+  };
+  for (int32_t k = 0; k < warmup; ++k) one();
+  int32_t done = 0;
+  double total = 0.0;
+  while (done < steps && (done < min_steps || total < max_seconds)) {
+    quiet.sink.str("");
+    const double t0 = omp_get_wtime();
+    one();
+    const double dt = omp_get_wtime() - t0;
+    seconds[done] = dt;
+    total += dt;
+    // the loop's per-iteration reports
+    const std::string log = quiet.sink.str();
+    int32_t its = 0;
+    float err = 0.0f;
+    for (size_t at = log.find("ERROR: "); at != std::string::npos; at = log.find("ERROR: ", at + 7)) {
+      ++its;
+      err = std::strtof(log.c_str() + at + 7, nullptr);
+    }
+    if (iterations) iterations[done] = its;
+    if (error_percent) error_percent[done] = err;
+    ++done;
+  }
+  return done;
 }
 
 }  // extern "C"

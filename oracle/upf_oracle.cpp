@@ -291,6 +291,7 @@ struct SimBase {
   virtual int get_rigid(float*, float*, float*, float*) const = 0;
   virtual void set_keep_fields(bool on) = 0;
   virtual void set_lagged(const float*, const float*, const float*) = 0;
+  virtual void get_lagged(float*, float*, float*) const = 0;
   virtual void set_literal(uint32_t mask) = 0;
 };
 
@@ -1039,6 +1040,14 @@ struct Sim : SimBase {
     }
   }
 
+  void get_lagged(float* pressure_prev, float* pressure, float* density) const override {
+    for (const Particle<R>& p : ps) {
+      pressure_prev[p.id] = float(p.p_prev);
+      pressure[p.id] = float(p.p_corr);
+      density[p.id] = float(p.rho_prev);
+    }
+  }
+
   void get(float* pos4, float* vel4, float* density, float* pressure, int32_t* type, uint32_t* id,
            uint32_t* key) const override {
     for (size_t i = 0; i < ps.size(); ++i) {
@@ -1456,6 +1465,10 @@ void orc_set_reference_literal(orc_sim* s, uint32_t mask) { s->impl->set_literal
 
 void orc_set_lagged(orc_sim* s, const float* pressure_prev, const float* pressure, const float* density) {
   s->impl->set_lagged(pressure_prev, pressure, density);
+}
+
+void orc_get_lagged(const orc_sim* s, float* pressure_prev, float* pressure, float* density) {
+  s->impl->get_lagged(pressure_prev, pressure, density);
 }
 
 void orc_get(const orc_sim* s, float* pos4, float* vel4, float* density, float* pressure,

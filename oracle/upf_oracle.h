@@ -94,6 +94,8 @@ void orc_set_reference_literal(orc_sim* s, uint32_t mask);
  * final correction pressure of the step before last and of the last step,
  * and the last step's predicted density */
 void orc_set_lagged(orc_sim* s, const float* pressure_prev, const float* pressure, const float* density);
+/* the same three arrays of the current state, per particle in creation order */
+void orc_get_lagged(const orc_sim* s, float* pressure_prev, float* pressure, float* density);
 /* current array order (sorted by key at the end of the last step) */
 void orc_get(const orc_sim* s, float* pos4, float* vel4, float* density, float* pressure,
              int32_t* type, uint32_t* id, uint32_t* key);

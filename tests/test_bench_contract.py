@@ -1,6 +1,7 @@
 """bench.py's output contract, checked on the CPU: the reference arm (the
-oracle, timed on the host cores) prints one JSON line with the keys the
-driver reads; the GPU arm, on a machine without a GPU, exits with an error
+reference's own step compiled from its sources where it covers the
+workload, else the oracle, timed on the host cores) prints one JSON line
+with the keys the driver reads; the GPU arm, on a machine without a GPU, exits with an error
 instead of falling back to the CPU."""
 import json
 import os

@@ -312,6 +312,39 @@ def test_rigid_deviations_measured_against_reference_step(oracle_lib, bit):
 
 
 @pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
+def test_reference_resumes_from_the_oracles_lagged_state(oracle_lib):
+    """The reference's step resumed mid-trajectory (the state and the lagged
+    PCISPH state of another run: the step before last's and the last step's
+    correction pressures and the last predicted density, as the CPU
+    baselines hand it over) continues the trajectory bit for bit: the oracle
+    runs 2 steps of the first dam case, the reference 3 more from its state,
+    against the oracle's own 3 more."""
+    from oracle import refstep
+    if not refstep.available():
+        pytest.skip("oracle/_ref/libupfref_physics.so not built")
+    g = np.load(GOLDEN_STEP)
+    p, pos, vel, typ, _ = step_case(g, "dam_st_pw")
+    o = oracle_lib.OracleSim(p, pos, vel, typ)
+    for _ in range(2):
+        o.step()
+    st = o.state()
+    lag = o.lagged()
+    order = np.argsort(st["id"])
+    pos2, vel2 = st["pos"][order], st["vel"][order]
+    for _ in range(3):
+        o.step()
+    want = o.state()
+    o.close()
+    r = refstep.reference_steps(p, pos2, vel2, typ, 3, lagged=lag)
+    wo, ro = np.argsort(want["id"]), np.argsort(r["id"])
+    liq = want["type"][wo] == 2
+    for k in ("pos", "vel"):
+        assert bits_equal(want[k][wo], r[k][ro]), k
+    for k in ("density", "pressure"):
+        assert bits_equal(want[k][wo][liq], r[k][ro][liq]), k
+
+
+@pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
 def test_step_fixture_regenerates_identically(oracle_lib):
     """The committed step fixture is what the compiled reference steps
     produce now (each case in a fresh process, oracle/refstep.py)."""
