@@ -499,12 +499,33 @@ def run_reference_step(args, threads, full):
 
 
 def batch_cpu_baseline(scs, seconds):
-    """The oracle on a bounded sample of the batch (every 64th scene), as
-    particle-steps/s converted to scene-steps/s by the batch's mean scene size."""
-    from oracle import pyoracle
+    """A bounded sample of the batch (every 64th scene) on the host cores,
+    as particle-steps/s converted to scene-steps/s by the batch's mean scene
+    size: the reference's own step (each scene in its own process, from rest,
+    an even share of `seconds` each) where it is compiled, else the oracle."""
+    from oracle import pyoracle, refstep
     pyoracle.build(with_ref=False)
     threads = os.cpu_count() or 1
     sample = scs[::64]
+    if refstep.available():
+        import unifiedparticleframeworkcuda_b200 as upf
+        parts, steps_total, secs = 0, 0, 0.0
+        for sc in sample:
+            p = upf.derive_params(sc.params)
+            r = refstep.reference_time(p, sc.pos, sc.vel, sc.type, None, "pcisph", threads=threads, warmup=1,
+                                       steps=100000, max_seconds=seconds / len(sample), min_steps=2)
+            parts += sc.n * r["seconds"].size
+            steps_total += r["seconds"].size
+            secs += float(r["seconds"].sum())
+        pps = parts / secs
+        mean_n = sum(sc.n for sc in scs) / len(scs)
+        return {"value": pps / mean_n, "unit": "scene-steps/s", "cores": threads, "kind": "reference",
+                "cpu_model": cpu_model(),
+                "sample": "the reference's own step (src/cpu/UnifiedPhysics.cpp, compiled from its sources, %d "
+                          "OpenMP threads) on %d of %d scenes (%d particles) from rest, each in its own process, "
+                          "%d steps in all after one warm-up each, %.1f s: %.3g particle-steps/s over the batch's "
+                          "mean scene size %.0f" % (threads, len(sample), len(scs), sum(sc.n for sc in sample),
+                                                    steps_total, secs, pps, mean_n)}
     sims = [make_oracle(sc, threads) for sc in sample]
     for o in sims:
         o.step()
