@@ -618,15 +618,14 @@ def run_batch(args, rank, world, local_rank):
     else:
         kname, achieved, kms = "k_pcisph_density<batched>", dens_gbs, prof.density_ms_total
 
-    # end to end: per step, upload all scenes' state from pinned host memory
-    # (the warmed state, read back once before), step, read the result back
-    # into pinned host memory; the asynchronous calls overlap the copies
-    # with the steps
+    # end to end: the same steps from the same checkpoint, the host carrying
+    # the trajectory. Per step: upload all scenes' positions and velocities
+    # from pinned host memory, step, read them back into the same host
+    # arrays and wait; the next step's input is that readback.
     b.restore(0)
+    b.reset_counters()
     hp = torch.empty((npart, 4), dtype=torch.float32, pin_memory=True)
     hv = torch.empty((npart, 4), dtype=torch.float32, pin_memory=True)
-    op = torch.empty((npart, 4), dtype=torch.float32, pin_memory=True)
-    ov = torch.empty((npart, 4), dtype=torch.float32, pin_memory=True)
     L = upf.lib()
     fp = C.POINTER(C.c_float)
     upf.check(L.upf_batch_download_state(b.handle, C.cast(hp.data_ptr(), fp), C.cast(hv.data_ptr(), fp)), "dl")
@@ -636,11 +635,12 @@ def run_batch(args, rank, world, local_rank):
             upf.check(L.upf_batch_upload_state_async(b.handle, C.cast(hp.data_ptr(), fp), C.cast(hv.data_ptr(), fp)),
                       "upf_batch_upload_state_async")
             b.step(1)
-            upf.check(L.upf_batch_download_state_async(b.handle, C.cast(op.data_ptr(), fp),
-                                                       C.cast(ov.data_ptr(), fp)), "upf_batch_download_state_async")
-        upf.check(L.upf_batch_wait_frames(b.handle), "upf_batch_wait_frames")
+            upf.check(L.upf_batch_download_state_async(b.handle, C.cast(hp.data_ptr(), fp),
+                                                       C.cast(hv.data_ptr(), fp)), "upf_batch_download_state_async")
+            upf.check(L.upf_batch_wait_frames(b.handle), "upf_batch_wait_frames")
 
     e2e_ms = timed(e2e_steps)
+    e2e_same = [st.total_iterations for st in b.stats()] == [st.total_iterations for st in stats]
     b.close()
 
     # baseline: the same scenes as single-scene systems, one after another
@@ -689,7 +689,9 @@ def run_batch(args, rank, world, local_rank):
         "phases_ms": {"sort": prof.sort_ms, "neighbors": prof.neighbors_ms, "forces": prof.forces_ms,
                       "loop": prof.loop_ms, "integrate": prof.integrate_ms, "iterations": prof.iterations},
         "e2e": {"value": ns * args.steps * world / (e2e_ms / 1e3), "unit": "scene-steps/s",
-                "h2d_bytes_per_step": npart * 32, "d2h_bytes_per_step": npart * 32},
+                "h2d_bytes_per_step": npart * 32, "d2h_bytes_per_step": npart * 32, "ms_per_step": e2e_ms / args.steps,
+                "input_of_each_step": "the previous step's readback (positions and velocities of every scene)",
+                "same_steps_as_value": bool(e2e_same)},
         "gpu_launches": args.steps * per_step + 3 * max_it,
         "clocks": clk.summary(),
     }
@@ -736,6 +738,25 @@ def run_adjoint(args, rank, world, local_rank):
             fwd.append(f)
             bwd.append(b)
     f_ms, b_ms = replicas.max_over_ranks(float(np.median(fwd)), float(np.median(bwd)))
+    # end to end: the calls a gradient-descent loop on the initial velocities
+    # makes, timed on the library stream: each trajectory uploads its initial
+    # velocities from host memory (upf_adjoint_forward), runs forward and
+    # backward, and reads the gradient back to the host
+    # (upf_adjoint_backward); the host then takes a small descent step
+    v0 = np.array(sc.vel, np.float32, copy=True)
+    e2e_ms = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        a.forward(v0)
+        ge, _ = a.backward()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+        v0[:, :3] -= 1e-2 * ge
+    e2e_med = replicas.max_over_ranks(float(np.median(e2e_ms)))[0]
     a.close()
     if rank != 0:
         return
@@ -751,8 +772,11 @@ def run_adjoint(args, rank, world, local_rank):
                    "grad_norm": float(np.linalg.norm(g)), "dloss_dviscosity": gm,
                    "timing": "median over the timed forward/backward pairs, CUDA events on the library stream",
                    "l2": "per-interval lists and intermediates ~0.9 GB (larger than L2)"},
-        "e2e": {"value": n * T * world / ((f_ms + b_ms) / 1e3), "unit": "particle-steps/s (forward + backward)",
-                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": n * 16 // T},
+        "e2e": {"value": n * T * world / (e2e_med / 1e3), "unit": "particle-steps/s (forward + backward)",
+                "h2d_bytes_per_step": n * 16 // T, "d2h_bytes_per_step": n * 16 // T,
+                "ms_per_trajectory": e2e_med,
+                "calls": "upf_adjoint_forward with the initial velocities from host memory, upf_adjoint_backward "
+                         "with the gradient read back; median over the timed trajectories"},
         "gpu_launches": None,
         "clocks": clk.summary(),
     }
