@@ -736,19 +736,27 @@ upf_status upf_batch_profile_step(upf_batch* b, upf_phase_times* out, uint64_t* 
   out->forces_ms = elapsed(ev[2], ev[3]);
   int launches = 4 + 1 + 4 + 1 + 1 + 2 + 1 + 1 + 1;  // sort stages, digits, reorder, cells, init, nlist, ext, loop init
   float loop = 0;
+  const uint32_t total_groups = b->n_slots / kSegAlign;
   for (int it = 0; it < 4096; ++it) {
-    // scenes still iterating before this iteration
+    // scenes still iterating before this iteration, and the groups the last
+    // loop control listed
+    uint32_t ngroups = total_groups;
     UPF_CUDA(cudaMemcpyAsync(h.data(), b->st_d, sizeof(DevState) * b->n_scenes, cudaMemcpyDeviceToHost, st));
+    if (it) UPF_CUDA(cudaMemcpyAsync(&ngroups, b->n_active_groups_d, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     UPF_CUDA(cudaStreamSynchronize(st));
     uint64_t act = 0;
     for (uint32_t s = 0; s < b->n_scenes; ++s)
       if (h[s].loop_active) act += b->count[s];
     if (!act) break;
     active += act;
+    // the passes the step graph runs: the full grid in the first iteration
+    // and while at least half of the groups iterate, then the resident
+    // passes over the listed groups (k_loop_ctl_batch's choice)
+    const bool full = 2 * ngroups >= total_groups;
     UPF_CUDA(cudaEventRecord(ev[4], st));
-    UPF_CUDA(batch_launch_loop_density(*b, st));
+    UPF_CUDA(full ? batch_launch_loop_density(*b, st) : batch_launch_loop_density_active(*b, st));
     UPF_CUDA(cudaEventRecord(ev[5], st));
-    UPF_CUDA(batch_launch_loop_pforce(*b, st));
+    UPF_CUDA(full ? batch_launch_loop_pforce(*b, st) : batch_launch_loop_pforce_active(*b, st));
     UPF_CUDA(cudaEventRecord(ev[6], st));
     UPF_CUDA(batch_launch_loop_ctl(*b, st));
     UPF_CUDA(cudaEventRecord(ev[7], st));

@@ -2211,8 +2211,9 @@ cudaError_t batch_launch_loop_ctl(BatchSystem& b, cudaStream_t st, cudaGraphCond
 }
 
 // The loop passes over the active groups only, on a resident grid.
-cudaError_t batch_launch_loop_active(BatchSystem& b, cudaStream_t st) {
-  constexpr int kR = 4;
+constexpr int kActiveRows = 4;
+static cudaError_t active_grid_of(BatchSystem& b) {
+  constexpr int kR = kActiveRows;
   if (!b.active_grid) {
     int dev = 0, sms = 0, per_sm_d = 0, per_sm_p = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -2224,15 +2225,29 @@ cudaError_t batch_launch_loop_active(BatchSystem& b, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     b.active_grid = (uint32_t)(sms * std::max(1, std::min(per_sm_d, per_sm_p)));
   }
-  const uint32_t n = b.n_slots;
-  k_pcisph_density_active<kR><<<b.active_grid, kSegAlign, 0, st>>>(b.view, n, b.active_groups_d, b.n_active_groups_d,
-                                                                   b.B.type, b.xs, b.nbr, b.ncnt, b.rho, b.press,
-                                                                   b.pq);
-  cudaError_t e = cudaGetLastError();
+  return cudaSuccess;
+}
+
+cudaError_t batch_launch_loop_density_active(BatchSystem& b, cudaStream_t st) {
+  cudaError_t e = active_grid_of(b);
   if (e != cudaSuccess) return e;
-  k_pcisph_pressure_force_active<kR><<<b.active_grid, kSegAlign, 0, st>>>(
-      b.view, n, b.active_groups_d, b.n_active_groups_d, b.B, b.nbr, b.lval, b.ncnt, b.pq, b.force, b.pforce, b.xs);
+  k_pcisph_density_active<kActiveRows><<<b.active_grid, kSegAlign, 0, st>>>(
+      b.view, b.n_slots, b.active_groups_d, b.n_active_groups_d, b.B.type, b.xs, b.nbr, b.ncnt, b.rho, b.press, b.pq);
   return cudaGetLastError();
+}
+
+cudaError_t batch_launch_loop_pforce_active(BatchSystem& b, cudaStream_t st) {
+  cudaError_t e = active_grid_of(b);
+  if (e != cudaSuccess) return e;
+  k_pcisph_pressure_force_active<kActiveRows><<<b.active_grid, kSegAlign, 0, st>>>(
+      b.view, b.n_slots, b.active_groups_d, b.n_active_groups_d, b.B, b.nbr, b.lval, b.ncnt, b.pq, b.force, b.pforce,
+      b.xs);
+  return cudaGetLastError();
+}
+
+cudaError_t batch_launch_loop_active(BatchSystem& b, cudaStream_t st) {
+  cudaError_t e = batch_launch_loop_density_active(b, st);
+  return e == cudaSuccess ? batch_launch_loop_pforce_active(b, st) : e;
 }
 
 // An IF node at the capture point of `st` (capturing into a graph) whose

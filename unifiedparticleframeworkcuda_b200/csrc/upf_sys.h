@@ -299,6 +299,10 @@ cudaError_t batch_launch_loop_init(BatchSystem& b, cudaStream_t st);
 cudaError_t batch_launch_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h, bool use_handle);
 cudaError_t batch_launch_loop_density(BatchSystem& b, cudaStream_t st);
 cudaError_t batch_launch_loop_pforce(BatchSystem& b, cudaStream_t st);
+// the same passes on a resident grid over the groups the last loop control
+// listed (n_active_groups_d)
+cudaError_t batch_launch_loop_density_active(BatchSystem& b, cudaStream_t st);
+cudaError_t batch_launch_loop_pforce_active(BatchSystem& b, cudaStream_t st);
 // the graph's loop body: [if most groups iterate: full-grid passes] [else:
 // resident passes over the active groups] loop control (sets all three)
 cudaError_t batch_capture_loop_body(BatchSystem& b, cudaStream_t st, cudaGraphConditionalHandle h);
