@@ -1288,7 +1288,7 @@ def main():
                                                 "[,density_mode,pforce_mode[,nlist_mode]]")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--ref-seconds", type=float, default=90.0,
+    ap.add_argument("--ref-seconds", type=float, default=60.0,
                     help="bound on the reference arm's timed steps on the host cores (at least 3 run)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
