@@ -167,13 +167,18 @@ def time_reference_step(args, p, sc, pos, vel, lagged, threads, warmup, steps, m
 
 
 def fp64_error(s, sc, threads):
-    """One step of system `s` from its checkpoint 0 against the FP64 oracle
-    from the same state: the largest differences of the liquid particles'
-    fields (positions absolute in m, the rest relative to the field's largest
-    magnitude) and both iteration counts."""
+    """One step of system `s` from its checkpoint 0 (the state at the start
+    of the timed steps) against the FP64 oracle from the same state: the
+    largest differences of the liquid particles' fields (positions absolute
+    in m, the rest relative to the field's largest magnitude) and both
+    iteration counts (0 for WCSPH)."""
     import unifiedparticleframeworkcuda_b200 as upf
     s.restore(0)
     o = oracle_from_system(s, sc, threads, fp64=True)
+    if sc.num_bodies:
+        # bodies assembled from their particles' current positions and
+        # velocities (FP64 sums on both sides)
+        o.set_rigid_bodies(sc.body, sc.num_bodies)
     s.step(1)
     s.synchronize()
     gi = s.stats().iterations
@@ -1259,8 +1264,7 @@ def run_ours(args, rank, world, local_rank):
         if dam:
             s.restore(0)  # the state at the start of the timed steps
         out["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds, system=s if dam else None)
-        if dam:
-            out["config"]["fp64_err"] = fp64_error(s, sc, os.cpu_count() or 1)
+        out["config"]["fp64_err"] = fp64_error(s, sc, os.cpu_count() or 1)
     print(json.dumps(out), flush=True)
     s.close()
 
