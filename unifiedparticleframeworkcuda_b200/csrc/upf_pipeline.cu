@@ -1084,9 +1084,12 @@ __global__ void __launch_bounds__(kSegAlign) k_pcisph_density_active(
 // the TMA ring or by direct loads (walk_lists).
 // Short TMA rings (at most 4 rows a stage) are held to 64 registers a thread
 // (four 256-thread CTAs an SM): two chunks of gathers in flight need them
-// (held to 40, the 4-row rings spilled).
-constexpr int pforce_min_blocks(bool direct, int threads, int rows) {
-  return (!direct && rows <= 4) ? 1024 / threads : 1;
+// (held to 40, the 4-row rings spilled). The batched pass keeps one chunk in
+// flight at 40 registers: its scenes converge unevenly, and the occupancy
+// pays more there than the second chunk.
+__host__ __device__ constexpr bool pforce_two_chunks(bool batch) { return !batch; }
+constexpr int pforce_min_blocks(bool batch, bool direct, int threads, int rows) {
+  return (!direct && rows <= 4) ? (pforce_two_chunks(batch) ? 1024 : 1536) / threads : 1;
 }
 
 template <bool kBatch, bool kDirect, int kThreads, int kRows>
@@ -1150,13 +1153,17 @@ __device__ __forceinline__ void pforce_block(
         gn[r] = __uint_as_float(val(r));
       }
     }
-    if (kp >= 0) accumulate(xp, gp, kp);
+    if constexpr (pforce_two_chunks(kBatch)) {
+      if (kp >= 0) accumulate(xp, gp, kp);
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-      xp[r] = xn[r];
-      gp[r] = gn[r];
+      for (int r = 0; r < kRows; ++r) {
+        xp[r] = xn[r];
+        gp[r] = gn[r];
+      }
+      kp = k0;
+    } else {
+      accumulate(xn, gn, k0);
     }
-    kp = k0;
   });
   if (kp >= 0) accumulate(xp, gp, kp);
   if (!ok && lane == 0) atomicOr(&st->error_flags, (uint32_t)ERR_TIMEOUT);
@@ -1169,7 +1176,7 @@ __device__ __forceinline__ void pforce_block(
 }
 
 template <bool kBatch, bool kDirect, int kThreads, int kRows>
-__global__ void __launch_bounds__(kThreads, pforce_min_blocks(kDirect, kThreads, kRows)) k_pcisph_pressure_force(
+__global__ void __launch_bounds__(kThreads, pforce_min_blocks(kBatch, kDirect, kThreads, kRows)) k_pcisph_pressure_force(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
     const __grid_constant__ CUtensorMap cmap, const __grid_constant__ CUtensorMap vmap,
     const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ lval, const uint32_t* __restrict__ ncnt,
