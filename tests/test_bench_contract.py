@@ -25,11 +25,12 @@ def _line(out):
     return json.loads(lines[0])
 
 
-@pytest.mark.parametrize("scene", ["c1", "c2"])
+@pytest.mark.parametrize("scene", ["c1", "c2", "c4"])
 def test_reference_arm_line(scene):
     # c2 at its full size, advanced on the host cores by one settle step
-    # (the default settle count takes minutes on a small host)
-    extra = ["--settle", "1"] if scene == "c2" else []
+    # (the default settle count takes minutes on a small host); the batch's
+    # sample bounded to a few seconds
+    extra = {"c2": ["--settle", "1"], "c4": ["--cpu-seconds", "4"]}.get(scene, [])
     r = _run(["--impl", "reference", "--scene", scene, "--steps", "2", "--warmup", "1"] + extra)
     assert r.returncode == 0, r.stderr[-2000:]
     d = _line(r.stdout)
@@ -39,6 +40,9 @@ def test_reference_arm_line(scene):
     assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2 and d["warmup"] == 1
     assert d["higher_is_better"] is True and d["n_gpus"] == 1
     assert d["config"]["workload"]
+    from oracle import refstep
+    if refstep.available():  # the reference's own step is compiled here
+        assert d["cpu_baseline"]["kind"] == "reference"
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
     e = d["e2e"]
