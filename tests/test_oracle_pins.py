@@ -345,6 +345,27 @@ def test_reference_resumes_from_the_oracles_lagged_state(oracle_lib):
 
 
 @pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
+def test_reference_timing_reports_the_loops_iterations(oracle_lib):
+    """The timed reference step (the CPU baselines' leg) counts each step's
+    predict-correct iterations from the loop's own per-iteration report: on
+    one thread they equal the oracle's counts for the same steps, and the
+    last reported error of each step is the oracle's final density error."""
+    from oracle import refstep
+    if not refstep.available():
+        pytest.skip("oracle/_ref/libupfref_physics.so not built")
+    g = np.load(GOLDEN_STEP)
+    p, pos, vel, typ, _ = step_case(g, "dam_st_pw")
+    r = refstep.reference_time(p, pos, vel, typ, None, "pcisph", threads=1, warmup=1, steps=3, max_seconds=1e9)
+    o = oracle_lib.OracleSim(p, pos, vel, typ)
+    o.step()
+    infos = [o.step() for _ in range(3)]
+    o.close()
+    assert r["seconds"].size == 3 and np.all(r["seconds"] > 0)
+    assert r["iterations"].tolist() == [int(i.iterations) for i in infos]
+    assert np.allclose(r["error_percent"], [float(i.density_error_percent) for i in infos], rtol=1e-5, atol=1e-4)
+
+
+@pytest.mark.skipif(not pyoracle.reference_present(), reason="reference tree not present")
 def test_step_fixture_regenerates_identically(oracle_lib):
     """The committed step fixture is what the compiled reference steps
     produce now (each case in a fresh process, oracle/refstep.py)."""
