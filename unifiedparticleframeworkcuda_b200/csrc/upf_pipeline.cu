@@ -1405,10 +1405,12 @@ __device__ __forceinline__ void walk_staged(const unsigned long long* __restrict
 // The predicted-density pass over staged neighbourhoods (density_block's
 // arithmetic, ComputePredictedDensityAndPressure, UnifiedPhysics.cpp:5456-5491).
 // Register caps (CTAs an SM the launch bounds ask for; six fit the shared
-// memory, 33-34 KB each): 4-entry batches are held to 48 registers, 8-entry
-// batches to 64 (density) and 80 (pressure force), the caps below which
-// they spill.
-constexpr int density_staged_min_blocks(int rows) { return rows == 4 ? 5 : 4; }
+// memory, 33-34 KB each): 4-entry batches of the density pass are held to 40
+// registers (six CTAs an SM; 8 bytes of spill, and 0.083 against 0.085 ms a
+// launch at five CTAs and 48 registers on the 1M dam), of the pressure-force
+// pass to 48; 8-entry batches to 64 (density) and 80 (pressure force), the
+// caps below which they spill.
+constexpr int density_staged_min_blocks(int rows) { return rows == 4 ? 6 : 4; }
 constexpr int pforce_staged_min_blocks(int rows) { return rows == 4 ? 5 : 3; }
 
 template <int kRows>
