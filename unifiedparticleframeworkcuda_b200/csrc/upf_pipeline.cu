@@ -874,8 +874,14 @@ __device__ __forceinline__ float3 solid_external(const DevParams& P, uint32_t i,
 // CalculateExternalForcesVersatilCouplingPCISPH (UnifiedPhysics.cpp:5252-5365):
 // liquid particles (then the first prediction of the loop), rigid and
 // granular particles (solid_external).
+// Held to five CTAs of 256 threads an SM (48 registers, a few dozen bytes of
+// spill) for one system: 0.223 against 0.240 ms a launch at four CTAs and 60
+// registers on the 1M dam. The batched pass, which spills more at that cap,
+// keeps the compiler's choice.
+constexpr int external_min_blocks(bool batch, int threads) { return batch ? 1 : 1280 / threads; }
+
 template <bool kBatch, int kThreads>
-__global__ void __launch_bounds__(kThreads) k_pcisph_external(
+__global__ void __launch_bounds__(kThreads, external_min_blocks(kBatch, kThreads)) k_pcisph_external(
     const __grid_constant__ DevParams Pk, const BatchView bv, uint32_t n, DynArrays B,
     const float* __restrict__ wvol, const int32_t* __restrict__ id_body, const uint32_t* __restrict__ nbr,
     const uint32_t* __restrict__ ncnt, const float* __restrict__ luts_plain, float4* __restrict__ force,
